@@ -1,0 +1,104 @@
+"""Regenerates the golden fixtures in this directory from the reference.
+
+Run from the repository root in a container where the reference sources are
+available (``python tests/golden/make_golden.py``); it builds the harness
+(oracle/_ref/cpref) from them if needed. The fixtures it writes are:
+
+* ``<scenario>.npz`` -- for every reference scenario in tests/scenarios.py:
+  the reference's CSR structure, right-hand side, Dirichlet mask, the values
+  of its first stiffness assembly (run with one thread, so the summation order
+  is the element order) and its converged state under tight tolerances;
+* ``ref_meshes.json`` -- SHA-256 digests of meshes made by the reference's own
+  generators (genRectWithHole, genRing, genRectangle);
+* ``ref_holePlatePlastPow.npz`` and ``ref_solverTest.npz`` -- the cell fields
+  and displacements of the VTK results shipped with the reference
+  (data/holePlatePlastPow.vtk, data/solverTest.vtk);
+* ``ref_tables.json`` -- the strain energies of data/aitken_*.txt and the
+  stress-strain points of data/diagramPow.txt / diagramLin.txt.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import oracle  # noqa: E402
+import scenarios  # noqa: E402
+from oracle import vtk  # noqa: E402
+
+REF = os.environ.get("CUPLAST_REFERENCE", "/root/reference")
+OUT = os.path.dirname(os.path.abspath(__file__))
+FIELDS = ["uv", "exx", "eyy", "gamma", "eps_i", "sxx", "syy", "tau", "sig_i", "table_s", "psi", "E_c", "nu_c",
+          "exx_p", "eyy_p", "gamma_p", "eps_p_i"]
+
+
+def scenario_fixtures(workdir):
+    for name, sc in scenarios.SCENARIOS.items():
+        if not sc.get("reference"):
+            continue
+        mesh_path = os.path.join(workdir, f"{name}.bin")
+        m, lines = scenarios.scenario_lines(name, mesh_path, extra=["dump_k 1", "dump_csr 1"])
+        oracle.write_mesh(mesh_path, m["node_xy"], elem3=m["elem3"], elem4=m["elem4"], borders=m["borders"])
+        r = oracle.run_reference(lines, threads=1)
+        arrays = {k: r[k] for k in ["rows", "cols", "adj_pos", "adj", "rp", "mask", "k_data"] + FIELDS}
+        arrays.update(outer_per_level=r["outer_per_level"], cg_per_level=r["cg_per_level"],
+                      err_per_level=r["err_per_level"], energy=r["energy"],
+                      mesh_digest=np.array(scenarios.mesh_digest(m)))
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **arrays)
+        print(name, "outer", r["outer_per_level"], "cg", r["cg_per_level"])
+
+
+def mesh_fixtures():
+    specs = ["hole -3 3 -2 2 0.5 48 32 1", "hole -3 3 -2 2 0.5 12 8 1", "hole -100 100 -100 100 20 16 16 1",
+             "ring 50 120 32 8 1", "ring 0.1 0.2 40 5 1", "rect -1 1 -1 1 4 4 1", "rect -3 3 -2 2 6 4 1"]
+    out = {}
+    for s in specs:
+        r = oracle.run_reference(["mode mesh", "mesh " + s])
+        off, borders = 0, []
+        for L in r["border_len"]:
+            borders.append(r["border_nodes"][off:off + L])
+            off += L
+        m = dict(node_xy=r["node_xy"].reshape(-1, 2), elem3=r["elem3"], elem4=r["elem4"], borders=borders)
+        out[s] = dict(digest=scenarios.mesh_digest(m), nodes=int(len(r["node_xy"]) // 2),
+                      count4=int(len(r["elem4"]) // 4), max_index_diff=int(r["max_index_diff"][0]))
+    with open(os.path.join(OUT, "ref_meshes.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
+def shipped_fixtures():
+    v = vtk.read_solution_vtk(os.path.join(REF, "data", "holePlatePlastPow.vtk"))
+    np.savez_compressed(os.path.join(OUT, "ref_holePlatePlastPow.npz"),
+                        displacement=v["point_fields"]["Displacement"][:, :2].ravel(), **v["cell_fields"])
+    v = vtk.read_solution_vtk(os.path.join(REF, "data", "solverTest.vtk"))
+    np.savez_compressed(os.path.join(OUT, "ref_solverTest.npz"),
+                        displacement=v["point_fields"]["Displacement"][:, :2].ravel(), **v["cell_fields"])
+    tables = {}
+    for name in ["aitken_plast1pow", "aitken_plast1", "aitken_elast1", "aitken_plast2pow", "aitken_plast2",
+                 "aitken_elast2"]:
+        rows = []
+        with open(os.path.join(REF, "data", name + ".txt")) as f:
+            next(f)
+            for line in f:
+                w = line.split()
+                rows.append([int(w[0]), float(w[1])])
+        tables[name] = rows
+    for name in ["diagramPow", "diagramLin"]:
+        with open(os.path.join(REF, "data", name + ".txt")) as f:
+            tables[name] = [[float(w) for w in line.split()] for line in f if line.strip()]
+    with open(os.path.join(OUT, "ref_tables.json"), "w") as f:
+        json.dump(tables, f, indent=1)
+
+
+if __name__ == "__main__":
+    import tempfile
+
+    if not oracle.have_reference():
+        oracle.build(with_reference=True)
+    with tempfile.TemporaryDirectory() as d:
+        scenario_fixtures(d)
+    mesh_fixtures()
+    shipped_fixtures()

@@ -1,0 +1,93 @@
+"""Parity scenarios shared by the golden-fixture script, the oracle pins and
+the GPU parity tests. Each scenario is a mesh plus the lines of a job in the
+harness syntax (material, diagram, loads). Units are those of the scenario
+(the configuration-style ones use mm and MPa).
+
+Scenarios with ``reference=True`` contain only what the reference supports
+(Q4, its BC types) and have golden fixtures made by running the reference.
+"""
+import numpy as np
+
+import meshgen
+
+E304, NU304 = 193000.0, 0.29
+TIGHT = ["cg_eps 1e-13", "outer_eps 1e-12", "max_outer 400"]
+
+# five-segment piecewise-linear diagram: elastic to (sy/E, sy), then tangent
+# slopes 20 GPa .. 0.5 GPa (geometric), segment widths 1e-3
+def piecewise_lines(E, sy, slopes=(20000.0, 7952.7, 3162.3, 1257.4, 500.0), width=1e-3):
+    pts = [(sy / E, sy)]
+    for h in slopes:
+        e, s = pts[-1]
+        pts.append((e + width, s + h * width))
+    flat = " ".join(f"{e!r} {s!r}" for e, s in pts)
+    return f"diagram piecewise {E!r} {len(pts)} {flat}"
+
+
+def _hole12():
+    return meshgen.hole_plate(-3.0, 3.0, -2.0, 2.0, 0.5, 12, 8)
+
+
+def _ogrid(n_c4, rad_n):
+    return meshgen.hole_plate(-100.0, 100.0, -100.0, 100.0, 20.0, n_c4, n_c4, rad_n=rad_n)
+
+
+def _ring():
+    return meshgen.ring(50.0, 100.0, 32, 8)
+
+
+_PT_LOADS = ["force 1 170 0 0", "force 3 -170 0 0", "fixvertaxis 0", "fixhoraxis 0"]
+_OGRID_LOADS = ["force 2 0 200 0", "fixborderhor 0", "fixpoint -100 -100"]
+
+
+def _ring_lines(mesh):
+    return ["force 0 200 0 1"] + [f"fixdof {d}" for d in meshgen.axis_dofs(mesh["node_xy"])]
+
+
+SCENARIOS = {
+    # plasticityTest material (src/Main.cpp:252-296) on a 320-element plate
+    "hole12_pow": dict(mesh=_hole12, reference=True,
+                       lines=[f"diagram power {E304} 170 1930 0.015", f"material {E304} {NU304} 1"] + _PT_LOADS),
+    # aitken_plast1 material: linear hardening K_T = 0.1 E
+    "hole12_lin": dict(mesh=_hole12, reference=True,
+                       lines=[f"diagram linear {E304} 170 19300", f"material {E304} {NU304} 1"] + _PT_LOADS),
+    "hole12_strain": dict(mesh=_hole12, reference=True,
+                          lines=[f"diagram linear {E304} 170 19300", f"material {E304} {NU304} 1", "plane strain"] + _PT_LOADS),
+    # configuration-1 style O-grid (16 circumferential x 8 radial), bilinear
+    # sy = 250, Et = 2 GPa, top traction 200 MPa in 10 increments
+    "ogrid16_bilin": dict(mesh=lambda: _ogrid(4, 8), reference=True, levels=10,
+                          lines=["diagram linear 210000 250 2000", "material 210000 0.3 1"] + _OGRID_LOADS),
+    # configuration-2 style hardening sy (1 + ep/e0)^n, 4 increments to 220 MPa
+    "ogrid16_hollomon": dict(mesh=lambda: _ogrid(4, 8), reference=True, levels=4,
+                             lines=["diagram hollomon 210000 250 0.002 0.2", "material 210000 0.3 1",
+                                    "force 2 0 220 0", "fixborderhor 0", "fixpoint -100 -100"]),
+    # configuration-4 style ring under internal pressure, piecewise diagram
+    "ring_pw": dict(mesh=_ring, reference=True, lines_fn=lambda m: [piecewise_lines(210000.0, 300.0), "material 210000 0.3 1"] + _ring_lines(m)),
+    # solverTest (src/Main.cpp:14-38): elastic 4x4 patch
+    "rect_elastic": dict(mesh=lambda: meshgen.rect(-1.0, 1.0, -1.0, 1.0, 4, 4), reference=True, mode="elastic",
+                         lines=[f"diagram linear {E304} 170000000 {E304}", f"material {E304} {NU304 * 1e-6!r} 1",
+                                "displ 2 0 0 0 1", "force 0 1 0 0"]),
+    # CST extension (no reference counterpart): configuration-1 style split
+    "ogrid16_t3": dict(mesh=lambda: meshgen.split_t3(_ogrid(4, 8)), reference=False, levels=10,
+                       lines=["diagram linear 210000 250 2000", "material 210000 0.3 1"] + _OGRID_LOADS),
+}
+
+
+def scenario_lines(name, mesh_path, mode=None, extra=()):
+    sc = SCENARIOS[name]
+    m = sc["mesh"]()
+    lines = list(sc.get("lines", [])) + (sc["lines_fn"](m) if "lines_fn" in sc else [])
+    lines = [f"mode {mode or sc.get('mode', 'phases')}", f"mesh file {mesh_path}",
+             f"levels {sc.get('levels', 1)}"] + TIGHT + lines + list(extra)
+    return m, lines
+
+
+def mesh_digest(m):
+    import hashlib
+
+    h = hashlib.sha256()
+    for k in ("node_xy", "elem3", "elem4"):
+        h.update(np.ascontiguousarray(np.asarray(m[k], dtype=np.float64 if k == "node_xy" else np.int32)).tobytes())
+    for b in m["borders"]:
+        h.update(np.asarray(b, dtype=np.int32).tobytes())
+    return h.hexdigest()
