@@ -1,0 +1,369 @@
+"""cudaplasticity_b200 -- Python front end of the B200 (sm_100a) implementation
+of CudaPlasticity's 2D elasto-plastic FEM hot path.
+
+Everything here calls the C ABI of the in-tree library libcuplast.so
+(include/cuplast.h, include/cuplast_host.h); the work itself runs in the
+library's CUDA kernels. Importing works without a GPU (mesh generation and
+load building are host code); device calls raise CuplastError when no CUDA
+device is present.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi as C
+from ._capi import (CP_DIAGRAM_ELASTIC, CP_DIAGRAM_HOLLOMON, CP_DIAGRAM_LINEAR, CP_DIAGRAM_PIECEWISE,  # noqa: F401
+                    CP_DIAGRAM_POWER, CP_PLANE_STRAIN, CP_PLANE_STRESS, CP_PREC_FP64, CP_PREC_MIXED)
+
+FIELDS = ["exx", "eyy", "gamma", "eps_i", "sxx", "syy", "tau", "sig_i", "table_s", "psi", "E_c", "nu_c",
+          "exx_p", "eyy_p", "gamma_p", "eps_p_i"]
+
+
+class CuplastError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        text = C.lib().cp_status_string(status).decode()
+        super().__init__(f"{text} ({status})" + (f": {msg}" if msg else ""))
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.P_double)
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.P_int)
+
+
+def _up(a):
+    return a.ctypes.data_as(C.P_ubyte)
+
+
+def version():
+    return C.lib().cp_version().decode()
+
+
+def device_count():
+    n = ctypes.c_int(0)
+    C.lib().cp_device_count(ctypes.byref(n))
+    return n.value
+
+
+# ------------------------------------------------------------------ material --
+
+def material(E, nu=0.3, h=1.0, rho=1.0, plane=CP_PLANE_STRESS, diagram="elastic", **kw):
+    """cp_material. diagram: 'elastic'; 'linear' (sigma_t, k_t); 'power'
+    (sigma_t, a, m); 'hollomon' (sigma_y, eps0, n); 'piecewise' (points:
+    [(eps, sigma), ...], elastic up to the first point)."""
+    m = C.cp_material()
+    m.E, m.nu, m.h, m.rho, m.plane = float(E), float(nu), float(h), float(rho), int(plane)
+    kind = {"elastic": CP_DIAGRAM_ELASTIC, "linear": CP_DIAGRAM_LINEAR, "power": CP_DIAGRAM_POWER,
+            "hollomon": CP_DIAGRAM_HOLLOMON, "piecewise": CP_DIAGRAM_PIECEWISE}[diagram]
+    m.diagram = kind
+    if kind == CP_DIAGRAM_LINEAR:
+        m.sigma_t, m.k_t = kw["sigma_t"], kw["k_t"]
+    elif kind == CP_DIAGRAM_POWER:
+        m.sigma_t, m.a, m.m = kw["sigma_t"], kw["a"], kw["m"]
+    elif kind == CP_DIAGRAM_HOLLOMON:
+        m.sigma_t, m.eps0, m.n = kw["sigma_y"], kw["eps0"], kw["n"]
+    elif kind == CP_DIAGRAM_PIECEWISE:
+        pts = kw["points"]
+        m.n_points = len(pts)
+        for i, (e, s) in enumerate(pts):
+            m.pw_eps[i], m.pw_sig[i] = e, s
+        m.sigma_t = pts[0][1]
+    return m
+
+
+# ---------------------------------------------------------------------- mesh --
+
+class Mesh:
+    """Host mesh (the drop-in Mesh class) with the reference's generators."""
+
+    def __init__(self):
+        self._h = C.c_p()
+        self._check(C.lib().cpx_mesh_create(ctypes.byref(self._h)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            C.lib().cpx_mesh_destroy(self._h)
+            self._h = None
+
+    @staticmethod
+    def _check(st):
+        if st != C.CP_OK:
+            raise CuplastError(st)
+
+    @classmethod
+    def rect(cls, x1, x2, y1, y2, n1, n2):
+        m = cls()
+        m._check(C.lib().cpx_mesh_gen_rect(m._h, x1, x2, y1, y2, n1, n2))
+        return m
+
+    @classmethod
+    def rect_with_hole(cls, x1, x2, y1, y2, hole_rad, n1, n2, rad_n=0):
+        m = cls()
+        m._check(C.lib().cpx_mesh_gen_rect_with_hole(m._h, x1, x2, y1, y2, hole_rad, n1, n2, rad_n))
+        return m
+
+    @classmethod
+    def ring(cls, a, b, n_phi, n_r):
+        m = cls()
+        m._check(C.lib().cpx_mesh_gen_ring(m._h, a, b, n_phi, n_r))
+        return m
+
+    @classmethod
+    def from_arrays(cls, node_xy, elem3=None, elem4=None, borders=()):
+        m = cls()
+        xy = np.ascontiguousarray(node_xy, dtype=np.float64).ravel()
+        e3 = np.ascontiguousarray(elem3 if elem3 is not None else np.zeros(0), dtype=np.int32).ravel()
+        e4 = np.ascontiguousarray(elem4 if elem4 is not None else np.zeros(0), dtype=np.int32).ravel()
+        bl = np.array([len(b) for b in borders], dtype=np.int32)
+        bn = np.ascontiguousarray(np.concatenate([np.asarray(b, np.int32) for b in borders]) if len(borders)
+                                  else np.zeros(1, np.int32), dtype=np.int32)
+        m._check(C.lib().cpx_mesh_set(m._h, xy.size // 2, _dp(xy), e3.size // 3, _ip(e3), e4.size // 4, _ip(e4),
+                                      len(borders), _ip(bl) if len(bl) else None, _ip(bn)))
+        return m
+
+    def split_t3(self):
+        self._check(C.lib().cpx_mesh_split_t3(self._h))
+        return self
+
+    def counts(self):
+        v = [ctypes.c_int() for _ in range(5)]
+        self._check(C.lib().cpx_mesh_counts(self._h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def arrays(self):
+        n, c3, c4, nb, bt = self.counts()
+        xy = np.zeros(2 * n)
+        e3 = np.zeros(max(3 * c3, 1), np.int32)
+        e4 = np.zeros(max(4 * c4, 1), np.int32)
+        bl = np.zeros(max(nb, 1), np.int32)
+        bn = np.zeros(max(bt, 1), np.int32)
+        self._check(C.lib().cpx_mesh_get(self._h, _dp(xy), _ip(e3), _ip(e4), _ip(bl), _ip(bn)))
+        borders, off = [], 0
+        for L in bl[:nb]:
+            borders.append(bn[off:off + L].copy())
+            off += L
+        return dict(node_xy=xy.reshape(-1, 2), elem3=e3[:3 * c3].reshape(-1, 3), elem4=e4[:4 * c4].reshape(-1, 4),
+                    borders=borders)
+
+    def max_index_diff(self):
+        v = ctypes.c_int()
+        self._check(C.lib().cpx_mesh_max_index_diff(self._h, ctypes.byref(v)))
+        return v.value
+
+
+class Loads:
+    """LoadConditions of the drop-in API (constant-valued loads)."""
+
+    def __init__(self):
+        self._h = C.c_p()
+        Mesh._check(C.lib().cpx_loads_create(ctypes.byref(self._h)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            C.lib().cpx_loads_destroy(self._h)
+            self._h = None
+
+    def _do(self, name, *args):
+        Mesh._check(getattr(C.lib(), name)(self._h, *args))
+        return self
+
+    def set_force(self, border, fx, fy, normal=False):
+        return self._do("cpx_loads_set_force", border, fx, fy, int(normal))
+
+    def set_displacement(self, border, ux, uy, fix_mid_x=False, fix_mid_y=False):
+        return self._do("cpx_loads_set_displacement", border, ux, uy, int(fix_mid_x), int(fix_mid_y))
+
+    def fix_border(self, b):
+        return self._do("cpx_loads_fix_border", b)
+
+    def fix_border_vert(self, b):
+        return self._do("cpx_loads_fix_border_vert", b)
+
+    def fix_border_hor(self, b):
+        return self._do("cpx_loads_fix_border_hor", b)
+
+    def fix_vert_axis(self, x):
+        return self._do("cpx_loads_fix_vert_axis", x)
+
+    def fix_hor_axis(self, y):
+        return self._do("cpx_loads_fix_hor_axis", y)
+
+    def fix_point(self, x, y):
+        return self._do("cpx_loads_fix_point", x, y)
+
+    def set_displ_point(self, x, y, ux, uy):
+        return self._do("cpx_loads_set_displ_point", x, y, ux, uy)
+
+    def set_force_point(self, x, y, fx, fy):
+        return self._do("cpx_loads_set_force_point", x, y, fx, fy)
+
+    def set_gravity(self, g=9.81, dx=0.0, dy=-1.0):
+        return self._do("cpx_loads_set_gravity", g, dx, dy)
+
+    def set_rotation(self, omega, ax=0.0, ay=0.0):
+        return self._do("cpx_loads_set_rotation", omega, ax, ay)
+
+    def fix_dof(self, dof):
+        return self._do("cpx_loads_fix_dof", int(dof))
+
+    def build(self, mesh, h=1.0, rho=1.0):
+        n = mesh.counts()[0]
+        rp, uv, mask = np.zeros(2 * n), np.zeros(2 * n), np.zeros(2 * n, np.uint8)
+        Mesh._check(C.lib().cpx_loads_build(mesh._h, self._h, h, rho, _dp(rp), _up(mask), _dp(uv)))
+        return rp, mask, uv
+
+
+# ------------------------------------------------------------------- device --
+
+class Context:
+    def __init__(self, device=0):
+        self._h = C.c_p()
+        st = C.lib().cp_context_create(device, ctypes.byref(self._h))
+        if st != C.CP_OK:
+            self._h = None
+            raise CuplastError(st)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            C.lib().cp_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def error(self):
+        return C.lib().cp_context_last_error(self._h).decode()
+
+    def check(self, st):
+        if st != C.CP_OK:
+            raise CuplastError(st, self.error())
+        return st
+
+
+def mesh_view(arrays):
+    """cp_mesh_view over numpy arrays (kept alive by the returned tuple)."""
+    xy = np.ascontiguousarray(arrays["node_xy"], dtype=np.float64).ravel()
+    e3 = np.ascontiguousarray(arrays.get("elem3", np.zeros(0)), dtype=np.int32).ravel()
+    e4 = np.ascontiguousarray(arrays.get("elem4", np.zeros(0)), dtype=np.int32).ravel()
+    v = C.cp_mesh_view(xy.size // 2, _dp(xy), e3.size // 3, _ip(e3) if e3.size else None, e4.size // 4,
+                       _ip(e4) if e4.size else None)
+    return v, (xy, e3, e4)
+
+
+def solve_opts(**kw):
+    o = C.cp_solve_opts()
+    C.lib().cp_solve_opts_default(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Instance:
+    """One problem on the device (cp_instance)."""
+
+    def __init__(self, ctx, mesh_arrays, mat):
+        self.ctx = ctx
+        self._h = C.c_p()
+        v, keep = mesh_view(mesh_arrays)
+        self.n_nodes = v.node_count
+        self.n_elem = v.count3 + v.count4
+        self.count3 = v.count3
+        self.count4 = v.count4
+        ctx.check(C.lib().cp_instance_create(ctx._h, ctypes.byref(v), ctypes.byref(mat), ctypes.byref(self._h)))
+        del keep
+
+    def close(self):
+        if getattr(self, "_h", None):
+            C.lib().cp_instance_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def sizes(self):
+        a, b, c, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong(), ctypes.c_longlong()
+        self.ctx.check(C.lib().cp_instance_sizes(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                                 ctypes.byref(d)))
+        return a.value, b.value, c.value, d.value
+
+    def set_loads(self, rp, mask, uv=None):
+        rp = np.ascontiguousarray(rp, np.float64)
+        mask = np.ascontiguousarray(mask, np.uint8)
+        uvp = None
+        if uv is not None:
+            uv = np.ascontiguousarray(uv, np.float64)
+            uvp = _dp(uv)
+        self.ctx.check(C.lib().cp_instance_set_loads(self._h, _dp(rp), _up(mask), uvp))
+
+    def set_level(self, lam):
+        self.ctx.check(C.lib().cp_instance_set_level(self._h, float(lam)))
+
+    def reset_state(self):
+        self.ctx.check(C.lib().cp_instance_reset_state(self._h))
+
+    def assemble(self, precision=CP_PREC_FP64):
+        self.ctx.check(C.lib().cp_assemble(self._h, precision))
+
+    def cg_solve(self, eps, max_iter=10_000_000):
+        it, rr = ctypes.c_longlong(), ctypes.c_double()
+        st = C.lib().cp_cg_solve(self._h, eps, max_iter, ctypes.byref(it), ctypes.byref(rr))
+        if st not in (C.CP_OK,):
+            raise CuplastError(st, self.ctx.error())
+        return it.value, rr.value
+
+    def secant_update(self):
+        r = ctypes.c_double()
+        self.ctx.check(C.lib().cp_secant_update(self._h, ctypes.byref(r)))
+        return r.value
+
+    def plastic_strains(self):
+        self.ctx.check(C.lib().cp_plastic_strains(self._h))
+
+    def solve(self, allow_not_converged=False, **kw):
+        o = solve_opts(**kw)
+        rep = C.cp_solve_report()
+        st = C.lib().cp_solve(self._h, ctypes.byref(o), ctypes.byref(rep))
+        if st != C.CP_OK and not (allow_not_converged and st == C.CP_ERR_NOT_CONVERGED):
+            raise CuplastError(st, self.ctx.error())
+        return {k: getattr(rep, k) for k, _ in C.cp_solve_report._fields_}
+
+    def csr(self):
+        n, ne, nnz, nadj = self.sizes()
+        rows, cols = np.zeros(2 * n + 1, np.int32), np.zeros(nnz, np.int32)
+        adj_pos, adj = np.zeros(n + 1, np.int32), np.zeros(max(nadj, 1), np.int32)
+        vals = np.zeros(nnz)
+        self.ctx.check(C.lib().cp_get_csr(self._h, _ip(rows), _ip(cols), _ip(adj_pos), _ip(adj), _dp(vals)))
+        return dict(rows=rows, cols=cols, adj_pos=adj_pos, adj=adj[:nadj], k_data=vals)
+
+    def slot_map(self):
+        ns = 9 * self.count3 + 16 * self.count4
+        s = np.zeros(max(ns, 1), np.int32)
+        self.ctx.check(C.lib().cp_get_slot_map(self._h, _ip(s)))
+        return s[:ns]
+
+    def field(self, name):
+        n = 2 * self.n_nodes if name in ("uv", "rp") else self.n_elem
+        out = np.zeros(n)
+        self.ctx.check(C.lib().cp_get_field(self._h, name.encode(), _dp(out)))
+        return out
+
+    def set_field(self, name, values):
+        v = np.ascontiguousarray(values, np.float64)
+        self.ctx.check(C.lib().cp_set_field(self._h, name.encode(), _dp(v)))
+
+    def state(self):
+        d = {k: self.field(k) for k in FIELDS}
+        d["uv"] = self.field("uv")
+        return d
+
+
+def footprint(mesh_arrays, precision=CP_PREC_FP64):
+    v, keep = mesh_view(mesh_arrays)
+    out = ctypes.c_size_t()
+    st = C.lib().cp_instance_footprint(ctypes.byref(v), precision, ctypes.byref(out))
+    if st != C.CP_OK:
+        raise CuplastError(st)
+    return out.value

@@ -1,0 +1,851 @@
+// Host orchestration of one problem instance and the extern "C" entry points
+// declared in include/cuplast.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <type_traits>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "cg.h"
+#include "internal.h"
+
+using cp::Error;
+
+struct cp_context {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string last_error;
+};
+
+namespace {
+
+__global__ void k_set_level(int n, double lam, const double2* b_full, const double2* u_full, const uchar2* mask,
+                            double2* b, double2* u) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double2 bf = b_full[i];
+        b[i] = make_double2(lam * bf.x, lam * bf.y);
+        const uchar2 m = mask[i];
+        double2 uu = u[i];
+        const double2 uf = u_full[i];
+        if (!m.x) uu.x = lam * uf.x;
+        if (!m.y) uu.y = lam * uf.y;
+        u[i] = uu;
+    }
+}
+
+__global__ void k_reset_state(int ne, double E, double nu, cp::ElemState st) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+        st.psi[e] = 1.0;
+        st.E_c[e] = E;
+        st.nu_c[e] = nu;
+        st.res_prev[e] = 0.0;
+        st.res_cur[e] = 0.0;
+        st.sig_i[e] = 0.0;
+        st.table_s[e] = 0.0;
+    }
+}
+
+__global__ void k_zero_double(double* p, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = 0.0;
+}
+
+__global__ void k_widen(const float* in, double* out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (double)in[i];
+}
+
+cp::MaterialDev to_dev(const cp_material& m) {
+    cp::MaterialDev d{};
+    d.E = m.E;
+    d.nu = m.nu;
+    d.h = m.h;
+    d.plane = m.plane;
+    d.diagram = m.diagram;
+    d.sigma_t = m.sigma_t;
+    d.k_t = m.k_t;
+    d.a = m.a;
+    d.m = m.m;
+    d.eps0 = m.eps0;
+    d.n = m.n;
+    d.n_points = m.n_points;
+    for (int i = 0; i < CP_MAX_PW; ++i) {
+        d.pw_eps[i] = m.pw_eps[i];
+        d.pw_sig[i] = m.pw_sig[i];
+    }
+    return d;
+}
+
+void validate_material(const cp_material& m) {
+    CP_CHECK(m.E > 0 && std::isfinite(m.E), CP_ERR_INVALID, "material: E must be positive");
+    CP_CHECK(m.nu > -1.0 && m.nu < 0.5, CP_ERR_INVALID, "material: nu must be in (-1, 0.5)");
+    CP_CHECK(m.h > 0, CP_ERR_INVALID, "material: thickness h must be positive");
+    CP_CHECK(m.plane == CP_PLANE_STRESS || m.plane == CP_PLANE_STRAIN, CP_ERR_INVALID, "material: bad plane condition");
+    CP_CHECK(m.diagram >= CP_DIAGRAM_ELASTIC && m.diagram <= CP_DIAGRAM_PIECEWISE, CP_ERR_INVALID,
+             "material: unknown diagram");
+    if (m.diagram == CP_DIAGRAM_PIECEWISE) {
+        CP_CHECK(m.n_points >= 2 && m.n_points <= CP_MAX_PW, CP_ERR_INVALID, "material: piecewise needs 2..16 points");
+        for (int i = 1; i < m.n_points; ++i)
+            CP_CHECK(m.pw_eps[i] > m.pw_eps[i - 1], CP_ERR_INVALID, "material: piecewise strains must increase");
+    }
+    if (m.diagram == CP_DIAGRAM_HOLLOMON)
+        CP_CHECK(m.eps0 > 0 && m.n > 0 && m.sigma_t > 0, CP_ERR_INVALID, "material: Hollomon needs sy, eps0, n > 0");
+}
+
+}  // namespace
+
+struct cp_instance {
+    cp_context* ctx = nullptr;
+    cp::DevMesh mesh;
+    cp::DevCsr csr;
+    cp_material mat_host{};
+    cp::MaterialDev mat{};
+    int n_nodes = 0, n_elem = 0;
+    double2 *u = nullptr, *b = nullptr, *b_full = nullptr, *u_full = nullptr;
+    uchar2* mask = nullptr;
+    double2 *r64 = nullptr, *z64a = nullptr, *z64b = nullptr, *q64 = nullptr, *s64 = nullptr;
+    float2 *r32 = nullptr, *z32a = nullptr, *z32b = nullptr, *q32 = nullptr, *s32 = nullptr;
+    double4* minv64 = nullptr;
+    float4* minv32 = nullptr;
+    cp::ElemState st{};
+    double* st_block = nullptr;
+    cp::CgScalars* sc = nullptr;
+    cp::OuterScalars* osc = nullptr;
+    double* partials = nullptr;
+    int max_blocks = 0;
+    cp::CgScalars* sc_h = nullptr;     // pinned
+    cp::OuterScalars* osc_h = nullptr;  // pinned
+    cudaGraphExec_t g64[2] = {nullptr, nullptr}, g32[2] = {nullptr, nullptr};  // [precond]
+    int body_iters = 8;
+    bool use_graph = true;  // CG loop as a CUDA graph with a device-side WHILE condition
+    bool loads_set = false;
+    long long launches = 0;  // kernels launched (graph nodes included)
+    int last_assembly = -1;  // precision of the last assembly
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+
+    template <typename T>
+    T* alloc(size_t count) {
+        void* p = nullptr;
+        size_t nb = std::max<size_t>(count, 1) * sizeof(T);
+        CP_CUDA(cudaMallocAsync(&p, nb, ctx->stream));
+        allocs.push_back(p);
+        bytes += nb;
+        return static_cast<T*>(p);
+    }
+
+    cudaStream_t s() const { return ctx->stream; }
+    int sms() const { return ctx->sm_count; }
+
+    template <typename T>
+    cp::CgArgs<T> cg_args(int precond = 0);
+};
+
+template <>
+cp::CgArgs<double> cp_instance::cg_args<double>(int precond) {
+    cp::CgArgs<double> a;
+    if (precond && !s64) {
+        s64 = alloc<double2>(n_nodes);
+        minv64 = alloc<double4>(n_nodes);
+    }
+    a.precond = precond;
+    a.s = s64;
+    a.minv = minv64;
+    a.n = n_nodes;
+    a.sm_count = sms();
+    a.max_blocks = max_blocks;
+    a.slice_ptr = csr.slice_ptr;
+    a.scol = csr.scol;
+    a.val = csr.val64;
+    a.b = b;
+    a.mask = mask;
+    a.x = u;
+    a.r = r64;
+    a.z0 = z64a;
+    a.z1 = z64b;
+    a.q = q64;
+    a.sc = sc;
+    a.partials = partials;
+    return a;
+}
+
+template <>
+cp::CgArgs<float> cp_instance::cg_args<float>(int precond) {
+    cp::CgArgs<float> a;
+    if (precond && !s32) {
+        s32 = alloc<float2>(n_nodes);
+        minv32 = alloc<float4>(n_nodes);
+    }
+    a.precond = precond;
+    a.s = s32;
+    a.minv = minv32;
+    a.n = n_nodes;
+    a.sm_count = sms();
+    a.max_blocks = max_blocks;
+    a.slice_ptr = csr.slice_ptr;
+    a.scol = csr.scol;
+    a.val = csr.val32;
+    a.b = b;
+    a.mask = mask;
+    a.x = u;
+    a.r = r32;
+    a.z0 = z32a;
+    a.z1 = z32b;
+    a.q = q32;
+    a.sc = sc;
+    a.partials = partials;
+    return a;
+}
+
+namespace {
+
+int fail(cp_context* ctx, const Error& e) {
+    if (ctx) ctx->last_error = e.msg;
+    return e.status;
+}
+
+template <typename F>
+int guarded(cp_context* ctx, F&& f) {
+    try {
+        f();
+        return CP_OK;
+    } catch (const Error& e) {
+        return fail(ctx, e);
+    } catch (const std::bad_alloc&) {
+        return fail(ctx, Error{CP_ERR_NOMEM, "host allocation failed"});
+    }
+}
+
+void grid1d(long long n, int sms, int& grid) {
+    long long g = (n + 255) / 256;
+    long long cap = (long long)sms * 8;
+    grid = (int)std::max<long long>(1, std::min(g, cap));
+}
+
+void ensure_fp32(cp_instance* I) {
+    if (I->csr.val32) return;
+    I->csr.val32 = I->alloc<float>(4 * (size_t)I->csr.sell_blocks);
+    I->r32 = I->alloc<float2>(I->n_nodes);
+    I->z32a = I->alloc<float2>(I->n_nodes);
+    I->z32b = I->alloc<float2>(I->n_nodes);
+    I->q32 = I->alloc<float2>(I->n_nodes);
+}
+
+void assemble(cp_instance* I, int precision) {
+    const bool want32 = precision == CP_PREC_MIXED;
+    if (want32) ensure_fp32(I);
+    cp::launch_assemble(I->mesh, I->csr, I->mat, I->st.E_c, I->st.nu_c, true, want32, I->s(), I->sms());
+    I->last_assembly = precision;
+    I->launches += 1;
+}
+
+// Runs CG iterations until the device flags convergence or an error: one
+// graph launch (WHILE node), or -- with graphs off, e.g. to profile the
+// kernels one by one -- chunks of direct launches with a host poll between.
+template <typename T>
+void run_cg_loop(cp_instance* I, const cp::CgArgs<T>& a, cudaGraphExec_t g) {
+    I->launches += 1;  // the init kernel launched before the loop
+    if (I->use_graph) {
+        CP_CUDA(cudaGraphLaunch(g, I->s()));
+        CP_CUDA(cudaMemcpyAsync(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost, I->s()));
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+        // the WHILE body (body_iters x (P, U) + the condition kernel) ran
+        // until the iteration that converged, at least once
+        const long long trips = std::max<long long>(1, (I->sc_h->iter + I->body_iters - 1) / I->body_iters);
+        I->launches += trips * (2LL * I->body_iters + 1);
+        return;
+    }
+    for (;;) {
+        for (int it = 0; it < I->body_iters; ++it) cp::cg_launch_iteration<T>(a, it & 1, I->s());
+        I->launches += 2LL * I->body_iters;
+        CP_CUDA(cudaMemcpyAsync(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost, I->s()));
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+        if (I->sc_h->converged || I->sc_h->status) return;
+    }
+}
+
+// Reference-semantics FP64 CG from the current u.
+void cg_fp64(cp_instance* I, double eps, long long max_iter, int precond = 0) {
+    auto a = I->cg_args<double>(precond);
+    if (I->use_graph && !I->g64[precond]) I->g64[precond] = cp::cg_build_while_graph<double>(a, I->body_iters, I->s());
+    cp::cg_launch_init<double>(a, I->csr.val64, true, eps * eps, max_iter, 0, -1.0, I->s());
+    run_cg_loop(I, a, I->g64[precond]);
+}
+
+// Mixed precision: FP64 defect correction around FP32 CG. Each step computes
+// r = m.(b - K64 u) in FP64 and runs CG on K32 from that residual (FP32
+// recurrences, u accumulated in FP64) to a relative reduction inner_tol; stops
+// when ||r64|| / ||b|| <= eps.
+void cg_mixed(cp_instance* I, double eps, double inner_tol, long long max_iter, long long* inner_total,
+              long long* fp64_spmv, double* rel_res, int precond = 0) {
+    auto a = I->cg_args<float>(precond);
+    if (I->use_graph && !I->g32[precond]) I->g32[precond] = cp::cg_build_while_graph<float>(a, I->body_iters, I->s());
+    long long total = 0;
+    for (int step = 0; step < 200; ++step) {
+        cp::cg_launch_init<float>(a, I->csr.val64, true, inner_tol * inner_tol, max_iter, 1, eps * eps, I->s());
+        ++*fp64_spmv;
+        run_cg_loop(I, a, I->g32[precond]);
+        const cp::CgScalars& h = *I->sc_h;
+        *rel_res = h.bb > 0 ? std::sqrt(h.res64 / h.bb) : 0.0;
+        if (h.lin_done) break;
+        total += h.iter;
+        if (h.status == CP_ERR_BREAKDOWN) throw Error{CP_ERR_BREAKDOWN, "FP32 inner CG broke down"};
+        if (total >= max_iter) break;
+    }
+    *inner_total += total;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI --
+
+extern "C" {
+
+CP_API const char* cp_version(void) { return "cuplast-b200 0.1.0 (sm_100a)"; }
+
+CP_API const char* cp_status_string(int s) {
+    switch (s) {
+    case CP_OK: return "ok";
+    case CP_ERR_INVALID: return "invalid argument";
+    case CP_ERR_CUDA: return "CUDA error";
+    case CP_ERR_NOMEM: return "out of device memory";
+    case CP_ERR_NOT_CONVERGED: return "iteration limit reached";
+    case CP_ERR_BREAKDOWN: return "numerical breakdown (NaN/Inf or non-positive curvature)";
+    case CP_ERR_MESH: return "malformed mesh";
+    case CP_ERR_UNSUPPORTED: return "unsupported";
+    case CP_ERR_BUSY: return "busy";
+    case CP_ERR_NO_DEVICE: return "no CUDA device";
+    case CP_ERR_CANCELLED: return "cancelled";
+    default: return "unknown status";
+    }
+}
+
+CP_API int cp_device_count(int* count) {
+    if (!count) return CP_ERR_INVALID;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    *count = (e == cudaSuccess) ? n : 0;
+    return CP_OK;
+}
+
+CP_API int cp_context_create(int device, cp_context** out) {
+    if (!out) return CP_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return CP_ERR_NO_DEVICE;
+    if (device < 0 || device >= n) return CP_ERR_INVALID;
+    cp_context* c = new (std::nothrow) cp_context();
+    if (!c) return CP_ERR_NOMEM;
+    c->device = device;
+    int rc = guarded(c, [&] {
+        CP_CUDA(cudaSetDevice(device));
+        CP_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+        CP_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        CP_CUDA(cudaEventCreate(&c->ev0));
+        CP_CUDA(cudaEventCreate(&c->ev1));
+    });
+    if (rc != CP_OK) {
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return CP_OK;
+}
+
+CP_API int cp_context_destroy(cp_context* ctx) {
+    if (!ctx) return CP_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return CP_OK;
+}
+
+CP_API const char* cp_context_last_error(const cp_context* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+CP_API int cp_context_synchronize(cp_context* ctx) {
+    if (!ctx) return CP_ERR_INVALID;
+    return guarded(ctx, [&] { CP_CUDA(cudaStreamSynchronize(ctx->stream)); });
+}
+
+CP_API int cp_instance_footprint(const cp_mesh_view* m, int precision, size_t* bytes) {
+    if (!m || !bytes || m->node_count <= 0 || m->count3 < 0 || m->count4 < 0) return CP_ERR_INVALID;
+    const size_t n = (size_t)m->node_count, ne = (size_t)m->count3 + (size_t)m->count4;
+    const size_t incs = 3 * (size_t)m->count3 + 4 * (size_t)m->count4;
+    // upper bound of the neighbour count: the reference's link capacity
+    const size_t nadj = 2 * (size_t)m->count3 + 3 * (size_t)m->count4;
+    const size_t nadj_est = std::min(nadj, incs * 3);
+    const size_t nnz = 4 * (nadj_est + n);
+    size_t b = n * 16 + ne * 16 + incs * 8 + (2 * n + 2) * 4 + nadj_est * 4;  // mesh + structure
+    b += nnz * 8;                                                              // K (FP64)
+    b += n * (16 * 8 + 2);                                                     // u, b, b_full, u_full, r, z, z, q, mask
+    b += ne * 18 * 8;                                                          // element state
+    if (precision == CP_PREC_MIXED) b += nnz * 4 + n * 8 * 4;
+    b += 1 << 20;                                                              // scalars, partials, graphs
+    *bytes = b;
+    return CP_OK;
+}
+
+CP_API int cp_instance_create(cp_context* ctx, const cp_mesh_view* mv, const cp_material* mat, cp_instance** out) {
+    if (!ctx || !mv || !mat || !out) return CP_ERR_INVALID;
+    *out = nullptr;
+    cp_instance* I = new (std::nothrow) cp_instance();
+    if (!I) return CP_ERR_NOMEM;
+    I->ctx = ctx;
+    if (const char* g = std::getenv("CUPLAST_NO_GRAPH")) I->use_graph = !(g[0] == '1');
+    int rc = guarded(ctx, [&] {
+        CP_CHECK(mv->node_count > 0 && mv->node_xy, CP_ERR_INVALID, "mesh: no nodes");
+        CP_CHECK(mv->count3 >= 0 && mv->count4 >= 0 && mv->count3 + mv->count4 > 0, CP_ERR_INVALID,
+                 "mesh: no elements");
+        CP_CHECK(mv->count3 == 0 || mv->elem3, CP_ERR_INVALID, "mesh: elem3 missing");
+        CP_CHECK(mv->count4 == 0 || mv->elem4, CP_ERR_INVALID, "mesh: elem4 missing");
+        CP_CHECK((long long)mv->count3 + mv->count4 < (1LL << 29), CP_ERR_UNSUPPORTED, "mesh: too many elements");
+        validate_material(*mat);
+        CP_CUDA(cudaSetDevice(ctx->device));
+        I->mat_host = *mat;
+        I->mat = to_dev(*mat);
+        I->n_nodes = mv->node_count;
+        I->n_elem = mv->count3 + mv->count4;
+        cudaStream_t s = I->s();
+        // mesh upload (the reference's meshToGPU, src/Mesh.cu:678-717)
+        I->mesh.n_nodes = mv->node_count;
+        I->mesh.c3 = mv->count3;
+        I->mesh.c4 = mv->count4;
+        I->mesh.xy = I->alloc<double2>(I->n_nodes);
+        std::vector<int4> e3((size_t)mv->count3), e4((size_t)mv->count4);
+        for (int e = 0; e < mv->count3; ++e)
+            e3[e] = make_int4(mv->elem3[3 * e], mv->elem3[3 * e + 1], mv->elem3[3 * e + 2], -1);
+        for (int e = 0; e < mv->count4; ++e)
+            e4[e] = make_int4(mv->elem4[4 * e], mv->elem4[4 * e + 1], mv->elem4[4 * e + 2], mv->elem4[4 * e + 3]);
+        I->mesh.e3 = I->alloc<int4>(e3.size());
+        I->mesh.e4 = I->alloc<int4>(e4.size());
+        CP_CUDA(cudaMemcpyAsync(I->mesh.xy, mv->node_xy, sizeof(double2) * I->n_nodes, cudaMemcpyHostToDevice, s));
+        if (!e3.empty()) CP_CUDA(cudaMemcpyAsync(I->mesh.e3, e3.data(), sizeof(int4) * e3.size(), cudaMemcpyHostToDevice, s));
+        if (!e4.empty()) CP_CUDA(cudaMemcpyAsync(I->mesh.e4, e4.data(), sizeof(int4) * e4.size(), cudaMemcpyHostToDevice, s));
+        // sparsity structure + slot map on the device
+        cp::setup_csr(I->mesh, I->csr, s, I->sms());
+        I->allocs.push_back(I->csr.inc_pos);
+        I->allocs.push_back(I->csr.adj_pos);
+        I->allocs.push_back(I->csr.inc);
+        I->allocs.push_back(I->csr.inc_k);
+        I->allocs.push_back(I->csr.adj);
+        I->bytes += (size_t)(2 * (I->n_nodes + 1)) * 4 + (3ull * mv->count3 + 4ull * mv->count4) * 8 + I->csr.nadj * 4;
+        CP_CHECK(I->csr.nnz < (1LL << 31), CP_ERR_UNSUPPORTED, "matrix too large for 32-bit CSR offsets");
+        I->allocs.push_back(I->csr.slice_ptr);
+        I->allocs.push_back(I->csr.scol);
+        I->bytes += ((size_t)I->csr.n_slices + 1 + (size_t)I->csr.sell_blocks) * 4;
+        I->csr.val64 = I->alloc<double>(4 * (size_t)I->csr.sell_blocks);
+        const int n = I->n_nodes, ne = I->n_elem;
+        I->u = I->alloc<double2>(n);
+        I->b = I->alloc<double2>(n);
+        I->b_full = I->alloc<double2>(n);
+        I->u_full = I->alloc<double2>(n);
+        I->mask = I->alloc<uchar2>(n);
+        I->r64 = I->alloc<double2>(n);
+        I->z64a = I->alloc<double2>(n);
+        I->z64b = I->alloc<double2>(n);
+        I->q64 = I->alloc<double2>(n);
+        CP_CUDA(cudaMemsetAsync(I->u, 0, sizeof(double2) * n, s));
+        CP_CUDA(cudaMemsetAsync(I->b, 0, sizeof(double2) * n, s));
+        CP_CUDA(cudaMemsetAsync(I->b_full, 0, sizeof(double2) * n, s));
+        CP_CUDA(cudaMemsetAsync(I->u_full, 0, sizeof(double2) * n, s));
+        CP_CUDA(cudaMemsetAsync(I->mask, 1, sizeof(uchar2) * n, s));
+        CP_CUDA(cudaMemsetAsync(I->z64a, 0, sizeof(double2) * n, s));
+        CP_CUDA(cudaMemsetAsync(I->z64b, 0, sizeof(double2) * n, s));
+        // element state: 18 arrays in one block
+        I->st_block = I->alloc<double>(18 * (size_t)ne);
+        double** f[] = {&I->st.exx, &I->st.eyy, &I->st.gam, &I->st.eps_i, &I->st.sxx, &I->st.syy,
+                        &I->st.tau, &I->st.sig_i, &I->st.table_s, &I->st.psi, &I->st.E_c, &I->st.nu_c,
+                        &I->st.exx_p, &I->st.eyy_p, &I->st.gam_p, &I->st.eps_p_i, &I->st.res_prev, &I->st.res_cur};
+        for (int k = 0; k < 18; ++k) *f[k] = I->st_block + (size_t)k * ne;
+        {
+            int g;
+            grid1d(18LL * ne, I->sms(), g);
+            k_zero_double<<<g, 256, 0, s>>>(I->st_block, 18LL * ne);
+        }
+        I->sc = I->alloc<cp::CgScalars>(1);
+        I->osc = I->alloc<cp::OuterScalars>(1);
+        CP_CUDA(cudaMemsetAsync(I->sc, 0, sizeof(cp::CgScalars), s));
+        CP_CUDA(cudaMemsetAsync(I->osc, 0, sizeof(cp::OuterScalars), s));
+        I->max_blocks = I->sms() * 8;
+        I->partials = I->alloc<double>(4 * (size_t)I->max_blocks);  // <= 4 sums per block
+        CP_CUDA(cudaMallocHost(&I->sc_h, sizeof(cp::CgScalars)));
+        CP_CUDA(cudaMallocHost(&I->osc_h, sizeof(cp::OuterScalars)));
+        {
+            int g;
+            grid1d(ne, I->sms(), g);
+            k_reset_state<<<g, 256, 0, s>>>(ne, I->mat.E, I->mat.nu, I->st);
+        }
+        CP_CUDA(cudaGetLastError());
+        CP_CUDA(cudaStreamSynchronize(s));
+    });
+    if (rc != CP_OK) {
+        cp_instance_destroy(I);
+        return rc;
+    }
+    *out = I;
+    return CP_OK;
+}
+
+CP_API int cp_instance_destroy(cp_instance* I) {
+    if (!I) return CP_ERR_INVALID;
+    if (I->ctx) {
+        cudaSetDevice(I->ctx->device);
+        cudaStreamSynchronize(I->ctx->stream);
+    }
+    for (int k = 0; k < 2; ++k) {
+        if (I->g64[k]) cudaGraphExecDestroy(I->g64[k]);
+        if (I->g32[k]) cudaGraphExecDestroy(I->g32[k]);
+    }
+    for (void* p : I->allocs) cudaFreeAsync(p, I->ctx->stream);
+    if (I->sc_h) cudaFreeHost(I->sc_h);
+    if (I->osc_h) cudaFreeHost(I->osc_h);
+    if (I->ctx) cudaStreamSynchronize(I->ctx->stream);
+    delete I;
+    return CP_OK;
+}
+
+CP_API int cp_instance_sizes(const cp_instance* I, int* nodes, int* elems, long long* nnz, long long* nadj) {
+    if (!I) return CP_ERR_INVALID;
+    if (nodes) *nodes = I->n_nodes;
+    if (elems) *elems = I->n_elem;
+    if (nnz) *nnz = I->csr.nnz;
+    if (nadj) *nadj = I->csr.nadj;
+    return CP_OK;
+}
+
+CP_API int cp_instance_set_loads(cp_instance* I, const double* rp, const unsigned char* mask, const double* uv) {
+    if (!I || !rp || !mask) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        const int n = I->n_nodes;
+        cudaStream_t s = I->s();
+        std::vector<unsigned char> m(2 * (size_t)n);
+        for (size_t i = 0; i < m.size(); ++i) m[i] = mask[i] ? 1 : 0;
+        CP_CUDA(cudaMemcpyAsync(I->b_full, rp, sizeof(double2) * n, cudaMemcpyHostToDevice, s));
+        CP_CUDA(cudaMemcpyAsync(I->mask, m.data(), 2 * (size_t)n, cudaMemcpyHostToDevice, s));
+        if (uv) {
+            CP_CUDA(cudaMemcpyAsync(I->u_full, uv, sizeof(double2) * n, cudaMemcpyHostToDevice, s));
+            CP_CUDA(cudaMemcpyAsync(I->u, uv, sizeof(double2) * n, cudaMemcpyHostToDevice, s));
+        } else {
+            CP_CUDA(cudaMemsetAsync(I->u_full, 0, sizeof(double2) * n, s));
+            CP_CUDA(cudaMemsetAsync(I->u, 0, sizeof(double2) * n, s));
+        }
+        int g;
+        grid1d(n, I->sms(), g);
+        k_set_level<<<g, 256, 0, s>>>(n, 1.0, I->b_full, I->u_full, I->mask, I->b, I->u);
+        CP_CUDA(cudaGetLastError());
+        CP_CUDA(cudaStreamSynchronize(s));
+        I->loads_set = true;
+    });
+}
+
+CP_API int cp_instance_set_level(cp_instance* I, double lam) {
+    if (!I) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        int g;
+        grid1d(I->n_nodes, I->sms(), g);
+        k_set_level<<<g, 256, 0, I->s()>>>(I->n_nodes, lam, I->b_full, I->u_full, I->mask, I->b, I->u);
+        CP_CUDA(cudaGetLastError());
+    });
+}
+
+CP_API int cp_instance_reset_state(cp_instance* I) {
+    if (!I) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        int g;
+        grid1d(I->n_elem, I->sms(), g);
+        k_reset_state<<<g, 256, 0, I->s()>>>(I->n_elem, I->mat.E, I->mat.nu, I->st);
+        CP_CUDA(cudaGetLastError());
+    });
+}
+
+CP_API int cp_assemble(cp_instance* I, int precision) {
+    if (!I || (precision != CP_PREC_FP64 && precision != CP_PREC_MIXED)) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        assemble(I, precision);
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+    });
+}
+
+CP_API int cp_cg_solve(cp_instance* I, double eps, long long max_iter, long long* iters, double* rel_res) {
+    if (!I || !(eps > 0) || max_iter <= 0) return CP_ERR_INVALID;
+    int st = CP_OK;
+    int rc = guarded(I->ctx, [&] {
+        CP_CHECK(I->loads_set, CP_ERR_INVALID, "loads not set");
+        CP_CHECK(I->last_assembly >= 0, CP_ERR_INVALID, "matrix not assembled");
+        cg_fp64(I, eps, max_iter);
+        if (iters) *iters = I->sc_h->iter;
+        if (rel_res) *rel_res = std::sqrt(I->sc_h->rr * I->sc_h->normB_inv);
+        st = I->sc_h->status;
+    });
+    return rc != CP_OK ? rc : st;
+}
+
+CP_API int cp_secant_update(cp_instance* I, double* rel_err) {
+    if (!I) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        cp::launch_update(I->mesh, I->mat, I->u, I->st, I->osc, I->partials, 0, I->s(), I->sms());
+        CP_CUDA(cudaMemcpyAsync(I->osc_h, I->osc, sizeof(cp::OuterScalars), cudaMemcpyDeviceToHost, I->s()));
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+        if (rel_err) *rel_err = I->osc_h->rel_err;
+    });
+}
+
+CP_API int cp_plastic_strains(cp_instance* I) {
+    if (!I) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        cp::launch_plastic(I->mesh, I->mat, I->st, I->s(), I->sms());
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+    });
+}
+
+CP_API void cp_solve_opts_default(cp_solve_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof *o);
+    o->precision = CP_PREC_FP64;
+    o->cg_tol = 1e-7;
+    o->outer_tol = 1e-5;
+    o->max_outer = 50;
+    o->max_cg = 200000;
+    o->levels = 1;
+    o->aitken = 0;
+    o->inner_tol = 1e-4;
+    o->adaptive_cg = 0;
+    o->precond = 0;
+}
+
+CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* rep) {
+    if (!I || !opts) return CP_ERR_INVALID;
+    cp_solve_report R{};
+    const cp_solve_opts o = *opts;
+    if (!(o.cg_tol > 0) || !(o.outer_tol > 0) || o.max_outer <= 0 || o.levels <= 0 || o.max_cg <= 0)
+        return CP_ERR_INVALID;
+    if (o.precision != CP_PREC_FP64 && o.precision != CP_PREC_MIXED) return CP_ERR_INVALID;
+    if (o.precond != 0 && o.precond != 1) return CP_ERR_INVALID;
+    int rc = guarded(I->ctx, [&] {
+        CP_CHECK(I->loads_set, CP_ERR_INVALID, "loads not set");
+        cudaStream_t s = I->s();
+        CP_CUDA(cudaEventRecord(I->ctx->ev0, s));
+        const long long launches0 = I->launches;
+        R.status = CP_OK;
+        for (int lev = 1; lev <= o.levels; ++lev) {
+            const double lam = (double)lev / o.levels;
+            int g;
+            grid1d(I->n_nodes, I->sms(), g);
+            k_set_level<<<g, 256, 0, s>>>(I->n_nodes, lam, I->b_full, I->u_full, I->mask, I->b, I->u);
+            grid1d(2LL * I->n_elem, I->sms(), g);
+            k_zero_double<<<g, 256, 0, s>>>(I->st.res_prev, 2LL * I->n_elem);  // res_prev, res_cur adjacent
+            I->launches += 2;
+            double rel_err = 1.0, w_prev = 1.0;
+            bool converged = false;
+            for (int it = 0; it < o.max_outer; ++it) {
+                // linear tolerance: tight once the secant iteration is close
+                double eps = o.cg_tol;
+                if (o.adaptive_cg && rel_err > 10.0 * o.outer_tol) eps = std::max(o.cg_tol, 1e-2 * rel_err);
+                assemble(I, o.precision);
+                if (o.precision == CP_PREC_FP64) {
+                    cg_fp64(I, eps, o.max_cg, o.precond ? 1 : 0);
+                    R.cg_iters += I->sc_h->iter;
+                    R.cg_rel_res = std::sqrt(I->sc_h->rr * I->sc_h->normB_inv);
+                    if (I->sc_h->status == CP_ERR_BREAKDOWN) throw Error{CP_ERR_BREAKDOWN, "CG broke down"};
+                } else {
+                    double rr = 0;
+                    cg_mixed(I, eps, o.inner_tol, o.max_cg, &R.cg_iters, &R.fp64_spmv, &rr, o.precond ? 1 : 0);
+                    R.cg_rel_res = rr;
+                }
+                cp::launch_update(I->mesh, I->mat, I->u, I->st, I->osc, I->partials, o.aitken, s, I->sms());
+                I->launches += 1;
+                CP_CUDA(cudaMemcpyAsync(I->osc_h, I->osc, sizeof(cp::OuterScalars), cudaMemcpyDeviceToHost, s));
+                CP_CUDA(cudaStreamSynchronize(s));
+                rel_err = I->osc_h->rel_err;
+                R.outer_iters += 1;
+                CP_CHECK(std::isfinite(rel_err), CP_ERR_BREAKDOWN, "secant iteration produced NaN");
+                if (o.aitken) {
+                    double w = 1.0;
+                    if (it > 0 && I->osc_h->a_den > 0) w = -w_prev * I->osc_h->a_num / I->osc_h->a_den;
+                    if (!(w >= 0.1)) w = 0.1;
+                    if (w > 10.0) w = 10.0;
+                    cp::launch_aitken_relax(I->mesh, I->mat, I->st, I->osc, w, s, I->sms());
+                    I->launches += 1;
+                    w_prev = w;
+                }
+                if (rel_err <= o.outer_tol && eps <= o.cg_tol) {
+                    converged = true;
+                    break;
+                }
+            }
+            R.rel_err = rel_err;
+            R.levels_done = lev;
+            if (!converged) {
+                R.status = CP_ERR_NOT_CONVERGED;
+                break;
+            }
+        }
+        cp::launch_plastic(I->mesh, I->mat, I->st, s, I->sms());
+        I->launches += 1;
+        R.kernel_launches = I->launches - launches0;
+        CP_CUDA(cudaEventRecord(I->ctx->ev1, s));
+        CP_CUDA(cudaEventSynchronize(I->ctx->ev1));
+        float ms = 0;
+        CP_CUDA(cudaEventElapsedTime(&ms, I->ctx->ev0, I->ctx->ev1));
+        R.seconds = ms * 1e-3;
+    });
+    if (rep) *rep = R;
+    if (rc != CP_OK) return rc;
+    return R.status;
+}
+
+CP_API int cp_bench_cg(cp_instance* I, int precision, int precond, int iters, double* ms_p, double* ms_u,
+                       double* bytes_p, double* bytes_u) {
+    if (!I || iters <= 0 || (precision != CP_PREC_FP64 && precision != CP_PREC_MIXED) || (precond & ~1)) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        CP_CHECK(I->loads_set, CP_ERR_INVALID, "loads not set");
+        cudaStream_t s = I->s();
+        assemble(I, precision);
+        std::vector<cudaEvent_t> ev(2 * (size_t)iters + 1);
+        for (auto& e : ev) CP_CUDA(cudaEventCreate(&e));
+        auto time_it = [&](auto a, const void* valA) {
+            using T = typename std::remove_cv<typename std::remove_reference<decltype(*a.val)>::type>::type;
+            cp::cg_launch_init<T>(a, valA, true, 0.0, (long long)iters + 8, precision == CP_PREC_MIXED, -1.0, s);
+            for (int it = 0; it < iters; ++it) {
+                CP_CUDA(cudaEventRecord(ev[2 * it], s));
+                cp::cg_launch_p<T>(a, it & 1, s);
+                CP_CUDA(cudaEventRecord(ev[2 * it + 1], s));
+                cp::cg_launch_u<T>(a, it & 1, s);
+            }
+            CP_CUDA(cudaEventRecord(ev[2 * (size_t)iters], s));
+        };
+        const double n = I->n_nodes, nnz = (double)I->csr.nnz;
+        double sv, sx;
+        if (precision == CP_PREC_FP64) {
+            time_it(I->cg_args<double>(precond), I->csr.val64);
+            sv = 8;
+            sx = 8;
+        } else {
+            time_it(I->cg_args<float>(precond), I->csr.val64);
+            sv = 4;
+            sx = 4;
+        }
+        CP_CUDA(cudaEventSynchronize(ev.back()));
+        double tp = 0, tu = 0;
+        for (int it = 0; it < iters; ++it) {
+            float a = 0, b = 0;
+            CP_CUDA(cudaEventElapsedTime(&a, ev[2 * it], ev[2 * it + 1]));
+            CP_CUDA(cudaEventElapsedTime(&b, ev[2 * it + 1], ev[2 * it + 2]));
+            tp += a;
+            tu += b;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        // algorithmic bytes per launch (2 DOFs per node, N = 2n):
+        //  P: values nnz*sv + block columns nnz/4*4 + read r, z + write z', Kz' (4 N sx)
+        //  U: read x (16 n), z', r, Kz' (3 N sx), mask (2 n); write x, r (16 n + N sx)
+        //     [+ block Jacobi: read M^-1 (4 n sx), write s (N sx)]
+        const double N = 2 * n;
+        if (ms_p) *ms_p = tp / iters;
+        if (ms_u) *ms_u = tu / iters;
+        if (bytes_p) *bytes_p = nnz * sv + nnz + 4 * N * sx;
+        if (bytes_u) *bytes_u = 32 * n + 4 * N * sx + 2 * n + (precond ? 4 * n * sx + N * sx : 0.0);
+    });
+}
+
+CP_API int cp_get_csr(cp_instance* I, int* rows, int* cols, int* adj_pos, int* adj, double* values) {
+    if (!I) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        cudaStream_t s = I->s();
+        const int n = I->n_nodes;
+        const long long nnz = I->csr.nnz;
+        int *d_rows = nullptr, *d_cols = nullptr;
+        if (rows || cols) {
+            CP_CUDA(cudaMallocAsync(&d_rows, sizeof(int) * (2 * (size_t)n + 1), s));
+            if (cols) CP_CUDA(cudaMallocAsync(&d_cols, sizeof(int) * (size_t)nnz, s));
+            cp::csr_rows_cols(I->mesh, I->csr, d_rows, d_cols, s);
+            if (rows) CP_CUDA(cudaMemcpyAsync(rows, d_rows, sizeof(int) * (2 * (size_t)n + 1), cudaMemcpyDeviceToHost, s));
+            if (cols) CP_CUDA(cudaMemcpyAsync(cols, d_cols, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToHost, s));
+        }
+        if (adj_pos) CP_CUDA(cudaMemcpyAsync(adj_pos, I->csr.adj_pos, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+        if (adj) CP_CUDA(cudaMemcpyAsync(adj, I->csr.adj, sizeof(int) * (size_t)I->csr.nadj, cudaMemcpyDeviceToHost, s));
+        double* d_vals = nullptr;
+        if (values) {
+            CP_CUDA(cudaMallocAsync(&d_vals, sizeof(double) * (size_t)nnz, s));
+            cp::csr_export_values(I->mesh, I->csr, d_vals, s);
+            CP_CUDA(cudaMemcpyAsync(values, d_vals, sizeof(double) * (size_t)nnz, cudaMemcpyDeviceToHost, s));
+        }
+        CP_CUDA(cudaStreamSynchronize(s));
+        if (d_rows) cudaFreeAsync(d_rows, s);
+        if (d_cols) cudaFreeAsync(d_cols, s);
+        if (d_vals) cudaFreeAsync(d_vals, s);
+        CP_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+CP_API int cp_get_slot_map(cp_instance* I, int* slots) {
+    if (!I || !slots) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        cudaStream_t s = I->s();
+        const size_t ns = 9 * (size_t)I->mesh.c3 + 16 * (size_t)I->mesh.c4;
+        int* d = nullptr;
+        CP_CUDA(cudaMallocAsync(&d, sizeof(int) * std::max<size_t>(ns, 1), s));
+        cp::csr_slot_map(I->mesh, I->csr, d, s);
+        CP_CUDA(cudaMemcpyAsync(slots, d, sizeof(int) * ns, cudaMemcpyDeviceToHost, s));
+        CP_CUDA(cudaStreamSynchronize(s));
+        cudaFreeAsync(d, s);
+        CP_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+static double* field_ptr(cp_instance* I, const char* name, size_t* count) {
+    struct F {
+        const char* n;
+        double* p;
+    } fs[] = {{"exx", I->st.exx},       {"eyy", I->st.eyy},     {"gamma", I->st.gam},    {"eps_i", I->st.eps_i},
+              {"sxx", I->st.sxx},       {"syy", I->st.syy},     {"tau", I->st.tau},      {"sig_i", I->st.sig_i},
+              {"table_s", I->st.table_s}, {"psi", I->st.psi},   {"E_c", I->st.E_c},      {"nu_c", I->st.nu_c},
+              {"exx_p", I->st.exx_p},   {"eyy_p", I->st.eyy_p}, {"gamma_p", I->st.gam_p}, {"eps_p_i", I->st.eps_p_i}};
+    if (!std::strcmp(name, "uv")) {
+        *count = 2 * (size_t)I->n_nodes;
+        return reinterpret_cast<double*>(I->u);
+    }
+    if (!std::strcmp(name, "rp")) {
+        *count = 2 * (size_t)I->n_nodes;
+        return reinterpret_cast<double*>(I->b);
+    }
+    for (auto& f : fs)
+        if (!std::strcmp(name, f.n)) {
+            *count = (size_t)I->n_elem;
+            return f.p;
+        }
+    return nullptr;
+}
+
+CP_API int cp_get_field(cp_instance* I, const char* name, double* out) {
+    if (!I || !name || !out) return CP_ERR_INVALID;
+    size_t count = 0;
+    double* p = field_ptr(I, name, &count);
+    if (!p) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        CP_CUDA(cudaMemcpyAsync(out, p, sizeof(double) * count, cudaMemcpyDeviceToHost, I->s()));
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+    });
+}
+
+CP_API int cp_set_field(cp_instance* I, const char* name, const double* in) {
+    if (!I || !name || !in) return CP_ERR_INVALID;
+    size_t count = 0;
+    double* p = field_ptr(I, name, &count);
+    if (!p) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        CP_CUDA(cudaMemcpyAsync(p, in, sizeof(double) * count, cudaMemcpyHostToDevice, I->s()));
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+    });
+}
+
+}  // extern "C"

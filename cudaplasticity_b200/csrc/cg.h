@@ -1,0 +1,65 @@
+// CG launch interface (kernels in cg.cu).
+#pragma once
+
+#include "internal.h"
+
+namespace cp {
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+    using type = double2;
+};
+template <>
+struct Vec2<float> {
+    using type = float2;
+};
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<double> {
+    using type = double4;
+};
+template <>
+struct Vec4<float> {
+    using type = float4;
+};
+
+// Everything the CG kernels touch, passed by value.
+template <typename T>
+struct CgArgs {
+    using V2 = typename Vec2<T>::type;
+    int n = 0;            // nodes (2 DOFs each)
+    int sm_count = 148;
+    int max_blocks = 0;   // capacity of the partials buffer (blocks)
+    const int* slice_ptr = nullptr;  // sliced layout (see DevCsr)
+    const int* scol = nullptr;
+    const T* val = nullptr;         // K in the recurrence type, 4 values per block
+    const double2* b = nullptr;     // right-hand side (FP64)
+    const uchar2* mask = nullptr;   // 1 = free DOF
+    double2* x = nullptr;           // solution, accumulated in FP64
+    V2* r = nullptr;
+    V2* s = nullptr;                // preconditioned residual M^-1 r (block Jacobi only)
+    typename Vec4<T>::type* minv = nullptr;  // inverse 2x2 diagonal blocks (block Jacobi only)
+    int precond = 0;                // 0: plain CG (reference), 1: 2x2 block-Jacobi PCG
+    V2* z0 = nullptr;
+    V2* z1 = nullptr;
+    V2* q = nullptr;
+    CgScalars* sc = nullptr;
+    double* partials = nullptr;     // >= 3 * max_blocks doubles
+};
+
+template <typename T>
+void cg_launch_init(const CgArgs<T>& a, const void* valA, bool valA_is_fp64, double eps2, long long max_iter,
+                    int relative_to_r0, double outer_eps2, cudaStream_t s);
+template <typename T>
+void cg_launch_iteration(const CgArgs<T>& a, int parity, cudaStream_t s);
+template <typename T>
+void cg_launch_p(const CgArgs<T>& a, int parity, cudaStream_t s);
+template <typename T>
+void cg_launch_u(const CgArgs<T>& a, int parity, cudaStream_t s);
+template <typename T>
+cudaGraphExec_t cg_build_while_graph(const CgArgs<T>& a, int body_iters, cudaStream_t s);
+
+}  // namespace cp

@@ -1,0 +1,168 @@
+// extern "C" wrappers of the host-side drop-in classes (include/cuplast_host.h).
+#include <exception>
+#include <new>
+#include <stdexcept>
+#include <vector>
+
+#include "../../include/cuplast/LoadConditions.hpp"
+#include "../../include/cuplast_host.h"
+
+struct cpx_mesh {
+    cuplast::Mesh m;
+};
+struct cpx_loads {
+    cuplast::LoadConditions l;
+};
+
+namespace {
+template <typename F>
+int guard(F&& f) {
+    try {
+        f();
+        return CP_OK;
+    } catch (const std::bad_alloc&) {
+        return CP_ERR_NOMEM;
+    } catch (const std::out_of_range&) {
+        return CP_ERR_INVALID;
+    } catch (const std::invalid_argument&) {
+        return CP_ERR_UNSUPPORTED;
+    } catch (...) {
+        return CP_ERR_INVALID;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+CP_API int cpx_mesh_create(cpx_mesh** out) {
+    if (!out) return CP_ERR_INVALID;
+    *out = new (std::nothrow) cpx_mesh();
+    return *out ? CP_OK : CP_ERR_NOMEM;
+}
+CP_API int cpx_mesh_destroy(cpx_mesh* m) {
+    delete m;
+    return CP_OK;
+}
+CP_API int cpx_mesh_gen_rect(cpx_mesh* m, double x1, double x2, double y1, double y2, int n1, int n2) {
+    if (!m || n1 <= 0 || n2 <= 0) return CP_ERR_INVALID;
+    return guard([&] { m->m.genRectangle(x1, x2, y1, y2, n1, n2); });
+}
+CP_API int cpx_mesh_gen_rect_with_hole(cpx_mesh* m, double x1, double x2, double y1, double y2, double r, int n1,
+                                       int n2, int rad_n) {
+    if (!m || n1 <= 0 || n2 <= 0 || !(r > 0)) return CP_ERR_INVALID;
+    return guard([&] { m->m.genRectWithHole(x1, x2, y1, y2, r, n1, n2, 1, rad_n); });
+}
+CP_API int cpx_mesh_gen_ring(cpx_mesh* m, double a, double b, int n_phi, int n_r) {
+    if (!m || n_phi < 3 || n_r <= 0 || !(b > a) || !(a > 0)) return CP_ERR_INVALID;
+    return guard([&] { m->m.genRing(a, b, n_phi, n_r); });
+}
+CP_API int cpx_mesh_split_t3(cpx_mesh* m) {
+    if (!m) return CP_ERR_INVALID;
+    return guard([&] { m->m.splitToTriangles(); });
+}
+CP_API int cpx_mesh_set(cpx_mesh* m, int nodes, const double* xy, int c3, const int* e3, int c4, const int* e4,
+                        int nb, const int* bl, const int* bn) {
+    if (!m || nodes <= 0 || !xy || c3 < 0 || c4 < 0 || nb < 0) return CP_ERR_INVALID;
+    return guard([&] {
+        std::vector<std::vector<int>> borders(nb);
+        int off = 0;
+        for (int b = 0; b < nb; ++b) {
+            borders[b].assign(bn + off, bn + off + bl[b]);
+            off += bl[b];
+        }
+        m->m.assign(nodes, xy, c3, e3, c4, e4, borders);
+    });
+}
+CP_API int cpx_mesh_counts(const cpx_mesh* m, int* nodes, int* c3, int* c4, int* nb, int* bt) {
+    if (!m) return CP_ERR_INVALID;
+    if (nodes) *nodes = m->m.nodeCount;
+    if (c3) *c3 = m->m.count3;
+    if (c4) *c4 = m->m.count4;
+    if (nb) *nb = m->m.bordersCount;
+    if (bt) {
+        int t = 0;
+        for (int b = 0; b < m->m.bordersCount; ++b) t += m->m.borderLength[b];
+        *bt = t;
+    }
+    return CP_OK;
+}
+CP_API int cpx_mesh_get(const cpx_mesh* m, double* xy, int* e3, int* e4, int* bl, int* bn) {
+    if (!m) return CP_ERR_INVALID;
+    const cuplast::Mesh& M = m->m;
+    if (xy)
+        for (int i = 0; i < M.nodeCount; ++i) {
+            xy[2 * i] = M.node[i].x;
+            xy[2 * i + 1] = M.node[i].y;
+        }
+    if (e3)
+        for (int i = 0; i < 3 * M.count3; ++i) e3[i] = M.elem3[i];
+    if (e4)
+        for (int i = 0; i < 4 * M.count4; ++i) e4[i] = M.elem4[i];
+    int off = 0;
+    for (int b = 0; b < M.bordersCount; ++b) {
+        if (bl) bl[b] = M.borderLength[b];
+        if (bn)
+            for (int j = 0; j < M.borderLength[b]; ++j) bn[off + j] = M.borders[b][j];
+        off += M.borderLength[b];
+    }
+    return CP_OK;
+}
+CP_API int cpx_mesh_max_index_diff(const cpx_mesh* m, int* out) {
+    if (!m || !out) return CP_ERR_INVALID;
+    *out = m->m.findMaxIndexDiff();
+    return CP_OK;
+}
+
+CP_API int cpx_loads_create(cpx_loads** out) {
+    if (!out) return CP_ERR_INVALID;
+    *out = new (std::nothrow) cpx_loads();
+    return *out ? CP_OK : CP_ERR_NOMEM;
+}
+CP_API int cpx_loads_destroy(cpx_loads* l) {
+    delete l;
+    return CP_OK;
+}
+#define CPX_L(body)                  \
+    if (!l) return CP_ERR_INVALID;   \
+    return guard([&] { body; });
+CP_API int cpx_loads_set_force(cpx_loads* l, int b, double fx, double fy, int normal) {
+    CPX_L(l->l.setForce(b, cuplast::vec2(fx, fy), normal != 0))
+}
+CP_API int cpx_loads_set_displacement(cpx_loads* l, int b, double ux, double uy, int mx, int my) {
+    CPX_L(l->l.setDisplacement(b, cuplast::vec2(ux, uy), mx != 0, my != 0))
+}
+CP_API int cpx_loads_fix_border(cpx_loads* l, int b) { CPX_L(l->l.fixBorder(b)) }
+CP_API int cpx_loads_fix_border_vert(cpx_loads* l, int b) { CPX_L(l->l.fixBorderVert(b)) }
+CP_API int cpx_loads_fix_border_hor(cpx_loads* l, int b) { CPX_L(l->l.fixBorderHor(b)) }
+CP_API int cpx_loads_fix_vert_axis(cpx_loads* l, double x) { CPX_L(l->l.fixVertAxis(x)) }
+CP_API int cpx_loads_fix_hor_axis(cpx_loads* l, double y) { CPX_L(l->l.fixHorAxis(y)) }
+CP_API int cpx_loads_fix_point(cpx_loads* l, double x, double y) { CPX_L(l->l.fixPoint(cuplast::vec2(x, y))) }
+CP_API int cpx_loads_set_displ_point(cpx_loads* l, double x, double y, double ux, double uy) {
+    CPX_L(l->l.setDisplPoint(cuplast::vec2(x, y), cuplast::vec2(ux, uy)))
+}
+CP_API int cpx_loads_set_force_point(cpx_loads* l, double x, double y, double fx, double fy) {
+    CPX_L(l->l.setForcePoint(cuplast::vec2(x, y), cuplast::vec2(fx, fy)))
+}
+CP_API int cpx_loads_set_gravity(cpx_loads* l, double g, double dx, double dy) {
+    CPX_L(l->l.setGravity(g, cuplast::vec2(dx, dy)))
+}
+CP_API int cpx_loads_set_rotation(cpx_loads* l, double w, double ax, double ay) {
+    CPX_L(l->l.setRotation(w, cuplast::vec2(ax, ay)))
+}
+CP_API int cpx_loads_fix_dof(cpx_loads* l, int dof) { CPX_L(l->l.fixDof(dof)) }
+#undef CPX_L
+
+CP_API int cpx_loads_build(const cpx_mesh* m, const cpx_loads* l, double h, double rho, double* rp,
+                           unsigned char* mask, double* uv) {
+    if (!m || !l || !rp || !mask || !uv) return CP_ERR_INVALID;
+    return guard([&] {
+        std::vector<double> r, u;
+        std::vector<unsigned char> k;
+        cuplast::buildConditions(m->m, l->l, h, rho, r, k, u);
+        std::copy(r.begin(), r.end(), rp);
+        std::copy(k.begin(), k.end(), mask);
+        std::copy(u.begin(), u.end(), uv);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,333 @@
+// Host mesh of the drop-in API: generators with the reference's node and
+// element numbering (so CSR ordering and results match it bit for bit).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <vector>
+
+#include "../../include/cuplast/Mesh.hpp"
+
+namespace cuplast {
+
+namespace {
+template <typename T>
+T* dup(const T* src, size_t n) {
+    T* p = new T[n ? n : 1];
+    if (n) std::memcpy(p, src, n * sizeof(T));
+    return p;
+}
+const double kPi = 3.141592653589793;
+}  // namespace
+
+void Mesh::clear() {
+    delete[] elem3;
+    delete[] elem4;
+    delete[] elem8;
+    delete[] node;
+    delete[] secOrdNodes;
+    for (int i = 0; i < bordersCount; ++i) delete[] borders[i];
+    delete[] borders;
+    delete[] borderLength;
+    elem3 = elem4 = elem8 = nullptr;
+    node = nullptr;
+    secOrdNodes = nullptr;
+    borders = nullptr;
+    borderLength = nullptr;
+    bordersCount = 0;
+    count3 = count4 = count8 = 0;
+    nodeCount = 0;
+    fillPos();
+}
+
+Mesh::Mesh(const Mesh& o) { *this = o; }
+
+Mesh& Mesh::operator=(const Mesh& o) {
+    if (this == &o) return *this;
+    clear();
+    useCuda = o.useCuda;
+    ramSaved = o.ramSaved;
+    count3 = o.count3;
+    count4 = o.count4;
+    count8 = o.count8;
+    nodeCount = o.nodeCount;
+    elem3 = dup(o.elem3, 3 * (size_t)count3);
+    elem4 = dup(o.elem4, 4 * (size_t)count4);
+    elem8 = dup(o.elem8, 8 * (size_t)count8);
+    node = dup(o.node, (size_t)nodeCount);
+    secOrdNodes = dup(o.secOrdNodes, (size_t)nodeCount);
+    bordersCount = o.bordersCount;
+    borderLength = dup(o.borderLength, (size_t)bordersCount);
+    borders = new int*[bordersCount ? bordersCount : 1];
+    for (int b = 0; b < bordersCount; ++b) borders[b] = dup(o.borders[b], (size_t)borderLength[b]);
+    fillPos();
+    return *this;
+}
+
+Mesh::~Mesh() { clear(); }
+
+void Mesh::assign(int nodes, const double* xy, int c3, const int* e3, int c4, const int* e4,
+                  const std::vector<std::vector<int>>& borderLists) {
+    clear();
+    nodeCount = nodes;
+    node = new vec2[nodes ? nodes : 1];
+    secOrdNodes = new bool[nodes ? nodes : 1];
+    for (int i = 0; i < nodes; ++i) {
+        node[i] = vec2(xy[2 * i], xy[2 * i + 1]);
+        secOrdNodes[i] = false;
+    }
+    count3 = c3;
+    count4 = c4;
+    elem3 = dup(e3, 3 * (size_t)c3);
+    elem4 = dup(e4, 4 * (size_t)c4);
+    elem8 = new int[1];
+    bordersCount = (int)borderLists.size();
+    borderLength = new int[bordersCount ? bordersCount : 1];
+    borders = new int*[bordersCount ? bordersCount : 1];
+    for (int b = 0; b < bordersCount; ++b) {
+        borderLength[b] = (int)borderLists[b].size();
+        borders[b] = dup(borderLists[b].data(), borderLists[b].size());
+    }
+    fillPos();
+}
+
+void Mesh::genRectangle(double x1, double x2, double y1, double y2, size_t N1, size_t N2, int order) {
+    if (order != 1) throw std::invalid_argument("second-order (Q8) meshes are not supported");
+    clear();
+    nodeCount = (int)((N1 + 1) * (N2 + 1));
+    count4 = (int)(N1 * N2);
+    node = new vec2[nodeCount];
+    secOrdNodes = new bool[nodeCount];
+    std::fill(secOrdNodes, secOrdNodes + nodeCount, false);
+    double h1 = (x2 - x1) / N1, h2 = (y2 - y1) / N2;
+    for (size_t i = 0; i <= N1; ++i)
+        for (size_t j = 0; j <= N2; ++j) node[i * (N2 + 1) + j] = vec2(x1 + h1 * i, y1 + h2 * j);
+    elem3 = new int[1];
+    elem8 = new int[1];
+    elem4 = new int[4 * (size_t)count4];
+    for (size_t i = 0; i < N1; ++i)
+        for (size_t j = 0; j < N2; ++j) {
+            size_t b = 4 * (i * N2 + j);
+            elem4[b] = (int)((i + 1) * (N2 + 1) + j + 1);
+            elem4[b + 1] = (int)(i * (N2 + 1) + j + 1);
+            elem4[b + 2] = (int)(i * (N2 + 1) + j);
+            elem4[b + 3] = (int)((i + 1) * (N2 + 1) + j);
+        }
+    bordersCount = 4;
+    borders = new int*[4];
+    borderLength = new int[4];
+    borderLength[0] = borderLength[2] = (int)N2 + 1;
+    borderLength[1] = borderLength[3] = (int)N1 + 1;
+    for (int b = 0; b < 4; ++b) borders[b] = new int[borderLength[b]];
+    for (size_t i = 0; i <= N2; ++i) {
+        borders[0][N2 - i] = (int)((N1 + 1) * (N2 + 1) - i - 1);
+        borders[2][N2 - i] = (int)i;
+    }
+    for (size_t i = 0; i <= N1; ++i) {
+        borders[1][N1 - i] = (int)((i + 1) * (N2 + 1) - 1);
+        borders[3][N1 - i] = (int)((N1 - i) * (N2 + 1));
+    }
+    fillPos();
+}
+
+void Mesh::genRectWithHole(double x1, double x2, double y1, double y2, double holeRad, size_t N1, size_t N2,
+                           int order, int radNOverride) {
+    if (order != 1) throw std::invalid_argument("second-order (Q8) meshes are not supported");
+    clear();
+    int borderN = (int)((N1 + N2) * 2);
+    int radN = (int)((N1 + N2) / 4);
+    radN = (int)std::round(double(radN) * (x2 - x1 + y2 - y1 - 4. * holeRad) * 2. / (x2 - x1 + y2 - y1));
+    if (radNOverride > 0) radN = radNOverride;
+    nodeCount = borderN * (radN + 1);
+    node = new vec2[nodeCount];
+    secOrdNodes = new bool[nodeCount];
+    std::fill(secOrdNodes, secOrdNodes + nodeCount, false);
+    bordersCount = 5;
+    borders = new int*[5];
+    borderLength = new int[5];
+    borderLength[0] = borderLength[2] = (int)N1 + 1;
+    borderLength[1] = borderLength[3] = (int)N2 + 1;
+    borderLength[4] = borderN + 1;
+    for (int b = 0; b < 5; ++b) borders[b] = new int[borderLength[b]];
+    int nodeId = 0;
+    double hx = (x2 - x1) / N1, hy = (y2 - y1) / N2;
+    for (size_t i = 0; i < N1; ++i, ++nodeId) {
+        node[nodeId] = vec2(x1 + i * hx, y1);
+        borders[0][i] = nodeId;
+    }
+    borders[0][borderLength[0] - 1] = nodeId;
+    for (size_t j = 0; j < N2; ++j, ++nodeId) {
+        node[nodeId] = vec2(x2, y1 + j * hy);
+        borders[1][j] = nodeId;
+    }
+    borders[1][borderLength[1] - 1] = nodeId;
+    for (size_t i = 0; i < N1; ++i, ++nodeId) {
+        node[nodeId] = vec2(x2 - i * hx, y2);
+        borders[2][i] = nodeId;
+    }
+    borders[2][borderLength[2] - 1] = nodeId;
+    for (size_t j = 0; j < N2; ++j, ++nodeId) {
+        node[nodeId] = vec2(x1, y2 - j * hy);
+        borders[3][j] = nodeId;
+    }
+    borders[3][borderLength[3] - 1] = 0;
+    double phi = 2. * kPi / borderN;
+    nodeId = radN * borderN;
+    vec2 center(0.5 * (x1 + x2), 0.5 * (y1 + y2));
+    double start = phi * (N1 + N2 * 1.5);
+    for (int i = 0; i < borderN; ++i, ++nodeId) {
+        node[nodeId] = center + vec2(std::cos(start + i * phi), std::sin(start + i * phi)) * holeRad;
+        borders[4][borderN - i - 1] = nodeId;
+    }
+    borders[4][borderLength[4] - 1] = nodeCount - 1;
+    vec2 rh = (node[radN * borderN] - node[0]) / radN;
+    for (int i = 1; i < radN; ++i) node[i * borderN] = node[0] + rh * i;
+    rh = (node[nodeCount - 1] - node[borderN - 1]) / radN;
+    for (int i = 1; i < radN; ++i) node[i * borderN + borderN - 1] = node[borderN - 1] + rh * i;
+    for (int j = 1; j < borderN; ++j) {
+        vec2 r2 = (node[radN * borderN + j] - node[j]) / radN;
+        for (int i = 1; i < radN; ++i) node[i * borderN + j] = node[j] + r2 * i;
+    }
+    count4 = borderN * radN;
+    elem3 = new int[1];
+    elem8 = new int[1];
+    elem4 = new int[4 * (size_t)count4];
+    for (int i = 0; i < radN; ++i)
+        for (int j = 0; j < borderN - 1; ++j) {
+            size_t b = 4 * ((size_t)j * radN + i);
+            elem4[b + 1] = (i + 1) * borderN + j;
+            elem4[b + 2] = i * borderN + j;
+            elem4[b + 3] = i * borderN + j + 1;
+            elem4[b + 0] = (i + 1) * borderN + j + 1;
+        }
+    for (int i = 0; i < radN; ++i) {
+        size_t b = 4 * ((size_t)(borderN - 1) * radN + i);
+        elem4[b + 1] = (i + 1) * borderN + borderN - 1;
+        elem4[b + 2] = i * borderN + borderN - 1;
+        elem4[b + 3] = i * borderN;
+        elem4[b + 0] = (i + 1) * borderN;
+    }
+    fillPos();
+    renumerateRing(borderN);
+}
+
+void Mesh::genRing(double a, double b, size_t N_phi, size_t N_r, int order) {
+    if (order != 1) throw std::invalid_argument("second-order (Q8) meshes are not supported");
+    clear();
+    nodeCount = (int)((N_r + 1) * N_phi);
+    node = new vec2[nodeCount];
+    secOrdNodes = new bool[nodeCount];
+    std::fill(secOrdNodes, secOrdNodes + nodeCount, false);
+    bordersCount = 2;
+    borders = new int*[2];
+    borderLength = new int[2];
+    borderLength[0] = borderLength[1] = (int)N_phi + 1;
+    for (int k = 0; k < 2; ++k) borders[k] = new int[borderLength[k]];
+    double h_r = (b - a) / N_r, h_phi = 2. * kPi / N_phi;
+    for (size_t j = 0; j < N_phi; ++j) {
+        for (size_t i = 0; i <= N_r; ++i) {
+            double r = b - h_r * i, ph = h_phi * j;
+            node[i * N_phi + j] = vec2(r * std::cos(ph), r * std::sin(ph));
+        }
+        borders[1][N_phi - j] = (int)j;
+        borders[0][j] = (int)(N_r * N_phi + j);
+    }
+    borders[1][0] = 0;
+    borders[0][borderLength[1] - 1] = (int)(N_r * N_phi);
+    count4 = (int)(N_r * N_phi);
+    elem3 = new int[1];
+    elem8 = new int[1];
+    elem4 = new int[4 * (size_t)count4];
+    for (size_t i = 0; i < N_r; ++i)
+        for (size_t j = 0; j + 1 < N_phi; ++j) {
+            size_t k = 4 * (j * N_r + i);
+            elem4[k] = (int)((i + 1) * N_phi + j + 1);
+            elem4[k + 3] = (int)(i * N_phi + j + 1);
+            elem4[k + 2] = (int)(i * N_phi + j);
+            elem4[k + 1] = (int)((i + 1) * N_phi + j);
+        }
+    for (size_t i = 0; i < N_r; ++i) {
+        size_t k = 4 * ((N_phi - 1) * N_r + i);
+        elem4[k] = (int)((i + 1) * N_phi);
+        elem4[k + 3] = (int)(i * N_phi);
+        elem4[k + 2] = (int)(i * N_phi + N_phi - 1);
+        elem4[k + 1] = (int)((i + 1) * N_phi + N_phi - 1);
+    }
+    fillPos();
+    renumerateRing((int)N_phi);
+}
+
+void Mesh::renumerateRing(int borderN) {
+    // Columns are numbered pairwise from both ends inwards, which keeps the
+    // index distance between neighbours small. For an odd column count the
+    // reference's last loop writes the old index instead of the new one
+    // (src/Mesh.cu:347-349); that is reproduced so the numbering matches it.
+    std::vector<int> newNodes(nodeCount, 0);
+    int newN = 0, radN = nodeCount / borderN, jBack = borderN - 1, jFront = 0;
+    while (jBack > jFront) {
+        for (int i = 0; i < radN; ++i) newNodes[i * borderN + jFront] = newN++;
+        for (int i = 0; i < radN; ++i) newNodes[i * borderN + jBack] = newN++;
+        ++jFront;
+        --jBack;
+    }
+    if (jBack == jFront)
+        for (int i = 0; i < radN; ++i) newNodes[newN++] = i * borderN + jFront;
+    for (int i = 0; i < 4 * count4; ++i) elem4[i] = newNodes[elem4[i]];
+    for (int b = 0; b < bordersCount; ++b)
+        for (int j = 0; j < borderLength[b]; ++j) borders[b][j] = newNodes[borders[b][j]];
+    std::vector<vec2> nodes(nodeCount);
+    for (int i = 0; i < nodeCount; ++i) nodes[newNodes[i]] = node[i];
+    std::copy(nodes.begin(), nodes.end(), node);
+}
+
+void Mesh::splitToTriangles() {
+    int* e3 = new int[6 * (size_t)count4 + 1];
+    for (int e = 0; e < count4; ++e) {
+        const int* q = elem4 + 4 * (size_t)e;
+        int* t = e3 + 6 * (size_t)e;
+        t[0] = q[0]; t[1] = q[1]; t[2] = q[2];
+        t[3] = q[0]; t[4] = q[2]; t[5] = q[3];
+    }
+    delete[] elem3;
+    elem3 = e3;
+    count3 = 2 * count4;
+    delete[] elem4;
+    elem4 = new int[1];
+    count4 = 0;
+    fillPos();
+}
+
+int Mesh::findMaxIndexDiff() const {
+    int mx = 0;
+    for (int e = 0; e < count3; ++e)
+        for (int i = 3 * e; i < 3 * (e + 1); ++i)
+            for (int j = i + 1; j < 3 * (e + 1); ++j) mx = std::max(mx, std::abs(elem3[i] - elem3[j]));
+    for (int e = 0; e < count4; ++e)
+        for (int i = 4 * e; i < 4 * (e + 1); ++i)
+            for (int j = i + 1; j < 4 * (e + 1); ++j) mx = std::max(mx, std::abs(elem4[i] - elem4[j]));
+    return mx;
+}
+
+double Mesh::elemSpace3(int e) const {
+    double s1 = 0., s2 = 0.;
+    for (int i = 3 * e + 1; i < 3 * (e + 1); ++i) {
+        s1 += node[elem3[i - 1]].x * node[elem3[i]].y;
+        s2 += node[elem3[i - 1]].y * node[elem3[i]].x;
+    }
+    s1 += node[elem3[3 * (e + 1) - 1]].x * node[elem3[3 * e]].y;
+    s2 += node[elem3[3 * (e + 1) - 1]].y * node[elem3[3 * e]].x;
+    return std::fabs(s1 - s2) * 0.5;
+}
+
+double Mesh::elemSpace4(int e) const {
+    double s1 = 0., s2 = 0.;
+    for (int i = 4 * e + 1; i < 4 * (e + 1); ++i) {
+        s1 += node[elem4[i - 1]].x * node[elem4[i]].y;
+        s2 += node[elem4[i - 1]].y * node[elem4[i]].x;
+    }
+    s1 += node[elem4[4 * (e + 1) - 1]].x * node[elem4[4 * e]].y;
+    s2 += node[elem4[4 * (e + 1) - 1]].y * node[elem4[4 * e]].x;
+    return std::fabs(s1 - s2) * 0.5;
+}
+
+}  // namespace cuplast

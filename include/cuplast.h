@@ -1,0 +1,185 @@
+/*
+ * cuplast.h -- C ABI of the B200 (sm_100a) implementation of CudaPlasticity's
+ * 2D elasto-plastic FEM hot path: element B / B^T D B stiffness, CSR sparsity
+ * and slot-map assembly, masked conjugate gradients, and the secant
+ * ("variable elastic parameters") plastic update inside the outer iterations.
+ *
+ * The reference exposes this path only through C++ classes (no C ABI). Each
+ * entry point below names the reference code it replaces; the C++ drop-in
+ * classes with the reference's names (include/cuplast/*.hpp) are written on
+ * top of these functions.
+ *
+ * Conventions: every function returns a cp_status (0 = CP_OK); on error the
+ * context keeps a message (cp_context_last_error). All array arguments are
+ * plain HOST pointers with the sizes stated; nothing here exposes CUDA or
+ * PyTorch types. DOF order is the reference's: (u_0, v_0, u_1, v_1, ...).
+ * Element numbering is the reference's: triangles first, then quads
+ * (Mesh::elemPos, src/Mesh.cuh:26-30).
+ */
+#ifndef CUPLAST_H
+#define CUPLAST_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define CP_API __attribute__((visibility("default")))
+#else
+#define CP_API
+#endif
+
+typedef enum {
+    CP_OK = 0,
+    CP_ERR_INVALID = 1,        /* bad argument */
+    CP_ERR_CUDA = 2,           /* a CUDA call failed */
+    CP_ERR_NOMEM = 3,          /* device memory exhausted / above the admission limit */
+    CP_ERR_NOT_CONVERGED = 4,  /* iteration cap reached */
+    CP_ERR_BREAKDOWN = 5,      /* NaN/Inf or a non-positive curvature in CG */
+    CP_ERR_MESH = 6,           /* malformed mesh (bad node index, degenerate element) */
+    CP_ERR_UNSUPPORTED = 7,
+    CP_ERR_BUSY = 8,
+    CP_ERR_NO_DEVICE = 9,      /* no CUDA device visible */
+    CP_ERR_CANCELLED = 10
+} cp_status;
+
+typedef struct cp_context cp_context;
+typedef struct cp_instance cp_instance;
+
+enum { CP_PLANE_STRESS = 0, CP_PLANE_STRAIN = 1 };           /* plainCondition, src/PlasticitySolver.cuh:15 */
+enum {
+    CP_DIAGRAM_ELASTIC = 0,   /* sigma = E eps */
+    CP_DIAGRAM_LINEAR = 1,    /* Material::setLinearPlast, src/Material.cu:14-17,29-35 */
+    CP_DIAGRAM_POWER = 2,     /* Material::setPowerPlast, src/Material.cu:19-23,37-43 */
+    CP_DIAGRAM_HOLLOMON = 3,  /* sigma = sigma_y (1 + eps_p / eps0)^n (new) */
+    CP_DIAGRAM_PIECEWISE = 4  /* elastic to (pw_eps[0], pw_sig[0]), then piecewise linear (new) */
+};
+enum { CP_PREC_FP64 = 0, CP_PREC_MIXED = 1 };
+#define CP_MAX_PW 16
+
+/* Material and hardening diagram (class Material, src/Material.cuh:9-40). */
+typedef struct {
+    double E, nu, h, rho;
+    int plane;
+    int diagram;
+    double sigma_t;   /* yield stress: sigmaT (linear/power) or sigma_y (Hollomon) */
+    double k_t;       /* linear: hardening modulus K_T */
+    double a, m;      /* power: A, m */
+    double eps0, n;   /* Hollomon */
+    int n_points;     /* piecewise: breakpoints, pw_eps ascending, pw_sig[k] = f(pw_eps[k]) */
+    double pw_eps[CP_MAX_PW], pw_sig[CP_MAX_PW];
+} cp_material;
+
+/* A mesh as the public arrays of class Mesh (src/Mesh.cuh:42-66). */
+typedef struct {
+    int node_count;
+    const double* node_xy;  /* 2 * node_count */
+    int count3;
+    const int* elem3;       /* 3 * count3 */
+    int count4;
+    const int* elem4;       /* 4 * count4 */
+} cp_mesh_view;
+
+typedef struct {
+    int precision;       /* CP_PREC_FP64: FP64 throughout; CP_PREC_MIXED: FP32 matrix + inner CG, FP64 defect correction */
+    double cg_tol;       /* linear solve: stop when ||r|| / ||b|| <= cg_tol (reference: 1e-7) */
+    double outer_tol;    /* secant iteration: stop when relErr <= outer_tol (reference: 1e-5) */
+    int max_outer;       /* per load level (reference CPU path: 50) */
+    long long max_cg;    /* per linear solve */
+    int levels;          /* load levels lambda_k = k / levels, k = 1..levels, each warm-started */
+    int aitken;          /* 1: Aitken-relaxed secant iteration (same fixed point) */
+    double inner_tol;    /* mixed precision: relative tolerance of each FP32 inner solve */
+    int adaptive_cg;     /* 1: linear tolerance follows the outer error (inexact early steps) */
+    int precond;         /* 0: unpreconditioned CG as the reference; 1: 2x2 block-Jacobi PCG (same solution) */
+} cp_solve_opts;
+
+typedef struct {
+    int status;
+    int outer_iters;      /* summed over levels */
+    long long cg_iters;   /* summed over all linear solves (FP32 inner iterations in mixed mode) */
+    long long fp64_spmv;  /* FP64 residual evaluations (mixed mode) */
+    double rel_err;       /* final relErr of the secant iteration */
+    double cg_rel_res;    /* final ||r|| / ||b|| of the last linear solve (FP64) */
+    double seconds;       /* device time of the solve (CUDA events) */
+    int levels_done;
+    long long kernel_launches;  /* kernels launched by the solve (graph nodes included) */
+} cp_solve_report;
+
+/* ------------------------------------------------------------ library --- */
+CP_API const char* cp_version(void);
+CP_API const char* cp_status_string(int status);
+CP_API int cp_device_count(int* count);
+
+/* ------------------------------------------------------------ context --- */
+/* One context per device and stream; all instances of a context run on its
+ * stream. Replaces the reference's implicit device 0 (src/Mesh.cuh:86-104). */
+CP_API int cp_context_create(int device, cp_context** out);
+CP_API int cp_context_destroy(cp_context* ctx);
+CP_API const char* cp_context_last_error(const cp_context* ctx);
+CP_API int cp_context_synchronize(cp_context* ctx);
+
+/* ----------------------------------------------------------- instance --- */
+/* Uploads the mesh, builds on the device the reference CSR structure of
+ * SparseSLAE(Mesh&, 2) (src/SparseSLAE.h:60-196) and the element-to-CSR slot
+ * map, and allocates the per-element secant state. Replaces the set-up part
+ * of PlasticitySolver::PlasticitySolver + solveCUDA
+ * (src/PlasticitySolver.cuh:236-338, src/PlasticitySolver.cu:469-485). */
+CP_API int cp_instance_create(cp_context* ctx, const cp_mesh_view* mesh, const cp_material* mat, cp_instance** out);
+CP_API int cp_instance_destroy(cp_instance* inst);
+/* Device bytes an instance of this mesh holds (for admission control). */
+CP_API int cp_instance_footprint(const cp_mesh_view* mesh, int precision, size_t* bytes);
+CP_API int cp_instance_sizes(const cp_instance* inst, int* node_count, int* elem_count, long long* nnz,
+                             long long* nadj);
+/* Right-hand side, Dirichlet mask (1 = free DOF, 0 = prescribed) and the
+ * prescribed/initial displacements, all of length 2 * node_count, as built by
+ * initConditions (src/PlasticitySolver.cu:812-1005). Resets uv. */
+CP_API int cp_instance_set_loads(cp_instance* inst, const double* rp, const unsigned char* mask, const double* uv);
+/* psi = 1, E_c = E, nu_c = nu (initPlastParams, src/PlasticitySolver.cu:385-415). */
+CP_API int cp_instance_reset_state(cp_instance* inst);
+/* Scales the loads to level lam: rp = lam * rp_full, uv[prescribed] = lam * uv_full. */
+CP_API int cp_instance_set_level(cp_instance* inst, double lam);
+
+/* ------------------------------------------------------------- phases --- */
+/* K(E_c, nu_c) into the CSR values: fillGlobalStiffness + insertKe4
+ * (src/PlasticitySolver.cu:1413-1499), no band matrix and no atomics. */
+CP_API int cp_assemble(cp_instance* inst, int precision);
+/* Masked CG from the current uv: ConjGradCuda::solve (src/ConjGradCuda.cu:185-231). */
+CP_API int cp_cg_solve(cp_instance* inst, double eps, long long max_iter, long long* iters, double* rel_res);
+/* Strain, stress, secant update and exit norm: strain4 + plastStress +
+ * exitCondition (src/PlasticitySolver.cu:1517-1549,1590-1610,1722-1735). */
+CP_API int cp_secant_update(cp_instance* inst, double* rel_err);
+/* Plastic strains: plastDeform (src/PlasticitySolver.cu:1641-1662). */
+CP_API int cp_plastic_strains(cp_instance* inst);
+/* The whole outer loop: solveCUDA (src/PlasticitySolver.cu:469-512). */
+CP_API void cp_solve_opts_default(cp_solve_opts* opts);
+CP_API int cp_solve(cp_instance* inst, const cp_solve_opts* opts, cp_solve_report* report);
+
+/* Kernel timing of the linear solver (no reference counterpart; the
+ * reference times whole solves only, src/Main.cpp:458-902): assembles K at
+ * the current state, starts a CG from the current uv and runs `iters`
+ * iterations as direct launches, with CUDA events around every SpMV (P) and
+ * update (U) kernel. Outputs the mean duration of each in milliseconds and
+ * the bytes each must move per launch (see DESIGN.md's roofline section).
+ * Leaves uv changed. */
+CP_API int cp_bench_cg(cp_instance* inst, int precision, int precond, int iters, double* ms_spmv, double* ms_update,
+                       double* bytes_spmv, double* bytes_update);
+
+/* ---------------------------------------------------------- read-back --- */
+/* Reference CSR arrays (SparseSLAE::rows/cols/adjPos/adj/data); any pointer
+ * may be NULL. values: the last assembly (FP64, or FP32 widened). */
+CP_API int cp_get_csr(cp_instance* inst, int* rows, int* cols, int* adj_pos, int* adj, double* values);
+/* slots[off_e + i*nen + j] = index in values of K(2*node_i, 2*node_j) of
+ * element e; off_e = 9e for triangles, 9*count3 + 16(e - count3) for quads. */
+CP_API int cp_get_slot_map(cp_instance* inst, int* slots);
+/* Fields by name: "uv" (2 * node_count) or per element "exx", "eyy", "gamma",
+ * "eps_i", "sxx", "syy", "tau", "sig_i", "table_s", "psi", "E_c", "nu_c",
+ * "exx_p", "eyy_p", "gamma_p", "eps_p_i" (PlasticitySolver::dataToRAM). */
+CP_API int cp_get_field(cp_instance* inst, const char* name, double* out);
+CP_API int cp_set_field(cp_instance* inst, const char* name, const double* in);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,71 @@
+// Mesh of the drop-in API: the public fields and generators of the
+// reference's class Mesh (src/Mesh.cuh:22-318), host side only. The device
+// copy lives in the solver instance (cp_instance), so there are no dev_*
+// fields and no meshToGPU / meshToRAM round trips.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "vec2.hpp"
+
+namespace cuplast {
+
+class CUPLAST_CXX_API Mesh {
+public:
+    bool useCuda = true;   // kept for source compatibility; the solver always runs on the GPU
+    bool ramSaved = true;
+
+    int count3 = 0, count4 = 0, count8 = 0;
+    int* elem3 = nullptr;
+    int* elem4 = nullptr;
+    int* elem8 = nullptr;
+    int elemPos[3] = {};
+
+    int nodeCount = 0;
+    vec2* node = nullptr;
+    bool* secOrdNodes = nullptr;
+
+    int bordersCount = 0;
+    int* borderLength = nullptr;
+    int** borders = nullptr;
+
+    Mesh() = default;
+    Mesh(const Mesh& other);
+    Mesh& operator=(const Mesh& other);
+    ~Mesh();
+
+    int elemCount() const { return elemPos[2]; }
+
+    // src/Mesh.cu:17-110
+    void genRectangle(double x1, double x2, double y1, double y2, size_t N1, size_t N2, int order = 1);
+    // src/Mesh.cu:112-246. radN > 0 overrides the reference's radial count
+    // (which it ties to the perimeter count): the O-grid of the benchmarks.
+    void genRectWithHole(double x1, double x2, double y1, double y2, double holeRad, size_t N1, size_t N2,
+                         int order = 1, int radN = 0);
+    // src/Mesh.cu:249-329
+    void genRing(double a, double b, size_t N_phi, size_t N_r, int order = 1);
+    // src/Mesh.cu:332-380
+    void renumerateRing(int borderN);
+    // Extension: every quad (n1,n2,n3,n4) becomes (n1,n2,n3), (n1,n3,n4).
+    void splitToTriangles();
+    // src/Mesh.cu:417-440
+    int findMaxIndexDiff() const;
+
+    double elemSpace3(int e) const;
+    double elemSpace4(int e) const;
+
+    // Replaces the arrays (takes copies).
+    void assign(int nodes, const double* xy, int c3, const int* e3, int c4, const int* e4,
+                const std::vector<std::vector<int>>& borderLists);
+
+private:
+    void clear();
+    void fillPos() {
+        elemPos[0] = count3;
+        elemPos[1] = elemPos[0] + count4;
+        elemPos[2] = elemPos[1] + count8;
+    }
+};
+
+}  // namespace cuplast

@@ -1,0 +1,62 @@
+/*
+ * cuplast_host.h -- C ABI over the host-side half of the drop-in API (the
+ * C++ classes Mesh and LoadConditions of include/cuplast/*.hpp), so that
+ * non-C++ callers (the Python package, tests, benchmarks) use the same mesh
+ * generators and the same right-hand-side / Dirichlet-mask construction as
+ * C++ users. No function here touches the GPU.
+ */
+#ifndef CUPLAST_HOST_H
+#define CUPLAST_HOST_H
+
+#include "cuplast.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cpx_mesh cpx_mesh;
+typedef struct cpx_loads cpx_loads;
+
+CP_API int cpx_mesh_create(cpx_mesh** out);
+CP_API int cpx_mesh_destroy(cpx_mesh* m);
+/* Mesh::genRectangle (src/Mesh.cu:17-110) */
+CP_API int cpx_mesh_gen_rect(cpx_mesh* m, double x1, double x2, double y1, double y2, int n1, int n2);
+/* Mesh::genRectWithHole (src/Mesh.cu:112-246); rad_n > 0 overrides the reference's radial count */
+CP_API int cpx_mesh_gen_rect_with_hole(cpx_mesh* m, double x1, double x2, double y1, double y2, double hole_rad,
+                                       int n1, int n2, int rad_n);
+/* Mesh::genRing (src/Mesh.cu:249-329) */
+CP_API int cpx_mesh_gen_ring(cpx_mesh* m, double a, double b, int n_phi, int n_r);
+/* every quad (n1,n2,n3,n4) -> triangles (n1,n2,n3), (n1,n3,n4) (extension) */
+CP_API int cpx_mesh_split_t3(cpx_mesh* m);
+CP_API int cpx_mesh_set(cpx_mesh* m, int node_count, const double* xy, int count3, const int* elem3, int count4,
+                        const int* elem4, int n_borders, const int* border_len, const int* border_nodes);
+CP_API int cpx_mesh_counts(const cpx_mesh* m, int* node_count, int* count3, int* count4, int* n_borders,
+                           int* border_total);
+CP_API int cpx_mesh_get(const cpx_mesh* m, double* xy, int* elem3, int* elem4, int* border_len, int* border_nodes);
+CP_API int cpx_mesh_max_index_diff(const cpx_mesh* m, int* out);
+
+CP_API int cpx_loads_create(cpx_loads** out);
+CP_API int cpx_loads_destroy(cpx_loads* l);
+/* LoadConditions setters (src/LoadConditions.cuh:70-179), constant-valued */
+CP_API int cpx_loads_set_force(cpx_loads* l, int border, double fx, double fy, int normal);
+CP_API int cpx_loads_set_displacement(cpx_loads* l, int border, double ux, double uy, int fix_mid_x, int fix_mid_y);
+CP_API int cpx_loads_fix_border(cpx_loads* l, int border);
+CP_API int cpx_loads_fix_border_vert(cpx_loads* l, int border);
+CP_API int cpx_loads_fix_border_hor(cpx_loads* l, int border);
+CP_API int cpx_loads_fix_vert_axis(cpx_loads* l, double x);
+CP_API int cpx_loads_fix_hor_axis(cpx_loads* l, double y);
+CP_API int cpx_loads_fix_point(cpx_loads* l, double x, double y);
+CP_API int cpx_loads_set_displ_point(cpx_loads* l, double x, double y, double ux, double uy);
+CP_API int cpx_loads_set_force_point(cpx_loads* l, double x, double y, double fx, double fy);
+CP_API int cpx_loads_set_gravity(cpx_loads* l, double g, double dx, double dy);
+CP_API int cpx_loads_set_rotation(cpx_loads* l, double omega, double ax, double ay);
+CP_API int cpx_loads_fix_dof(cpx_loads* l, int dof);
+/* initConditions (src/PlasticitySolver.cu:812-1005): rp, mask (1 = free) and
+ * the prescribed displacements, each 2 * node_count long. */
+CP_API int cpx_loads_build(const cpx_mesh* m, const cpx_loads* l, double h, double rho, double* rp,
+                           unsigned char* mask, double* uv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

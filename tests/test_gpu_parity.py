@@ -1,0 +1,182 @@
+"""GPU parity of the product (CUDA kernels through the C ABI) against the
+reference's golden fixtures and the oracle, on the same seeded inputs.
+
+Bars: integer work (CSR rows/cols/adjacency, slot maps, Dirichlet mask)
+bit-exact; assembled FP64 values within 1e-13 of the row scale (summation
+order differs); converged FP64 state within 1e-10 relative L2 (each field
+normalised by its natural scale, tests/parity.py) with the identical yielded
+set; the mixed-precision mode within 1e-8 of the FP64 oracle."""
+import os
+
+import numpy as np
+import pytest
+
+import cudaplasticity_b200 as cp
+import oracle
+import product_runner
+import scenarios
+from parity import FIELDS, field_error, worst, yielded
+
+pytestmark = pytest.mark.gpu
+
+REF_SCEN = [n for n, s in scenarios.SCENARIOS.items() if s.get("reference")]
+FP64_TOL = 1e-10
+MIXED_TOL = 1e-8
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = cp.Context(0)
+    yield c
+    c.close()
+
+
+def load_golden(golden_dir, name):
+    return dict(np.load(os.path.join(golden_dir, f"{name}.npz")))
+
+
+def scenario(name, workdir):
+    return scenarios.scenario_lines(name, os.path.join(workdir, f"{name}.bin"))
+
+
+@pytest.mark.parametrize("name", REF_SCEN)
+def test_structure_and_assembly_match_reference(name, ctx, golden_dir, workdir):
+    g = load_golden(golden_dir, name)
+    m, lines = scenario(name, workdir)
+    r = product_runner.run(ctx, lines, m, want_k=True)
+    for k in ["rows", "cols", "adj_pos", "adj", "mask"]:
+        assert np.array_equal(r[k], g[k]), k
+    # first assembly at E_c = E, nu_c = nu: values equal up to summation order
+    rows = g["rows"]
+    scale = np.repeat(np.maximum.reduceat(np.abs(g["k_data"]), rows[:-1]), np.diff(rows))
+    assert np.max(np.abs(r["k_data"] - g["k_data"]) / scale) < 1e-13
+    # the product's matrix is exactly symmetric (it assembles K(i,j) and
+    # K(j,i) from the same products)
+    n = len(rows) - 1
+    K = {(i, c): v for i in range(n) for c, v in zip(r["cols"][rows[i]:rows[i + 1]], r["k_data"][rows[i]:rows[i + 1]])}
+    assert all(K[(c, i)] == v for (i, c), v in K.items())
+
+
+@pytest.mark.parametrize("name", REF_SCEN)
+def test_converged_state_matches_reference(name, ctx, golden_dir, workdir):
+    g = load_golden(golden_dir, name)
+    m, lines = scenario(name, workdir)
+    r = product_runner.run(ctx, lines, m)
+    k, err, errs = worst(r, g)
+    assert err <= FP64_TOL, (k, err, errs)
+    assert np.array_equal(yielded(r), yielded(g))
+    assert list(r["report"]["levels_done"] for _ in [0]) == [scenarios.SCENARIOS[name].get("levels", 1)]
+
+
+def test_slot_map_matches_oracle(ctx, workdir):
+    for name in ["hole12_pow", "ogrid16_t3", "ring_pw"]:
+        m, lines = scenario(name, workdir)
+        path = os.path.join(workdir, f"{name}.bin")
+        oracle.write_mesh(path, m["node_xy"], elem3=m["elem3"], elem4=m["elem4"], borders=m["borders"])
+        o = oracle.run_oracle(["mode csr", f"mesh file {path}", "material 1 0.3 1"])
+        r = product_runner.run(ctx, lines, m, want_k=True, max_outer=1, outer_tol=1e300)
+        assert np.array_equal(r["slots"], o["slots"]), name
+        assert np.array_equal(r["rows"], o["rows"]) and np.array_equal(r["cols"], o["cols"]), name
+
+
+def test_triangles_match_oracle(ctx, workdir):
+    """CST extension: no reference counterpart; the oracle restatement is the bar."""
+    name = "ogrid16_t3"
+    m, lines = scenario(name, workdir)
+    path = os.path.join(workdir, f"{name}.bin")
+    oracle.write_mesh(path, m["node_xy"], elem3=m["elem3"], elem4=m["elem4"], borders=m["borders"])
+    o = oracle.run_oracle(lines + ["dump_k 1"])
+    r = product_runner.run(ctx, lines, m, want_k=True)
+    assert np.max(np.abs(r["k_data"] - o["k_data"])) <= 1e-13 * np.max(np.abs(o["k_data"]))
+    k, err, errs = worst(r, o)
+    assert err <= FP64_TOL, (k, err, errs)
+    assert np.array_equal(yielded(r), yielded(o))
+
+
+@pytest.mark.parametrize("name", ["hole12_pow", "ogrid16_bilin", "ring_pw"])
+def test_aitken_and_adaptive_cg_reach_the_same_fixed_point(name, ctx, golden_dir, workdir):
+    g = load_golden(golden_dir, name)
+    m, lines = scenario(name, workdir)
+    plain = product_runner.run(ctx, lines, m)
+    fast = product_runner.run(ctx, lines, m, aitken=1, adaptive_cg=1)
+    k, err, errs = worst(fast, g)
+    assert err <= FP64_TOL, (k, err, errs)
+    assert np.array_equal(yielded(fast), yielded(g))
+    assert fast["report"]["outer_iters"] < plain["report"]["outer_iters"]
+
+
+@pytest.mark.parametrize("name", ["hole12_pow", "ogrid16_bilin", "ogrid16_hollomon"])
+def test_mixed_precision_within_1e8_of_fp64_reference(name, ctx, golden_dir, workdir):
+    """FP32 matrix values and inner CG, FP64 defect correction / u / dot-product
+    reductions / secant update: error stated against the FP64 golden state."""
+    g = load_golden(golden_dir, name)
+    m, lines = scenario(name, workdir)
+    r = product_runner.run(ctx, lines, m, precision=cp.CP_PREC_MIXED, aitken=1, adaptive_cg=1, inner_tol=1e-3)
+    for k in ["uv", "sig_i", "eps_p_i"]:
+        assert field_error(k, r, g) <= MIXED_TOL, (k, field_error(k, r, g))
+    assert np.array_equal(yielded(r, 1e-9), yielded(g, 1e-9))
+
+
+def test_cg_phase_reference_semantics(ctx, golden_dir, workdir):
+    """One elastic solve through the phase entry points: assemble, CG from the
+    current u, secant update; against the oracle's first outer iteration."""
+    name = "hole12_lin"
+    m, lines = scenario(name, workdir)
+    job, (rp, mask, uv) = product_runner.build_inputs(lines, m)
+    inst = cp.Instance(ctx, m, product_runner.material_of(job))
+    inst.set_loads(rp, mask, uv)
+    inst.assemble()
+    it, rel = inst.cg_solve(1e-13)
+    assert rel <= 1e-13 and it > 10
+    rel_err = inst.secant_update()
+    path = os.path.join(workdir, f"{name}.bin")
+    oracle.write_mesh(path, m["node_xy"], elem4=m["elem4"], borders=m["borders"])
+    o = oracle.run_oracle([ln for ln in lines if not ln.startswith(("max_outer", "mode"))] +
+                          ["mode phases", "max_outer 1"])
+    assert abs(rel_err - o["err_per_level"][0]) <= 1e-9 * abs(o["err_per_level"][0])
+    for k in ["uv", "sig_i", "E_c"]:
+        assert field_error(k, inst.state(), o) <= 1e-10
+    inst.close()
+
+
+def test_malformed_mesh_is_rejected(ctx):
+    mat = cp.material(1.0)
+    bad = dict(node_xy=np.zeros((3, 2)), elem4=np.array([[0, 1, 2, 7]]), borders=[])
+    with pytest.raises(cp.CuplastError) as e:
+        cp.Instance(ctx, bad, mat)
+    assert e.value.status == cp._capi.CP_ERR_MESH
+    degenerate = dict(node_xy=np.zeros((4, 2)), elem4=np.array([[0, 1, 1, 3]]), borders=[])
+    with pytest.raises(cp.CuplastError):
+        cp.Instance(ctx, degenerate, mat)
+
+
+def test_iteration_cap_reports_not_converged(ctx, workdir):
+    m, lines = scenario("hole12_pow", workdir)
+    job, (rp, mask, uv) = product_runner.build_inputs(lines, m)
+    inst = cp.Instance(ctx, m, product_runner.material_of(job))
+    inst.set_loads(rp, mask, uv)
+    rep = inst.solve(allow_not_converged=True, cg_tol=1e-13, outer_tol=1e-12, max_outer=3)
+    assert rep["status"] == cp._capi.CP_ERR_NOT_CONVERGED and rep["outer_iters"] == 3
+    # a CG cap too: status comes back from the device, no hang
+    inst.reset_state()
+    inst.assemble()
+    with pytest.raises(cp.CuplastError) as e:
+        inst.cg_solve(1e-30, max_iter=5)
+    assert e.value.status == cp._capi.CP_ERR_NOT_CONVERGED
+    inst.close()
+
+
+def test_singular_system_terminates(ctx):
+    """No Dirichlet conditions: K is singular; the solve must end with an
+    error status (breakdown or iteration cap) instead of hanging."""
+    m = cp.Mesh.rect(0, 1, 0, 1, 2, 2).arrays()
+    inst = cp.Instance(ctx, m, cp.material(1000.0))
+    rp = np.zeros(2 * inst.n_nodes)
+    rp[-2] = 1.0
+    inst.set_loads(rp, np.ones(2 * inst.n_nodes, np.uint8))
+    try:
+        rep = inst.solve(allow_not_converged=True, max_cg=2000, max_outer=2, cg_tol=1e-14)
+        assert rep["cg_iters"] <= 2 * 2000
+    except cp.CuplastError as e:
+        assert e.status == cp._capi.CP_ERR_BREAKDOWN
+    inst.close()

@@ -1,0 +1,106 @@
+"""CPU tests of the product's boundary and host logic (no GPU compute):
+the C ABI library loads and exports every declared symbol; the host-side
+drop-in classes (mesh generators, load/BC builder) reproduce the reference
+bit for bit; device entry points fail cleanly without a device."""
+import glob
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+import cudaplasticity_b200 as cp
+import meshgen
+import scenarios
+from cudaplasticity_b200 import _capi
+from conftest import ROOT, have_gpu
+
+import product_runner
+
+
+def declared_functions():
+    names = []
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        txt = open(h).read()
+        names += re.findall(r"CP_API\s+[\w\s\*]+?\b(\w+)\s*\(", txt)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _capi.lib()
+    names = declared_functions()
+    assert len(names) >= 40
+    for n in names:
+        assert hasattr(lib, n), n
+    # and the ctypes table covers all of them
+    assert set(names) == set(_capi.declared_symbols())
+
+
+def test_version_and_status_strings():
+    assert "sm_100a" in cp.version()
+    assert _capi.lib().cp_status_string(4).decode() == "iteration limit reached"
+
+
+def _digest_of(m):
+    a = m.arrays()
+    return scenarios.mesh_digest(dict(node_xy=a["node_xy"], elem3=a["elem3"], elem4=a["elem4"], borders=a["borders"]))
+
+
+def test_product_mesh_generators_match_reference(golden_dir):
+    ref = json.load(open(os.path.join(golden_dir, "ref_meshes.json")))
+    makers = {
+        "hole -3 3 -2 2 0.5 48 32 1": lambda: cp.Mesh.rect_with_hole(-3, 3, -2, 2, 0.5, 48, 32),
+        "hole -3 3 -2 2 0.5 12 8 1": lambda: cp.Mesh.rect_with_hole(-3, 3, -2, 2, 0.5, 12, 8),
+        "hole -100 100 -100 100 20 16 16 1": lambda: cp.Mesh.rect_with_hole(-100, 100, -100, 100, 20, 16, 16),
+        "ring 50 120 32 8 1": lambda: cp.Mesh.ring(50, 120, 32, 8),
+        "ring 0.1 0.2 40 5 1": lambda: cp.Mesh.ring(0.1, 0.2, 40, 5),
+        "rect -1 1 -1 1 4 4 1": lambda: cp.Mesh.rect(-1, 1, -1, 1, 4, 4),
+        "rect -3 3 -2 2 6 4 1": lambda: cp.Mesh.rect(-3, 3, -2, 2, 6, 4),
+    }
+    for spec, mk in makers.items():
+        m = mk()
+        assert _digest_of(m) == ref[spec]["digest"], spec
+        assert m.max_index_diff() == ref[spec]["max_index_diff"], spec
+
+
+def test_product_ogrid_matches_test_generator():
+    """The O-grid with a free radial count (benchmark meshes) and the T3 split."""
+    a = cp.Mesh.rect_with_hole(-100, 100, -100, 100, 20, 16, 16, rad_n=64).arrays()
+    b = meshgen.hole_plate(-100, 100, -100, 100, 20, 16, 16, rad_n=64)
+    assert np.array_equal(a["node_xy"], b["node_xy"]) and np.array_equal(a["elem4"], b["elem4"])
+    t = cp.Mesh.rect_with_hole(-100, 100, -100, 100, 20, 4, 4, rad_n=8).split_t3().arrays()
+    tb = meshgen.split_t3(meshgen.hole_plate(-100, 100, -100, 100, 20, 4, 4, rad_n=8))
+    assert np.array_equal(t["elem3"], tb["elem3"]) and t["elem4"].size == 0
+
+
+@pytest.mark.parametrize("name", [n for n, s in scenarios.SCENARIOS.items() if s.get("reference")])
+def test_product_loads_match_reference(name, golden_dir, workdir):
+    """initConditions restated in the C++ drop-in classes: the right-hand side
+    and the Dirichlet mask equal the reference's bit for bit."""
+    g = np.load(os.path.join(golden_dir, f"{name}.npz"))
+    m, lines = scenarios.scenario_lines(name, os.path.join(workdir, "m.bin"))
+    _, (rp, mask, uv) = product_runner.build_inputs(lines, m)
+    assert np.array_equal(mask, g["mask"])
+    assert np.array_equal(rp, g["rp"])
+
+
+def test_loads_reject_bad_border():
+    m = cp.Mesh.rect(0, 1, 0, 1, 2, 2)
+    with pytest.raises(cp.CuplastError):
+        cp.Loads().set_force(9, 1.0, 0.0).build(m)
+
+
+def test_footprint_is_host_only():
+    m = meshgen.hole_plate(-100, 100, -100, 100, 20, 16, 16, rad_n=64)
+    f64 = cp.footprint(m, cp.CP_PREC_FP64)
+    fmx = cp.footprint(m, cp.CP_PREC_MIXED)
+    assert fmx > f64 > 4160 * 36 * 8
+
+
+@pytest.mark.skipif(have_gpu(), reason="checks the no-device path")
+def test_device_calls_fail_cleanly_without_gpu():
+    assert cp.device_count() == 0
+    with pytest.raises(cp.CuplastError) as e:
+        cp.Context(0)
+    assert e.value.status == _capi.CP_ERR_NO_DEVICE
