@@ -300,7 +300,7 @@ def run_product_arm(args):
     roofline = {"bound": "hbm", "kernel": "k_cg_p<double> (SpMV+dot) on the 2.1M-DOF config-2 mesh",
                 "achieved": bp / (mp * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                 "frac": bp / (mp * 1e-3) / 1e9 / peak, "traffic": 402.7e6,
-                "traffic_note": "dram read+write of one k_cg_p<double> launch, ncu, profiles/cg_spmv_fp64_2M.md",
+                "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one k_cg_p<double> launch (ncu capture)",
                 "bytes_per_launch": bp, "ms_per_launch": mp, "peak_kind": peak_kind}
 
     cpu = None

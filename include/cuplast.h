@@ -161,8 +161,10 @@ CP_API int cp_solve(cp_instance* inst, const cp_solve_opts* opts, cp_solve_repor
  * the current state, starts a CG from the current uv and runs `iters`
  * iterations as direct launches, with CUDA events around every SpMV (P) and
  * update (U) kernel. Outputs the mean duration of each in milliseconds and
- * the bytes each must move per launch (see DESIGN.md's roofline section).
- * Leaves uv changed. */
+ * the algorithmic bytes each must move per launch: P reads the values, one
+ * 4-byte column per 2x2 block, r and z, and writes z' and K z'; U reads x,
+ * z', r, K z' and the mask and writes x and r (plus M^-1 and s with block
+ * Jacobi). Leaves uv changed. */
 CP_API int cp_bench_cg(cp_instance* inst, int precision, int precond, int iters, double* ms_spmv, double* ms_update,
                        double* bytes_spmv, double* bytes_update);
 
