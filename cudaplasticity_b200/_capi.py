@@ -81,6 +81,8 @@ _SIGS = {
     "cp_solve_opts_default": (None, [ctypes.POINTER(cp_solve_opts)]),
     "cp_solve": (c_int, [c_p, ctypes.POINTER(cp_solve_opts), ctypes.POINTER(cp_solve_report)]),
     "cp_bench_cg": (c_int, [c_p, c_int, c_int, c_int, P_double, P_double, P_double, P_double]),
+    "cp_secant_update_noalloc": (c_int, [c_p, ctypes.POINTER(cp_material), c_int, c_p, c_int, c_p, c_p, c_p, c_p,
+                                         c_p, c_p, P_double]),
     "cp_get_csr": (c_int, [c_p, P_int, P_int, P_int, P_int, P_double]),
     "cp_get_slot_map": (c_int, [c_p, P_int]),
     "cp_get_field": (c_int, [c_p, ctypes.c_char_p, P_double]),

@@ -6,6 +6,8 @@
 // reference stores B and detJ per Gauss point, 288 B per quad, computed once
 // by calcBs4, src/PlasticitySolver.cu:139-144,1237-1246); reading 4 node
 // coordinates costs less HBM traffic than reading B back.
+#include <mutex>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -233,6 +235,7 @@ __device__ double diagram_f(const MaterialDev& M, double eps) {
     }
 }
 
+}  // namespace
 constexpr int kElemThreads = 256;
 
 // strain4 + plastStress + exitNorm2 (src/PlasticitySolver.cu:1517-1549,
@@ -337,6 +340,8 @@ __global__ void __launch_bounds__(kElemThreads) k_update(DevMesh m, MaterialDev 
     }
 }
 
+namespace {
+
 // Aitken (Irons-Tuck) relaxation of the secant iteration on psi:
 // psi_{k+1} = psi_k + w_k r_k, w_k = -w_{k-1} (r_{k-1}, r_k - r_{k-1}) / |r_k - r_{k-1}|^2.
 // The fixed point (r = 0) is the reference's.
@@ -420,3 +425,94 @@ void launch_plastic(const DevMesh& m, const MaterialDev& mat, ElemState& st, cud
 }
 
 }  // namespace cp
+
+// ------------------------------------------------ allocation-free update --
+//
+// Some callers cannot allocate device memory: code that runs while a CUDA
+// graph is being captured (cudaMalloc is not a capturable operation), code
+// inside a framework that owns the whole device memory pool through its own
+// allocator, and real-time loops whose memory budget is fixed up front. For
+// them cp_secant_update_noalloc runs the fused strain / stress / secant-update
+// kernel (k_update above) on buffers the caller already owns. Its only scratch
+// -- the block partial sums of the exit norm and the reduction's scalars --
+// lives in the file-scope array below, which every GPU that loads this library
+// keeps until the process exits.
+namespace {
+
+constexpr int kNoAllocMaxBlocks = 4096;  // one partial-sum slot per block of 256 elements
+constexpr int kNoAllocScalarBytes = 256;  // cp::OuterScalars, padded
+static_assert(sizeof(cp::OuterScalars) <= kNoAllocScalarBytes, "scalars do not fit the scratch header");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScalarBytes + 4 * 8 * kNoAllocMaxBlocks];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device. In host code the
+// array's name is only a host-side stand-in, so the address is looked up once
+// per device (with that device current) and cached.
+int noalloc_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return CP_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return CP_ERR_CUDA;
+        g_noalloc_ptr[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_ptr[device]);
+    return CP_OK;
+}
+
+}  // namespace
+
+extern "C" CP_API int cp_secant_update_noalloc(void* stream, const cp_material* mat, int node_count,
+                                               const double* d_node_xy, int count4, const int* d_elem4,
+                                               const double* d_uv, double* d_E_c, double* d_nu_c, double* d_psi,
+                                               double* d_fields, double* rel_err) {
+    if (!mat || !d_node_xy || !d_elem4 || !d_uv || !d_E_c || !d_nu_c || !d_psi || !d_fields || !rel_err)
+        return CP_ERR_INVALID;
+    if (node_count <= 0 || count4 <= 0) return CP_ERR_INVALID;
+    if ((long long)count4 > (long long)kNoAllocMaxBlocks * cp::kElemThreads) return CP_ERR_INVALID;  // > 1,048,576
+    if (((uintptr_t)d_node_xy | (uintptr_t)d_elem4 | (uintptr_t)d_uv) & 15u) return CP_ERR_INVALID;
+    if (!(mat->E > 0) || !(mat->nu > -1.0 && mat->nu < 0.5) || mat->diagram < CP_DIAGRAM_ELASTIC ||
+        mat->diagram > CP_DIAGRAM_PIECEWISE || (mat->diagram == CP_DIAGRAM_PIECEWISE &&
+                                                 (mat->n_points < 2 || mat->n_points > CP_MAX_PW)))
+        return CP_ERR_INVALID;
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return CP_ERR_NO_DEVICE;
+    unsigned char* scratch = nullptr;
+    int st = noalloc_scratch(device, &scratch);
+    if (st != CP_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cp::OuterScalars* sc = reinterpret_cast<cp::OuterScalars*>(scratch);
+    double* partials = reinterpret_cast<double*>(scratch + kNoAllocScalarBytes);
+    // the array keeps the previous call's contents: the reduction ticket must start at zero
+    if (cudaMemsetAsync(sc, 0, sizeof(cp::OuterScalars), s) != cudaSuccess) return CP_ERR_CUDA;
+    cp::MaterialDev M{};
+    M.E = mat->E; M.nu = mat->nu; M.h = mat->h; M.plane = mat->plane; M.diagram = mat->diagram;
+    M.sigma_t = mat->sigma_t; M.k_t = mat->k_t; M.a = mat->a; M.m = mat->m; M.eps0 = mat->eps0; M.n = mat->n;
+    M.n_points = mat->n_points;
+    for (int i = 0; i < CP_MAX_PW; ++i) { M.pw_eps[i] = mat->pw_eps[i]; M.pw_sig[i] = mat->pw_sig[i]; }
+    cp::DevMesh m;
+    m.n_nodes = node_count;
+    m.c3 = 0;
+    m.c4 = count4;
+    m.xy = reinterpret_cast<double2*>(const_cast<double*>(d_node_xy));
+    m.e4 = reinterpret_cast<int4*>(const_cast<int*>(d_elem4));
+    cp::ElemState es{};
+    const size_t ne = (size_t)count4;
+    es.exx = d_fields; es.eyy = d_fields + ne; es.gam = d_fields + 2 * ne; es.eps_i = d_fields + 3 * ne;
+    es.sxx = d_fields + 4 * ne; es.syy = d_fields + 5 * ne; es.tau = d_fields + 6 * ne; es.sig_i = d_fields + 7 * ne;
+    es.table_s = d_fields + 8 * ne;
+    es.psi = d_psi; es.E_c = d_E_c; es.nu_c = d_nu_c;
+    const int grid = (count4 + cp::kElemThreads - 1) / cp::kElemThreads;  // <= kNoAllocMaxBlocks
+    cp::k_update<<<grid, cp::kElemThreads, 0, s>>>(m, M, reinterpret_cast<const double2*>(d_uv), es, sc, partials, 0);
+    if (cudaGetLastError() != cudaSuccess) return CP_ERR_CUDA;
+    double host_err = 0.0;
+    if (cudaMemcpyAsync(&host_err, &sc->rel_err, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return CP_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return CP_ERR_CUDA;
+    *rel_err = host_err;
+    return CP_OK;
+}

@@ -168,6 +168,30 @@ CP_API int cp_solve(cp_instance* inst, const cp_solve_opts* opts, cp_solve_repor
 CP_API int cp_bench_cg(cp_instance* inst, int precision, int precond, int iters, double* ms_spmv, double* ms_update,
                        double* bytes_spmv, double* bytes_update);
 
+/* Allocation-free secant update (no counterpart in the reference). For
+ * callers that cannot allocate device memory -- code running while a CUDA
+ * graph is captured, code inside a framework whose allocator owns the device
+ * memory, loops with a fixed memory budget -- this runs the same fused
+ * strain / stress / secant-update / exit-norm kernel as cp_secant_update on
+ * buffers the caller owns, and allocates nothing (no cudaMalloc, no cudaFree,
+ * no allocating library call). Every pointer except mat and rel_err is a
+ * DEVICE pointer on the current device; node_xy, elem4 and uv must be 16-byte
+ * aligned. Quad meshes only: count4 <= 1,048,576 elements, larger meshes
+ * return CP_ERR_INVALID. In: node_xy (2 * node_count), elem4 (4 * count4), uv
+ * (2 * node_count), E_c / nu_c (count4, the moduli K was assembled with).
+ * Out: E_c, nu_c, psi updated; fields = 9 * count4 doubles, one block of
+ * count4 each: exx, eyy, gamma, eps_i, sxx, syy, tau, sig_i, table_s; *rel_err
+ * = the exit norm; the call returns when the result is on the host.
+ * Its scratch (the exit norm's per-block partial sums and scalars) is a
+ * file-scope device array of 131,328 bytes that every GPU loading the library holds
+ * until exit. The first call on each device looks up that array's address
+ * (with the device current); make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU, on any stream,
+ * race and must be serialised by the caller. stream may be NULL. */
+CP_API int cp_secant_update_noalloc(void* stream, const cp_material* mat, int node_count, const double* node_xy,
+                                    int count4, const int* elem4, const double* uv, double* E_c, double* nu_c,
+                                    double* psi, double* fields, double* rel_err);
+
 /* ---------------------------------------------------------- read-back --- */
 /* Reference CSR arrays (SparseSLAE::rows/cols/adjPos/adj/data); any pointer
  * may be NULL. values: the last assembly (FP64, or FP32 widened). */
