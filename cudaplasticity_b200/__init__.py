@@ -360,6 +360,93 @@ class Instance:
         return d
 
 
+def _report(rep):
+    return {k: getattr(rep, k) for k, _ in C.cp_solve_report._fields_}
+
+
+class Batch:
+    """Many instances solved together in mixed precision (cp_batch): one CUDA
+    graph advances every instance's own state machine; instances join between
+    runs and are harvested when done."""
+
+    def __init__(self, ctx, **opts):
+        self.ctx = ctx
+        o = C.cp_batch_opts()
+        C.lib().cp_batch_opts_default(ctypes.byref(o))
+        for k, v in opts.items():
+            setattr(o, k, v)
+        self.opts = o
+        self._h = C.c_p()
+        ctx.check(C.lib().cp_batch_create(ctx._h, ctypes.byref(o), ctypes.byref(self._h)))
+        self._slots = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            C.lib().cp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def add(self, inst, **solve_kw):
+        """Adds an Instance (loads set) with cp_solve options; mixed precision."""
+        kw = dict(solve_kw)
+        kw["precision"] = CP_PREC_MIXED
+        o = solve_opts(**kw)
+        slot = ctypes.c_int(-1)
+        self.ctx.check(C.lib().cp_batch_add(self._h, inst._h, ctypes.byref(o), ctypes.byref(slot)))
+        self._slots[slot.value] = inst
+        return slot.value
+
+    def launch(self, any_done=False, max_trips=0):
+        until = C.CP_BATCH_RUN_ANY_DONE if any_done else C.CP_BATCH_RUN_ALL
+        self.ctx.check(C.lib().cp_batch_launch(self._h, until, int(max_trips)))
+
+    def wait(self):
+        a, d = ctypes.c_int(), ctypes.c_int()
+        self.ctx.check(C.lib().cp_batch_wait(self._h, ctypes.byref(a), ctypes.byref(d)))
+        return a.value, d.value
+
+    def interrupt(self):
+        self.ctx.check(C.lib().cp_batch_interrupt(self._h))
+
+    def run(self, any_done=False, max_trips=0):
+        self.launch(any_done, max_trips)
+        return self.wait()
+
+    def harvest(self):
+        """[(slot, Instance, report dict)] of the finished instances."""
+        cap = max(len(self._slots), 1)
+        slots = np.zeros(cap, np.int32)
+        hs = (C.c_p * cap)()
+        reps = (C.cp_solve_report * cap)()
+        n = ctypes.c_int()
+        self.ctx.check(C.lib().cp_batch_harvest(self._h, cap, _ip(slots), hs, reps, ctypes.byref(n)))
+        out = []
+        for i in range(n.value):
+            inst = self._slots.pop(int(slots[i]))
+            out.append((int(slots[i]), inst, _report(reps[i])))
+        return out
+
+    def autotune(self):
+        ms = ctypes.c_double()
+        self.ctx.check(C.lib().cp_batch_autotune(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def tile(self, bucket):
+        v = ctypes.c_int()
+        self.ctx.check(C.lib().cp_batch_get_tile(self._h, bucket, ctypes.byref(v)))
+        return v.value
+
+    def set_tile(self, bucket, slices):
+        self.ctx.check(C.lib().cp_batch_set_tile(self._h, bucket, slices))
+
+    def stats(self):
+        t, k, r = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        self.ctx.check(C.lib().cp_batch_stats(self._h, ctypes.byref(t), ctypes.byref(k), ctypes.byref(r)))
+        return dict(trips=t.value, kernel_launches=k.value, runs=r.value)
+
+
 def footprint(mesh_arrays, precision=CP_PREC_FP64):
     v, keep = mesh_view(mesh_arrays)
     out = ctypes.c_size_t()

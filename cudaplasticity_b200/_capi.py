@@ -57,6 +57,13 @@ class cp_solve_report(ctypes.Structure):
                 ("kernel_launches", c_ll)]
 
 
+class cp_batch_opts(ctypes.Structure):
+    _fields_ = [("max_instances", c_int), ("cg_per_trip", c_int), ("elem_per_trip", c_int), ("max_width", c_int),
+                ("cg_blocks_per_sm", c_int)]
+
+
+CP_BATCH_RUN_ALL, CP_BATCH_RUN_ANY_DONE = 0, 1
+
 # name -> (restype, argtypes)
 _SIGS = {
     "cp_version": (ctypes.c_char_p, []),
@@ -83,6 +90,19 @@ _SIGS = {
     "cp_bench_cg": (c_int, [c_p, c_int, c_int, c_int, P_double, P_double, P_double, P_double]),
     "cp_secant_update_noalloc": (c_int, [c_p, ctypes.POINTER(cp_material), c_int, c_p, c_int, c_p, c_p, c_p, c_p,
                                          c_p, c_p, P_double]),
+    "cp_batch_opts_default": (None, [ctypes.POINTER(cp_batch_opts)]),
+    "cp_batch_create": (c_int, [c_p, ctypes.POINTER(cp_batch_opts), ctypes.POINTER(c_p)]),
+    "cp_batch_destroy": (c_int, [c_p]),
+    "cp_batch_add": (c_int, [c_p, c_p, ctypes.POINTER(cp_solve_opts), P_int]),
+    "cp_batch_launch": (c_int, [c_p, c_int, c_ll]),
+    "cp_batch_wait": (c_int, [c_p, P_int, P_int]),
+    "cp_batch_interrupt": (c_int, [c_p]),
+    "cp_batch_run": (c_int, [c_p, c_int, c_ll, P_int, P_int]),
+    "cp_batch_harvest": (c_int, [c_p, c_int, P_int, ctypes.POINTER(c_p), ctypes.POINTER(cp_solve_report), P_int]),
+    "cp_batch_set_tile": (c_int, [c_p, c_int, c_int]),
+    "cp_batch_get_tile": (c_int, [c_p, c_int, P_int]),
+    "cp_batch_autotune": (c_int, [c_p, P_double]),
+    "cp_batch_stats": (c_int, [c_p, P_ll, P_ll, P_ll]),
     "cp_get_csr": (c_int, [c_p, P_int, P_int, P_int, P_int, P_double]),
     "cp_get_slot_map": (c_int, [c_p, P_int]),
     "cp_get_field": (c_int, [c_p, ctypes.c_char_p, P_double]),

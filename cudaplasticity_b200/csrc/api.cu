@@ -12,17 +12,10 @@
 #include <vector>
 
 #include "cg.h"
+#include "instance.h"
 #include "internal.h"
 
 using cp::Error;
-
-struct cp_context {
-    int device = 0;
-    int sm_count = 148;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::string last_error;
-};
 
 namespace {
 
@@ -100,53 +93,6 @@ void validate_material(const cp_material& m) {
 }
 
 }  // namespace
-
-struct cp_instance {
-    cp_context* ctx = nullptr;
-    cp::DevMesh mesh;
-    cp::DevCsr csr;
-    cp_material mat_host{};
-    cp::MaterialDev mat{};
-    int n_nodes = 0, n_elem = 0;
-    double2 *u = nullptr, *b = nullptr, *b_full = nullptr, *u_full = nullptr;
-    uchar2* mask = nullptr;
-    double2 *r64 = nullptr, *z64a = nullptr, *z64b = nullptr, *q64 = nullptr, *s64 = nullptr;
-    float2 *r32 = nullptr, *z32a = nullptr, *z32b = nullptr, *q32 = nullptr, *s32 = nullptr;
-    double4* minv64 = nullptr;
-    float4* minv32 = nullptr;
-    cp::ElemState st{};
-    double* st_block = nullptr;
-    cp::CgScalars* sc = nullptr;
-    cp::OuterScalars* osc = nullptr;
-    double* partials = nullptr;
-    int max_blocks = 0;
-    cp::CgScalars* sc_h = nullptr;     // pinned
-    cp::OuterScalars* osc_h = nullptr;  // pinned
-    cudaGraphExec_t g64[2] = {nullptr, nullptr}, g32[2] = {nullptr, nullptr};  // [precond]
-    int body_iters = 8;
-    bool use_graph = true;  // CG loop as a CUDA graph with a device-side WHILE condition
-    bool loads_set = false;
-    long long launches = 0;  // kernels launched (graph nodes included)
-    int last_assembly = -1;  // precision of the last assembly
-    size_t bytes = 0;
-    std::vector<void*> allocs;
-
-    template <typename T>
-    T* alloc(size_t count) {
-        void* p = nullptr;
-        size_t nb = std::max<size_t>(count, 1) * sizeof(T);
-        CP_CUDA(cudaMallocAsync(&p, nb, ctx->stream));
-        allocs.push_back(p);
-        bytes += nb;
-        return static_cast<T*>(p);
-    }
-
-    cudaStream_t s() const { return ctx->stream; }
-    int sms() const { return ctx->sm_count; }
-
-    template <typename T>
-    cp::CgArgs<T> cg_args(int precond = 0);
-};
 
 template <>
 cp::CgArgs<double> cp_instance::cg_args<double>(int precond) {
@@ -303,6 +249,16 @@ void cg_mixed(cp_instance* I, double eps, double inner_tol, long long max_iter, 
 }
 
 }  // namespace
+
+void cp::instance_prepare_mixed(cp_instance* I, int precond) {
+    const bool fresh = !I->csr.val32;
+    ensure_fp32(I);
+    if (fresh) {
+        CP_CUDA(cudaMemsetAsync(I->z32a, 0, sizeof(float2) * I->n_nodes, I->s()));
+        CP_CUDA(cudaMemsetAsync(I->z32b, 0, sizeof(float2) * I->n_nodes, I->s()));
+    }
+    if (precond) (void)I->cg_args<float>(1);  // allocates s32 / minv32 once
+}
 
 // ------------------------------------------------------------------ C ABI --
 
@@ -497,6 +453,7 @@ CP_API int cp_instance_create(cp_context* ctx, const cp_mesh_view* mv, const cp_
 }
 
 CP_API int cp_instance_destroy(cp_instance* I) {
+    if (I && I->in_batch) return CP_ERR_BUSY;  // owned by a batch until harvested
     if (!I) return CP_ERR_INVALID;
     if (I->ctx) {
         cudaSetDevice(I->ctx->device);
@@ -524,6 +481,7 @@ CP_API int cp_instance_sizes(const cp_instance* I, int* nodes, int* elems, long 
 }
 
 CP_API int cp_instance_set_loads(cp_instance* I, const double* rp, const unsigned char* mask, const double* uv) {
+    if (I && I->in_batch) return CP_ERR_BUSY;  // owned by a batch until harvested
     if (!I || !rp || !mask) return CP_ERR_INVALID;
     return guarded(I->ctx, [&] {
         const int n = I->n_nodes;
@@ -549,6 +507,7 @@ CP_API int cp_instance_set_loads(cp_instance* I, const double* rp, const unsigne
 }
 
 CP_API int cp_instance_set_level(cp_instance* I, double lam) {
+    if (I && I->in_batch) return CP_ERR_BUSY;  // owned by a batch until harvested
     if (!I) return CP_ERR_INVALID;
     return guarded(I->ctx, [&] {
         int g;
@@ -559,6 +518,7 @@ CP_API int cp_instance_set_level(cp_instance* I, double lam) {
 }
 
 CP_API int cp_instance_reset_state(cp_instance* I) {
+    if (I && I->in_batch) return CP_ERR_BUSY;  // owned by a batch until harvested
     if (!I) return CP_ERR_INVALID;
     return guarded(I->ctx, [&] {
         int g;
@@ -569,6 +529,7 @@ CP_API int cp_instance_reset_state(cp_instance* I) {
 }
 
 CP_API int cp_assemble(cp_instance* I, int precision) {
+    if (I && I->in_batch) return CP_ERR_BUSY;  // owned by a batch until harvested
     if (!I || (precision != CP_PREC_FP64 && precision != CP_PREC_MIXED)) return CP_ERR_INVALID;
     return guarded(I->ctx, [&] {
         assemble(I, precision);
@@ -577,6 +538,7 @@ CP_API int cp_assemble(cp_instance* I, int precision) {
 }
 
 CP_API int cp_cg_solve(cp_instance* I, double eps, long long max_iter, long long* iters, double* rel_res) {
+    if (I && I->in_batch) return CP_ERR_BUSY;  // owned by a batch until harvested
     if (!I || !(eps > 0) || max_iter <= 0) return CP_ERR_INVALID;
     int st = CP_OK;
     int rc = guarded(I->ctx, [&] {
@@ -591,6 +553,7 @@ CP_API int cp_cg_solve(cp_instance* I, double eps, long long max_iter, long long
 }
 
 CP_API int cp_secant_update(cp_instance* I, double* rel_err) {
+    if (I && I->in_batch) return CP_ERR_BUSY;  // owned by a batch until harvested
     if (!I) return CP_ERR_INVALID;
     return guarded(I->ctx, [&] {
         cp::launch_update(I->mesh, I->mat, I->u, I->st, I->osc, I->partials, 0, I->s(), I->sms());
@@ -601,6 +564,7 @@ CP_API int cp_secant_update(cp_instance* I, double* rel_err) {
 }
 
 CP_API int cp_plastic_strains(cp_instance* I) {
+    if (I && I->in_batch) return CP_ERR_BUSY;  // owned by a batch until harvested
     if (!I) return CP_ERR_INVALID;
     return guarded(I->ctx, [&] {
         cp::launch_plastic(I->mesh, I->mat, I->st, I->s(), I->sms());
@@ -624,6 +588,7 @@ CP_API void cp_solve_opts_default(cp_solve_opts* o) {
 }
 
 CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* rep) {
+    if (I && I->in_batch) return CP_ERR_BUSY;  // owned by a batch until harvested
     if (!I || !opts) return CP_ERR_INVALID;
     cp_solve_report R{};
     const cp_solve_opts o = *opts;
@@ -706,6 +671,7 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
 
 CP_API int cp_bench_cg(cp_instance* I, int precision, int precond, int iters, double* ms_p, double* ms_u,
                        double* bytes_p, double* bytes_u) {
+    if (I && I->in_batch) return CP_ERR_BUSY;
     if (!I || iters <= 0 || (precision != CP_PREC_FP64 && precision != CP_PREC_MIXED) || (precond & ~1)) return CP_ERR_INVALID;
     return guarded(I->ctx, [&] {
         CP_CHECK(I->loads_set, CP_ERR_INVALID, "loads not set");
@@ -838,6 +804,7 @@ CP_API int cp_get_field(cp_instance* I, const char* name, double* out) {
 }
 
 CP_API int cp_set_field(cp_instance* I, const char* name, const double* in) {
+    if (I && I->in_batch) return CP_ERR_BUSY;  // owned by a batch until harvested
     if (!I || !name || !in) return CP_ERR_INVALID;
     size_t count = 0;
     double* p = field_ptr(I, name, &count);

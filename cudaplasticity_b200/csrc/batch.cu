@@ -1,0 +1,1153 @@
+// Batched mixed-precision solves: many independent instances on one GPU.
+//
+// Every instance runs the single-instance algorithm of cp_solve in its
+// mixed-precision form (outer secant iteration of the reference's
+// PlasticitySolver::solveCUDA, src/PlasticitySolver.cu:469-512; masked CG of
+// ConjGradCuda::solve, src/ConjGradCuda.cu:185-231, here with FP32 values and
+// recurrences inside FP64 defect correction) as its own state machine on the
+// device:
+//
+//   LEVEL -> ASM -> INIT -> (P -> U)* -> INIT ... -> UPD -> RELAX -> ASM ...
+//                                         (level converged) -> LEVEL / PLASTIC -> DONE
+//
+// The instances' nodes and elements are cut into tiles; one work list holds
+// every (instance, tile) pair. Three persistent kernels walk that list, each
+// acting only on the tiles whose instance is in one of its phases:
+//   k_batch_cg    INIT (FP64 residual, FP32 restart), P (SpMV + direction),
+//                 U (axpy / residual / preconditioner)
+//   k_batch_asm   ASM (FP64 + FP32 values of K, node gather, no atomics)
+//   k_batch_elem  LEVEL, UPD (strain / stress / secant / exit norm),
+//                 RELAX (Aitken), PLASTIC
+// Each tile writes one partial sum per 32-node slice or 32-element group; the
+// last tile of an instance to arrive (per-instance ticket) reduces that
+// instance's partials in index order with a fixed thread assignment and moves
+// the instance to its next phase. The sums therefore do not depend on the
+// tiling, on the grid, or on the other instances in the batch.
+//
+// One CUDA graph drives a run: a WHILE node whose body is
+//   elem x E, asm, cg x C, condition
+// and every launch advances every instance in a matching phase by one step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "elements.cuh"
+#include "instance.h"
+#include "internal.h"
+
+namespace cp {
+namespace {
+
+constexpr int kThreads = 128;  // 4 warps; every kernel of the batch
+constexpr int kWarps = kThreads / 32;
+constexpr int kBuckets = 24;
+
+enum : int {
+    PH_FREE = 0,
+    PH_LEVEL,
+    PH_ASM,
+    PH_INIT,
+    PH_P,
+    PH_U,
+    PH_UPD,
+    PH_RELAX,
+    PH_PLASTIC,
+    PH_DONE,
+    PH_COUNT
+};
+
+// Read-only description of one instance (written by the host at add).
+struct BDesc {
+    DevMesh m;
+    int n_slices, n_groups;  // 32-node slices, 32-element groups
+    const int* slice_ptr;
+    const int* scol;
+    const int* inc_pos;
+    const int* inc;
+    const uint32_t* inc_k;
+    double* val64;
+    float* val32;
+    double2* x;
+    double2* b;
+    const double2* b_full;
+    const double2* u_full;
+    const uchar2* mask;
+    float2 *r, *z0, *z1, *q, *s;
+    float4* minv;
+    ElemState st;
+    MaterialDev mat;
+    double* part;  // 4 per slice / group
+    double cg_tol, outer_tol, inner_tol;
+    long long max_cg;
+    int max_outer, levels, aitken, adaptive, precond;
+};
+
+// Mutable state of one instance.
+struct BState {
+    int phase, status, level, levels_done;
+    int outer_it, outer_total, restarts, parity;
+    unsigned int ticket;
+    int pad;
+    long long iter, lin_iters, cg_total, fp64_spmv;
+    double rr, rho, alpha, beta, normB_inv, eps2_inner, bb, res64;
+    double eps, rel_err, w_prev, omega, cg_rel_res;
+    unsigned long long t_first, t_done;  // %globaltimer, ns
+};
+
+// Run control. The host writes it before every launch.
+struct BCtl {
+    int n_tiles;
+    int active;
+    int done;
+    int exit_on_done;  // stop once done >= exit_on_done (0: never)
+    long long trips, max_trips;
+    int pop[PH_COUNT];  // instances per phase
+    const volatile int* stop;  // host-mapped interrupt flag
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void set_phase(BState* S, BCtl* c, int ph) {
+    atomicSub(&c->pop[S->phase], 1);
+    atomicAdd(&c->pop[ph], 1);
+    S->phase = ph;
+}
+
+__device__ __forceinline__ void finish(BState* S, BCtl* c, int status) {
+    if (status) S->status = status;
+    S->t_done = global_ns();
+    set_phase(S, c, PH_DONE);
+    atomicAdd(&c->done, 1);
+    atomicSub(&c->active, 1);
+}
+
+// Every thread of the block: true in the block whose tile is the instance's
+// last to arrive in this launch.
+__device__ __forceinline__ bool arrive(BState* S, int ntiles, int* sh_flag) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int t = atomicAdd(&S->ticket, 1u);
+        *sh_flag = (t == (unsigned int)ntiles - 1u);
+    }
+    __syncthreads();
+    const bool last = *sh_flag != 0;
+    if (last) __threadfence();
+    return last;
+}
+
+// Sums of the first K of the 4 partials per unit over units [0, n), fixed
+// assignment (thread t takes units t, t + 128, ...) and a fixed tree.
+// Results valid in thread 0.
+template <int K>
+__device__ __forceinline__ void reduce_parts(const double* part, int n, double* out, double* sh) {
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+        const volatile double* p = part + 4 * (size_t)i;
+#pragma unroll
+        for (int k = 0; k < K; ++k) a[k] += p[k];
+    }
+#pragma unroll
+    for (int k = 0; k < K; k += 2) {
+        const double2 s = block_sum2(a[k], k + 1 < K ? a[k + 1] : 0.0, sh);
+        out[k] = s.x;
+        if (k + 1 < K) out[k + 1] = s.y;
+    }
+}
+
+__device__ __forceinline__ int tile_phase(const BState* S, int* sh) {
+    __syncthreads();
+    if (threadIdx.x == 0) *sh = *(const volatile int*)&S->phase;
+    __syncthreads();
+    return *sh;
+}
+
+// Linear tolerance of the next solve (cp_solve: inexact early steps with
+// the adaptive option, tight once the secant iteration is close).
+__device__ __forceinline__ double next_eps(const BDesc& d, double rel_err) {
+    return (d.adaptive && rel_err > 10.0 * d.outer_tol) ? fmax(d.cg_tol, 1e-2 * rel_err) : d.cg_tol;
+}
+
+// After the update (and Aitken): next level, plastic strains, or another
+// outer iteration (cp_solve's loop body).
+__device__ __forceinline__ void decide(const BDesc& d, BState* S, BCtl* c) {
+    const bool conv = S->rel_err <= d.outer_tol && S->eps <= d.cg_tol;
+    if (conv) {
+        S->levels_done = S->level;
+        if (S->level < d.levels) {
+            S->level += 1;
+            set_phase(S, c, PH_LEVEL);
+        } else {
+            set_phase(S, c, PH_PLASTIC);
+        }
+    } else if (S->outer_it >= d.max_outer) {
+        S->levels_done = S->level;
+        S->status = CP_ERR_NOT_CONVERGED;
+        set_phase(S, c, PH_PLASTIC);
+    } else {
+        S->eps = next_eps(d, S->rel_err);
+        set_phase(S, c, PH_ASM);
+    }
+}
+
+// ------------------------------------------------------------ CG phases --
+
+// INIT: r = m.(b - K64 x) in FP64, stored in FP32; z = 0; block-Jacobi
+// inverse and s = M^-1 r. Sums (r32, r32), (r64, r64), (b, b), (r32, s).
+__device__ void tile_init(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
+    const int pre = d.precond;
+    for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
+        const int n = 32 * sl + lane;
+        const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
+        double s_rr = 0.0, s_r64 = 0.0, s_bb = 0.0, s_rho = 0.0;
+        if (n < d.m.n_nodes) {
+            double k0 = 0.0, k1 = 0.0;
+            for (int k = 0; k < wd; ++k) {
+                const long long bi = base + 32LL * k + lane;
+                const int col = __ldg(d.scol + bi);
+                const double2* vp = reinterpret_cast<const double2*>(d.val64 + 4 * bi);
+                const double2 lo = __ldg(vp), hi = __ldg(vp + 1);
+                const double2 xc = d.x[col];
+                k0 += lo.x * xc.x + lo.y * xc.y;
+                k1 += hi.x * xc.x + hi.y * xc.y;
+            }
+            const double2 bb = d.b[n];
+            const uchar2 m = d.mask[n];
+            const double r0 = m.x ? bb.x - k0 : 0.0, r1 = m.y ? bb.y - k1 : 0.0;
+            const float2 rt = make_float2((float)r0, (float)r1);
+            d.r[n] = rt;
+            d.z0[n] = make_float2(0.f, 0.f);
+            s_rr = (double)rt.x * (double)rt.x + (double)rt.y * (double)rt.y;
+            if (pre) {
+                const double2* dp = reinterpret_cast<const double2*>(d.val64 + 4 * ((long long)base + lane));
+                const double2 dlo = __ldg(dp), dhi = __ldg(dp + 1);
+                double i00 = 0, i01 = 0, i10 = 0, i11 = 0;
+                if (m.x && m.y) {
+                    const double det = dlo.x * dhi.y - dlo.y * dhi.x;
+                    i00 = dhi.y / det; i01 = -dlo.y / det; i10 = -dhi.x / det; i11 = dlo.x / det;
+                } else if (m.x) {
+                    i00 = 1.0 / dlo.x;
+                } else if (m.y) {
+                    i11 = 1.0 / dhi.y;
+                }
+                const float4 mi = make_float4((float)i00, (float)i01, (float)i10, (float)i11);
+                d.minv[n] = mi;
+                const float2 sv = make_float2(mi.x * rt.x + mi.y * rt.y, mi.z * rt.x + mi.w * rt.y);
+                d.s[n] = sv;
+                s_rho = (double)rt.x * (double)sv.x + (double)rt.y * (double)sv.y;
+            }
+            s_r64 = r0 * r0 + r1 * r1;
+            s_bb = bb.x * bb.x + bb.y * bb.y;
+        }
+        s_rr = warp_sum(s_rr);
+        s_r64 = warp_sum(s_r64);
+        s_bb = warp_sum(s_bb);
+        s_rho = warp_sum(s_rho);
+        if (lane == 0) {
+            double* p = d.part + 4 * (size_t)sl;
+            p[0] = s_rr; p[1] = s_r64; p[2] = s_bb; p[3] = s_rho;
+        }
+    }
+    if (!arrive(S, tl.w, shf)) return;
+    double t[4];
+    reduce_parts<4>(d.part, d.n_slices, t, sh);
+    if (threadIdx.x == 0) {
+        const double rr = t[0], res64 = t[1], bb = t[2];
+        S->ticket = 0;
+        S->fp64_spmv += 1;
+        S->restarts += 1;
+        S->bb = bb;
+        S->res64 = res64;
+        S->cg_rel_res = bb > 0.0 ? sqrt(res64 / bb) : 0.0;
+        if (!(rr == rr) || !(bb == bb) || !(res64 == res64)) {
+            finish(S, c, CP_ERR_BREAKDOWN);
+        } else if (res64 <= S->eps * S->eps * bb || rr == 0.0 || S->restarts > 200 || S->lin_iters >= d.max_cg) {
+            set_phase(S, c, PH_UPD);  // the linear solve meets its tolerance (or its caps)
+        } else {
+            S->rr = rr;
+            S->rho = pre ? t[3] : rr;
+            S->normB_inv = 1.0 / rr;  // inner solve: reduction relative to its start
+            S->eps2_inner = d.inner_tol * d.inner_tol;
+            S->iter = 0;
+            S->alpha = 0.0;
+            S->beta = 0.0;
+            S->parity = 0;
+            set_phase(S, c, PH_P);
+        }
+    }
+}
+
+// P: z' = s + beta z (own node), q = K32 z' gathered from the neighbours,
+// (q, z').
+__device__ void tile_p(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
+    const int par = S->parity;
+    const float beta = (float)S->beta;
+    const float2* __restrict__ zo = par ? d.z1 : d.z0;
+    float2* __restrict__ zn = par ? d.z0 : d.z1;
+    const float2* __restrict__ rs = d.precond ? d.s : d.r;
+    for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
+        const int n = 32 * sl + lane;
+        const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
+        double dot = 0.0;
+        if (n < d.m.n_nodes) {
+            float k0 = 0.f, k1 = 0.f;
+#pragma unroll 3
+            for (int k = 0; k < wd; ++k) {
+                const long long bi = base + 32LL * k + lane;
+                const int col = __ldg(d.scol + bi);
+                const float4 v = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
+                const float2 rc = rs[col], zc = zo[col];
+                const float wx = rc.x + beta * zc.x, wy = rc.y + beta * zc.y;
+                k0 += v.x * wx + v.y * wy;
+                k1 += v.z * wx + v.w * wy;
+            }
+            const float2 rn = rs[n], zon = zo[n];
+            const float2 zz = make_float2(rn.x + beta * zon.x, rn.y + beta * zon.y);
+            zn[n] = zz;
+            d.q[n] = make_float2(k0, k1);
+            dot = (double)k0 * (double)zz.x + (double)k1 * (double)zz.y;
+        }
+        dot = warp_sum(dot);
+        if (lane == 0) d.part[4 * (size_t)sl] = dot;
+    }
+    if (!arrive(S, tl.w, shf)) return;
+    double t[4];
+    reduce_parts<1>(d.part, d.n_slices, t, sh);
+    if (threadIdx.x == 0) {
+        const double pAz = t[0];
+        S->ticket = 0;
+        const double alpha = S->rho / pAz;
+        if (!(pAz > 0.0) || !(alpha == alpha)) {
+            finish(S, c, CP_ERR_BREAKDOWN);
+        } else {
+            S->alpha = alpha;
+            set_phase(S, c, PH_U);
+        }
+    }
+}
+
+// U: x += alpha z' (FP64), r -= m.alpha q, s = M^-1 r; (r, r), (r, s).
+__device__ void tile_u(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
+    const float2* __restrict__ zn = S->parity ? d.z0 : d.z1;
+    const double alpha = S->alpha;
+    const float alpha_t = (float)alpha;
+    const int pre = d.precond;
+    for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
+        const int n = 32 * sl + lane;
+        double s_rr = 0.0, s_rs = 0.0;
+        if (n < d.m.n_nodes) {
+            const float2 z = zn[n], q = d.q[n];
+            const uchar2 m = d.mask[n];
+            double2 x = d.x[n];
+            x.x += alpha * (double)z.x;
+            x.y += alpha * (double)z.y;
+            d.x[n] = x;
+            float2 r = d.r[n];
+            if (m.x) r.x -= alpha_t * q.x;
+            if (m.y) r.y -= alpha_t * q.y;
+            d.r[n] = r;
+            s_rr = (double)r.x * (double)r.x + (double)r.y * (double)r.y;
+            if (pre) {
+                const float4 mi = d.minv[n];
+                const float2 sv = make_float2(mi.x * r.x + mi.y * r.y, mi.z * r.x + mi.w * r.y);
+                d.s[n] = sv;
+                s_rs = (double)r.x * (double)sv.x + (double)r.y * (double)sv.y;
+            }
+        }
+        s_rr = warp_sum(s_rr);
+        s_rs = warp_sum(s_rs);
+        if (lane == 0) {
+            d.part[4 * (size_t)sl] = s_rr;
+            d.part[4 * (size_t)sl + 1] = s_rs;
+        }
+    }
+    if (!arrive(S, tl.w, shf)) return;
+    double t[4];
+    reduce_parts<2>(d.part, d.n_slices, t, sh);
+    if (threadIdx.x == 0) {
+        const double rn = t[0];
+        const double rho_new = pre ? t[1] : rn;
+        S->ticket = 0;
+        S->beta = rho_new / S->rho;
+        S->rho = rho_new;
+        S->rr = rn;
+        S->iter += 1;
+        S->lin_iters += 1;
+        S->cg_total += 1;
+        S->parity ^= 1;
+        if (!(rn == rn)) finish(S, c, CP_ERR_BREAKDOWN);
+        else if (rn * S->normB_inv <= S->eps2_inner) set_phase(S, c, PH_INIT);  // restart from the FP64 residual
+        else if (S->lin_iters >= d.max_cg) set_phase(S, c, PH_UPD);
+        else set_phase(S, c, PH_P);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_batch_cg(const BDesc* __restrict__ D, BState* SS,
+                                                       const int4* __restrict__ tiles, BCtl* c) {
+    __shared__ double sh[2 * kWarps];
+    __shared__ int shf, shp;
+    {
+        const volatile int* pop = c->pop;
+        if (pop[PH_INIT] + pop[PH_P] + pop[PH_U] == 0) return;
+    }
+    const int nt = c->n_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int4 tl = tiles[t];
+        BState* S = SS + tl.x;
+        const int ph = tile_phase(S, &shp);
+        if (ph == PH_P) tile_p(D[tl.x], S, c, tl, sh, &shf);
+        else if (ph == PH_U) tile_u(D[tl.x], S, c, tl, sh, &shf);
+        else if (ph == PH_INIT) tile_init(D[tl.x], S, c, tl, sh, &shf);
+    }
+}
+
+// The SpMV of the P phase for the autotuner: the same loads and arithmetic,
+// with the results written to a sink of the batch (one value per thread)
+// instead of the instance's z' and q, so that the instances' state is left
+// untouched whatever phase they are in.
+__global__ void __launch_bounds__(kThreads) k_batch_probe(const BDesc* __restrict__ D, const BState* SS,
+                                                          const int4* __restrict__ tiles, int nt, float beta,
+                                                          float2* sink) {
+    float2 acc = make_float2(0.f, 0.f);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int4 tl = tiles[t];
+        const BDesc& d = D[tl.x];
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
+        const int par = SS[tl.x].parity;
+        const float2* __restrict__ zo = par ? d.z1 : d.z0;
+        const float2* __restrict__ rs = d.precond ? d.s : d.r;
+        for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
+            const int n = 32 * sl + lane;
+            const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
+            if (n < d.m.n_nodes) {
+                float k0 = 0.f, k1 = 0.f;
+#pragma unroll 3
+                for (int k = 0; k < wd; ++k) {
+                    const long long bi = base + 32LL * k + lane;
+                    const int col = __ldg(d.scol + bi);
+                    const float4 v = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
+                    const float2 rc = rs[col], zc = zo[col];
+                    const float wx = rc.x + beta * zc.x, wy = rc.y + beta * zc.y;
+                    k0 += v.x * wx + v.y * wy;
+                    k1 += v.z * wx + v.w * wy;
+                }
+                acc.x += k0;
+                acc.y += k1;
+            }
+        }
+    }
+    sink[blockIdx.x * kThreads + threadIdx.x] = acc;
+}
+
+// ------------------------------------------------------ assembly phase --
+
+// ASM: K(E_c, nu_c) in FP64 and FP32, one warp per 32-node slice, the
+// slice's blocks accumulated in the warp's shared-memory region (each lane
+// only touches its own node's blocks; element order) and written once,
+// coalesced. Same arithmetic as the single-instance assembly.
+__global__ void __launch_bounds__(kThreads) k_batch_asm(const BDesc* __restrict__ D, BState* SS,
+                                                        const int4* __restrict__ tiles, BCtl* c, int max_width) {
+    extern __shared__ double sacc[];
+    __shared__ int shf, shp;
+    {
+        const volatile int* pop = c->pop;
+        if (pop[PH_ASM] == 0) return;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double* acc = sacc + (size_t)w * 128 * max_width;
+    const int nt = c->n_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int4 tl = tiles[t];
+        BState* S = SS + tl.x;
+        if (tile_phase(S, &shp) != PH_ASM) continue;
+        const BDesc& d = D[tl.x];
+        const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
+        for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
+            const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
+            const int len = 128 * wd;
+            for (int i = lane; i < len; i += 32) acc[i] = 0.0;
+            __syncwarp();
+            const int n = 32 * sl + lane;
+            if (n < d.m.n_nodes) {
+                double* nb = acc + 4 * lane;
+                for (int q = d.inc_pos[n]; q < d.inc_pos[n + 1]; ++q) {
+                    const int code = d.inc[q];
+                    const int e = code >> 2, i = code & 3;
+                    const Dmat dm = form_d(d.mat.plane, d.st.E_c[e], d.st.nu_c[e]);
+                    element_rows(d.m, e, i, d.inc_k[q], dm, d.mat.h, nb);
+                }
+            }
+            __syncwarp();
+            double* o64 = d.val64 + 4LL * base;
+            float* o32 = d.val32 + 4LL * base;
+            for (int i = lane; i < len; i += 32) {
+                const double v = acc[i];
+                o64[i] = v;
+                o32[i] = (float)v;
+            }
+            __syncwarp();
+        }
+        if (arrive(S, tl.w, &shf) && threadIdx.x == 0) {
+            S->ticket = 0;
+            set_phase(S, c, PH_INIT);
+        }
+    }
+}
+
+// --------------------------------------------------- element phases --
+
+__global__ void __launch_bounds__(kThreads) k_batch_elem(const BDesc* __restrict__ D, BState* SS,
+                                                         const int4* __restrict__ tiles, BCtl* c) {
+    __shared__ double sh[2 * kWarps];
+    __shared__ int shf, shp;
+    {
+        const volatile int* pop = c->pop;
+        if (pop[PH_LEVEL] + pop[PH_UPD] + pop[PH_RELAX] + pop[PH_PLASTIC] == 0) return;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nt = c->n_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int4 tl = tiles[t];
+        BState* S = SS + tl.x;
+        const int ph = tile_phase(S, &shp);
+        if (ph != PH_LEVEL && ph != PH_UPD && ph != PH_RELAX && ph != PH_PLASTIC) continue;
+        const BDesc& d = D[tl.x];
+        const int ne = d.m.c3 + d.m.c4;
+        const int g0 = tl.y * tl.z, g1 = min(g0 + tl.z, d.n_groups);
+        if (ph == PH_LEVEL) {
+            // k_set_level and the Aitken history reset of cp_solve
+            const double lam = (double)S->level / d.levels;
+            const int s1 = min(g0 + tl.z, d.n_slices);
+            for (int sl = g0 + w; sl < s1; sl += kWarps) {
+                const int n = 32 * sl + lane;
+                if (n < d.m.n_nodes) {
+                    const double2 bf = d.b_full[n];
+                    d.b[n] = make_double2(lam * bf.x, lam * bf.y);
+                    const uchar2 m = d.mask[n];
+                    double2 uu = d.x[n];
+                    const double2 uf = d.u_full[n];
+                    if (!m.x) uu.x = lam * uf.x;
+                    if (!m.y) uu.y = lam * uf.y;
+                    d.x[n] = uu;
+                }
+            }
+            for (int g = g0 + w; g < g1; g += kWarps) {
+                const int e = 32 * g + lane;
+                if (e < ne) {
+                    d.st.res_prev[e] = 0.0;
+                    d.st.res_cur[e] = 0.0;
+                }
+            }
+            if (arrive(S, tl.w, &shf) && threadIdx.x == 0) {
+                S->ticket = 0;
+                if (S->t_first == 0) S->t_first = global_ns();
+                S->outer_it = 0;
+                S->rel_err = 1.0;
+                S->w_prev = 1.0;
+                S->eps = next_eps(d, 1.0);
+                set_phase(S, c, PH_ASM);
+            }
+        } else if (ph == PH_UPD) {
+            for (int g = g0 + w; g < g1; g += kWarps) {
+                const int e = 32 * g + lane;
+                double s_num = 0.0, s_den = 0.0, s_an = 0.0, s_ad = 0.0;
+                if (e < ne) update_element(d.m, d.mat, d.x, d.st, e, d.aitken, s_num, s_den, s_an, s_ad);
+                s_num = warp_sum(s_num);
+                s_den = warp_sum(s_den);
+                s_an = warp_sum(s_an);
+                s_ad = warp_sum(s_ad);
+                if (lane == 0) {
+                    double* p = d.part + 4 * (size_t)g;
+                    p[0] = s_num; p[1] = s_den; p[2] = s_an; p[3] = s_ad;
+                }
+            }
+            if (arrive(S, tl.w, &shf)) {
+                double r[4];
+                reduce_parts<4>(d.part, d.n_groups, r, sh);
+                if (threadIdx.x == 0) {
+                    S->ticket = 0;
+                    const double rel = sqrt(r[0] / r[1]);
+                    S->rel_err = rel;
+                    S->outer_it += 1;
+                    S->outer_total += 1;
+                    S->lin_iters = 0;
+                    S->restarts = 0;
+                    if (!isfinite(rel)) {
+                        finish(S, c, CP_ERR_BREAKDOWN);
+                    } else if (d.aitken) {
+                        double om = 1.0;
+                        if (S->outer_it > 1 && r[3] > 0) om = -S->w_prev * r[2] / r[3];
+                        if (!(om >= 0.1)) om = 0.1;
+                        if (om > 10.0) om = 10.0;
+                        S->omega = om;
+                        S->w_prev = om;
+                        set_phase(S, c, PH_RELAX);
+                    } else {
+                        decide(d, S, c);
+                    }
+                }
+            }
+        } else if (ph == PH_RELAX) {
+            const double om = S->omega;
+            for (int g = g0 + w; g < g1; g += kWarps) {
+                const int e = 32 * g + lane;
+                if (e < ne) relax_element(d.mat, d.st, e, om);
+            }
+            if (arrive(S, tl.w, &shf) && threadIdx.x == 0) {
+                S->ticket = 0;
+                decide(d, S, c);
+            }
+        } else {  // PH_PLASTIC
+            for (int g = g0 + w; g < g1; g += kWarps) {
+                const int e = 32 * g + lane;
+                if (e < ne) plastic_element(d.mat, d.st, e);
+            }
+            if (arrive(S, tl.w, &shf) && threadIdx.x == 0) {
+                S->ticket = 0;
+                finish(S, c, 0);
+            }
+        }
+    }
+}
+
+__global__ void k_batch_cond(BCtl* c, cudaGraphConditionalHandle h) {
+    c->trips += 1;
+    bool go = c->active > 0 && (c->max_trips <= 0 || c->trips < c->max_trips) &&
+              !(c->exit_on_done > 0 && c->done >= c->exit_on_done);
+    if (go && c->stop && *c->stop) go = false;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+int bucket_of(int n_slices) {
+    int b = 0;
+    while ((2 << b) <= n_slices && b + 1 < kBuckets) ++b;
+    return b;
+}
+
+}  // namespace
+}  // namespace cp
+
+using namespace cp;
+
+struct cp_batch {
+    cp_context* ctx = nullptr;
+    cp_batch_opts o{};
+    int cap = 0;
+    std::vector<cp_instance*> inst;      // per slot (nullptr: free)
+    std::vector<BDesc> desc;             // host copies
+    std::vector<BState> state;           // host copies, refreshed after each run
+    std::vector<int> listed;             // slots in the batch, in admission order
+    int tile_slices[kBuckets];
+    BDesc* d_desc = nullptr;
+    BState* d_state = nullptr;
+    int4* d_tiles = nullptr;
+    BCtl* d_ctl = nullptr;
+    int tiles_cap = 0;
+    int4* h_tiles = nullptr;  // pinned
+    BState* h_state = nullptr;  // pinned
+    BCtl* h_ctl = nullptr;  // pinned
+    int* h_stop = nullptr;  // host-mapped
+    int* d_stop = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int grid_cg = 0, grid_elem = 0, grid_asm = 0;
+    float2* d_sink = nullptr;  // autotuner probe output
+    size_t asm_smem = 0;
+    bool running = false;
+    int last_tiles = 0;
+    long long trips = 0, launches = 0, runs = 0;
+};
+
+namespace {
+
+int bfail(cp_batch* b, const Error& e) {
+    if (b && b->ctx) b->ctx->last_error = e.msg;
+    return e.status;
+}
+
+template <typename F>
+int bguard(cp_batch* b, F&& f) {
+    try {
+        f();
+        return CP_OK;
+    } catch (const Error& e) {
+        return bfail(b, e);
+    } catch (const std::bad_alloc&) {
+        return bfail(b, Error{CP_ERR_NOMEM, "host allocation failed"});
+    }
+}
+
+int default_tile(int bucket) {
+    // 4 slices (one per warp) for small instances, up to 16 for large ones
+    return bucket < 6 ? 4 : (bucket < 9 ? 8 : 16);
+}
+
+void ensure_tiles(cp_batch* b, int need) {
+    if (need <= b->tiles_cap) return;
+    int nc = std::max(need, 2 * b->tiles_cap);
+    if (b->d_tiles) CP_CUDA(cudaFree(b->d_tiles));
+    if (b->h_tiles) CP_CUDA(cudaFreeHost(b->h_tiles));
+    b->d_tiles = nullptr;
+    b->h_tiles = nullptr;
+    CP_CUDA(cudaMalloc(&b->d_tiles, sizeof(int4) * (size_t)nc));
+    CP_CUDA(cudaMallocHost(&b->h_tiles, sizeof(int4) * (size_t)nc));
+    b->tiles_cap = nc;
+    // the graph holds the work-list pointer: rebuild it
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+}
+
+int tiles_of(const BDesc& d, int S) {
+    const int a = (d.n_slices + S - 1) / S, g = (d.n_groups + S - 1) / S;
+    return std::max(a, g);
+}
+
+// Work list of the listed, unfinished instances; returns the tile count.
+int build_tiles(cp_batch* b, const std::vector<int>& slots, bool only_active, const int* S_override) {
+    int total = 0;
+    for (int sl : slots) {
+        if (only_active && b->state[sl].phase == PH_DONE) continue;
+        const int S = S_override ? *S_override : b->tile_slices[bucket_of(b->desc[sl].n_slices)];
+        total += tiles_of(b->desc[sl], S);
+    }
+    ensure_tiles(b, std::max(total, 1));
+    int k = 0;
+    for (int sl : slots) {
+        if (only_active && b->state[sl].phase == PH_DONE) continue;
+        const int S = S_override ? *S_override : b->tile_slices[bucket_of(b->desc[sl].n_slices)];
+        const int nt = tiles_of(b->desc[sl], S);
+        for (int t = 0; t < nt; ++t) b->h_tiles[k++] = make_int4(sl, t, S, nt);
+    }
+    return k;
+}
+
+// Round-robin order across instances, so that the persistent grid's blocks
+// take tiles of many instances at once (the last tile of a large instance is
+// not left to run alone).
+void interleave_tiles(cp_batch* b, int n) {
+    std::vector<int4> out;
+    out.reserve(n);
+    std::vector<std::pair<int, int>> ranges;  // [begin, end) per instance
+    int i = 0;
+    while (i < n) {
+        int j = i;
+        while (j < n && b->h_tiles[j].x == b->h_tiles[i].x) ++j;
+        ranges.push_back({i, j});
+        i = j;
+    }
+    bool more = true;
+    for (int r = 0; more; ++r) {
+        more = false;
+        for (auto& rg : ranges)
+            if (rg.first + r < rg.second) {
+                out.push_back(b->h_tiles[rg.first + r]);
+                more = true;
+            }
+    }
+    std::memcpy(b->h_tiles, out.data(), sizeof(int4) * (size_t)n);
+}
+
+void build_graph(cp_batch* b) {
+    cudaStream_t s = b->ctx->stream;
+    cudaGraph_t g;
+    CP_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    CP_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    CP_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &p));
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    CP_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    for (int k = 0; k < b->o.elem_per_trip; ++k)
+        k_batch_elem<<<b->grid_elem, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
+    k_batch_asm<<<b->grid_asm, kThreads, b->asm_smem, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl,
+                                                           b->o.max_width);
+    for (int k = 0; k < b->o.cg_per_trip; ++k)
+        k_batch_cg<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
+    k_batch_cond<<<1, 1, 0, s>>>(b->d_ctl, h);
+    cudaGraph_t captured = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &captured);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        CP_CUDA(e);
+    }
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    CP_CUDA(e);
+}
+
+cp_solve_report report_of(const BState& S) {
+    cp_solve_report r{};
+    r.status = S.status;
+    r.outer_iters = S.outer_total;
+    r.cg_iters = S.cg_total;
+    r.fp64_spmv = S.fp64_spmv;
+    r.rel_err = S.rel_err;
+    r.cg_rel_res = S.cg_rel_res;
+    r.levels_done = S.levels_done;
+    r.seconds = (S.t_done > S.t_first && S.t_first) ? (double)(S.t_done - S.t_first) * 1e-9 : 0.0;
+    r.kernel_launches = 0;
+    return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+CP_API void cp_batch_opts_default(cp_batch_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof *o);
+    o->max_instances = 1024;
+    o->cg_per_trip = 16;
+    o->elem_per_trip = 3;
+    o->max_width = 16;
+    o->cg_blocks_per_sm = 0;
+}
+
+CP_API int cp_batch_create(cp_context* ctx, const cp_batch_opts* opts, cp_batch** out) {
+    if (!ctx || !out) return CP_ERR_INVALID;
+    *out = nullptr;
+    cp_batch_opts o;
+    cp_batch_opts_default(&o);
+    if (opts) o = *opts;
+    if (o.max_instances <= 0 || o.max_instances > (1 << 20) || o.cg_per_trip <= 0 || o.elem_per_trip < 3 ||
+        o.max_width < 1 || o.max_width > 48 || o.cg_blocks_per_sm < 0 || o.cg_blocks_per_sm > 16)
+        return CP_ERR_INVALID;
+    cp_batch* b = new (std::nothrow) cp_batch();
+    if (!b) return CP_ERR_NOMEM;
+    b->ctx = ctx;
+    b->o = o;
+    b->cap = o.max_instances;
+    for (int k = 0; k < kBuckets; ++k) b->tile_slices[k] = default_tile(k);
+    int rc = bguard(b, [&] {
+        CP_CUDA(cudaSetDevice(ctx->device));
+        b->inst.assign(b->cap, nullptr);
+        b->desc.assign(b->cap, BDesc{});
+        b->state.assign(b->cap, BState{});
+        CP_CUDA(cudaMalloc(&b->d_desc, sizeof(BDesc) * (size_t)b->cap));
+        CP_CUDA(cudaMalloc(&b->d_state, sizeof(BState) * (size_t)b->cap));
+        CP_CUDA(cudaMemset(b->d_state, 0, sizeof(BState) * (size_t)b->cap));
+        CP_CUDA(cudaMalloc(&b->d_ctl, sizeof(BCtl)));
+        CP_CUDA(cudaMemset(b->d_ctl, 0, sizeof(BCtl)));
+        CP_CUDA(cudaMallocHost(&b->h_state, sizeof(BState) * (size_t)b->cap));
+        CP_CUDA(cudaMallocHost(&b->h_ctl, sizeof(BCtl)));
+        CP_CUDA(cudaHostAlloc(&b->h_stop, 64, cudaHostAllocMapped));
+        *b->h_stop = 0;
+        CP_CUDA(cudaHostGetDevicePointer((void**)&b->d_stop, b->h_stop, 0));
+        ensure_tiles(b, 1024);
+        int per_sm = 0;
+        CP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cg, kThreads, 0));
+        if (o.cg_blocks_per_sm > 0) per_sm = std::min(per_sm, o.cg_blocks_per_sm);
+        b->grid_cg = ctx->sm_count * std::max(1, per_sm);
+        CP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_elem, kThreads, 0));
+        b->grid_elem = ctx->sm_count * std::max(1, std::min(per_sm, 8));
+        b->asm_smem = (size_t)kWarps * 128 * o.max_width * sizeof(double);
+        CP_CUDA(cudaFuncSetAttribute(k_batch_asm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->asm_smem));
+        CP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_asm, kThreads, b->asm_smem));
+        b->grid_asm = ctx->sm_count * std::max(1, per_sm);
+        CP_CUDA(cudaMalloc(&b->d_sink, sizeof(float2) * (size_t)b->grid_cg * kThreads));
+    });
+    if (rc != CP_OK) {
+        cp_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return CP_OK;
+}
+
+CP_API int cp_batch_destroy(cp_batch* b) {
+    if (!b) return CP_ERR_INVALID;
+    if (b->ctx) {
+        cudaSetDevice(b->ctx->device);
+        cudaStreamSynchronize(b->ctx->stream);
+    }
+    for (int sl : b->listed)
+        if (b->inst[sl]) b->inst[sl]->in_batch = false;
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->d_desc) cudaFree(b->d_desc);
+    if (b->d_state) cudaFree(b->d_state);
+    if (b->d_tiles) cudaFree(b->d_tiles);
+    if (b->d_ctl) cudaFree(b->d_ctl);
+    if (b->h_tiles) cudaFreeHost(b->h_tiles);
+    if (b->h_state) cudaFreeHost(b->h_state);
+    if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    if (b->h_stop) cudaFreeHost(b->h_stop);
+    if (b->d_sink) cudaFree(b->d_sink);
+    delete b;
+    return CP_OK;
+}
+
+CP_API int cp_batch_add(cp_batch* b, cp_instance* I, const cp_solve_opts* opts, int* slot) {
+    if (!b || !I || !opts) return CP_ERR_INVALID;
+    if (b->running) return CP_ERR_BUSY;
+    if (I->in_batch) return CP_ERR_BUSY;
+    const cp_solve_opts o = *opts;
+    if (o.precision != CP_PREC_MIXED) return CP_ERR_UNSUPPORTED;
+    if (!(o.cg_tol > 0) || !(o.outer_tol > 0) || !(o.inner_tol > 0 && o.inner_tol < 1) || o.max_outer <= 0 ||
+        o.levels <= 0 || o.max_cg <= 0 || (o.precond & ~1))
+        return CP_ERR_INVALID;
+    return bguard(b, [&] {
+        CP_CHECK(I->loads_set, CP_ERR_INVALID, "loads not set");
+        CP_CHECK(I->ctx && I->ctx->device == b->ctx->device, CP_ERR_INVALID, "instance on another device");
+        CP_CHECK(I->csr.max_width <= b->o.max_width, CP_ERR_UNSUPPORTED,
+                 "node degree above the batch's assembly width (cp_batch_opts.max_width)");
+        int sl = -1;
+        for (int k = 0; k < b->cap; ++k)
+            if (!b->inst[k]) {
+                sl = k;
+                break;
+            }
+        CP_CHECK(sl >= 0, CP_ERR_BUSY, "no free batch slot");
+        CP_CUDA(cudaSetDevice(b->ctx->device));
+        instance_prepare_mixed(I, o.precond);
+        BDesc d{};
+        d.m = I->mesh;
+        d.n_slices = I->csr.n_slices;
+        d.n_groups = (I->n_elem + 31) / 32;
+        d.slice_ptr = I->csr.slice_ptr;
+        d.scol = I->csr.scol;
+        d.inc_pos = I->csr.inc_pos;
+        d.inc = I->csr.inc;
+        d.inc_k = I->csr.inc_k;
+        d.val64 = I->csr.val64;
+        d.val32 = I->csr.val32;
+        d.x = I->u;
+        d.b = I->b;
+        d.b_full = I->b_full;
+        d.u_full = I->u_full;
+        d.mask = I->mask;
+        d.r = I->r32;
+        d.z0 = I->z32a;
+        d.z1 = I->z32b;
+        d.q = I->q32;
+        d.s = I->s32;
+        d.minv = I->minv32;
+        d.st = I->st;
+        d.mat = I->mat;
+        d.part = I->alloc<double>(4 * (size_t)std::max(d.n_slices, d.n_groups));
+        d.cg_tol = o.cg_tol;
+        d.outer_tol = o.outer_tol;
+        d.inner_tol = o.inner_tol;
+        d.max_cg = o.max_cg;
+        d.max_outer = o.max_outer;
+        d.levels = o.levels;
+        d.aitken = o.aitken ? 1 : 0;
+        d.adaptive = o.adaptive_cg ? 1 : 0;
+        d.precond = o.precond;
+        CP_CUDA(cudaStreamSynchronize(I->s()));  // buffers of the instance's own stream are ready
+        BState S{};
+        S.phase = PH_LEVEL;
+        S.level = 1;
+        S.rel_err = 1.0;
+        S.w_prev = 1.0;
+        b->desc[sl] = d;
+        b->state[sl] = S;
+        CP_CUDA(cudaMemcpyAsync(b->d_desc + sl, &b->desc[sl], sizeof(BDesc), cudaMemcpyHostToDevice, b->ctx->stream));
+        CP_CUDA(cudaMemcpyAsync(b->d_state + sl, &b->state[sl], sizeof(BState), cudaMemcpyHostToDevice,
+                                b->ctx->stream));
+        CP_CUDA(cudaStreamSynchronize(b->ctx->stream));
+        b->inst[sl] = I;
+        I->in_batch = true;
+        b->listed.push_back(sl);
+        if (slot) *slot = sl;
+    });
+}
+
+CP_API int cp_batch_launch(cp_batch* b, int until, long long max_trips) {
+    if (!b || (until != CP_BATCH_RUN_ALL && until != CP_BATCH_RUN_ANY_DONE)) return CP_ERR_INVALID;
+    if (b->running) return CP_ERR_BUSY;
+    return bguard(b, [&] {
+        cudaStream_t s = b->ctx->stream;
+        CP_CUDA(cudaSetDevice(b->ctx->device));
+        const int nt = build_tiles(b, b->listed, true, nullptr);
+        interleave_tiles(b, nt);
+        if (!b->graph) build_graph(b);
+        BCtl c{};
+        c.n_tiles = nt;
+        int active = 0, done = 0;
+        for (int sl : b->listed) {
+            const int ph = b->state[sl].phase;
+            c.pop[ph] += 1;
+            if (ph == PH_DONE) ++done;
+            else ++active;
+        }
+        c.active = active;
+        c.done = 0;
+        c.exit_on_done = until == CP_BATCH_RUN_ANY_DONE ? 1 : 0;
+        c.trips = 0;
+        c.max_trips = max_trips;
+        c.stop = b->d_stop;
+        *b->h_ctl = c;
+        *(volatile int*)b->h_stop = 0;
+        if (nt > 0) CP_CUDA(cudaMemcpyAsync(b->d_tiles, b->h_tiles, sizeof(int4) * (size_t)nt, cudaMemcpyHostToDevice, s));
+        CP_CUDA(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BCtl), cudaMemcpyHostToDevice, s));
+        b->last_tiles = nt;
+        if (active > 0) {
+            CP_CUDA(cudaGraphLaunch(b->graph, s));
+            b->runs += 1;
+        }
+        CP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(BCtl), cudaMemcpyDeviceToHost, s));
+        // states of the listed slots (contiguous copy of the slot range in use)
+        int lo = b->cap, hi = -1;
+        for (int sl : b->listed) {
+            lo = std::min(lo, sl);
+            hi = std::max(hi, sl);
+        }
+        if (hi >= lo)
+            CP_CUDA(cudaMemcpyAsync(b->h_state + lo, b->d_state + lo, sizeof(BState) * (size_t)(hi - lo + 1),
+                                    cudaMemcpyDeviceToHost, s));
+        b->running = true;
+    });
+}
+
+CP_API int cp_batch_interrupt(cp_batch* b) {
+    if (!b || !b->h_stop) return CP_ERR_INVALID;
+    *(volatile int*)b->h_stop = 1;
+    return CP_OK;
+}
+
+CP_API int cp_batch_wait(cp_batch* b, int* active, int* done) {
+    if (!b) return CP_ERR_INVALID;
+    if (!b->running) {
+        int a = 0, d = 0;
+        for (int sl : b->listed) (b->state[sl].phase == PH_DONE ? d : a) += 1;
+        if (active) *active = a;
+        if (done) *done = d;
+        return CP_OK;
+    }
+    return bguard(b, [&] {
+        b->running = false;
+        CP_CUDA(cudaStreamSynchronize(b->ctx->stream));
+        const long long trips = b->h_ctl->trips;
+        b->trips += trips;
+        b->launches += trips * (long long)(b->o.elem_per_trip + 1 + b->o.cg_per_trip + 1);
+        int a = 0, d = 0;
+        for (int sl : b->listed) {
+            b->state[sl] = b->h_state[sl];
+            (b->state[sl].phase == PH_DONE ? d : a) += 1;
+        }
+        if (active) *active = a;
+        if (done) *done = d;
+    });
+}
+
+CP_API int cp_batch_run(cp_batch* b, int until, long long max_trips, int* active, int* done) {
+    int rc = cp_batch_launch(b, until, max_trips);
+    if (rc != CP_OK) return rc;
+    return cp_batch_wait(b, active, done);
+}
+
+CP_API int cp_batch_harvest(cp_batch* b, int cap, int* slots, cp_instance** insts, cp_solve_report* reports,
+                            int* count) {
+    if (!b || cap < 0 || !count) return CP_ERR_INVALID;
+    if (b->running) return CP_ERR_BUSY;
+    int k = 0;
+    std::vector<int> keep;
+    for (int sl : b->listed) {
+        if (b->state[sl].phase == PH_DONE && k < cap) {
+            if (slots) slots[k] = sl;
+            if (insts) insts[k] = b->inst[sl];
+            if (reports) reports[k] = report_of(b->state[sl]);
+            b->inst[sl]->in_batch = false;
+            b->inst[sl] = nullptr;
+            b->state[sl] = BState{};
+            ++k;
+        } else {
+            keep.push_back(sl);
+        }
+    }
+    b->listed.swap(keep);
+    *count = k;
+    return CP_OK;
+}
+
+CP_API int cp_batch_set_tile(cp_batch* b, int bucket, int slices) {
+    if (!b || bucket < 0 || bucket >= kBuckets || slices < 1 || slices > 1024) return CP_ERR_INVALID;
+    b->tile_slices[bucket] = slices;
+    return CP_OK;
+}
+
+CP_API int cp_batch_get_tile(const cp_batch* b, int bucket, int* slices) {
+    if (!b || bucket < 0 || bucket >= kBuckets || !slices) return CP_ERR_INVALID;
+    *slices = b->tile_slices[bucket];
+    return CP_OK;
+}
+
+CP_API int cp_batch_autotune(cp_batch* b, double* ms_per_sweep) {
+    if (!b) return CP_ERR_INVALID;
+    if (b->running) return CP_ERR_BUSY;
+    return bguard(b, [&] {
+        cudaStream_t s = b->ctx->stream;
+        CP_CUDA(cudaSetDevice(b->ctx->device));
+        cudaEvent_t e0, e1;
+        CP_CUDA(cudaEventCreate(&e0));
+        CP_CUDA(cudaEventCreate(&e1));
+        const int cands[] = {4, 8, 16, 32, 64};
+        double total = 0.0;
+        for (int bk = 0; bk < kBuckets; ++bk) {
+            std::vector<int> slots;
+            for (int sl : b->listed)
+                if (bucket_of(b->desc[sl].n_slices) == bk && b->state[sl].phase != PH_DONE) slots.push_back(sl);
+            if (slots.empty()) continue;
+            double best = 1e30;
+            int best_S = b->tile_slices[bk];
+            for (int S : cands) {
+                const int nt = build_tiles(b, slots, true, &S);
+                interleave_tiles(b, nt);
+                CP_CUDA(cudaMemcpyAsync(b->d_tiles, b->h_tiles, sizeof(int4) * (size_t)nt, cudaMemcpyHostToDevice, s));
+                k_batch_probe<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, nt, 0.5f, b->d_sink);  // warm
+                CP_CUDA(cudaEventRecord(e0, s));
+                const int reps = 5;
+                for (int r = 0; r < reps; ++r)
+                    k_batch_probe<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, nt, 0.5f,
+                                                                  b->d_sink);
+                CP_CUDA(cudaEventRecord(e1, s));
+                CP_CUDA(cudaEventSynchronize(e1));
+                CP_CUDA(cudaGetLastError());
+                float ms = 0;
+                CP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                const double t = ms / reps;
+                if (t < best) {
+                    best = t;
+                    best_S = S;
+                }
+            }
+            b->tile_slices[bk] = best_S;
+            total += best;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (ms_per_sweep) *ms_per_sweep = total;
+    });
+}
+
+CP_API int cp_batch_stats(const cp_batch* b, long long* trips, long long* launches, long long* runs) {
+    if (!b) return CP_ERR_INVALID;
+    if (trips) *trips = b->trips;
+    if (launches) *launches = b->launches;
+    if (runs) *runs = b->runs;
+    return CP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,76 @@
+// Host-side definitions of the opaque handles cp_context and cp_instance
+// (include/cuplast.h), shared by the translation units that drive them.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "cg.h"
+#include "internal.h"
+
+struct cp_context {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string last_error;
+};
+
+struct cp_instance {
+    cp_context* ctx = nullptr;
+    cp::DevMesh mesh;
+    cp::DevCsr csr;
+    cp_material mat_host{};
+    cp::MaterialDev mat{};
+    int n_nodes = 0, n_elem = 0;
+    double2 *u = nullptr, *b = nullptr, *b_full = nullptr, *u_full = nullptr;
+    uchar2* mask = nullptr;
+    double2 *r64 = nullptr, *z64a = nullptr, *z64b = nullptr, *q64 = nullptr, *s64 = nullptr;
+    float2 *r32 = nullptr, *z32a = nullptr, *z32b = nullptr, *q32 = nullptr, *s32 = nullptr;
+    double4* minv64 = nullptr;
+    float4* minv32 = nullptr;
+    cp::ElemState st{};
+    double* st_block = nullptr;
+    cp::CgScalars* sc = nullptr;
+    cp::OuterScalars* osc = nullptr;
+    double* partials = nullptr;
+    int max_blocks = 0;
+    cp::CgScalars* sc_h = nullptr;     // pinned
+    cp::OuterScalars* osc_h = nullptr;  // pinned
+    cudaGraphExec_t g64[2] = {nullptr, nullptr}, g32[2] = {nullptr, nullptr};  // [precond]
+    int body_iters = 8;
+    bool use_graph = true;  // CG loop as a CUDA graph with a device-side WHILE condition
+    bool loads_set = false;
+    bool in_batch = false;  // owned by a cp_batch until harvested: no other call may touch it
+    long long launches = 0;  // kernels launched (graph nodes included)
+    int last_assembly = -1;  // precision of the last assembly
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+
+    template <typename T>
+    T* alloc(size_t count) {
+        void* p = nullptr;
+        size_t nb = std::max<size_t>(count, 1) * sizeof(T);
+        CP_CUDA(cudaMallocAsync(&p, nb, ctx->stream));
+        allocs.push_back(p);
+        bytes += nb;
+        return static_cast<T*>(p);
+    }
+
+    cudaStream_t s() const { return ctx->stream; }
+    int sms() const { return ctx->sm_count; }
+
+    template <typename T>
+    cp::CgArgs<T> cg_args(int precond = 0);
+};
+
+
+namespace cp {
+// Allocates (once) what the mixed-precision solve needs beyond the FP64
+// instance: FP32 values and recurrence vectors, and with precond the FP32
+// block-Jacobi vectors. Stream-ordered on the instance's context stream.
+void instance_prepare_mixed(cp_instance* I, int precond);
+}  // namespace cp

@@ -192,6 +192,68 @@ CP_API int cp_secant_update_noalloc(void* stream, const cp_material* mat, int no
                                     int count4, const int* elem4, const double* uv, double* E_c, double* nu_c,
                                     double* psi, double* fields, double* rel_err);
 
+/* ------------------------------------------------------------- batch --- */
+/* Many independent instances solved together on one GPU (no counterpart in
+ * the reference, which solves one mesh per process, src/Main.cpp:1193-1227).
+ * Each instance runs the same algorithm as cp_solve in mixed precision (FP32
+ * values and inner CG inside FP64 defect correction, FP64 secant update), as
+ * its own device-side state machine: level -> assemble -> defect-correction
+ * CG -> secant update -> Aitken -> ... -> plastic strains. One captured CUDA
+ * graph drives every instance: a device WHILE loop over a body of phase-
+ * filtered kernels that walk a work list of (instance, tile) entries, so
+ * instances of different sizes advance concurrently with no host round trip;
+ * an instance that finishes its linear solve continues while others are
+ * still iterating. Every cross-tile sum is reduced per instance in a fixed
+ * order, so an instance's result does not depend on what else is in the
+ * batch. Instances are added between runs and harvested when done. */
+typedef struct cp_batch cp_batch;
+
+typedef struct {
+    int max_instances;   /* slots */
+    int cg_per_trip;     /* CG kernel launches per graph trip (each advances every CG instance by half an iteration) */
+    int elem_per_trip;   /* element-phase launches per trip (>= 3: update, Aitken, next level) */
+    int max_width;       /* assembly limit on blocks per node row (node degree + 1) */
+    int cg_blocks_per_sm;  /* persistent grid of the CG kernel: 0 = occupancy limit */
+} cp_batch_opts;
+
+enum { CP_BATCH_RUN_ALL = 0, CP_BATCH_RUN_ANY_DONE = 1 };
+
+CP_API void cp_batch_opts_default(cp_batch_opts* opts);
+CP_API int cp_batch_create(cp_context* ctx, const cp_batch_opts* opts, cp_batch** out);
+CP_API int cp_batch_destroy(cp_batch* b);
+/* Adds an instance (loads set; it may belong to another context on the same
+ * device) with its solve options; opts->precision must be CP_PREC_MIXED.
+ * From here until it is harvested the batch owns the instance: every other
+ * call on it returns CP_ERR_BUSY. Not allowed while a run is in flight. */
+CP_API int cp_batch_add(cp_batch* b, cp_instance* inst, const cp_solve_opts* opts, int* slot);
+/* Starts a run on the batch's stream and returns: the graph loops until every
+ * listed instance is done (CP_BATCH_RUN_ALL), or until at least one finishes
+ * (CP_BATCH_RUN_ANY_DONE), or after max_trips trips (<= 0: no limit), or when
+ * cp_batch_interrupt is called. */
+CP_API int cp_batch_launch(cp_batch* b, int until, long long max_trips);
+/* Waits for the run; *active = instances still running, *done = instances
+ * ready to harvest. */
+CP_API int cp_batch_wait(cp_batch* b, int* active, int* done);
+/* Asks a run in flight to stop at the end of its current trip (thread-safe,
+ * through host-mapped memory; used by schedulers that have new work). */
+CP_API int cp_batch_interrupt(cp_batch* b);
+CP_API int cp_batch_run(cp_batch* b, int until, long long max_trips, int* active, int* done);
+/* Removes up to cap finished instances: their slots, handles and reports
+ * (report->seconds = device time from the instance's first to its last phase). */
+CP_API int cp_batch_harvest(cp_batch* b, int cap, int* slots, cp_instance** insts, cp_solve_report* reports,
+                            int* count);
+/* Slices (32 nodes) per work-list tile for instances whose slice count lies
+ * in [2^bucket, 2^(bucket+1)); buckets 0..23. */
+CP_API int cp_batch_set_tile(cp_batch* b, int bucket, int slices);
+CP_API int cp_batch_get_tile(const cp_batch* b, int bucket, int* slices);
+/* Autotuner: times the CG kernel's SpMV over the listed instances of each
+ * size bucket for every candidate tile size (4..64 slices; state is left
+ * unchanged) and keeps the fastest per bucket. ms_per_sweep (may be NULL):
+ * the tuned time of one SpMV sweep over all listed instances. */
+CP_API int cp_batch_autotune(cp_batch* b, double* ms_per_sweep);
+/* Counters of the batch since creation: graph trips and kernel launches. */
+CP_API int cp_batch_stats(const cp_batch* b, long long* trips, long long* kernel_launches, long long* runs);
+
 /* ---------------------------------------------------------- read-back --- */
 /* Reference CSR arrays (SparseSLAE::rows/cols/adjPos/adj/data); any pointer
  * may be NULL. values: the last assembly (FP64, or FP32 widened). */
