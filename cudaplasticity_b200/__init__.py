@@ -7,7 +7,9 @@ library's CUDA kernels. Importing works without a GPU (mesh generation and
 load building are host code); device calls raise CuplastError when no CUDA
 device is present.
 """
+import atexit
 import ctypes
+import weakref
 
 import numpy as np
 
@@ -428,6 +430,13 @@ class Batch:
             out.append((int(slots[i]), inst, _report(reps[i])))
         return out
 
+    def progress(self, slot):
+        """(phase, level, report dict) of the instance in slot, as of the last run."""
+        ph, lv = ctypes.c_int(), ctypes.c_int()
+        rep = C.cp_solve_report()
+        self.ctx.check(C.lib().cp_batch_progress(self._h, slot, ctypes.byref(ph), ctypes.byref(lv), ctypes.byref(rep)))
+        return ph.value, lv.value, _report(rep)
+
     def autotune(self):
         ms = ctypes.c_double()
         self.ctx.check(C.lib().cp_batch_autotune(self._h, ctypes.byref(ms)))
@@ -445,6 +454,101 @@ class Batch:
         t, k, r = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
         self.ctx.check(C.lib().cp_batch_stats(self._h, ctypes.byref(t), ctypes.byref(k), ctypes.byref(r)))
         return dict(trips=t.value, kernel_launches=k.value, runs=r.value)
+
+
+class _Handed(Instance):
+    """An instance created by the library (a server result). It lives on the
+    server's streams: it is freed before the server (Server.close frees the
+    ones still open)."""
+
+    def __init__(self, server, handle, n_nodes, n_elem, count3, count4):
+        self.ctx = server.ctx
+        self._server = server
+        self._h = handle
+        self.n_nodes, self.n_elem, self.count3, self.count4 = n_nodes, n_elem, count3, count4
+
+
+_LIVE_SERVERS = weakref.WeakSet()
+
+
+@atexit.register
+def _close_servers():
+    for srv in list(_LIVE_SERVERS):
+        srv.close()
+
+
+class Server:
+    """Solve service (cp_server): requests are submitted as they arrive and
+    solved with continuous batching on one GPU; wait() hands back each
+    request's results."""
+
+    def __init__(self, device=0, hbm_reserve=0.05, max_bytes=0, max_inflight=1024, trip_quantum=0, **batch):
+        o = C.cp_server_opts()
+        C.lib().cp_server_opts_default(ctypes.byref(o))
+        o.device, o.hbm_reserve, o.max_bytes = device, hbm_reserve, int(max_bytes)
+        o.max_inflight, o.trip_quantum = max_inflight, int(trip_quantum)
+        for k, v in batch.items():
+            setattr(o.batch, k, v)
+        self._h = C.c_p()
+        st = C.lib().cp_server_create(ctypes.byref(o), ctypes.byref(self._h))
+        if st != C.CP_OK:
+            self._h = None
+            raise CuplastError(st)
+        self.ctx = Context(device)  # for error strings
+        self._meta = {}
+        self._handed = weakref.WeakSet()
+        _LIVE_SERVERS.add(self)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for inst in list(self._handed):
+                inst.close()
+            C.lib().cp_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, mesh_arrays, mat, rp, mask, uv=None, **solve_kw):
+        v, keep = mesh_view(mesh_arrays)
+        rp = np.ascontiguousarray(rp, np.float64)
+        mask = np.ascontiguousarray(mask, np.uint8)
+        uvp = None
+        if uv is not None:
+            uv = np.ascontiguousarray(uv, np.float64)
+            uvp = _dp(uv)
+        kw = dict(solve_kw)
+        kw["precision"] = CP_PREC_MIXED
+        o = solve_opts(**kw)
+        rid = ctypes.c_longlong()
+        st = C.lib().cp_server_submit(self._h, ctypes.byref(v), ctypes.byref(mat), _dp(rp), _up(mask), uvp,
+                                      ctypes.byref(o), ctypes.byref(rid))
+        if st != C.CP_OK:
+            raise CuplastError(st)
+        self._meta[rid.value] = (v.node_count, v.count3 + v.count4, v.count3, v.count4)
+        del keep
+        return rid.value
+
+    def wait(self, rid, timeout=-1.0):
+        """(Instance with the results, report dict, latency seconds)."""
+        h = C.c_p()
+        rep = C.cp_solve_report()
+        lat = ctypes.c_double()
+        st = C.lib().cp_server_wait(self._h, rid, float(timeout), ctypes.byref(h), ctypes.byref(rep),
+                                    ctypes.byref(lat))
+        if st != C.CP_OK:
+            raise CuplastError(st)
+        meta = self._meta.pop(rid)
+        inst = _Handed(self, h, *meta)
+        self._handed.add(inst)
+        return inst, _report(rep), lat.value
+
+    def stats(self):
+        s = C.cp_server_stats()
+        st = C.lib().cp_server_get_stats(self._h, ctypes.byref(s))
+        if st != C.CP_OK:
+            raise CuplastError(st)
+        return {k: getattr(s, k) for k, _ in C.cp_server_stats._fields_}
 
 
 def footprint(mesh_arrays, precision=CP_PREC_FP64):

@@ -64,6 +64,17 @@ class cp_batch_opts(ctypes.Structure):
 
 CP_BATCH_RUN_ALL, CP_BATCH_RUN_ANY_DONE = 0, 1
 
+
+class cp_server_opts(ctypes.Structure):
+    _fields_ = [("device", c_int), ("hbm_reserve", c_double), ("max_bytes", ctypes.c_size_t),
+                ("max_inflight", c_int), ("trip_quantum", c_ll), ("batch", cp_batch_opts)]
+
+
+class cp_server_stats(ctypes.Structure):
+    _fields_ = [("submitted", c_ll), ("admitted", c_ll), ("completed", c_ll), ("failed", c_ll), ("rejected", c_ll),
+                ("inflight", c_ll), ("pending", c_ll), ("runs", c_ll), ("trips", c_ll), ("busy_seconds", c_double),
+                ("peak_bytes", ctypes.c_size_t)]
+
 # name -> (restype, argtypes)
 _SIGS = {
     "cp_version": (ctypes.c_char_p, []),
@@ -103,6 +114,15 @@ _SIGS = {
     "cp_batch_get_tile": (c_int, [c_p, c_int, P_int]),
     "cp_batch_autotune": (c_int, [c_p, P_double]),
     "cp_batch_stats": (c_int, [c_p, P_ll, P_ll, P_ll]),
+    "cp_batch_progress": (c_int, [c_p, c_int, P_int, P_int, ctypes.POINTER(cp_solve_report)]),
+    "cp_server_opts_default": (None, [ctypes.POINTER(cp_server_opts)]),
+    "cp_server_create": (c_int, [ctypes.POINTER(cp_server_opts), ctypes.POINTER(c_p)]),
+    "cp_server_destroy": (c_int, [c_p]),
+    "cp_server_submit": (c_int, [c_p, ctypes.POINTER(cp_mesh_view), ctypes.POINTER(cp_material), P_double, P_ubyte,
+                                 P_double, ctypes.POINTER(cp_solve_opts), P_ll]),
+    "cp_server_wait": (c_int, [c_p, c_ll, c_double, ctypes.POINTER(c_p), ctypes.POINTER(cp_solve_report),
+                               P_double]),
+    "cp_server_get_stats": (c_int, [c_p, ctypes.POINTER(cp_server_stats)]),
     "cp_get_csr": (c_int, [c_p, P_int, P_int, P_int, P_int, P_double]),
     "cp_get_slot_map": (c_int, [c_p, P_int]),
     "cp_get_field": (c_int, [c_p, ctypes.c_char_p, P_double]),

@@ -7,14 +7,23 @@
 // recurrences inside FP64 defect correction) as its own state machine on the
 // device:
 //
-//   LEVEL -> ASM -> INIT -> (P -> U)* -> INIT ... -> UPD -> RELAX -> ASM ...
-//                                         (level converged) -> LEVEL / PLASTIC -> DONE
+//   LEVEL -> ASM -> INIT -> (P -> U [-> RR])* -> UPD -> RELAX -> ASM ...
+//                           (level converged) -> LEVEL / PLASTIC -> DONE
+//
+// The linear solve is one preconditioned CG on the FP32 values with FP32
+// recurrences ("reliable updates"): INIT computes the residual b - K64 x in
+// FP64 once; whenever the recursive FP32 residual has dropped by inner_tol
+// since the last replacement, or meets the solve's tolerance, RR replaces it
+// by the FP64 residual b - K64 x (x itself accumulates in FP64) and the
+// search direction carries on, so the Krylov space is kept; the solve ends
+// when the FP64 residual meets the tolerance.
 //
 // The instances' nodes and elements are cut into tiles; one work list holds
 // every (instance, tile) pair. Three persistent kernels walk that list, each
 // acting only on the tiles whose instance is in one of its phases:
-//   k_batch_cg    INIT (FP64 residual, FP32 restart), P (SpMV + direction),
-//                 U (axpy / residual / preconditioner)
+//   k_batch_cg    INIT (FP64 residual), P (SpMV + direction),
+//                 U (axpy / residual / preconditioner), RR (FP64 residual
+//                 replacement)
 //   k_batch_asm   ASM (FP64 + FP32 values of K, node gather, no atomics)
 //   k_batch_elem  LEVEL, UPD (strain / stress / secant / exit norm),
 //                 RELAX (Aitken), PLASTIC
@@ -54,6 +63,7 @@ enum : int {
     PH_INIT,
     PH_P,
     PH_U,
+    PH_RR,
     PH_UPD,
     PH_RELAX,
     PH_PLASTIC,
@@ -90,11 +100,11 @@ struct BDesc {
 // Mutable state of one instance.
 struct BState {
     int phase, status, level, levels_done;
-    int outer_it, outer_total, restarts, parity;
+    int outer_it, outer_total, parity, pad0;
     unsigned int ticket;
     int pad;
     long long iter, lin_iters, cg_total, fp64_spmv;
-    double rr, rho, alpha, beta, normB_inv, eps2_inner, bb, res64;
+    double rr, rho, rho_prev, alpha, beta, rr_ref, eps2_inner, bb, res64;
     double eps, rel_err, w_prev, omega, cg_rel_res;
     unsigned long long t_first, t_done;  // %globaltimer, ns
 };
@@ -266,23 +276,91 @@ __device__ void tile_init(const BDesc& d, BState* S, BCtl* c, int4 tl, double* s
         const double rr = t[0], res64 = t[1], bb = t[2];
         S->ticket = 0;
         S->fp64_spmv += 1;
-        S->restarts += 1;
         S->bb = bb;
         S->res64 = res64;
         S->cg_rel_res = bb > 0.0 ? sqrt(res64 / bb) : 0.0;
         if (!(rr == rr) || !(bb == bb) || !(res64 == res64)) {
             finish(S, c, CP_ERR_BREAKDOWN);
-        } else if (res64 <= S->eps * S->eps * bb || rr == 0.0 || S->restarts > 200 || S->lin_iters >= d.max_cg) {
-            set_phase(S, c, PH_UPD);  // the linear solve meets its tolerance (or its caps)
+        } else if (res64 <= S->eps * S->eps * bb || rr == 0.0 || S->lin_iters >= d.max_cg) {
+            set_phase(S, c, PH_UPD);  // the linear solve meets its tolerance (or its cap)
         } else {
             S->rr = rr;
+            S->rr_ref = rr;
             S->rho = pre ? t[3] : rr;
-            S->normB_inv = 1.0 / rr;  // inner solve: reduction relative to its start
             S->eps2_inner = d.inner_tol * d.inner_tol;
             S->iter = 0;
             S->alpha = 0.0;
             S->beta = 0.0;
             S->parity = 0;
+            set_phase(S, c, PH_P);
+        }
+    }
+}
+
+// RR: the recursive residual is replaced by the FP64 residual of the FP64
+// solution, r = m.(b - K64 x) (stored in FP32), s = M^-1 r with the
+// preconditioner of INIT; the search direction is kept and beta is recomputed
+// from the replaced residual. Sums (r32, r32), (r64, r64), -, (r32, s).
+__device__ void tile_rr(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
+    const int pre = d.precond;
+    for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
+        const int n = 32 * sl + lane;
+        const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
+        double s_rr = 0.0, s_r64 = 0.0, s_rho = 0.0;
+        if (n < d.m.n_nodes) {
+            double k0 = 0.0, k1 = 0.0;
+            for (int k = 0; k < wd; ++k) {
+                const long long bi = base + 32LL * k + lane;
+                const int col = __ldg(d.scol + bi);
+                const double2* vp = reinterpret_cast<const double2*>(d.val64 + 4 * bi);
+                const double2 lo = __ldg(vp), hi = __ldg(vp + 1);
+                const double2 xc = d.x[col];
+                k0 += lo.x * xc.x + lo.y * xc.y;
+                k1 += hi.x * xc.x + hi.y * xc.y;
+            }
+            const double2 bb = d.b[n];
+            const uchar2 m = d.mask[n];
+            const double r0 = m.x ? bb.x - k0 : 0.0, r1 = m.y ? bb.y - k1 : 0.0;
+            const float2 rt = make_float2((float)r0, (float)r1);
+            d.r[n] = rt;
+            s_rr = (double)rt.x * (double)rt.x + (double)rt.y * (double)rt.y;
+            if (pre) {
+                const float4 mi = d.minv[n];
+                const float2 sv = make_float2(mi.x * rt.x + mi.y * rt.y, mi.z * rt.x + mi.w * rt.y);
+                d.s[n] = sv;
+                s_rho = (double)rt.x * (double)sv.x + (double)rt.y * (double)sv.y;
+            }
+            s_r64 = r0 * r0 + r1 * r1;
+        }
+        s_rr = warp_sum(s_rr);
+        s_r64 = warp_sum(s_r64);
+        s_rho = warp_sum(s_rho);
+        if (lane == 0) {
+            double* p = d.part + 4 * (size_t)sl;
+            p[0] = s_rr; p[1] = s_r64; p[2] = 0.0; p[3] = s_rho;
+        }
+    }
+    if (!arrive(S, tl.w, shf)) return;
+    double t[4];
+    reduce_parts<4>(d.part, d.n_slices, t, sh);
+    if (threadIdx.x == 0) {
+        const double rr = t[0], res64 = t[1];
+        S->ticket = 0;
+        S->fp64_spmv += 1;
+        S->res64 = res64;
+        S->cg_rel_res = S->bb > 0.0 ? sqrt(res64 / S->bb) : 0.0;
+        if (!(rr == rr) || !(res64 == res64)) {
+            finish(S, c, CP_ERR_BREAKDOWN);
+        } else if (res64 <= S->eps * S->eps * S->bb || rr == 0.0 || S->lin_iters >= d.max_cg) {
+            set_phase(S, c, PH_UPD);
+        } else {
+            const double rho_new = pre ? t[3] : rr;
+            S->beta = rho_new / S->rho_prev;
+            S->rho = rho_new;
+            S->rr = rr;
+            S->rr_ref = rr;
             set_phase(S, c, PH_P);
         }
     }
@@ -383,6 +461,7 @@ __device__ void tile_u(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, 
         const double rn = t[0];
         const double rho_new = pre ? t[1] : rn;
         S->ticket = 0;
+        S->rho_prev = S->rho;
         S->beta = rho_new / S->rho;
         S->rho = rho_new;
         S->rr = rn;
@@ -391,7 +470,7 @@ __device__ void tile_u(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, 
         S->cg_total += 1;
         S->parity ^= 1;
         if (!(rn == rn)) finish(S, c, CP_ERR_BREAKDOWN);
-        else if (rn * S->normB_inv <= S->eps2_inner) set_phase(S, c, PH_INIT);  // restart from the FP64 residual
+        else if (rn <= S->eps * S->eps * S->bb || rn <= S->eps2_inner * S->rr_ref) set_phase(S, c, PH_RR);
         else if (S->lin_iters >= d.max_cg) set_phase(S, c, PH_UPD);
         else set_phase(S, c, PH_P);
     }
@@ -403,7 +482,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_cg(const BDesc* __restrict__
     __shared__ int shf, shp;
     {
         const volatile int* pop = c->pop;
-        if (pop[PH_INIT] + pop[PH_P] + pop[PH_U] == 0) return;
+        if (pop[PH_INIT] + pop[PH_P] + pop[PH_U] + pop[PH_RR] == 0) return;
     }
     const int nt = c->n_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
@@ -412,6 +491,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_cg(const BDesc* __restrict__
         const int ph = tile_phase(S, &shp);
         if (ph == PH_P) tile_p(D[tl.x], S, c, tl, sh, &shf);
         else if (ph == PH_U) tile_u(D[tl.x], S, c, tl, sh, &shf);
+        else if (ph == PH_RR) tile_rr(D[tl.x], S, c, tl, sh, &shf);
         else if (ph == PH_INIT) tile_init(D[tl.x], S, c, tl, sh, &shf);
     }
 }
@@ -587,7 +667,6 @@ __global__ void __launch_bounds__(kThreads) k_batch_elem(const BDesc* __restrict
                     S->outer_it += 1;
                     S->outer_total += 1;
                     S->lin_iters = 0;
-                    S->restarts = 0;
                     if (!isfinite(rel)) {
                         finish(S, c, CP_ERR_BREAKDOWN);
                     } else if (d.aitken) {
@@ -1140,6 +1219,16 @@ CP_API int cp_batch_autotune(cp_batch* b, double* ms_per_sweep) {
         cudaEventDestroy(e1);
         if (ms_per_sweep) *ms_per_sweep = total;
     });
+}
+
+CP_API int cp_batch_progress(const cp_batch* b, int slot, int* phase, int* level, cp_solve_report* report) {
+    if (!b || slot < 0 || slot >= b->cap || !b->inst[slot]) return CP_ERR_INVALID;
+    if (b->running) return CP_ERR_BUSY;
+    const BState& S = b->state[slot];
+    if (phase) *phase = S.phase;
+    if (level) *level = S.level;
+    if (report) *report = report_of(S);
+    return CP_OK;
 }
 
 CP_API int cp_batch_stats(const cp_batch* b, long long* trips, long long* launches, long long* runs) {

@@ -195,17 +195,21 @@ CP_API int cp_secant_update_noalloc(void* stream, const cp_material* mat, int no
 /* ------------------------------------------------------------- batch --- */
 /* Many independent instances solved together on one GPU (no counterpart in
  * the reference, which solves one mesh per process, src/Main.cpp:1193-1227).
- * Each instance runs the same algorithm as cp_solve in mixed precision (FP32
- * values and inner CG inside FP64 defect correction, FP64 secant update), as
- * its own device-side state machine: level -> assemble -> defect-correction
- * CG -> secant update -> Aitken -> ... -> plastic strains. One captured CUDA
- * graph drives every instance: a device WHILE loop over a body of phase-
- * filtered kernels that walk a work list of (instance, tile) entries, so
- * instances of different sizes advance concurrently with no host round trip;
- * an instance that finishes its linear solve continues while others are
- * still iterating. Every cross-tile sum is reduced per instance in a fixed
- * order, so an instance's result does not depend on what else is in the
- * batch. Instances are added between runs and harvested when done. */
+ * Each instance runs cp_solve's outer algorithm (load levels, assembly,
+ * linear solve, secant update, optional Aitken relaxation) in mixed
+ * precision: FP32 values and FP32 CG recurrences, with the solution u
+ * accumulated in FP64, every dot product reduced in FP64, and the recursive
+ * residual replaced by the FP64 residual b - K64 u whenever it has dropped by
+ * inner_tol since the last replacement or meets cg_tol (the linear solve ends
+ * on the FP64 residual); the secant update is FP64. Every instance is its own
+ * device-side state machine. One captured CUDA graph drives all of them: a
+ * device WHILE loop over a body of phase-filtered kernels that walk a work
+ * list of (instance, tile) entries, so instances of different sizes advance
+ * concurrently with no host round trip; an instance that finishes its linear
+ * solve continues while others are still iterating. Every cross-tile sum is
+ * reduced per instance in a fixed order, so an instance's result does not
+ * depend on what else is in the batch. Instances are added between runs and
+ * harvested when done. */
 typedef struct cp_batch cp_batch;
 
 typedef struct {
@@ -251,8 +255,64 @@ CP_API int cp_batch_get_tile(const cp_batch* b, int bucket, int* slices);
  * unchanged) and keeps the fastest per bucket. ms_per_sweep (may be NULL):
  * the tuned time of one SpMV sweep over all listed instances. */
 CP_API int cp_batch_autotune(cp_batch* b, double* ms_per_sweep);
+/* Progress of the instance in a slot as of the end of the last run: phase
+ * (1 level set-up, 2 assembly, 3 first FP64 residual, 4-5 CG, 6 FP64
+ * residual replacement, 7 secant update, 8 Aitken, 9 plastic strains,
+ * 10 done), load level, and the counters of its report so far. */
+CP_API int cp_batch_progress(const cp_batch* b, int slot, int* phase, int* level, cp_solve_report* report);
 /* Counters of the batch since creation: graph trips and kernel launches. */
 CP_API int cp_batch_stats(const cp_batch* b, long long* trips, long long* kernel_launches, long long* runs);
+
+/* ------------------------------------------------------------ server --- */
+/* A solve service on one GPU (no counterpart in the reference): requests of
+ * uneven sizes (mesh, material / hardening diagram, loads, load levels) are
+ * submitted from any thread as they arrive; a scheduler thread admits them
+ * in arrival order while their device footprint (cp_instance_footprint) fits
+ * into the free device memory minus a reserve and a batch slot is free, sets
+ * each one up on its own stream while the batch's graph keeps running, then
+ * makes the running graph stop at its next trip so that the new instances
+ * join, and harvests finished ones. Every request's matrix, displacements and
+ * plastic state stay on the device from admission to completion; requests
+ * that arrive while others are on the GPU overlap with them (continuous
+ * batching). Each result is the one the same request gives alone. */
+typedef struct cp_server cp_server;
+
+typedef struct {
+    int device;
+    double hbm_reserve;      /* fraction of the device memory kept free (admission limit) */
+    size_t max_bytes;        /* limit on the sum of admitted footprints (0: free memory only) */
+    int max_inflight;        /* requests on the device at once (<= batch slots) */
+    long long trip_quantum;  /* graph trips per run before the scheduler looks again (<= 0: until one finishes) */
+    cp_batch_opts batch;
+} cp_server_opts;
+
+typedef struct {
+    long long submitted, admitted, completed, failed, rejected;
+    long long inflight, pending;
+    long long runs, trips;
+    double busy_seconds;     /* host time with a run in flight */
+    size_t peak_bytes;       /* largest sum of admitted footprints */
+} cp_server_stats;
+
+CP_API void cp_server_opts_default(cp_server_opts* opts);
+CP_API int cp_server_create(const cp_server_opts* opts, cp_server** out);
+/* Stops the scheduler; requests not yet completed are cancelled
+ * (CP_ERR_CANCELLED to their waiters); instances not yet taken are freed. */
+CP_API int cp_server_destroy(cp_server* s);
+/* Copies the request and returns at once; *id identifies it. opts->precision
+ * must be CP_PREC_MIXED. A request larger than the whole admission limit is
+ * rejected here with CP_ERR_NOMEM. */
+CP_API int cp_server_submit(cp_server* s, const cp_mesh_view* mesh, const cp_material* mat, const double* rp,
+                            const unsigned char* mask, const double* uv, const cp_solve_opts* opts, long long* id);
+/* Waits (timeout_s < 0: without limit) until request id completes; returns
+ * CP_ERR_BUSY on timeout. On completion hands over the instance with the
+ * results (read them with cp_get_field; free it with cp_instance_destroy
+ * before cp_server_destroy: it lives on the server's streams),
+ * its report (report->status: the solve's own status) and the latency from
+ * submission to completion in seconds. Each id can be taken once. */
+CP_API int cp_server_wait(cp_server* s, long long id, double timeout_s, cp_instance** inst, cp_solve_report* report,
+                          double* latency_s);
+CP_API int cp_server_get_stats(cp_server* s, cp_server_stats* stats);
 
 /* ---------------------------------------------------------- read-back --- */
 /* Reference CSR arrays (SparseSLAE::rows/cols/adjPos/adj/data); any pointer

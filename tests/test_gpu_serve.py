@@ -1,0 +1,116 @@
+"""GPU tests of the solve service (cp_server_*), through the C ABI.
+
+Requests arrive from a separate thread at random times while others are on
+the device (continuous batching); each result must be bit-identical to the
+same request solved alone, admission must respect the byte budget, and a
+request larger than the budget is rejected at submission."""
+import random
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import cudaplasticity_b200 as cp
+from cudaplasticity_b200 import workload
+
+pytestmark = pytest.mark.gpu
+
+GEN = dict(dof_min=600, dof_max=6000)
+# Some seeded requests converge slowly (heavy plasticity); the cap keeps the
+# test short, and a capped request must still equal its capped solve alone.
+KW = dict(cg_tol=1e-10, outer_tol=1e-7, max_outer=120, max_cg=2_000_000, precond=1, aitken=1, adaptive_cg=1,
+          inner_tol=1e-3)
+
+
+def alone(ctx, w):
+    inst = cp.Instance(ctx, w["mesh"], w["material"])
+    inst.set_loads(w["rp"], w["mask"], w["uv"])
+    b = cp.Batch(ctx, max_instances=1)
+    b.add(inst, levels=w["levels"], **KW)
+    while b.run()[0]:
+        pass
+    (_, inst_b, rep), = b.harvest()
+    st = inst_b.state()
+    inst_b.close()
+    b.close()
+    return st, rep
+
+
+def submit_all(server, ws, rate_hz, seed=7):
+    """Submits the requests from a thread at Poisson arrival times; returns ids."""
+    ids = [None] * len(ws)
+    rng = random.Random(seed)
+
+    def run():
+        for k, w in enumerate(ws):
+            time.sleep(rng.expovariate(rate_hz))
+            ids[k] = server.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"], **KW)
+
+    t = threading.Thread(target=run)
+    t.start()
+    return t, ids
+
+
+def test_served_results_equal_alone():
+    ws = [workload.instance(i, increments=(1, 3), **GEN) for i in range(30, 38)]
+    ctx = cp.Context(0)
+    ref = [alone(ctx, w) for w in ws]
+    srv = cp.Server(max_inflight=4)
+    try:
+        t, ids = submit_all(srv, ws, rate_hz=200.0)
+        t.join()
+        lat = []
+        for k, rid in enumerate(ids):
+            inst, rep, latency = srv.wait(rid, timeout=300.0)
+            assert rep["status"] == ref[k][1]["status"], (rep, ref[k][1])
+            st = inst.state()
+            for f in cp.FIELDS + ["uv"]:
+                assert np.array_equal(st[f], ref[k][0][f]), (k, f)
+            assert rep["outer_iters"] == ref[k][1]["outer_iters"] and rep["cg_iters"] == ref[k][1]["cg_iters"]
+            lat.append(latency)
+            inst.close()
+        s = srv.stats()
+        assert s["completed"] == len(ws) and s["admitted"] == len(ws)
+        assert s["runs"] >= 2 and all(x > 0 for x in lat)
+    finally:
+        srv.close()
+        ctx.close()
+
+
+def test_admission_respects_byte_budget():
+    ws = [workload.instance(i, **GEN) for i in range(40, 46)]
+    fps = [cp.footprint(w["mesh"], cp.CP_PREC_MIXED) for w in ws]
+    budget = int(1.5 * max(fps))
+    ctx = cp.Context(0)
+    ref = [alone(ctx, w) for w in ws]
+    srv = cp.Server(max_bytes=budget)
+    try:
+        ids = [srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"], **KW)
+               for w in ws]
+        for k, rid in enumerate(ids):
+            inst, rep, _ = srv.wait(rid, timeout=300.0)
+            assert rep["status"] == ref[k][1]["status"]
+            assert np.array_equal(inst.field("uv"), ref[k][0]["uv"])
+            inst.close()
+        s = srv.stats()
+        assert 0 < s["peak_bytes"] <= budget
+        assert s["completed"] == len(ws)
+        with pytest.raises(cp.CuplastError) as e:
+            big = workload.instance(0)  # far above the budget
+            srv.submit(big["mesh"], big["material"], big["rp"], big["mask"], big["uv"], **KW)
+        assert e.value.status == cp._capi.CP_ERR_NOMEM
+        assert srv.stats()["rejected"] == 1
+    finally:
+        srv.close()
+        ctx.close()
+
+
+def test_destroy_with_requests_in_flight_returns():
+    ws = [workload.instance(i, **GEN) for i in range(50, 54)]
+    srv = cp.Server(max_inflight=2)
+    for w in ws:
+        srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"], **KW)
+    t0 = time.time()
+    srv.close()
+    assert time.time() - t0 < 60.0
