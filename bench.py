@@ -15,6 +15,21 @@ the reference). ``--impl reference`` runs the reference implementation's own
 CPU path (oracle/_ref/cpref, built from its sources) on the same job with all
 host cores.
 
+Beside the headline, the line carries the batched and served forms on the
+seeded config-4 / config-5 request streams (cudaplasticity_b200/workload.py):
+  batched  closed-loop saturation throughput of the batched mixed-precision
+           engine: a batch of 512 resident instances of the config-4 stream
+           (DOF log-uniform in [2k, 200k], plates and rings, 5-segment
+           diagrams), refilled from the stream as solves finish, converged
+           solves counted over a fixed window; the SpMV sweep over all 512
+           resident instances timed live (CG GB/s);
+  plain    the plain FP64 drop-in, one request at a time, on a seeded sample
+           of the requests the batched window completed (same solver
+           options), and the mixed-precision results' error against it;
+  served   the solve service (cp_server) under Poisson arrivals of config-5
+           requests (DOF log-uniform in [2k, 500k], 5-30 load increments),
+           host buffers in and results out: solves/s and p50/p99 latency.
+
 Multi-GPU: the path does not shard (one solve is one small instance), so N GPUs
 run N independent replicas ("replicas only"); value = solves of all ranks /
 max-over-ranks time.
@@ -175,6 +190,224 @@ def flush_l2(ctx_dev):
     torch.cuda.synchronize(ctx_dev)
 
 
+
+BATCH_KW = dict(cg_tol=1e-10, outer_tol=1e-6, max_outer=2000, max_cg=5_000_000, precond=1, aitken=1, adaptive_cg=1,
+                inner_tol=1e-3)
+
+
+def batched_leg(ctx, window_s=20.0, warm_s=3.0, slots=512, pool_size=768, seed=20261203):
+    """The batched engine on the config-4 stream.
+
+    saturation: closed loop, a batch of `slots` resident instances refilled
+        from the stream as solves finish; converged solves per second over a
+        window, and the SpMV sweep over all resident instances (CG GB/s).
+        Quick requests finish first, so this is a throughput, not a comparison.
+    The like-for-like comparison with the plain drop-in is compare_leg.
+    """
+    import numpy as np
+
+    import cudaplasticity_b200 as cp
+    from cudaplasticity_b200 import workload
+
+    def make(i):
+        w = workload.instance(i, seed=seed)
+        inst = cp.Instance(ctx, w["mesh"], w["material"])
+        inst.set_loads(w["rp"], w["mask"], w["uv"])
+        return w, inst
+
+    # --- saturation ---
+    pool = [make(i) for i in range(pool_size)]
+    b = cp.Batch(ctx, max_instances=slots)
+    nxt = 0
+    for _ in range(slots):
+        b.add(pool[nxt][1], levels=1, **BATCH_KW)
+        nxt += 1
+    b.run(max_trips=2)
+    ms_sweep = b.autotune()
+    blocks = nodes = 0
+    for _, inst in pool[:slots]:
+        n, ne, nnz, nadj = inst.sizes()
+        blocks += nnz // 4
+        nodes += n
+    # algorithmic bytes of one SpMV sweep (P phase, FP32): 4 values + one
+    # column per 2x2 block, read r (or s) and z, write z' and K z'
+    bytes_sweep = blocks * 20 + nodes * 4 * 8
+    by_inst = {id(p[1]): p for p in pool}
+    done = []
+    t0 = time.perf_counter()
+    t_start = None
+    while True:
+        now = time.perf_counter() - t0
+        if t_start is None and now >= warm_s:
+            t_start, launches_start = now, b.stats()["kernel_launches"]
+        if now >= warm_s + window_s:
+            break
+        b.run(max_trips=200)
+        for slot, inst, rep in b.harvest():
+            done.append((time.perf_counter() - t0, by_inst[id(inst)], rep))
+            if nxt < len(pool):
+                b.add(pool[nxt][1], levels=1, **BATCH_KW)
+                nxt += 1
+    t_end = time.perf_counter() - t0
+    counted = [d for d in done if d[0] > t_start]
+    launches_sat = b.stats()["kernel_launches"] - launches_start
+    b.close()  # releases the instances still in flight (not counted)
+    for _, inst in pool:
+        inst.close()
+    saturation = {
+        "slots": slots, "window_s": round(t_end - t_start, 2), "completed": len(counted),
+        "solves_per_s": len(counted) / (t_end - t_start), "statuses": sorted({d[2]["status"] for d in counted}),
+        "mean_dof_completed": float(sum(d[1][0]["params"]["dof"] for d in counted) / max(1, len(counted))),
+        "resident_dof": int(2 * nodes), "gpu_launches": int(launches_sat),
+        "spmv_sweep": {"ms": ms_sweep, "bytes": bytes_sweep, "gbs": bytes_sweep / (ms_sweep * 1e-3) / 1e9,
+                       "kernel": "k_batch_cg P phase (autotuner probe), all resident instances"},
+    }
+
+    return {
+        "workload": "config-4 stream: seeded instances (base seed %d), DOF log-uniform [2k, 200k], plates / rings, "
+                    "5-segment piecewise diagrams, 1 load level, CG 1e-10, outer 1e-6; batched = mixed precision, "
+                    "plain = FP64 drop-in one request at a time, same solver options" % seed,
+        "saturation": saturation,
+    }
+
+
+def compare_leg(ctx, n_requests, max_outer=300, seed=20261203):
+    """Like for like: the plain FP64 drop-in solves the first n requests of
+    the config-4 stream one at a time; the batched mixed-precision engine
+    then solves exactly the same requests (fresh instances) to completion.
+    Same solver options and caps for both, wall clock for both, and the error
+    of each mixed-precision result against its FP64 result. Requests that hit
+    the outer cap count as solved by both (same cap) and are listed."""
+    import numpy as np
+
+    import cudaplasticity_b200 as cp
+    from cudaplasticity_b200 import workload
+
+    kw = dict(BATCH_KW, max_outer=max_outer)
+
+    def make(i):
+        w = workload.instance(i, seed=seed)
+        inst = cp.Instance(ctx, w["mesh"], w["material"])
+        inst.set_loads(w["rp"], w["mask"], w["uv"])
+        return w, inst
+
+    plain, t_plain = {}, 0.0
+    for k in range(n_requests):
+        w, inst = make(k)
+        t1 = time.perf_counter()
+        rep = inst.solve(allow_not_converged=True, precision=cp.CP_PREC_FP64, levels=1, **kw)
+        t_plain += time.perf_counter() - t1
+        plain[k] = (inst.state(), rep, w["params"]["dof"])
+        inst.close()
+    ids = sorted(plain)
+    insts = {i: make(i)[1] for i in ids}
+    b = cp.Batch(ctx, max_instances=len(ids))
+    for i in ids:
+        b.add(insts[i], levels=1, **kw)
+    b.run(max_trips=1)
+    b.autotune()  # tile sizes per size bucket of this set (state unchanged)
+    reps = {}
+    for slot, inst, rep in b.harvest():
+        reps[id(inst)] = rep
+    launches0 = b.stats()["kernel_launches"]
+    t1 = time.perf_counter()
+    while True:
+        active, _ = b.run()
+        for slot, inst, rep in b.harvest():
+            reps[id(inst)] = rep
+        if active == 0:
+            break
+    t_batch = time.perf_counter() - t1
+    launches_fixed = b.stats()["kernel_launches"] - launches0
+    errs = {"uv": 0.0, "sig_i": 0.0, "eps_p_i": 0.0}
+    statuses = set()
+    for i in ids:
+        mixed = insts[i].state()
+        ref = plain[i][0]
+        statuses.add(reps[id(insts[i])]["status"])
+        for f in errs:
+            nrm = np.linalg.norm(ref[f])
+            errs[f] = max(errs[f], float(np.linalg.norm(mixed[f] - ref[f]) / nrm) if nrm > 0 else 0.0)
+        insts[i].close()
+    b.close()
+    fixed = {
+        "workload": "first %d requests of the config-4 stream (base seed %d), outer cap %d, CG 1e-10, outer 1e-6"
+                    % (n_requests, seed, max_outer),
+        "requests": len(ids), "dof": [plain[i][2] for i in ids],
+        "capped": [i for i in ids if plain[i][1]["status"] != 0],
+        "plain_fp64_dropin": {"seconds": t_plain, "solves_per_s": len(ids) / t_plain,
+                              "statuses": sorted({plain[i][1]["status"] for i in ids})},
+        "batched_mixed": {"seconds": t_batch, "solves_per_s": len(ids) / t_batch, "statuses": sorted(statuses),
+                          "gpu_launches": int(launches_fixed)},
+        "speedup_vs_plain": t_plain / t_batch,
+        "max_rel_err_mixed_vs_fp64": errs,
+    }
+    return fixed
+
+
+def served_leg(rate_hz=10.0, submit_s=20.0, drain_s=25.0, seed=20270101):
+    """The solve service under Poisson arrivals of config-5 requests."""
+    import random
+
+    import numpy as np
+
+    import cudaplasticity_b200 as cp
+    from cudaplasticity_b200 import workload
+
+    rng = random.Random(seed)
+    srv = cp.Server()
+    ids, t_sub, h2d = [], [], 0
+    t0 = time.perf_counter()
+    k = 0
+    next_t = rng.expovariate(rate_hz)
+    while next_t < submit_s:
+        w = workload.instance(k, seed=seed, dof_min=2000, dof_max=500000, increments=(5, 30))
+        now = time.perf_counter() - t0
+        if next_t > now:
+            time.sleep(next_t - now)
+        ids.append(srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"], **BATCH_KW))
+        t_sub.append(time.perf_counter() - t0)
+        h2d += sum(w["mesh"][a].nbytes for a in ("node_xy", "elem4")) + w["rp"].nbytes + w["mask"].nbytes + w["uv"].nbytes
+        k += 1
+        next_t += rng.expovariate(rate_hz)
+    deadline = t0 + submit_s + drain_s
+    lat, statuses, d2h, last_done = [], [], 0, 0.0
+    pending = list(ids)
+    while pending and time.perf_counter() < deadline:
+        still = []
+        for rid in pending:
+            try:
+                inst, rep, latency = srv.wait(rid, timeout=0.0)
+            except cp.CuplastError as e:
+                if e.status == cp._capi.CP_ERR_BUSY:
+                    still.append(rid)
+                    continue
+                raise
+            st = inst.state()
+            d2h += sum(v.nbytes for v in st.values())
+            inst.close()
+            lat.append(latency)
+            statuses.append(rep["status"])
+            last_done = time.perf_counter() - t0
+        pending = still
+        time.sleep(0.02)
+    stats = srv.stats()
+    srv.close()
+    n = len(lat)
+    return {
+        "workload": "config-5 stream: Poisson arrivals, DOF log-uniform [2k, 500k], 5-30 load increments, "
+                    "mixed precision, CG 1e-10, outer 1e-6",
+        "rate_hz": rate_hz, "submitted": len(ids), "completed": n,
+        "solves_per_s": n / last_done if last_done > 0 else 0.0,
+        "p50_s": float(np.percentile(lat, 50)) if n else None,
+        "p99_s": float(np.percentile(lat, 99)) if n else None,
+        "censored": len(ids) - n, "statuses": sorted(set(statuses)),
+        "h2d_bytes": int(h2d), "d2h_bytes": int(d2h), "server": {k: stats[k] for k in
+                                                               ("admitted", "completed", "runs", "trips",
+                                                                "busy_seconds", "peak_bytes")},
+    }
+
+
 def run_product_arm(args):
     import numpy as np
 
@@ -310,6 +543,12 @@ def run_product_arm(args):
                "sample": "one full config-1 solve (10 levels, CG 1e-10, outer 1e-6), reference CPU path, "
                          f"{c['outer']} outer / {c['cg']} CG iterations"}
 
+    batched = served = None
+    if rank == 0 and not args.skip_batched:
+        batched = batched_leg(ctx, window_s=args.batched_window)
+    if rank == 0 and not args.skip_served:
+        served = served_leg(rate_hz=args.serve_rate, submit_s=args.serve_window, drain_s=args.serve_window + 5)
+
     launches = sum(r["kernel_launches"] for r in reps)
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times), "higher_is_better": True,
@@ -320,7 +559,7 @@ def run_product_arm(args):
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches), "roofline": roofline, "roofline_this_workload": roof_small,
             "cg_large_mesh": cg_large, "cpu_baseline": cpu, "clocks": clocks.summary(),
-            "accuracy_vs_tight_fp64": accuracy,
+            "accuracy_vs_tight_fp64": accuracy, "batched": batched, "served": served,
             "detail": {"outer_iters": reps[-1]["outer_iters"], "cg_iters": reps[-1]["cg_iters"],
                        "step_seconds": times}}
     if rank == 0:
@@ -330,6 +569,33 @@ def run_product_arm(args):
         dist.destroy_process_group()
 
 
+def batched_probe(n, trips):
+    """A fixed slice of batched work for profilers: n resident config-4
+    instances, then `trips` graph trips; prints the time per trip."""
+    import cudaplasticity_b200 as cp
+    from cudaplasticity_b200 import workload
+
+    ctx = cp.Context(0)
+    insts = []
+    for i in range(n):
+        w = workload.instance(i)
+        inst = cp.Instance(ctx, w["mesh"], w["material"])
+        inst.set_loads(w["rp"], w["mask"], w["uv"])
+        insts.append(inst)
+    b = cp.Batch(ctx, max_instances=n)
+    for inst in insts:
+        b.add(inst, levels=1, **BATCH_KW)
+    b.run(max_trips=3)
+    t0 = time.perf_counter()
+    b.run(max_trips=trips)
+    dt = time.perf_counter() - t0
+    print(json.dumps({"batched_probe": n, "trips": trips, "ms_per_trip": 1e3 * dt / trips, "stats": b.stats()}))
+    b.close()
+    for inst in insts:
+        inst.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -337,7 +603,27 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU-baseline leg")
+    ap.add_argument("--skip-batched", action="store_true", help="omit the batched (config-4 stream) leg")
+    ap.add_argument("--skip-served", action="store_true", help="omit the served (config-5 stream) leg")
+    ap.add_argument("--batched-window", type=float, default=20.0, help="seconds counted in the saturation run")
+    ap.add_argument("--compare", type=int, metavar="N",
+                    help="like-for-like run only: the first N config-4 requests, plain FP64 one at a time vs batched")
+    ap.add_argument("--compare-max-outer", type=int, default=300)
+    ap.add_argument("--serve-rate", type=float, default=10.0, help="Poisson arrival rate of the served leg")
+    ap.add_argument("--serve-window", type=float, default=20.0, help="seconds of arrivals in the served leg")
+    ap.add_argument("--batched-probe", type=int, nargs=2, metavar=("N", "TRIPS"),
+                    help="profiling aid: N resident config-4 instances, TRIPS graph trips, then exit")
     args = ap.parse_args()
+    if args.batched_probe:
+        batched_probe(*args.batched_probe)
+        return
+    if args.compare:
+        import cudaplasticity_b200 as cp
+
+        ctx = cp.Context(0)
+        print(json.dumps({"compare": compare_leg(ctx, args.compare, max_outer=args.compare_max_outer)}), flush=True)
+        ctx.close()
+        return
     if args.impl == "reference":
         run_reference_arm(args)
     else:

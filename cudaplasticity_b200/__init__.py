@@ -221,8 +221,12 @@ class Loads:
 # ------------------------------------------------------------------- device --
 
 class Context:
+    """cp_context. Instances and batches made on it are closed with it
+    (batches first), so no handle outlives its context."""
+
     def __init__(self, device=0):
         self._h = C.c_p()
+        self._deps = weakref.WeakSet()
         st = C.lib().cp_context_create(device, ctypes.byref(self._h))
         if st != C.CP_OK:
             self._h = None
@@ -230,6 +234,13 @@ class Context:
 
     def close(self):
         if getattr(self, "_h", None):
+            deps = list(getattr(self, "_deps", ()))
+            for d in deps:
+                if isinstance(d, Batch):
+                    d.close()
+            for d in deps:
+                if not isinstance(d, Batch):
+                    d.close()
             C.lib().cp_context_destroy(self._h)
             self._h = None
 
@@ -275,6 +286,7 @@ class Instance:
         self.count3 = v.count3
         self.count4 = v.count4
         ctx.check(C.lib().cp_instance_create(ctx._h, ctypes.byref(v), ctypes.byref(mat), ctypes.byref(self._h)))
+        ctx._deps.add(self)
         del keep
 
     def close(self):
@@ -380,6 +392,7 @@ class Batch:
         self.opts = o
         self._h = C.c_p()
         ctx.check(C.lib().cp_batch_create(ctx._h, ctypes.byref(o), ctypes.byref(self._h)))
+        ctx._deps.add(self)
         self._slots = {}
 
     def close(self):

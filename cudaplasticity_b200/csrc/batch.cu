@@ -7,23 +7,22 @@
 // recurrences inside FP64 defect correction) as its own state machine on the
 // device:
 //
-//   LEVEL -> ASM -> INIT -> (P -> U [-> RR])* -> UPD -> RELAX -> ASM ...
+//   LEVEL -> ASM -> RES -> W -> ITER* [-> RES -> W -> ITER*] -> UPD -> RELAX -> ASM ...
 //                           (level converged) -> LEVEL / PLASTIC -> DONE
 //
 // The linear solve is one preconditioned CG on the FP32 values with FP32
-// recurrences ("reliable updates"): INIT computes the residual b - K64 x in
-// FP64 once; whenever the recursive FP32 residual has dropped by inner_tol
-// since the last replacement, or meets the solve's tolerance, RR replaces it
-// by the FP64 residual b - K64 x (x itself accumulates in FP64) and the
-// search direction carries on, so the Krylov space is kept; the solve ends
-// when the FP64 residual meets the tolerance.
+// recurrences ("reliable updates"): RES computes the residual b - K64 x in
+// FP64 at the start; whenever the recursive FP32 residual has dropped by
+// inner_tol since the last replacement, or meets the solve's tolerance, RES
+// replaces it by the FP64 residual of the FP64 solution and the search
+// direction carries on, so the Krylov space is kept; the solve ends when the
+// FP64 residual meets the tolerance. One CG iteration is one launch (the
+// Chronopoulos-Gear form, see the CG section).
 //
 // The instances' nodes and elements are cut into tiles; one work list holds
 // every (instance, tile) pair. Three persistent kernels walk that list, each
 // acting only on the tiles whose instance is in one of its phases:
-//   k_batch_cg    INIT (FP64 residual), P (SpMV + direction),
-//                 U (axpy / residual / preconditioner), RR (FP64 residual
-//                 replacement)
+//   k_batch_cg    RES (FP64 residual), W (w = K u), ITER (one CG iteration)
 //   k_batch_asm   ASM (FP64 + FP32 values of K, node gather, no atomics)
 //   k_batch_elem  LEVEL, UPD (strain / stress / secant / exit norm),
 //                 RELAX (Aitken), PLASTIC
@@ -40,6 +39,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -60,10 +60,9 @@ enum : int {
     PH_FREE = 0,
     PH_LEVEL,
     PH_ASM,
-    PH_INIT,
-    PH_P,
-    PH_U,
-    PH_RR,
+    PH_RES,
+    PH_W,
+    PH_ITER,
     PH_UPD,
     PH_RELAX,
     PH_PLASTIC,
@@ -87,11 +86,11 @@ struct BDesc {
     const double2* b_full;
     const double2* u_full;
     const uchar2* mask;
-    float2 *r, *z0, *z1, *q, *s;
+    float2 *rA, *rB, *wA, *wB, *kA, *kB, *p, *u;  // FP32 CG vectors (A/B: by parity)
     float4* minv;
     ElemState st;
     MaterialDev mat;
-    double* part;  // 4 per slice / group
+    double* part;  // 8 per slice / group
     double cg_tol, outer_tol, inner_tol;
     long long max_cg;
     int max_outer, levels, aitken, adaptive, precond;
@@ -100,11 +99,11 @@ struct BDesc {
 // Mutable state of one instance.
 struct BState {
     int phase, status, level, levels_done;
-    int outer_it, outer_total, parity, pad0;
+    int outer_it, outer_total, parity, res_kind;  // res_kind: 0 first residual of a solve, 1 replacement
     unsigned int ticket;
     int pad;
     long long iter, lin_iters, cg_total, fp64_spmv;
-    double rr, rho, rho_prev, alpha, beta, rr_ref, eps2_inner, bb, res64;
+    double rr, gamma, alpha, beta, rr_ref, eps2_inner, bb, res64;
     double eps, rel_err, w_prev, omega, cg_rel_res;
     unsigned long long t_first, t_done;  // %globaltimer, ns
 };
@@ -118,6 +117,7 @@ struct BCtl {
     long long trips, max_trips;
     int pop[PH_COUNT];  // instances per phase
     const volatile int* stop;  // host-mapped interrupt flag
+    int go;                    // condition of the last trip (direct launches)
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -155,14 +155,17 @@ __device__ __forceinline__ bool arrive(BState* S, int ntiles, int* sh_flag) {
     return last;
 }
 
-// Sums of the first K of the 4 partials per unit over units [0, n), fixed
+// Sums of the first K of the 8 partials per unit over units [0, n), fixed
 // assignment (thread t takes units t, t + 128, ...) and a fixed tree.
 // Results valid in thread 0.
+constexpr int kPart = 8;
 template <int K>
 __device__ __forceinline__ void reduce_parts(const double* part, int n, double* out, double* sh) {
-    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    double a[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) a[k] = 0.0;
     for (int i = threadIdx.x; i < n; i += kThreads) {
-        const volatile double* p = part + 4 * (size_t)i;
+        const volatile double* p = part + kPart * (size_t)i;
 #pragma unroll
         for (int k = 0; k < K; ++k) a[k] += p[k];
     }
@@ -210,17 +213,39 @@ __device__ __forceinline__ void decide(const BDesc& d, BState* S, BCtl* c) {
 }
 
 // ------------------------------------------------------------ CG phases --
+//
+// The linear solve is preconditioned CG in the Chronopoulos-Gear form: the
+// same iterates as the standard recurrence in exact arithmetic, with both
+// inner products of an iteration taken together, so one iteration is one
+// launch with one reduction. With M the 2x2 block-Jacobi inverse (identity
+// without preconditioning), u = M r, w = K u, p the direction, kp = K p:
+//   p = u + beta p, kp = w + beta kp, x += alpha p, r -= m.alpha kp,
+//   u = M r, w = K u, gamma = (r, u), delta = (w, u),
+//   beta' = gamma' / gamma, alpha' = gamma' / (K p', p') with
+//   (K p', p') = delta' + beta' ((w', p) + (kp, u')) + beta'^2 (kp, p).
+// K u needs the new u of the neighbours, which each thread recomputes from
+// the neighbours' old r, w, kp (double-buffered by the instance's parity),
+// so no second pass is needed. RES (FP64 residual of the FP64 solution, at
+// the start and at every replacement) and W (w = K u after it) bracket the
+// iterations; r, u, w, kp, p are FP32, x and every sum are FP64.
 
-// INIT: r = m.(b - K64 x) in FP64, stored in FP32; z = 0; block-Jacobi
-// inverse and s = M^-1 r. Sums (r32, r32), (r64, r64), (b, b), (r32, s).
-__device__ void tile_init(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
+__device__ __forceinline__ float2 mvec(const float4& m, float2 v) {
+    return make_float2(m.x * v.x + m.y * v.y, m.z * v.x + m.w * v.y);
+}
+
+// RES: r = m.(b - K64 x) in FP64 (stored in FP32), u = M r; at the start of
+// a solve also the block-Jacobi inverse, p = kp = 0. Sums (r32, r32),
+// (r64, r64), (b, b).
+__device__ void tile_res(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
-    const int pre = d.precond;
+    const int pre = d.precond, first = S->res_kind == 0;
+    const int par = S->parity;
+    float2* __restrict__ r = par ? d.rB : d.rA;
     for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
         const int n = 32 * sl + lane;
         const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
-        double s_rr = 0.0, s_r64 = 0.0, s_bb = 0.0, s_rho = 0.0;
+        double s_rr = 0.0, s_r64 = 0.0, s_bb = 0.0;
         if (n < d.m.n_nodes) {
             double k0 = 0.0, k1 = 0.0;
             for (int k = 0; k < wd; ++k) {
@@ -236,110 +261,45 @@ __device__ void tile_init(const BDesc& d, BState* S, BCtl* c, int4 tl, double* s
             const uchar2 m = d.mask[n];
             const double r0 = m.x ? bb.x - k0 : 0.0, r1 = m.y ? bb.y - k1 : 0.0;
             const float2 rt = make_float2((float)r0, (float)r1);
-            d.r[n] = rt;
-            d.z0[n] = make_float2(0.f, 0.f);
-            s_rr = (double)rt.x * (double)rt.x + (double)rt.y * (double)rt.y;
+            r[n] = rt;
+            float2 u = rt;
             if (pre) {
-                const double2* dp = reinterpret_cast<const double2*>(d.val64 + 4 * ((long long)base + lane));
-                const double2 dlo = __ldg(dp), dhi = __ldg(dp + 1);
-                double i00 = 0, i01 = 0, i10 = 0, i11 = 0;
-                if (m.x && m.y) {
-                    const double det = dlo.x * dhi.y - dlo.y * dhi.x;
-                    i00 = dhi.y / det; i01 = -dlo.y / det; i10 = -dhi.x / det; i11 = dlo.x / det;
-                } else if (m.x) {
-                    i00 = 1.0 / dlo.x;
-                } else if (m.y) {
-                    i11 = 1.0 / dhi.y;
+                float4 mi;
+                if (first) {
+                    // inverse of the node's 2x2 diagonal block, restricted to its free DOFs
+                    const double2* dp = reinterpret_cast<const double2*>(d.val64 + 4 * ((long long)base + lane));
+                    const double2 dlo = __ldg(dp), dhi = __ldg(dp + 1);
+                    double i00 = 0, i01 = 0, i10 = 0, i11 = 0;
+                    if (m.x && m.y) {
+                        const double det = dlo.x * dhi.y - dlo.y * dhi.x;
+                        i00 = dhi.y / det; i01 = -dlo.y / det; i10 = -dhi.x / det; i11 = dlo.x / det;
+                    } else if (m.x) {
+                        i00 = 1.0 / dlo.x;
+                    } else if (m.y) {
+                        i11 = 1.0 / dhi.y;
+                    }
+                    mi = make_float4((float)i00, (float)i01, (float)i10, (float)i11);
+                    d.minv[n] = mi;
+                } else {
+                    mi = d.minv[n];
                 }
-                const float4 mi = make_float4((float)i00, (float)i01, (float)i10, (float)i11);
-                d.minv[n] = mi;
-                const float2 sv = make_float2(mi.x * rt.x + mi.y * rt.y, mi.z * rt.x + mi.w * rt.y);
-                d.s[n] = sv;
-                s_rho = (double)rt.x * (double)sv.x + (double)rt.y * (double)sv.y;
+                u = mvec(mi, rt);
             }
+            d.u[n] = u;
+            if (first) {
+                d.p[n] = make_float2(0.f, 0.f);
+                (par ? d.kB : d.kA)[n] = make_float2(0.f, 0.f);
+            }
+            s_rr = (double)rt.x * (double)rt.x + (double)rt.y * (double)rt.y;
             s_r64 = r0 * r0 + r1 * r1;
             s_bb = bb.x * bb.x + bb.y * bb.y;
         }
         s_rr = warp_sum(s_rr);
         s_r64 = warp_sum(s_r64);
         s_bb = warp_sum(s_bb);
-        s_rho = warp_sum(s_rho);
         if (lane == 0) {
-            double* p = d.part + 4 * (size_t)sl;
-            p[0] = s_rr; p[1] = s_r64; p[2] = s_bb; p[3] = s_rho;
-        }
-    }
-    if (!arrive(S, tl.w, shf)) return;
-    double t[4];
-    reduce_parts<4>(d.part, d.n_slices, t, sh);
-    if (threadIdx.x == 0) {
-        const double rr = t[0], res64 = t[1], bb = t[2];
-        S->ticket = 0;
-        S->fp64_spmv += 1;
-        S->bb = bb;
-        S->res64 = res64;
-        S->cg_rel_res = bb > 0.0 ? sqrt(res64 / bb) : 0.0;
-        if (!(rr == rr) || !(bb == bb) || !(res64 == res64)) {
-            finish(S, c, CP_ERR_BREAKDOWN);
-        } else if (res64 <= S->eps * S->eps * bb || rr == 0.0 || S->lin_iters >= d.max_cg) {
-            set_phase(S, c, PH_UPD);  // the linear solve meets its tolerance (or its cap)
-        } else {
-            S->rr = rr;
-            S->rr_ref = rr;
-            S->rho = pre ? t[3] : rr;
-            S->eps2_inner = d.inner_tol * d.inner_tol;
-            S->iter = 0;
-            S->alpha = 0.0;
-            S->beta = 0.0;
-            S->parity = 0;
-            set_phase(S, c, PH_P);
-        }
-    }
-}
-
-// RR: the recursive residual is replaced by the FP64 residual of the FP64
-// solution, r = m.(b - K64 x) (stored in FP32), s = M^-1 r with the
-// preconditioner of INIT; the search direction is kept and beta is recomputed
-// from the replaced residual. Sums (r32, r32), (r64, r64), -, (r32, s).
-__device__ void tile_rr(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
-    const int pre = d.precond;
-    for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
-        const int n = 32 * sl + lane;
-        const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
-        double s_rr = 0.0, s_r64 = 0.0, s_rho = 0.0;
-        if (n < d.m.n_nodes) {
-            double k0 = 0.0, k1 = 0.0;
-            for (int k = 0; k < wd; ++k) {
-                const long long bi = base + 32LL * k + lane;
-                const int col = __ldg(d.scol + bi);
-                const double2* vp = reinterpret_cast<const double2*>(d.val64 + 4 * bi);
-                const double2 lo = __ldg(vp), hi = __ldg(vp + 1);
-                const double2 xc = d.x[col];
-                k0 += lo.x * xc.x + lo.y * xc.y;
-                k1 += hi.x * xc.x + hi.y * xc.y;
-            }
-            const double2 bb = d.b[n];
-            const uchar2 m = d.mask[n];
-            const double r0 = m.x ? bb.x - k0 : 0.0, r1 = m.y ? bb.y - k1 : 0.0;
-            const float2 rt = make_float2((float)r0, (float)r1);
-            d.r[n] = rt;
-            s_rr = (double)rt.x * (double)rt.x + (double)rt.y * (double)rt.y;
-            if (pre) {
-                const float4 mi = d.minv[n];
-                const float2 sv = make_float2(mi.x * rt.x + mi.y * rt.y, mi.z * rt.x + mi.w * rt.y);
-                d.s[n] = sv;
-                s_rho = (double)rt.x * (double)sv.x + (double)rt.y * (double)sv.y;
-            }
-            s_r64 = r0 * r0 + r1 * r1;
-        }
-        s_rr = warp_sum(s_rr);
-        s_r64 = warp_sum(s_r64);
-        s_rho = warp_sum(s_rho);
-        if (lane == 0) {
-            double* p = d.part + 4 * (size_t)sl;
-            p[0] = s_rr; p[1] = s_r64; p[2] = 0.0; p[3] = s_rho;
+            double* p = d.part + kPart * (size_t)sl;
+            p[0] = s_rr; p[1] = s_r64; p[2] = s_bb; p[3] = 0.0;
         }
     }
     if (!arrive(S, tl.w, shf)) return;
@@ -349,37 +309,37 @@ __device__ void tile_rr(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh,
         const double rr = t[0], res64 = t[1];
         S->ticket = 0;
         S->fp64_spmv += 1;
+        if (first) S->bb = t[2];
+        const double bb = S->bb;
         S->res64 = res64;
-        S->cg_rel_res = S->bb > 0.0 ? sqrt(res64 / S->bb) : 0.0;
-        if (!(rr == rr) || !(res64 == res64)) {
+        S->cg_rel_res = bb > 0.0 ? sqrt(res64 / bb) : 0.0;
+        if (!(rr == rr) || !(bb == bb) || !(res64 == res64)) {
             finish(S, c, CP_ERR_BREAKDOWN);
-        } else if (res64 <= S->eps * S->eps * S->bb || rr == 0.0 || S->lin_iters >= d.max_cg) {
-            set_phase(S, c, PH_UPD);
+        } else if (res64 <= S->eps * S->eps * bb || rr == 0.0 || S->lin_iters >= d.max_cg) {
+            set_phase(S, c, PH_UPD);  // the linear solve meets its tolerance (or its cap)
         } else {
-            const double rho_new = pre ? t[3] : rr;
-            S->beta = rho_new / S->rho_prev;
-            S->rho = rho_new;
             S->rr = rr;
             S->rr_ref = rr;
-            set_phase(S, c, PH_P);
+            set_phase(S, c, PH_W);
         }
     }
 }
 
-// P: z' = s + beta z (own node), q = K32 z' gathered from the neighbours,
-// (q, z').
-__device__ void tile_p(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
+// W: w = K32 u (u of RES, read from the neighbours); gamma = (r, u),
+// delta = (w, u) and, for the direction that carries on after a
+// replacement, (w, p), (kp, u), (kp, p); the step scalars of the next
+// iteration (see tile_iter for the expansion).
+__device__ void tile_w(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
     const int par = S->parity;
-    const float beta = (float)S->beta;
-    const float2* __restrict__ zo = par ? d.z1 : d.z0;
-    float2* __restrict__ zn = par ? d.z0 : d.z1;
-    const float2* __restrict__ rs = d.precond ? d.s : d.r;
+    const float2* __restrict__ r = par ? d.rB : d.rA;
+    const float2* __restrict__ kv = par ? d.kB : d.kA;
+    float2* __restrict__ wv = par ? d.wB : d.wA;
     for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
         const int n = 32 * sl + lane;
         const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
-        double dot = 0.0;
+        double s_g = 0.0, s_d = 0.0, s_wp = 0.0, s_ku = 0.0, s_kp = 0.0;
         if (n < d.m.n_nodes) {
             float k0 = 0.f, k1 = 0.f;
 #pragma unroll 3
@@ -387,92 +347,159 @@ __device__ void tile_p(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, 
                 const long long bi = base + 32LL * k + lane;
                 const int col = __ldg(d.scol + bi);
                 const float4 v = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
-                const float2 rc = rs[col], zc = zo[col];
-                const float wx = rc.x + beta * zc.x, wy = rc.y + beta * zc.y;
-                k0 += v.x * wx + v.y * wy;
-                k1 += v.z * wx + v.w * wy;
+                const float2 uc = d.u[col];
+                k0 += v.x * uc.x + v.y * uc.y;
+                k1 += v.z * uc.x + v.w * uc.y;
             }
-            const float2 rn = rs[n], zon = zo[n];
-            const float2 zz = make_float2(rn.x + beta * zon.x, rn.y + beta * zon.y);
-            zn[n] = zz;
-            d.q[n] = make_float2(k0, k1);
-            dot = (double)k0 * (double)zz.x + (double)k1 * (double)zz.y;
+            wv[n] = make_float2(k0, k1);
+            const float2 un = d.u[n], rn = r[n], pn = d.p[n], kn = kv[n];
+            s_g = (double)rn.x * (double)un.x + (double)rn.y * (double)un.y;
+            s_d = (double)k0 * (double)un.x + (double)k1 * (double)un.y;
+            s_wp = (double)k0 * (double)pn.x + (double)k1 * (double)pn.y;
+            s_ku = (double)kn.x * (double)un.x + (double)kn.y * (double)un.y;
+            s_kp = (double)kn.x * (double)pn.x + (double)kn.y * (double)pn.y;
         }
-        dot = warp_sum(dot);
-        if (lane == 0) d.part[4 * (size_t)sl] = dot;
+        s_g = warp_sum(s_g);
+        s_d = warp_sum(s_d);
+        s_wp = warp_sum(s_wp);
+        s_ku = warp_sum(s_ku);
+        s_kp = warp_sum(s_kp);
+        if (lane == 0) {
+            double* p = d.part + kPart * (size_t)sl;
+            p[0] = s_g; p[1] = s_d; p[2] = 0.0; p[3] = s_wp; p[4] = s_ku; p[5] = s_kp;
+        }
     }
     if (!arrive(S, tl.w, shf)) return;
-    double t[4];
-    reduce_parts<1>(d.part, d.n_slices, t, sh);
+    double t[6];
+    reduce_parts<6>(d.part, d.n_slices, t, sh);
     if (threadIdx.x == 0) {
-        const double pAz = t[0];
+        const double g = t[0];
         S->ticket = 0;
-        const double alpha = S->rho / pAz;
-        if (!(pAz > 0.0) || !(alpha == alpha)) {
+        // the first solve starts with p = kp = 0; after a replacement the
+        // direction carries on with beta from the replaced residual
+        const double beta = S->res_kind != 0 ? g / S->gamma : 0.0;
+        const double den = t[1] + beta * (t[3] + t[4]) + beta * beta * t[5];
+        const double alpha = g / den;
+        if (!(den > 0.0) || !(g > 0.0) || !(alpha == alpha)) {
             finish(S, c, CP_ERR_BREAKDOWN);
         } else {
+            S->gamma = g;
             S->alpha = alpha;
-            set_phase(S, c, PH_U);
+            S->beta = beta;
+            set_phase(S, c, PH_ITER);
         }
     }
 }
 
-// U: x += alpha z' (FP64), r -= m.alpha q, s = M^-1 r; (r, r), (r, s).
-__device__ void tile_u(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
+// ITER: one CG iteration (see the section comment).
+__device__ void tile_iter(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
-    const float2* __restrict__ zn = S->parity ? d.z0 : d.z1;
+    const int par = S->parity, pre = d.precond;
+    const float2* __restrict__ ro = par ? d.rB : d.rA;
+    const float2* __restrict__ wo = par ? d.wB : d.wA;
+    const float2* __restrict__ ko = par ? d.kB : d.kA;
+    float2* __restrict__ rn_ = par ? d.rA : d.rB;
+    float2* __restrict__ wn_ = par ? d.wA : d.wB;
+    float2* __restrict__ kn_ = par ? d.kA : d.kB;
     const double alpha = S->alpha;
-    const float alpha_t = (float)alpha;
-    const int pre = d.precond;
+    const float a = (float)alpha, bt = (float)S->beta;
     for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
         const int n = 32 * sl + lane;
-        double s_rr = 0.0, s_rs = 0.0;
+        const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
+        double s_g = 0.0, s_d = 0.0, s_rr = 0.0, s_wp = 0.0, s_ku = 0.0, s_kp = 0.0;
         if (n < d.m.n_nodes) {
-            const float2 z = zn[n], q = d.q[n];
+            // own node
+            const float2 un = d.u[n], pn = d.p[n], wn = wo[n], kn = ko[n];
             const uchar2 m = d.mask[n];
+            const float2 p = make_float2(un.x + bt * pn.x, un.y + bt * pn.y);
+            const float2 kp = make_float2(wn.x + bt * kn.x, wn.y + bt * kn.y);
             double2 x = d.x[n];
-            x.x += alpha * (double)z.x;
-            x.y += alpha * (double)z.y;
-            d.x[n] = x;
-            float2 r = d.r[n];
-            if (m.x) r.x -= alpha_t * q.x;
-            if (m.y) r.y -= alpha_t * q.y;
-            d.r[n] = r;
-            s_rr = (double)r.x * (double)r.x + (double)r.y * (double)r.y;
-            if (pre) {
-                const float4 mi = d.minv[n];
-                const float2 sv = make_float2(mi.x * r.x + mi.y * r.y, mi.z * r.x + mi.w * r.y);
-                d.s[n] = sv;
-                s_rs = (double)r.x * (double)sv.x + (double)r.y * (double)sv.y;
+            x.x += alpha * (double)p.x;
+            x.y += alpha * (double)p.y;
+            float2 r = ro[n];
+            if (m.x) r.x -= a * kp.x;
+            if (m.y) r.y -= a * kp.y;
+            const float2 u = pre ? mvec(d.minv[n], r) : r;
+            // w = K u with the neighbours' new u recomputed from their old values
+            float k0 = 0.f, k1 = 0.f;
+#pragma unroll 3
+            for (int k = 0; k < wd; ++k) {
+                const long long bi = base + 32LL * k + lane;
+                const int col = __ldg(d.scol + bi);
+                const float4 v = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
+                float2 uc;
+                if (k == 0) {
+                    uc = u;  // block 0 is the node itself
+                } else {
+                    const float2 rc = ro[col], wc = wo[col], kc = ko[col];
+                    float2 rr2 = make_float2(rc.x - a * (wc.x + bt * kc.x), rc.y - a * (wc.y + bt * kc.y));
+                    if (pre) {
+                        uc = mvec(d.minv[col], rr2);  // zero rows and columns at prescribed DOFs
+                    } else {
+                        const uchar2 mc = d.mask[col];
+                        uc = make_float2(mc.x ? rr2.x : 0.f, mc.y ? rr2.y : 0.f);
+                    }
+                }
+                k0 += v.x * uc.x + v.y * uc.y;
+                k1 += v.z * uc.x + v.w * uc.y;
             }
+            d.p[n] = p;
+            kn_[n] = kp;
+            d.x[n] = x;
+            rn_[n] = r;
+            d.u[n] = u;
+            wn_[n] = make_float2(k0, k1);
+            s_g = (double)r.x * (double)u.x + (double)r.y * (double)u.y;
+            s_d = (double)k0 * (double)u.x + (double)k1 * (double)u.y;
+            s_rr = (double)r.x * (double)r.x + (double)r.y * (double)r.y;
+            s_wp = (double)k0 * (double)p.x + (double)k1 * (double)p.y;
+            s_ku = (double)kp.x * (double)u.x + (double)kp.y * (double)u.y;
+            s_kp = (double)kp.x * (double)p.x + (double)kp.y * (double)p.y;
         }
+        s_g = warp_sum(s_g);
+        s_d = warp_sum(s_d);
         s_rr = warp_sum(s_rr);
-        s_rs = warp_sum(s_rs);
+        s_wp = warp_sum(s_wp);
+        s_ku = warp_sum(s_ku);
+        s_kp = warp_sum(s_kp);
         if (lane == 0) {
-            d.part[4 * (size_t)sl] = s_rr;
-            d.part[4 * (size_t)sl + 1] = s_rs;
+            double* p = d.part + kPart * (size_t)sl;
+            p[0] = s_g; p[1] = s_d; p[2] = s_rr; p[3] = s_wp; p[4] = s_ku; p[5] = s_kp;
         }
     }
     if (!arrive(S, tl.w, shf)) return;
-    double t[4];
-    reduce_parts<2>(d.part, d.n_slices, t, sh);
+    double t[6];
+    reduce_parts<6>(d.part, d.n_slices, t, sh);
     if (threadIdx.x == 0) {
-        const double rn = t[0];
-        const double rho_new = pre ? t[1] : rn;
+        const double g = t[0], rn = t[2];
         S->ticket = 0;
-        S->rho_prev = S->rho;
-        S->beta = rho_new / S->rho;
-        S->rho = rho_new;
-        S->rr = rn;
+        S->parity ^= 1;
         S->iter += 1;
         S->lin_iters += 1;
         S->cg_total += 1;
-        S->parity ^= 1;
-        if (!(rn == rn)) finish(S, c, CP_ERR_BREAKDOWN);
-        else if (rn <= S->eps * S->eps * S->bb || rn <= S->eps2_inner * S->rr_ref) set_phase(S, c, PH_RR);
-        else if (S->lin_iters >= d.max_cg) set_phase(S, c, PH_UPD);
-        else set_phase(S, c, PH_P);
+        S->rr = rn;
+        // (K p', p') of the next direction p' = u + beta p, K p' = w + beta kp,
+        // expanded from this iteration's vectors: the step is computed as in
+        // standard CG, with no recurrence identity that a residual
+        // replacement or FP32 rounding would break
+        const double beta = g / S->gamma;
+        const double den = t[1] + beta * (t[3] + t[4]) + beta * beta * t[5];
+        if (!(rn == rn) || !(g == g)) {
+            finish(S, c, CP_ERR_BREAKDOWN);
+        } else if (rn <= S->eps * S->eps * S->bb || rn <= S->eps2_inner * S->rr_ref || !(den > 0.0) || !(g > 0.0)) {
+            // converged in the FP32 recurrence (or its step degenerated): check
+            // against the FP64 residual, which restarts the scalars
+            S->res_kind = 1;
+            set_phase(S, c, PH_RES);
+        } else if (S->lin_iters >= d.max_cg) {
+            set_phase(S, c, PH_UPD);
+        } else {
+            S->beta = beta;
+            S->alpha = g / den;
+            S->gamma = g;
+            set_phase(S, c, PH_ITER);
+        }
     }
 }
 
@@ -482,26 +509,25 @@ __global__ void __launch_bounds__(kThreads) k_batch_cg(const BDesc* __restrict__
     __shared__ int shf, shp;
     {
         const volatile int* pop = c->pop;
-        if (pop[PH_INIT] + pop[PH_P] + pop[PH_U] + pop[PH_RR] == 0) return;
+        if (pop[PH_RES] + pop[PH_W] + pop[PH_ITER] == 0) return;
     }
     const int nt = c->n_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int4 tl = tiles[t];
         BState* S = SS + tl.x;
         const int ph = tile_phase(S, &shp);
-        if (ph == PH_P) tile_p(D[tl.x], S, c, tl, sh, &shf);
-        else if (ph == PH_U) tile_u(D[tl.x], S, c, tl, sh, &shf);
-        else if (ph == PH_RR) tile_rr(D[tl.x], S, c, tl, sh, &shf);
-        else if (ph == PH_INIT) tile_init(D[tl.x], S, c, tl, sh, &shf);
+        if (ph == PH_ITER) tile_iter(D[tl.x], S, c, tl, sh, &shf);
+        else if (ph == PH_W) tile_w(D[tl.x], S, c, tl, sh, &shf);
+        else if (ph == PH_RES) tile_res(D[tl.x], S, c, tl, sh, &shf);
     }
 }
 
-// The SpMV of the P phase for the autotuner: the same loads and arithmetic,
-// with the results written to a sink of the batch (one value per thread)
-// instead of the instance's z' and q, so that the instances' state is left
-// untouched whatever phase they are in.
+// The SpMV of an iteration for the autotuner: the same loads and arithmetic
+// as ITER's neighbour loop, with the results written to a sink of the batch
+// (one value per thread) instead of the instance's vectors, so that the
+// instances' state is left untouched whatever phase they are in.
 __global__ void __launch_bounds__(kThreads) k_batch_probe(const BDesc* __restrict__ D, const BState* SS,
-                                                          const int4* __restrict__ tiles, int nt, float beta,
+                                                          const int4* __restrict__ tiles, int nt, float a, float bt,
                                                           float2* sink) {
     float2 acc = make_float2(0.f, 0.f);
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
@@ -509,9 +535,10 @@ __global__ void __launch_bounds__(kThreads) k_batch_probe(const BDesc* __restric
         const BDesc& d = D[tl.x];
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
         const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
-        const int par = SS[tl.x].parity;
-        const float2* __restrict__ zo = par ? d.z1 : d.z0;
-        const float2* __restrict__ rs = d.precond ? d.s : d.r;
+        const int par = SS[tl.x].parity, pre = d.precond;
+        const float2* __restrict__ ro = par ? d.rB : d.rA;
+        const float2* __restrict__ wo = par ? d.wB : d.wA;
+        const float2* __restrict__ ko = par ? d.kB : d.kA;
         for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
             const int n = 32 * sl + lane;
             const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
@@ -522,10 +549,11 @@ __global__ void __launch_bounds__(kThreads) k_batch_probe(const BDesc* __restric
                     const long long bi = base + 32LL * k + lane;
                     const int col = __ldg(d.scol + bi);
                     const float4 v = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
-                    const float2 rc = rs[col], zc = zo[col];
-                    const float wx = rc.x + beta * zc.x, wy = rc.y + beta * zc.y;
-                    k0 += v.x * wx + v.y * wy;
-                    k1 += v.z * wx + v.w * wy;
+                    const float2 rc = ro[col], wc = wo[col], kc = ko[col];
+                    const float2 rr2 = make_float2(rc.x - a * (wc.x + bt * kc.x), rc.y - a * (wc.y + bt * kc.y));
+                    const float2 uc = pre ? mvec(d.minv[col], rr2) : rr2;
+                    k0 += v.x * uc.x + v.y * uc.y;
+                    k1 += v.z * uc.x + v.w * uc.y;
                 }
                 acc.x += k0;
                 acc.y += k1;
@@ -585,7 +613,9 @@ __global__ void __launch_bounds__(kThreads) k_batch_asm(const BDesc* __restrict_
         }
         if (arrive(S, tl.w, &shf) && threadIdx.x == 0) {
             S->ticket = 0;
-            set_phase(S, c, PH_INIT);
+            S->res_kind = 0;
+            S->eps2_inner = d.inner_tol * d.inner_tol;
+            set_phase(S, c, PH_RES);
         }
     }
 }
@@ -653,7 +683,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_elem(const BDesc* __restrict
                 s_an = warp_sum(s_an);
                 s_ad = warp_sum(s_ad);
                 if (lane == 0) {
-                    double* p = d.part + 4 * (size_t)g;
+                    double* p = d.part + kPart * (size_t)g;
                     p[0] = s_num; p[1] = s_den; p[2] = s_an; p[3] = s_ad;
                 }
             }
@@ -705,13 +735,22 @@ __global__ void __launch_bounds__(kThreads) k_batch_elem(const BDesc* __restrict
     }
 }
 
-__global__ void k_batch_cond(BCtl* c, cudaGraphConditionalHandle h) {
+__device__ __forceinline__ bool trip_condition(BCtl* c) {
     c->trips += 1;
     bool go = c->active > 0 && (c->max_trips <= 0 || c->trips < c->max_trips) &&
               !(c->exit_on_done > 0 && c->done >= c->exit_on_done);
     if (go && c->stop && *c->stop) go = false;
-    cudaGraphSetConditional(h, go ? 1u : 0u);
+    c->go = go ? 1 : 0;
+    return go;
 }
+
+__global__ void k_batch_cond(BCtl* c, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, trip_condition(c) ? 1u : 0u);
+}
+
+// The same condition for runs launched kernel by kernel (profilers cannot
+// see kernel nodes of a graph with a conditional node).
+__global__ void k_batch_cond_direct(BCtl* c) { trip_condition(c); }
 
 int bucket_of(int n_slices) {
     int b = 0;
@@ -748,6 +787,7 @@ struct cp_batch {
     float2* d_sink = nullptr;  // autotuner probe output
     size_t asm_smem = 0;
     bool running = false;
+    bool use_graph = true;  // false (CUPLAST_NO_GRAPH=1): trips launched kernel by kernel, for profilers
     int last_tiles = 0;
     long long trips = 0, launches = 0, runs = 0;
 };
@@ -843,6 +883,30 @@ void interleave_tiles(cp_batch* b, int n) {
     std::memcpy(b->h_tiles, out.data(), sizeof(int4) * (size_t)n);
 }
 
+// One trip: element phases, assembly, CG launches.
+void launch_body(cp_batch* b, cudaStream_t s) {
+    for (int k = 0; k < b->o.elem_per_trip; ++k)
+        k_batch_elem<<<b->grid_elem, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
+    k_batch_asm<<<b->grid_asm, kThreads, b->asm_smem, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl,
+                                                           b->o.max_width);
+    for (int k = 0; k < b->o.cg_per_trip; ++k)
+        k_batch_cg<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
+}
+
+// Direct launches: trip after trip with the condition read back each time.
+void run_direct(cp_batch* b) {
+    cudaStream_t s = b->ctx->stream;
+    for (;;) {
+        launch_body(b, s);
+        k_batch_cond_direct<<<1, 1, 0, s>>>(b->d_ctl);
+        CP_CUDA(cudaGetLastError());
+        int go = 0;
+        CP_CUDA(cudaMemcpyAsync(&go, &b->d_ctl->go, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CP_CUDA(cudaStreamSynchronize(s));
+        if (!go) return;
+    }
+}
+
 void build_graph(cp_batch* b) {
     cudaStream_t s = b->ctx->stream;
     cudaGraph_t g;
@@ -858,12 +922,7 @@ void build_graph(cp_batch* b) {
     CP_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &p));
     cudaGraph_t body = p.conditional.phGraph_out[0];
     CP_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    for (int k = 0; k < b->o.elem_per_trip; ++k)
-        k_batch_elem<<<b->grid_elem, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
-    k_batch_asm<<<b->grid_asm, kThreads, b->asm_smem, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl,
-                                                           b->o.max_width);
-    for (int k = 0; k < b->o.cg_per_trip; ++k)
-        k_batch_cg<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
+    launch_body(b, s);
     k_batch_cond<<<1, 1, 0, s>>>(b->d_ctl, h);
     cudaGraph_t captured = nullptr;
     cudaError_t e = cudaStreamEndCapture(s, &captured);
@@ -918,6 +977,7 @@ CP_API int cp_batch_create(cp_context* ctx, const cp_batch_opts* opts, cp_batch*
     b->ctx = ctx;
     b->o = o;
     b->cap = o.max_instances;
+    if (const char* g = std::getenv("CUPLAST_NO_GRAPH")) b->use_graph = !(g[0] == '1');
     for (int k = 0; k < kBuckets; ++k) b->tile_slices[k] = default_tile(k);
     int rc = bguard(b, [&] {
         CP_CUDA(cudaSetDevice(ctx->device));
@@ -1016,15 +1076,17 @@ CP_API int cp_batch_add(cp_batch* b, cp_instance* I, const cp_solve_opts* opts, 
         d.b_full = I->b_full;
         d.u_full = I->u_full;
         d.mask = I->mask;
-        d.r = I->r32;
-        d.z0 = I->z32a;
-        d.z1 = I->z32b;
-        d.q = I->q32;
-        d.s = I->s32;
+        {
+            const size_t nn = (size_t)I->n_nodes;
+            float2* v = I->alloc<float2>(8 * nn);
+            CP_CUDA(cudaMemsetAsync(v, 0, sizeof(float2) * 8 * nn, I->s()));
+            d.rA = v; d.rB = v + nn; d.wA = v + 2 * nn; d.wB = v + 3 * nn;
+            d.kA = v + 4 * nn; d.kB = v + 5 * nn; d.p = v + 6 * nn; d.u = v + 7 * nn;
+        }
         d.minv = I->minv32;
         d.st = I->st;
         d.mat = I->mat;
-        d.part = I->alloc<double>(4 * (size_t)std::max(d.n_slices, d.n_groups));
+        d.part = I->alloc<double>(kPart * (size_t)std::max(d.n_slices, d.n_groups));
         d.cg_tol = o.cg_tol;
         d.outer_tol = o.outer_tol;
         d.inner_tol = o.inner_tol;
@@ -1061,7 +1123,7 @@ CP_API int cp_batch_launch(cp_batch* b, int until, long long max_trips) {
         CP_CUDA(cudaSetDevice(b->ctx->device));
         const int nt = build_tiles(b, b->listed, true, nullptr);
         interleave_tiles(b, nt);
-        if (!b->graph) build_graph(b);
+        if (b->use_graph && !b->graph) build_graph(b);
         BCtl c{};
         c.n_tiles = nt;
         int active = 0, done = 0;
@@ -1083,7 +1145,8 @@ CP_API int cp_batch_launch(cp_batch* b, int until, long long max_trips) {
         CP_CUDA(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BCtl), cudaMemcpyHostToDevice, s));
         b->last_tiles = nt;
         if (active > 0) {
-            CP_CUDA(cudaGraphLaunch(b->graph, s));
+            if (b->use_graph) CP_CUDA(cudaGraphLaunch(b->graph, s));
+            else run_direct(b);
             b->runs += 1;
         }
         CP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(BCtl), cudaMemcpyDeviceToHost, s));
@@ -1195,12 +1258,13 @@ CP_API int cp_batch_autotune(cp_batch* b, double* ms_per_sweep) {
                 const int nt = build_tiles(b, slots, true, &S);
                 interleave_tiles(b, nt);
                 CP_CUDA(cudaMemcpyAsync(b->d_tiles, b->h_tiles, sizeof(int4) * (size_t)nt, cudaMemcpyHostToDevice, s));
-                k_batch_probe<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, nt, 0.5f, b->d_sink);  // warm
+                k_batch_probe<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, nt, 0.5f, 0.5f,
+                                                             b->d_sink);  // warm
                 CP_CUDA(cudaEventRecord(e0, s));
                 const int reps = 5;
                 for (int r = 0; r < reps; ++r)
                     k_batch_probe<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, nt, 0.5f,
-                                                                  b->d_sink);
+                                                                  0.5f, b->d_sink);
                 CP_CUDA(cudaEventRecord(e1, s));
                 CP_CUDA(cudaEventSynchronize(e1));
                 CP_CUDA(cudaGetLastError());

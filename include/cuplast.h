@@ -201,7 +201,8 @@ CP_API int cp_secant_update_noalloc(void* stream, const cp_material* mat, int no
  * accumulated in FP64, every dot product reduced in FP64, and the recursive
  * residual replaced by the FP64 residual b - K64 u whenever it has dropped by
  * inner_tol since the last replacement or meets cg_tol (the linear solve ends
- * on the FP64 residual); the secant update is FP64. Every instance is its own
+ * on the FP64 residual); CG runs in the Chronopoulos-Gear form, one reduction
+ * and one kernel launch per iteration; the secant update is FP64. Every instance is its own
  * device-side state machine. One captured CUDA graph drives all of them: a
  * device WHILE loop over a body of phase-filtered kernels that walk a work
  * list of (instance, tile) entries, so instances of different sizes advance
@@ -256,9 +257,9 @@ CP_API int cp_batch_get_tile(const cp_batch* b, int bucket, int* slices);
  * the tuned time of one SpMV sweep over all listed instances. */
 CP_API int cp_batch_autotune(cp_batch* b, double* ms_per_sweep);
 /* Progress of the instance in a slot as of the end of the last run: phase
- * (1 level set-up, 2 assembly, 3 first FP64 residual, 4-5 CG, 6 FP64
- * residual replacement, 7 secant update, 8 Aitken, 9 plastic strains,
- * 10 done), load level, and the counters of its report so far. */
+ * (1 level set-up, 2 assembly, 3 FP64 residual (first or replacement),
+ * 4 w = K u, 5 CG iteration, 6 secant update, 7 Aitken, 8 plastic strains,
+ * 9 done), load level, and the counters of its report so far. */
 CP_API int cp_batch_progress(const cp_batch* b, int slot, int* phase, int* level, cp_solve_report* report);
 /* Counters of the batch since creation: graph trips and kernel launches. */
 CP_API int cp_batch_stats(const cp_batch* b, long long* trips, long long* kernel_launches, long long* runs);
