@@ -543,9 +543,10 @@ def run_product_arm(args):
                "sample": "one full config-1 solve (10 levels, CG 1e-10, outer 1e-6), reference CPU path, "
                          f"{c['outer']} outer / {c['cg']} CG iterations"}
 
-    batched = served = None
+    batched = served = roof_batched = None
     if rank == 0 and not args.skip_batched:
         batched = batched_leg(ctx, window_s=args.batched_window)
+        roof_batched = cg_kernel_roofline(ctx)
     if rank == 0 and not args.skip_served:
         served = served_leg(rate_hz=args.serve_rate, submit_s=args.serve_window, drain_s=args.serve_window + 5)
 
@@ -559,7 +560,8 @@ def run_product_arm(args):
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches), "roofline": roofline, "roofline_this_workload": roof_small,
             "cg_large_mesh": cg_large, "cpu_baseline": cpu, "clocks": clocks.summary(),
-            "accuracy_vs_tight_fp64": accuracy, "batched": batched, "served": served,
+            "accuracy_vs_tight_fp64": accuracy, "batched": batched, "roofline_batched": roof_batched,
+            "served": served,
             "detail": {"outer_iters": reps[-1]["outer_iters"], "cg_iters": reps[-1]["cg_iters"],
                        "step_seconds": times}}
     if rank == 0:
@@ -569,9 +571,64 @@ def run_product_arm(args):
         dist.destroy_process_group()
 
 
+CG_ONLY_KW = dict(cg_tol=1e-12, outer_tol=1e-9, max_outer=50, max_cg=5_000_000, precond=1, aitken=1, adaptive_cg=0,
+                  inner_tol=1e-3)
+
+
+def cg_kernel_roofline(ctx, n=512, warm_trips=3, trips=10, seed=20261203):
+    """Live roofline of the batched CG iteration kernel (k_batch_cg, ITER
+    phase): n resident config-4 instances with tight, non-adaptive linear
+    solves, so every launch after the warm-up is a CG iteration of every
+    instance; CUDA-event time per iteration of the whole batch and the
+    algorithmic bytes one iteration must move."""
+    import cudaplasticity_b200 as cp
+    from cudaplasticity_b200 import workload
+
+    insts = []
+    for i in range(n):
+        w = workload.instance(i, seed=seed)
+        inst = cp.Instance(ctx, w["mesh"], w["material"])
+        inst.set_loads(w["rp"], w["mask"], w["uv"])
+        insts.append(inst)
+    b = cp.Batch(ctx, max_instances=n)
+    for inst in insts:
+        b.add(inst, levels=1, **CG_ONLY_KW)
+    b.run(max_trips=warm_trips)
+    b.autotune()
+    cg0 = [b.progress(s)[2]["cg_iters"] for s in range(n)]
+    b.run(max_trips=trips)
+    sec = b.last_run_ms() * 1e-3  # CUDA events around the run on the batch's stream
+    done_iters = [b.progress(s)[2]["cg_iters"] - cg0[s] for s in range(n)]
+    phases = [b.progress(s)[0] for s in range(n)]
+    # per 2x2 block: 4 FP32 values + one column; per node: read the 32-byte
+    # record, p, w, kp, r (FP32 pairs), x (FP64 pair), mask, block-Jacobi
+    # inverse; write p, kp, x, r, w and the new record
+    per_iter = []
+    nodes = 0
+    for inst in insts:
+        nn, ne, nnz, nadj = inst.sizes()
+        per_iter.append(20.0 * (nnz // 4) + 178.0 * nn)
+        nodes += nn
+    b.close()
+    for inst in insts:
+        inst.close()
+    moved = sum(k * bi for k, bi in zip(done_iters, per_iter))
+    iters = max(done_iters)  # launches of the iteration kernel that did work
+    bytes_iter = moved / iters
+    peak, peak_kind = measured_peak_hbm()
+    us = 1e6 * sec / iters
+    gbs = moved / sec / 1e9
+    return {"bound": "hbm", "kernel": "k_batch_cg (CG iteration of %d resident instances, %d DOF)" % (n, 2 * nodes),
+            "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak, "traffic": None,
+            "bytes_per_launch": bytes_iter, "ms_per_launch": us * 1e-3, "peak_kind": peak_kind,
+            "iterations_timed": iters, "instance_iterations": int(sum(done_iters)),
+            "in_cg_at_end": phases.count(5)}
+
+
 def batched_probe(n, trips):
-    """A fixed slice of batched work for profilers: n resident config-4
-    instances, then `trips` graph trips; prints the time per trip."""
+    """A fixed slice of batched CG work for profilers: n resident config-4
+    instances with tight, non-adaptive linear solves (every launch after the
+    first trips is a CG iteration), `trips` graph trips; prints the time."""
     import cudaplasticity_b200 as cp
     from cudaplasticity_b200 import workload
 
@@ -584,12 +641,14 @@ def batched_probe(n, trips):
         insts.append(inst)
     b = cp.Batch(ctx, max_instances=n)
     for inst in insts:
-        b.add(inst, levels=1, **BATCH_KW)
+        b.add(inst, levels=1, **CG_ONLY_KW)
     b.run(max_trips=3)
+    ms = b.autotune()
     t0 = time.perf_counter()
     b.run(max_trips=trips)
     dt = time.perf_counter() - t0
-    print(json.dumps({"batched_probe": n, "trips": trips, "ms_per_trip": 1e3 * dt / trips, "stats": b.stats()}))
+    print(json.dumps({"batched_probe": n, "trips": trips, "ms_per_trip": 1e3 * dt / trips, "stats": b.stats(),
+                      "autotune_ms_per_sweep": ms, "tiles": [b.tile(k) for k in range(4, 14)]}))
     b.close()
     for inst in insts:
         inst.close()

@@ -463,6 +463,12 @@ class Batch:
     def set_tile(self, bucket, slices):
         self.ctx.check(C.lib().cp_batch_set_tile(self._h, bucket, slices))
 
+    def last_run_ms(self):
+        """Device time of the last run (CUDA events on the batch's stream)."""
+        v = ctypes.c_double()
+        self.ctx.check(C.lib().cp_batch_last_run_ms(self._h, ctypes.byref(v)))
+        return v.value
+
     def stats(self):
         t, k, r = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
         self.ctx.check(C.lib().cp_batch_stats(self._h, ctypes.byref(t), ctypes.byref(k), ctypes.byref(r)))

@@ -114,6 +114,7 @@ _SIGS = {
     "cp_batch_get_tile": (c_int, [c_p, c_int, P_int]),
     "cp_batch_autotune": (c_int, [c_p, P_double]),
     "cp_batch_stats": (c_int, [c_p, P_ll, P_ll, P_ll]),
+    "cp_batch_last_run_ms": (c_int, [c_p, P_double]),
     "cp_batch_progress": (c_int, [c_p, c_int, P_int, P_int, ctypes.POINTER(cp_solve_report)]),
     "cp_server_opts_default": (None, [ctypes.POINTER(cp_server_opts)]),
     "cp_server_create": (c_int, [ctypes.POINTER(cp_server_opts), ctypes.POINTER(c_p)]),

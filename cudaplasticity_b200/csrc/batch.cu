@@ -86,7 +86,9 @@ struct BDesc {
     const double2* b_full;
     const double2* u_full;
     const uchar2* mask;
-    float2 *rA, *rB, *wA, *wB, *kA, *kB, *p, *u;  // FP32 CG vectors (A/B: by parity)
+    float2 *r, *w, *kp, *p;  // FP32 CG vectors, own node only
+    float4 *gA, *gB;         // read by the neighbours, A/B by parity: node n's 32-byte record is
+                             // g[2n] = (u, M w), g[2n+1] = (M kp, 0): one L2 sector per neighbour
     float4* minv;
     ElemState st;
     MaterialDev mat;
@@ -214,34 +216,41 @@ __device__ __forceinline__ void decide(const BDesc& d, BState* S, BCtl* c) {
 
 // ------------------------------------------------------------ CG phases --
 //
-// The linear solve is preconditioned CG in the Chronopoulos-Gear form: the
-// same iterates as the standard recurrence in exact arithmetic, with both
-// inner products of an iteration taken together, so one iteration is one
-// launch with one reduction. With M the 2x2 block-Jacobi inverse (identity
-// without preconditioning), u = M r, w = K u, p the direction, kp = K p:
-//   p = u + beta p, kp = w + beta kp, x += alpha p, r -= m.alpha kp,
-//   u = M r, w = K u, gamma = (r, u), delta = (w, u),
-//   beta' = gamma' / gamma, alpha' = gamma' / (K p', p') with
-//   (K p', p') = delta' + beta' ((w', p) + (kp, u')) + beta'^2 (kp, p).
-// K u needs the new u of the neighbours, which each thread recomputes from
-// the neighbours' old r, w, kp (double-buffered by the instance's parity),
-// so no second pass is needed. RES (FP64 residual of the FP64 solution, at
+// The linear solve is preconditioned CG with one reduction per iteration
+// (the Chronopoulos-Gear arrangement): with M the 2x2 block-Jacobi inverse
+// (the Dirichlet mask without preconditioning), u = M r, w = K u, p the
+// direction, kp = K p, an iteration is
+//   p' = u + beta p, kp' = w + beta kp, x += alpha p', r' = m.(r - alpha kp'),
+//   u' = u - alpha (M w + beta M kp), w' = K u',
+//   gamma' = (r', u'), beta' = gamma' / gamma, alpha' = gamma' / (K p'', p'')
+// with (K p'', p'') = (w', u') + beta' ((w', p') + (kp', u')) + beta'^2 (kp', p')
+// expanded from this iteration's vectors, as standard CG computes its step.
+// K u' needs the neighbours' new u, which each thread recomputes from the
+// neighbours' u, M w and M kp, packed in one 32-byte record per node (one L2
+// sector per neighbour; double-buffered by the instance's parity). The node
+// itself uses the same formula, so every thread sees one vector u'.
+// One iteration is one launch. RES (FP64 residual of the FP64 solution, at
 // the start and at every replacement) and W (w = K u after it) bracket the
 // iterations; r, u, w, kp, p are FP32, x and every sum are FP64.
 
 __device__ __forceinline__ float2 mvec(const float4& m, float2 v) {
     return make_float2(m.x * v.x + m.y * v.y, m.z * v.x + m.w * v.y);
 }
+// M v: the block-Jacobi inverse, or the mask without preconditioning.
+__device__ __forceinline__ float2 apply_m(const BDesc& d, int n, float2 v) {
+    if (d.precond) return mvec(d.minv[n], v);
+    const uchar2 m = d.mask[n];
+    return make_float2(m.x ? v.x : 0.f, m.y ? v.y : 0.f);
+}
 
 // RES: r = m.(b - K64 x) in FP64 (stored in FP32), u = M r; at the start of
-// a solve also the block-Jacobi inverse, p = kp = 0. Sums (r32, r32),
-// (r64, r64), (b, b).
+// a solve also the block-Jacobi inverse and p = kp = M kp = 0. Sums
+// (r32, r32), (r64, r64), (b, b).
 __device__ void tile_res(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
     const int pre = d.precond, first = S->res_kind == 0;
     const int par = S->parity;
-    float2* __restrict__ r = par ? d.rB : d.rA;
     for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
         const int n = 32 * sl + lane;
         const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
@@ -261,34 +270,30 @@ __device__ void tile_res(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh
             const uchar2 m = d.mask[n];
             const double r0 = m.x ? bb.x - k0 : 0.0, r1 = m.y ? bb.y - k1 : 0.0;
             const float2 rt = make_float2((float)r0, (float)r1);
-            r[n] = rt;
-            float2 u = rt;
-            if (pre) {
-                float4 mi;
-                if (first) {
-                    // inverse of the node's 2x2 diagonal block, restricted to its free DOFs
-                    const double2* dp = reinterpret_cast<const double2*>(d.val64 + 4 * ((long long)base + lane));
-                    const double2 dlo = __ldg(dp), dhi = __ldg(dp + 1);
-                    double i00 = 0, i01 = 0, i10 = 0, i11 = 0;
-                    if (m.x && m.y) {
-                        const double det = dlo.x * dhi.y - dlo.y * dhi.x;
-                        i00 = dhi.y / det; i01 = -dlo.y / det; i10 = -dhi.x / det; i11 = dlo.x / det;
-                    } else if (m.x) {
-                        i00 = 1.0 / dlo.x;
-                    } else if (m.y) {
-                        i11 = 1.0 / dhi.y;
-                    }
-                    mi = make_float4((float)i00, (float)i01, (float)i10, (float)i11);
-                    d.minv[n] = mi;
-                } else {
-                    mi = d.minv[n];
+            d.r[n] = rt;
+            if (pre && first) {
+                // inverse of the node's 2x2 diagonal block, restricted to its free DOFs
+                const double2* dp = reinterpret_cast<const double2*>(d.val64 + 4 * ((long long)base + lane));
+                const double2 dlo = __ldg(dp), dhi = __ldg(dp + 1);
+                double i00 = 0, i01 = 0, i10 = 0, i11 = 0;
+                if (m.x && m.y) {
+                    const double det = dlo.x * dhi.y - dlo.y * dhi.x;
+                    i00 = dhi.y / det; i01 = -dlo.y / det; i10 = -dhi.x / det; i11 = dlo.x / det;
+                } else if (m.x) {
+                    i00 = 1.0 / dlo.x;
+                } else if (m.y) {
+                    i11 = 1.0 / dhi.y;
                 }
-                u = mvec(mi, rt);
+                d.minv[n] = make_float4((float)i00, (float)i01, (float)i10, (float)i11);
             }
-            d.u[n] = u;
+            float4* g = par ? d.gB : d.gA;
+            const float2 u = apply_m(d, n, rt);
+            reinterpret_cast<float2*>(g + 2 * (size_t)n)[0] = u;
             if (first) {
-                d.p[n] = make_float2(0.f, 0.f);
-                (par ? d.kB : d.kA)[n] = make_float2(0.f, 0.f);
+                const float2 z = make_float2(0.f, 0.f);
+                d.p[n] = z;
+                d.kp[n] = z;
+                g[2 * (size_t)n + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
             s_rr = (double)rt.x * (double)rt.x + (double)rt.y * (double)rt.y;
             s_r64 = r0 * r0 + r1 * r1;
@@ -299,12 +304,12 @@ __device__ void tile_res(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh
         s_bb = warp_sum(s_bb);
         if (lane == 0) {
             double* p = d.part + kPart * (size_t)sl;
-            p[0] = s_rr; p[1] = s_r64; p[2] = s_bb; p[3] = 0.0;
+            p[0] = s_rr; p[1] = s_r64; p[2] = s_bb;
         }
     }
     if (!arrive(S, tl.w, shf)) return;
     double t[4];
-    reduce_parts<4>(d.part, d.n_slices, t, sh);
+    reduce_parts<3>(d.part, d.n_slices, t, sh);
     if (threadIdx.x == 0) {
         const double rr = t[0], res64 = t[1];
         S->ticket = 0;
@@ -325,17 +330,14 @@ __device__ void tile_res(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh
     }
 }
 
-// W: w = K32 u (u of RES, read from the neighbours); gamma = (r, u),
-// delta = (w, u) and, for the direction that carries on after a
-// replacement, (w, p), (kp, u), (kp, p); the step scalars of the next
-// iteration (see tile_iter for the expansion).
+// W: w = K32 u (u of RES, read from the neighbours), M w; gamma = (r, u),
+// (w, u) and, for the direction that carries on after a replacement, (w, p),
+// (kp, u), (kp, p): the step scalars of the next iteration.
 __device__ void tile_w(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
     const int par = S->parity;
-    const float2* __restrict__ r = par ? d.rB : d.rA;
-    const float2* __restrict__ kv = par ? d.kB : d.kA;
-    float2* __restrict__ wv = par ? d.wB : d.wA;
+    float4* __restrict__ g = par ? d.gB : d.gA;
     for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
         const int n = 32 * sl + lane;
         const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
@@ -347,12 +349,16 @@ __device__ void tile_w(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, 
                 const long long bi = base + 32LL * k + lane;
                 const int col = __ldg(d.scol + bi);
                 const float4 v = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
-                const float2 uc = d.u[col];
+                const float2 uc = reinterpret_cast<const float2*>(g + 2 * (size_t)col)[0];
                 k0 += v.x * uc.x + v.y * uc.y;
                 k1 += v.z * uc.x + v.w * uc.y;
             }
-            wv[n] = make_float2(k0, k1);
-            const float2 un = d.u[n], rn = r[n], pn = d.p[n], kn = kv[n];
+            const float2 wn = make_float2(k0, k1);
+            d.w[n] = wn;
+            const float2 un = reinterpret_cast<const float2*>(g + 2 * (size_t)n)[0];
+            const float2 mw = apply_m(d, n, wn);
+            g[2 * (size_t)n] = make_float4(un.x, un.y, mw.x, mw.y);
+            const float2 rn = d.r[n], pn = d.p[n], kn = d.kp[n];
             s_g = (double)rn.x * (double)un.x + (double)rn.y * (double)un.y;
             s_d = (double)k0 * (double)un.x + (double)k1 * (double)un.y;
             s_wp = (double)k0 * (double)pn.x + (double)k1 * (double)pn.y;
@@ -395,77 +401,66 @@ __device__ void tile_w(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, 
 __device__ void tile_iter(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
-    const int par = S->parity, pre = d.precond;
-    const float2* __restrict__ ro = par ? d.rB : d.rA;
-    const float2* __restrict__ wo = par ? d.wB : d.wA;
-    const float2* __restrict__ ko = par ? d.kB : d.kA;
-    float2* __restrict__ rn_ = par ? d.rA : d.rB;
-    float2* __restrict__ wn_ = par ? d.wA : d.wB;
-    float2* __restrict__ kn_ = par ? d.kA : d.kB;
+    const int par = S->parity;
+    const float4* __restrict__ go = par ? d.gB : d.gA;
+    float4* __restrict__ gn = par ? d.gA : d.gB;
     const double alpha = S->alpha;
     const float a = (float)alpha, bt = (float)S->beta;
     for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
         const int n = 32 * sl + lane;
         const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
-        double s_g = 0.0, s_d = 0.0, s_rr = 0.0, s_wp = 0.0, s_ku = 0.0, s_kp = 0.0;
+        double s_g = 0.0, s_d = 0.0, s_rr = 0.0, s_x = 0.0, s_kp = 0.0;
         if (n < d.m.n_nodes) {
             // own node
-            const float2 un = d.u[n], pn = d.p[n], wn = wo[n], kn = ko[n];
+            const float4 g0 = __ldg(go + 2 * (size_t)n), g1 = __ldg(go + 2 * (size_t)n + 1);
+            const float2 u0 = make_float2(g0.x, g0.y), mw0 = make_float2(g0.z, g0.w), mk0 = make_float2(g1.x, g1.y);
+            const float2 pn = d.p[n], wn = d.w[n], kn = d.kp[n];
             const uchar2 m = d.mask[n];
-            const float2 p = make_float2(un.x + bt * pn.x, un.y + bt * pn.y);
+            const float2 p = make_float2(u0.x + bt * pn.x, u0.y + bt * pn.y);
             const float2 kp = make_float2(wn.x + bt * kn.x, wn.y + bt * kn.y);
+            const float2 u = make_float2(u0.x - a * (mw0.x + bt * mk0.x), u0.y - a * (mw0.y + bt * mk0.y));
             double2 x = d.x[n];
             x.x += alpha * (double)p.x;
             x.y += alpha * (double)p.y;
-            float2 r = ro[n];
+            float2 r = d.r[n];
             if (m.x) r.x -= a * kp.x;
             if (m.y) r.y -= a * kp.y;
-            const float2 u = pre ? mvec(d.minv[n], r) : r;
-            // w = K u with the neighbours' new u recomputed from their old values
+            // w' = K u' with the neighbours' u' from their u, M w, M kp
             float k0 = 0.f, k1 = 0.f;
 #pragma unroll 3
             for (int k = 0; k < wd; ++k) {
                 const long long bi = base + 32LL * k + lane;
                 const int col = __ldg(d.scol + bi);
                 const float4 v = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
-                float2 uc;
-                if (k == 0) {
-                    uc = u;  // block 0 is the node itself
-                } else {
-                    const float2 rc = ro[col], wc = wo[col], kc = ko[col];
-                    float2 rr2 = make_float2(rc.x - a * (wc.x + bt * kc.x), rc.y - a * (wc.y + bt * kc.y));
-                    if (pre) {
-                        uc = mvec(d.minv[col], rr2);  // zero rows and columns at prescribed DOFs
-                    } else {
-                        const uchar2 mc = d.mask[col];
-                        uc = make_float2(mc.x ? rr2.x : 0.f, mc.y ? rr2.y : 0.f);
-                    }
-                }
-                k0 += v.x * uc.x + v.y * uc.y;
-                k1 += v.z * uc.x + v.w * uc.y;
+                const float4 c0 = __ldg(go + 2 * (size_t)col), c1 = __ldg(go + 2 * (size_t)col + 1);
+                const float ux = c0.x - a * (c0.z + bt * c1.x), uy = c0.y - a * (c0.w + bt * c1.y);
+                k0 += v.x * ux + v.y * uy;
+                k1 += v.z * ux + v.w * uy;
             }
+            const float2 w2 = make_float2(k0, k1);
             d.p[n] = p;
-            kn_[n] = kp;
+            d.kp[n] = kp;
             d.x[n] = x;
-            rn_[n] = r;
-            d.u[n] = u;
-            wn_[n] = make_float2(k0, k1);
+            d.r[n] = r;
+            d.w[n] = w2;
+            const float2 mw = apply_m(d, n, w2), mk = apply_m(d, n, kp);
+            gn[2 * (size_t)n] = make_float4(u.x, u.y, mw.x, mw.y);
+            gn[2 * (size_t)n + 1] = make_float4(mk.x, mk.y, 0.f, 0.f);
             s_g = (double)r.x * (double)u.x + (double)r.y * (double)u.y;
             s_d = (double)k0 * (double)u.x + (double)k1 * (double)u.y;
             s_rr = (double)r.x * (double)r.x + (double)r.y * (double)r.y;
-            s_wp = (double)k0 * (double)p.x + (double)k1 * (double)p.y;
-            s_ku = (double)kp.x * (double)u.x + (double)kp.y * (double)u.y;
+            s_x = ((double)k0 * (double)p.x + (double)k1 * (double)p.y) +
+                  ((double)kp.x * (double)u.x + (double)kp.y * (double)u.y);  // (w', p') + (kp', u')
             s_kp = (double)kp.x * (double)p.x + (double)kp.y * (double)p.y;
         }
         s_g = warp_sum(s_g);
         s_d = warp_sum(s_d);
         s_rr = warp_sum(s_rr);
-        s_wp = warp_sum(s_wp);
-        s_ku = warp_sum(s_ku);
+        s_x = warp_sum(s_x);
         s_kp = warp_sum(s_kp);
         if (lane == 0) {
             double* p = d.part + kPart * (size_t)sl;
-            p[0] = s_g; p[1] = s_d; p[2] = s_rr; p[3] = s_wp; p[4] = s_ku; p[5] = s_kp;
+            p[0] = s_g; p[1] = s_d; p[2] = s_rr; p[3] = s_x; p[4] = 0.0; p[5] = s_kp;
         }
     }
     if (!arrive(S, tl.w, shf)) return;
@@ -479,10 +474,6 @@ __device__ void tile_iter(const BDesc& d, BState* S, BCtl* c, int4 tl, double* s
         S->lin_iters += 1;
         S->cg_total += 1;
         S->rr = rn;
-        // (K p', p') of the next direction p' = u + beta p, K p' = w + beta kp,
-        // expanded from this iteration's vectors: the step is computed as in
-        // standard CG, with no recurrence identity that a residual
-        // replacement or FP32 rounding would break
         const double beta = g / S->gamma;
         const double den = t[1] + beta * (t[3] + t[4]) + beta * beta * t[5];
         if (!(rn == rn) || !(g == g)) {
@@ -503,7 +494,9 @@ __device__ void tile_iter(const BDesc& d, BState* S, BCtl* c, int4 tl, double* s
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_batch_cg(const BDesc* __restrict__ D, BState* SS,
+// 8 resident blocks per SM (64 registers): the CG iteration is bound by the
+// latency of its gathers, and the occupancy pays for the few spills.
+__global__ void __launch_bounds__(kThreads, 8) k_batch_cg(const BDesc* __restrict__ D, BState* SS,
                                                        const int4* __restrict__ tiles, BCtl* c) {
     __shared__ double sh[2 * kWarps];
     __shared__ int shf, shp;
@@ -522,42 +515,61 @@ __global__ void __launch_bounds__(kThreads) k_batch_cg(const BDesc* __restrict__
     }
 }
 
-// The SpMV of an iteration for the autotuner: the same loads and arithmetic
-// as ITER's neighbour loop, with the results written to a sink of the batch
-// (one value per thread) instead of the instance's vectors, so that the
-// instances' state is left untouched whatever phase they are in.
+// The work of an iteration for the autotuner, with the same per-tile costs
+// as ITER: the phase read, the own-node and neighbour loads and arithmetic,
+// the per-slice sums, a fence and a ticket per tile, and the last tile's
+// pass over the slice sums. Everything it writes goes to scratch arrays of
+// the batch (sink, one ticket per slot, sums), so the instances' state is
+// left untouched whatever phase they are in.
 __global__ void __launch_bounds__(kThreads) k_batch_probe(const BDesc* __restrict__ D, const BState* SS,
                                                           const int4* __restrict__ tiles, int nt, float a, float bt,
-                                                          float2* sink) {
+                                                          float2* sink, unsigned int* tickets, double* sums) {
+    __shared__ double sh[2 * kWarps];
+    __shared__ int shf, shp;
     float2 acc = make_float2(0.f, 0.f);
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int4 tl = tiles[t];
         const BDesc& d = D[tl.x];
+        (void)tile_phase(SS + tl.x, &shp);
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
         const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
-        const int par = SS[tl.x].parity, pre = d.precond;
-        const float2* __restrict__ ro = par ? d.rB : d.rA;
-        const float2* __restrict__ wo = par ? d.wB : d.wA;
-        const float2* __restrict__ ko = par ? d.kB : d.kA;
+        const int par = SS[tl.x].parity;
+        const float4* __restrict__ go = par ? d.gB : d.gA;
         for (int sl = sl0 + w; sl < sl1; sl += kWarps) {
             const int n = 32 * sl + lane;
             const int base = d.slice_ptr[sl], wd = (d.slice_ptr[sl + 1] - base) >> 5;
+            double s0 = 0.0;
             if (n < d.m.n_nodes) {
+                const float4 g0 = go[2 * (size_t)n], g1 = go[2 * (size_t)n + 1];
+                const float2 u0 = make_float2(g0.x, g0.y), mw0 = make_float2(g0.z, g0.w), mk0 = make_float2(g1.x, g1.y);
+                const float2 pn = d.p[n], wn = d.w[n], kn = d.kp[n], rn = d.r[n];
+                const double2 xn = d.x[n];
                 float k0 = 0.f, k1 = 0.f;
 #pragma unroll 3
                 for (int k = 0; k < wd; ++k) {
                     const long long bi = base + 32LL * k + lane;
                     const int col = __ldg(d.scol + bi);
                     const float4 v = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
-                    const float2 rc = ro[col], wc = wo[col], kc = ko[col];
-                    const float2 rr2 = make_float2(rc.x - a * (wc.x + bt * kc.x), rc.y - a * (wc.y + bt * kc.y));
-                    const float2 uc = pre ? mvec(d.minv[col], rr2) : rr2;
-                    k0 += v.x * uc.x + v.y * uc.y;
-                    k1 += v.z * uc.x + v.w * uc.y;
+                    const float4 c0 = go[2 * (size_t)col], c1 = go[2 * (size_t)col + 1];
+                    const float ux = c0.x - a * (c0.z + bt * c1.x), uy = c0.y - a * (c0.w + bt * c1.y);
+                    k0 += v.x * ux + v.y * uy;
+                    k1 += v.z * ux + v.w * uy;
                 }
-                acc.x += k0;
-                acc.y += k1;
+                acc.x += k0 + u0.x + mw0.x + mk0.x + pn.x + wn.x + kn.x + rn.x + (float)xn.x;
+                acc.y += k1 + u0.y + mw0.y + mk0.y + pn.y + wn.y + kn.y + rn.y + (float)xn.y;
+                s0 = (double)k0 * (double)u0.x;
             }
+            s0 = warp_sum(s0);
+            if (lane == 0) sums[blockIdx.x] = s0;
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) shf = (atomicAdd(tickets + tl.x, 1u) % (unsigned)tl.w) == (unsigned)tl.w - 1u;
+        __syncthreads();
+        if (shf) {
+            double r[6];
+            reduce_parts<6>(d.part, d.n_slices, r, sh);  // reads only
+            if (threadIdx.x == 0) sums[blockIdx.x] += r[0];
         }
     }
     sink[blockIdx.x * kThreads + threadIdx.x] = acc;
@@ -784,12 +796,17 @@ struct cp_batch {
     int* d_stop = nullptr;
     cudaGraphExec_t graph = nullptr;
     int grid_cg = 0, grid_elem = 0, grid_asm = 0;
-    float2* d_sink = nullptr;  // autotuner probe output
+    float2* d_sink = nullptr;           // autotuner probe output
+    unsigned int* d_ptickets = nullptr;  // autotuner probe tickets (one per slot)
+    double* d_psums = nullptr;           // autotuner probe sums (one per block)
     size_t asm_smem = 0;
     bool running = false;
     bool use_graph = true;  // false (CUPLAST_NO_GRAPH=1): trips launched kernel by kernel, for profilers
     int last_tiles = 0;
     long long trips = 0, launches = 0, runs = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // bracket each run on the batch's stream
+    bool timed = false;
+    double last_run_ms = 0.0;
 };
 
 namespace {
@@ -839,18 +856,33 @@ int tiles_of(const BDesc& d, int S) {
 }
 
 // Work list of the listed, unfinished instances; returns the tile count.
-int build_tiles(cp_batch* b, const std::vector<int>& slots, bool only_active, const int* S_override) {
+// Tile sizes come from the table of the instance's size bucket; with
+// `shrink`, when the active instances hold too few slices to give every
+// block of the persistent grid a tile, tiles shrink (down to one slice per
+// warp) so that the remaining work still spreads over the whole GPU.
+int build_tiles(cp_batch* b, const std::vector<int>& slots, bool only_active, const int* S_override, bool shrink) {
+    long long slices = 0;
+    for (int sl : slots)
+        if (!(only_active && b->state[sl].phase == PH_DONE)) slices += b->desc[sl].n_slices;
+    int cap = 1 << 30;
+    if (shrink && !S_override) {
+        cap = kWarps;
+        while ((long long)cap * 2 * b->grid_cg <= slices && cap < 64) cap *= 2;
+    }
+    auto S_of = [&](int sl) {
+        if (S_override) return *S_override;
+        return std::min(b->tile_slices[bucket_of(b->desc[sl].n_slices)], cap);
+    };
     int total = 0;
     for (int sl : slots) {
         if (only_active && b->state[sl].phase == PH_DONE) continue;
-        const int S = S_override ? *S_override : b->tile_slices[bucket_of(b->desc[sl].n_slices)];
-        total += tiles_of(b->desc[sl], S);
+        total += tiles_of(b->desc[sl], S_of(sl));
     }
     ensure_tiles(b, std::max(total, 1));
     int k = 0;
     for (int sl : slots) {
         if (only_active && b->state[sl].phase == PH_DONE) continue;
-        const int S = S_override ? *S_override : b->tile_slices[bucket_of(b->desc[sl].n_slices)];
+        const int S = S_of(sl);
         const int nt = tiles_of(b->desc[sl], S);
         for (int t = 0; t < nt; ++t) b->h_tiles[k++] = make_int4(sl, t, S, nt);
     }
@@ -1005,7 +1037,12 @@ CP_API int cp_batch_create(cp_context* ctx, const cp_batch_opts* opts, cp_batch*
         CP_CUDA(cudaFuncSetAttribute(k_batch_asm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->asm_smem));
         CP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_asm, kThreads, b->asm_smem));
         b->grid_asm = ctx->sm_count * std::max(1, per_sm);
+        CP_CUDA(cudaEventCreate(&b->ev0));
+        CP_CUDA(cudaEventCreate(&b->ev1));
         CP_CUDA(cudaMalloc(&b->d_sink, sizeof(float2) * (size_t)b->grid_cg * kThreads));
+        CP_CUDA(cudaMalloc(&b->d_ptickets, sizeof(unsigned int) * (size_t)b->cap));
+        CP_CUDA(cudaMemset(b->d_ptickets, 0, sizeof(unsigned int) * (size_t)b->cap));
+        CP_CUDA(cudaMalloc(&b->d_psums, sizeof(double) * (size_t)b->grid_cg));
     });
     if (rc != CP_OK) {
         cp_batch_destroy(b);
@@ -1032,7 +1069,11 @@ CP_API int cp_batch_destroy(cp_batch* b) {
     if (b->h_state) cudaFreeHost(b->h_state);
     if (b->h_ctl) cudaFreeHost(b->h_ctl);
     if (b->h_stop) cudaFreeHost(b->h_stop);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->d_sink) cudaFree(b->d_sink);
+    if (b->d_ptickets) cudaFree(b->d_ptickets);
+    if (b->d_psums) cudaFree(b->d_psums);
     delete b;
     return CP_OK;
 }
@@ -1078,10 +1119,12 @@ CP_API int cp_batch_add(cp_batch* b, cp_instance* I, const cp_solve_opts* opts, 
         d.mask = I->mask;
         {
             const size_t nn = (size_t)I->n_nodes;
-            float2* v = I->alloc<float2>(8 * nn);
-            CP_CUDA(cudaMemsetAsync(v, 0, sizeof(float2) * 8 * nn, I->s()));
-            d.rA = v; d.rB = v + nn; d.wA = v + 2 * nn; d.wB = v + 3 * nn;
-            d.kA = v + 4 * nn; d.kB = v + 5 * nn; d.p = v + 6 * nn; d.u = v + 7 * nn;
+            float2* v = I->alloc<float2>(4 * nn);
+            float4* g = I->alloc<float4>(4 * nn);
+            CP_CUDA(cudaMemsetAsync(v, 0, sizeof(float2) * 4 * nn, I->s()));
+            CP_CUDA(cudaMemsetAsync(g, 0, sizeof(float4) * 4 * nn, I->s()));
+            d.r = v; d.w = v + nn; d.kp = v + 2 * nn; d.p = v + 3 * nn;
+            d.gA = g; d.gB = g + 2 * nn;
         }
         d.minv = I->minv32;
         d.st = I->st;
@@ -1121,7 +1164,7 @@ CP_API int cp_batch_launch(cp_batch* b, int until, long long max_trips) {
     return bguard(b, [&] {
         cudaStream_t s = b->ctx->stream;
         CP_CUDA(cudaSetDevice(b->ctx->device));
-        const int nt = build_tiles(b, b->listed, true, nullptr);
+        const int nt = build_tiles(b, b->listed, true, nullptr, true);
         interleave_tiles(b, nt);
         if (b->use_graph && !b->graph) build_graph(b);
         BCtl c{};
@@ -1144,9 +1187,13 @@ CP_API int cp_batch_launch(cp_batch* b, int until, long long max_trips) {
         if (nt > 0) CP_CUDA(cudaMemcpyAsync(b->d_tiles, b->h_tiles, sizeof(int4) * (size_t)nt, cudaMemcpyHostToDevice, s));
         CP_CUDA(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(BCtl), cudaMemcpyHostToDevice, s));
         b->last_tiles = nt;
+        b->timed = false;
         if (active > 0) {
+            CP_CUDA(cudaEventRecord(b->ev0, s));
             if (b->use_graph) CP_CUDA(cudaGraphLaunch(b->graph, s));
             else run_direct(b);
+            CP_CUDA(cudaEventRecord(b->ev1, s));
+            b->timed = true;
             b->runs += 1;
         }
         CP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(BCtl), cudaMemcpyDeviceToHost, s));
@@ -1181,6 +1228,9 @@ CP_API int cp_batch_wait(cp_batch* b, int* active, int* done) {
     return bguard(b, [&] {
         b->running = false;
         CP_CUDA(cudaStreamSynchronize(b->ctx->stream));
+        float ms = 0.f;
+        if (b->timed) CP_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+        b->last_run_ms = ms;
         const long long trips = b->h_ctl->trips;
         b->trips += trips;
         b->launches += trips * (long long)(b->o.elem_per_trip + 1 + b->o.cg_per_trip + 1);
@@ -1245,43 +1295,53 @@ CP_API int cp_batch_autotune(cp_batch* b, double* ms_per_sweep) {
         cudaEvent_t e0, e1;
         CP_CUDA(cudaEventCreate(&e0));
         CP_CUDA(cudaEventCreate(&e1));
-        const int cands[] = {4, 8, 16, 32, 64};
-        double total = 0.0;
-        for (int bk = 0; bk < kBuckets; ++bk) {
-            std::vector<int> slots;
-            for (int sl : b->listed)
-                if (bucket_of(b->desc[sl].n_slices) == bk && b->state[sl].phase != PH_DONE) slots.push_back(sl);
-            if (slots.empty()) continue;
-            double best = 1e30;
-            int best_S = b->tile_slices[bk];
-            for (int S : cands) {
-                const int nt = build_tiles(b, slots, true, &S);
-                interleave_tiles(b, nt);
-                CP_CUDA(cudaMemcpyAsync(b->d_tiles, b->h_tiles, sizeof(int4) * (size_t)nt, cudaMemcpyHostToDevice, s));
+        std::vector<int> active;
+        for (int sl : b->listed)
+            if (b->state[sl].phase != PH_DONE) active.push_back(sl);
+        // one sweep of the probe over every active instance with the current table
+        auto sweep = [&]() {
+            const int nt = build_tiles(b, active, true, nullptr, false);
+            interleave_tiles(b, nt);
+            CP_CUDA(cudaMemcpyAsync(b->d_tiles, b->h_tiles, sizeof(int4) * (size_t)nt, cudaMemcpyHostToDevice, s));
+            k_batch_probe<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, nt, 0.5f, 0.5f, b->d_sink,
+                                                         b->d_ptickets, b->d_psums);  // warm
+            const int reps = 3;
+            CP_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < reps; ++r)
                 k_batch_probe<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, nt, 0.5f, 0.5f,
-                                                             b->d_sink);  // warm
-                CP_CUDA(cudaEventRecord(e0, s));
-                const int reps = 5;
-                for (int r = 0; r < reps; ++r)
-                    k_batch_probe<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, nt, 0.5f,
-                                                                  0.5f, b->d_sink);
-                CP_CUDA(cudaEventRecord(e1, s));
-                CP_CUDA(cudaEventSynchronize(e1));
-                CP_CUDA(cudaGetLastError());
-                float ms = 0;
-                CP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-                const double t = ms / reps;
-                if (t < best) {
-                    best = t;
-                    best_S = S;
+                                                             b->d_sink, b->d_ptickets, b->d_psums);
+            CP_CUDA(cudaEventRecord(e1, s));
+            CP_CUDA(cudaEventSynchronize(e1));
+            CP_CUDA(cudaGetLastError());
+            float ms = 0;
+            CP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            return (double)ms / reps;
+        };
+        bool present[kBuckets] = {};
+        for (int sl : active) present[bucket_of(b->desc[sl].n_slices)] = true;
+        // coordinate descent: one bucket at a time against the whole set,
+        // largest buckets first (they carry most of the work)
+        const int cands[] = {4, 8, 16, 32, 64};
+        double best = active.empty() ? 0.0 : sweep();
+        for (int pass = 0; pass < 2 && !active.empty(); ++pass)
+            for (int bk = kBuckets - 1; bk >= 0; --bk) {
+                if (!present[bk]) continue;
+                const int keep = b->tile_slices[bk];
+                int best_S = keep;
+                for (int S : cands) {
+                    if (S == keep) continue;
+                    b->tile_slices[bk] = S;
+                    const double t = sweep();
+                    if (t < best) {
+                        best = t;
+                        best_S = S;
+                    }
                 }
+                b->tile_slices[bk] = best_S;
             }
-            b->tile_slices[bk] = best_S;
-            total += best;
-        }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        if (ms_per_sweep) *ms_per_sweep = total;
+        if (ms_per_sweep) *ms_per_sweep = best;
     });
 }
 
@@ -1292,6 +1352,13 @@ CP_API int cp_batch_progress(const cp_batch* b, int slot, int* phase, int* level
     if (phase) *phase = S.phase;
     if (level) *level = S.level;
     if (report) *report = report_of(S);
+    return CP_OK;
+}
+
+CP_API int cp_batch_last_run_ms(const cp_batch* b, double* ms) {
+    if (!b || !ms) return CP_ERR_INVALID;
+    if (b->running) return CP_ERR_BUSY;
+    *ms = b->last_run_ms;
     return CP_OK;
 }
 

@@ -261,6 +261,9 @@ CP_API int cp_batch_autotune(cp_batch* b, double* ms_per_sweep);
  * 4 w = K u, 5 CG iteration, 6 secant update, 7 Aitken, 8 plastic strains,
  * 9 done), load level, and the counters of its report so far. */
 CP_API int cp_batch_progress(const cp_batch* b, int slot, int* phase, int* level, cp_solve_report* report);
+/* Device time of the last completed run in milliseconds (CUDA events
+ * recorded on the batch's stream around the run's graph). */
+CP_API int cp_batch_last_run_ms(const cp_batch* b, double* ms);
 /* Counters of the batch since creation: graph trips and kernel launches. */
 CP_API int cp_batch_stats(const cp_batch* b, long long* trips, long long* kernel_launches, long long* runs);
 
