@@ -9,6 +9,7 @@ device is present.
 """
 import atexit
 import ctypes
+import os
 import weakref
 
 import numpy as np
@@ -111,6 +112,13 @@ class Mesh:
     def ring(cls, a, b, n_phi, n_r):
         m = cls()
         m._check(C.lib().cpx_mesh_gen_ring(m._h, a, b, n_phi, n_r))
+        return m
+
+    @classmethod
+    def load(cls, path):
+        """Mesh::loadFromFile: an .inp file (nodes, S3/S4 elements, *MPC borders)."""
+        m = cls()
+        m._check(C.lib().cpx_mesh_load_inp(m._h, os.fspath(path).encode()))
         return m
 
     @classmethod

@@ -56,6 +56,10 @@ CP_API int cpx_mesh_gen_ring(cpx_mesh* m, double a, double b, int n_phi, int n_r
     if (!m || n_phi < 3 || n_r <= 0 || !(b > a) || !(a > 0)) return CP_ERR_INVALID;
     return guard([&] { m->m.genRing(a, b, n_phi, n_r); });
 }
+CP_API int cpx_mesh_load_inp(cpx_mesh* m, const char* path) {
+    if (!m || !path) return CP_ERR_INVALID;
+    return guard([&] { m->m.loadFromFile(path); });
+}
 CP_API int cpx_mesh_split_t3(cpx_mesh* m) {
     if (!m) return CP_ERR_INVALID;
     return guard([&] { m->m.splitToTriangles(); });

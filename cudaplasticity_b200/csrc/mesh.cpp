@@ -3,7 +3,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <fstream>
+#include <sstream>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 #include "../../include/cuplast/Mesh.hpp"
@@ -328,6 +331,127 @@ double Mesh::elemSpace4(int e) const {
     s1 += node[elem4[4 * (e + 1) - 1]].x * node[elem4[4 * e]].y;
     s2 += node[elem4[4 * (e + 1) - 1]].y * node[elem4[4 * e]].x;
     return std::fabs(s1 - s2) * 0.5;
+}
+
+
+// ------------------------------------------------------------ .inp files --
+//
+// Mesh::loadFromFile (src/Mesh.cu:725-937), same reading rules:
+//  * a section starts at a line equal to "*NODE", starting with "*ELEMENT"
+//    (blocks of every "TYPE=S3" / "TYPE=S4" / "TYPE=S8R" in it) or equal to
+//    "*MPC"; its data lines run up to the first empty line or line starting
+//    with '*', and that line is consumed with the block (so a section header
+//    right after a block's last data line is not seen);
+//  * commas count as blanks; node lines are "id x y ...", element lines
+//    "id n1 n2 ..." with 1-based ids; the element id is ignored;
+//  * consecutive "*MPC" sections are the borders in order, one line per
+//    border node: its first four characters are blanked, the next integer is
+//    the node id;
+//  * every MPC section brings one reference node in the *NODE list, so the
+//    mesh has (node lines - MPC sections) nodes and node lines with a larger
+//    id are dropped.
+// Quadratic (S8R) elements are counted and rejected: this library has no
+// 8-node element.
+namespace {
+
+bool is_data(const std::string& l) { return !l.empty() && l[0] != '*'; }
+
+std::string blank_commas(std::string l) {
+    for (char& c : l)
+        if (c == ',') c = ' ';
+    return l;
+}
+
+}  // namespace
+
+bool Mesh::loadFromFile(const std::string& fileName) {
+    if (fileName.size() < 4 || fileName.substr(fileName.size() - 4) != ".inp")
+        throw std::out_of_range("unknown mesh file format (expected .inp)");
+    std::ifstream file(fileName);
+    if (!file) throw std::out_of_range("there is no such file: " + fileName);
+    std::vector<std::string> lines;
+    for (std::string l; std::getline(file, l);) lines.push_back(l);
+
+    std::vector<std::pair<int, vec2>> nodeLines;
+    std::vector<int> e3, e4;
+    int c8 = 0;
+    std::vector<std::vector<int>> borderLists;
+    size_t at = 0;
+    auto next = [&](std::string& l) {
+        if (at >= lines.size()) return false;
+        l = lines[at++];
+        return true;
+    };
+    // reads one data block; returns with `line` holding the consumed terminator
+    auto block = [&](std::string& line, auto&& onData) {
+        while (next(line)) {
+            if (!is_data(line)) return;
+            onData(line);
+        }
+        line.clear();
+    };
+    std::string line;
+    while (next(line)) {
+        if (line == "*NODE") {
+            block(line, [&](const std::string& l) {
+                std::istringstream ss(blank_commas(l));
+                int id = 0;
+                vec2 p;
+                ss >> id >> p.x >> p.y;
+                nodeLines.push_back({id - 1, p});
+            });
+        } else if (line.compare(0, 8, "*ELEMENT") == 0) {
+            // the scan goes on over the terminator of each block it reads
+            for (size_t i = 0; i < line.length(); ++i) {
+                if (line.compare(i, 5, "TYPE=") != 0) continue;
+                i += 5;
+                const bool t3 = line.compare(i, 2, "S3") == 0, t4 = line.compare(i, 2, "S4") == 0;
+                const bool t8 = line.compare(i, 3, "S8R") == 0;
+                if (!(t3 || t4 || t8)) continue;
+                const int nn = t3 ? 3 : (t4 ? 4 : 8);
+                std::vector<int>& dst = t3 ? e3 : e4;
+                block(line, [&](const std::string& l) {
+                    if (t8) {
+                        ++c8;
+                        return;
+                    }
+                    std::istringstream ss(blank_commas(l));
+                    int id = 0;
+                    ss >> id;
+                    for (int k = 0; k < nn; ++k) {
+                        int v = 0;
+                        ss >> v;
+                        dst.push_back(v - 1);
+                    }
+                });
+            }
+        } else if (line == "*MPC") {
+            for (;;) {
+                std::vector<int> b;
+                block(line, [&](const std::string& l) {
+                    std::string t = blank_commas(l);
+                    for (size_t k = 0; k < 4 && k < t.size(); ++k) t[k] = ' ';
+                    std::istringstream ss(t);
+                    int v = 0;
+                    ss >> v;
+                    b.push_back(v - 1);
+                });
+                borderLists.push_back(b);
+                if (line != "*MPC") break;
+            }
+        }
+    }
+    if (c8 > 0) throw std::invalid_argument("quadratic (S8R) elements are not supported");
+    const int nodes = (int)nodeLines.size() - (int)borderLists.size();
+    if (nodes <= 0) throw std::out_of_range("mesh file has no nodes");
+    std::vector<double> xy(2 * (size_t)nodes, 0.0);
+    for (const auto& nl : nodeLines)
+        if (nl.first >= 0 && nl.first < nodes) {
+            xy[2 * (size_t)nl.first] = nl.second.x;
+            xy[2 * (size_t)nl.first + 1] = nl.second.y;
+        }
+    assign(nodes, xy.data(), (int)(e3.size() / 3), e3.data(), (int)(e4.size() / 4), e4.data(), borderLists);
+    return true;
 }
 
 }  // namespace cuplast

@@ -55,6 +55,12 @@ public:
     double elemSpace3(int e) const;
     double elemSpace4(int e) const;
 
+    // src/Mesh.cu:725-937: a mesh from an .inp file (nodes, S3/S4 element
+    // blocks, *MPC border blocks); true when loaded. Throws
+    // std::out_of_range on a bad file, std::invalid_argument for quadratic
+    // (S8R) elements.
+    bool loadFromFile(const std::string& fileName);
+
     // Replaces the arrays (takes copies).
     void assign(int nodes, const double* xy, int c3, const int* e3, int c4, const int* e4,
                 const std::vector<std::vector<int>>& borderLists);

@@ -26,6 +26,10 @@ CP_API int cpx_mesh_gen_rect_with_hole(cpx_mesh* m, double x1, double x2, double
                                        int n1, int n2, int rad_n);
 /* Mesh::genRing (src/Mesh.cu:249-329) */
 CP_API int cpx_mesh_gen_ring(cpx_mesh* m, double a, double b, int n_phi, int n_r);
+/* Mesh::loadFromFile (src/Mesh.cu:725-937): an .inp file with *NODE, *ELEMENT
+ * (TYPE=S3, S4) and *MPC border blocks. CP_ERR_INVALID for a bad file,
+ * CP_ERR_UNSUPPORTED for quadratic (S8R) elements. */
+CP_API int cpx_mesh_load_inp(cpx_mesh* m, const char* path);
 /* every quad (n1,n2,n3,n4) -> triangles (n1,n2,n3), (n1,n3,n4) (extension) */
 CP_API int cpx_mesh_split_t3(cpx_mesh* m);
 CP_API int cpx_mesh_set(cpx_mesh* m, int node_count, const double* xy, int count3, const int* elem3, int count4,

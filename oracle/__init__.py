@@ -21,6 +21,9 @@ from . import cpbin
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "cpref")
+# the same harness with the reference's Mesh.cu built at -O0, for its .inp
+# loader (see the Makefile)
+REF_BIN_INP = os.path.join(HERE, "_ref", "cpref_inp")
 
 _lib = None
 
@@ -65,7 +68,7 @@ def run_oracle(lines, workdir=None):
         return cpbin.read(out)
 
 
-def run_reference(lines, threads=None, workdir=None):
+def run_reference(lines, threads=None, workdir=None, binary=None):
     """Runs the reference's CPU path through the harness (no GPU is used:
     the child sees no CUDA device, so the reference selects its CPU path)."""
     if not have_reference():
@@ -77,7 +80,8 @@ def run_reference(lines, threads=None, workdir=None):
     with tempfile.TemporaryDirectory(dir=workdir) as d:
         job, out = os.path.join(d, "job.txt"), os.path.join(d, "out.bin")
         _write_job(lines, job)
-        subprocess.run([REF_BIN, job, out], check=True, env=env, stdout=subprocess.DEVNULL)
+        subprocess.run([binary or REF_BIN, job, out], check=True, env=env, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL)
         return cpbin.read(out)
 
 

@@ -19,6 +19,7 @@
  *   mesh ring a b Nphi Nr order              (Mesh::genRing, src/Mesh.cu:249)
  *   mesh rect x1 x2 y1 y2 N1 N2 order        (Mesh::genRectangle, src/Mesh.cu:17)
  *   mesh file path.bin                       (arrays written by the test helpers)
+ *   mesh inp path.inp                        (Mesh::loadFromFile, src/Mesh.cu:725)
  *   material E nu h
  *   diagram linear E sigmaT K_T              (Material::setLinearPlast)
  *   diagram power E sigmaT A m               (Material::setPowerPlast)
@@ -31,6 +32,9 @@
  *   cg_eps e | outer_eps e | max_outer n | levels k (load factors k/n for k=1..n)
  *   dump_k 1 | dump_csr 1
  */
+#include <unistd.h>
+#include <csetjmp>
+#include <csignal>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -135,6 +139,9 @@ static Job parseJob(const char* path) {
     return j;
 }
 
+static sigjmp_buf g_trap;
+static void on_trap(int) { siglongjmp(g_trap, 1); }
+
 static void buildMesh(const Job& j, Mesh& mesh) {
     const auto& s = j.meshSpec;
     auto d = [&](int i) { return atof(s[i].c_str()); };
@@ -142,6 +149,29 @@ static void buildMesh(const Job& j, Mesh& mesh) {
     if (s[0] == "hole") mesh.genRectWithHole(d(1), d(2), d(3), d(4), d(5), n(6), n(7), (int)n(8));
     else if (s[0] == "ring") mesh.genRing(d(1), d(2), n(3), n(4), (int)n(5));
     else if (s[0] == "rect") mesh.genRectangle(d(1), d(2), d(3), d(4), n(5), n(6), (int)n(7));
+    else if (s[0] == "inp") {
+        // the reference looks the file up relative to the working directory
+        std::string path = s[1], dir = ".", name = path;
+        const size_t cut = path.rfind('/');
+        if (cut != std::string::npos) { dir = path.substr(0, cut); name = path.substr(cut + 1); }
+        if (chdir(dir.c_str()) != 0) { fprintf(stderr, "cannot enter %s\n", dir.c_str()); exit(2); }
+        mesh.useCuda = false;
+        // loadFromFile is declared bool but ends without a return (undefined
+        // behaviour). Built at -O0 (the cpref_inp binary) the compiler puts a
+        // trap instruction exactly there, after the whole load: catch it and
+        // come back with the loaded mesh.
+        struct sigaction sa = {}, old = {};
+        sa.sa_handler = on_trap;
+        sigemptyset(&sa.sa_mask);
+        sigaction(SIGILL, &sa, &old);
+        try {
+            if (sigsetjmp(g_trap, 1) == 0) mesh.loadFromFile(name);
+        } catch (const char* e) {
+            fprintf(stderr, "loadFromFile: %s\n", e);
+            exit(3);
+        }
+        sigaction(SIGILL, &old, nullptr);
+    }
     else if (s[0] == "file") {
         cpbin_file f;
         if (cpbin_read(s[1].c_str(), &f) != 0) { fprintf(stderr, "cannot read mesh file\n"); exit(2); }

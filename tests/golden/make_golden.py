@@ -14,7 +14,10 @@ available (``python tests/golden/make_golden.py``); it builds the harness
   and displacements of the VTK results shipped with the reference
   (data/holePlatePlastPow.vtk, data/solverTest.vtk);
 * ``ref_tables.json`` -- the strain energies of data/aitken_*.txt and the
-  stress-strain points of data/diagramPow.txt / diagramLin.txt.
+  stress-strain points of data/diagramPow.txt / diagramLin.txt;
+* ``inp_<name>.inp`` and ``inp_<name>.npz`` -- small .inp mesh files written
+  here (the reference ships none) and the arrays the reference's own
+  Mesh::loadFromFile makes of them.
 """
 import json
 import os
@@ -93,8 +96,74 @@ def shipped_fixtures():
         json.dump(tables, f, indent=1)
 
 
+def write_inp_files():
+    """Two .inp inputs: ``mixed`` (a 12 x 8 O-grid plate with every other quad
+    split into triangles, nodes listed out of order, four *MPC border blocks
+    with one reference node each, comment lines between sections) and
+    ``quirks`` (a section header right after a block's last data line, which
+    the reference's reader consumes with the block, a blank-line terminator,
+    comma-free lines, a file that ends inside an *MPC block)."""
+    sys.path.insert(0, ROOT)
+    import cudaplasticity_b200 as cp
+
+    m = cp.Mesh.rect_with_hole(-3.0, 3.0, -2.0, 2.0, 0.5, 12, 8).arrays()
+    xy, e4, borders = m["node_xy"], m["elem4"], m["borders"]
+    n = len(xy)
+    tri, quad = [], []
+    for k, q in enumerate(e4):
+        if k % 2 == 0:
+            tri += [(q[0], q[1], q[2]), (q[0], q[2], q[3])]
+        else:
+            quad.append(tuple(q))
+    rng = np.random.default_rng(5)
+    order = rng.permutation(n)
+    L = ["*HEADING", "mixed S3/S4 mesh for the loader pins", "*NODE"]
+    L += [f"{i + 1:6d}, {float(xy[i, 0])!r}, {float(xy[i, 1])!r}" for i in order]
+    L += [f"{n + b + 1:6d}, 0.0, 0.0" for b in range(len(borders))]  # one reference node per *MPC block
+    L += ["**", "*ELEMENT, TYPE=S3, ELSET=TRI"]
+    L += [f"{k + 1}, {a + 1}, {b + 1}, {c + 1}" for k, (a, b, c) in enumerate(tri)]
+    L += ["**", "*ELEMENT, TYPE=S4R, ELSET=QUAD"]
+    L += [f"{len(tri) + k + 1}, " + ", ".join(str(v + 1) for v in q) for k, q in enumerate(quad)]
+    L += ["**"]
+    for b, nodes in enumerate(borders):
+        L += ["*MPC"] + [f"BEAM, {v + 1}, {n + b + 1}" for v in nodes]
+    L += ["**", "*END"]
+    with open(os.path.join(OUT, "inp_mixed.inp"), "w") as f:
+        f.write("\n".join(L) + "\n")
+
+    r = cp.Mesh.rect(0.0, 2.0, 0.0, 1.0, 4, 2).arrays()
+    xy, e4, borders = r["node_xy"], r["elem4"], r["borders"]
+    n = len(xy)
+    L = ["*NODE"] + [f"{i + 1} {float(xy[i, 0])!r} {float(xy[i, 1])!r}" for i in range(n)]
+    L += [f"{n + b + 1} 9.0 9.0" for b in range(2)]
+    L += ["*ELEMENT, TYPE=S3"]  # consumed as the terminator of the *NODE block: its data lines are skipped
+    L += ["1, 1, 2, 3"]
+    L += ["", "*ELEMENT, TYPE=S4"] + [f"{k + 1} " + " ".join(str(v + 1) for v in q) for k, q in enumerate(e4)]
+    L += ["", "*MPC"] + [f"BEAM, {v + 1}, {n + 1}" for v in borders[0]]
+    L += ["*MPC"] + [f"BEAM, {v + 1}, {n + 2}" for v in borders[2]]
+    with open(os.path.join(OUT, "inp_quirks.inp"), "w") as f:
+        f.write("\n".join(L) + "\n")
+
+
+def inp_fixtures():
+    write_inp_files()
+    for name in ["mixed", "quirks"]:
+        r = oracle.run_reference(["mode mesh", "mesh inp " + os.path.join(OUT, f"inp_{name}.inp")],
+                                 binary=oracle.REF_BIN_INP)
+        np.savez_compressed(os.path.join(OUT, f"inp_{name}.npz"),
+                            **{k: r[k] for k in ["node_xy", "elem3", "elem4", "elem8", "border_len", "border_nodes"]})
+        print("inp", name, "nodes", len(r["node_xy"]) // 2, "tri", len(r["elem3"]) // 3, "quad", len(r["elem4"]) // 4,
+              "borders", list(r["border_len"]))
+
+
 if __name__ == "__main__":
     import tempfile
+
+    if "--inp" in sys.argv:  # only the .inp loader pins
+        if not oracle.have_reference():
+            oracle.build(with_reference=True)
+        inp_fixtures()
+        sys.exit(0)
 
     if not oracle.have_reference():
         oracle.build(with_reference=True)
@@ -102,3 +171,4 @@ if __name__ == "__main__":
         scenario_fixtures(d)
     mesh_fixtures()
     shipped_fixtures()
+    inp_fixtures()

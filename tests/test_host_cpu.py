@@ -104,3 +104,34 @@ def test_device_calls_fail_cleanly_without_gpu():
     with pytest.raises(cp.CuplastError) as e:
         cp.Context(0)
     assert e.value.status == _capi.CP_ERR_NO_DEVICE
+
+
+@pytest.mark.parametrize("name", ["mixed", "quirks"])
+def test_inp_loader_matches_reference(name, golden_dir):
+    """Mesh::loadFromFile (src/Mesh.cu:725-937): the product's reader gives
+    the arrays the reference's own reader made of the same file, bit for bit
+    (fixtures from tests/golden/make_golden.py). ``quirks`` covers the
+    reference's rule that a block's terminating line is consumed with it."""
+    g = dict(np.load(os.path.join(golden_dir, f"inp_{name}.npz")))
+    a = cp.Mesh.load(os.path.join(golden_dir, f"inp_{name}.inp")).arrays()
+    assert np.array_equal(a["node_xy"].ravel(), g["node_xy"])
+    assert np.array_equal(a["elem3"].ravel(), g["elem3"])
+    assert np.array_equal(a["elem4"].ravel(), g["elem4"])
+    assert len(g["elem8"]) == 0
+    assert [len(b) for b in a["borders"]] == list(g["border_len"])
+    assert np.array_equal(np.concatenate(a["borders"]), g["border_nodes"])
+
+
+def test_inp_loader_rejects_bad_files(tmp_path):
+    with pytest.raises(cp.CuplastError) as e:
+        cp.Mesh.load(tmp_path / "mesh.msh")
+    assert e.value.status == _capi.CP_ERR_INVALID
+    with pytest.raises(cp.CuplastError) as e:
+        cp.Mesh.load(tmp_path / "missing.inp")
+    assert e.value.status == _capi.CP_ERR_INVALID
+    q8 = tmp_path / "q8.inp"
+    q8.write_text("*NODE\n" + "".join(f"{i + 1}, {i % 3}.0, {i // 3}.0\n" for i in range(9)) +
+                  "**\n*ELEMENT, TYPE=S8R\n1, 1, 3, 9, 7, 2, 6, 8, 4\n")
+    with pytest.raises(cp.CuplastError) as e:
+        cp.Mesh.load(q8)
+    assert e.value.status == _capi.CP_ERR_UNSUPPORTED
