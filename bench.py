@@ -271,7 +271,7 @@ def batched_leg(ctx, window_s=20.0, warm_s=3.0, slots=512, pool_size=768, seed=2
     }
 
 
-def compare_leg(ctx, n_requests, max_outer=300, seed=20261203):
+def compare_leg(ctx, n_requests, max_outer=100, seed=20261203):
     """Like for like: the plain FP64 drop-in solves the first n requests of
     the config-4 stream one at a time; the batched mixed-precision engine
     then solves exactly the same requests (fresh instances) to completion.
@@ -296,9 +296,12 @@ def compare_leg(ctx, n_requests, max_outer=300, seed=20261203):
         w, inst = make(k)
         t1 = time.perf_counter()
         rep = inst.solve(allow_not_converged=True, precision=cp.CP_PREC_FP64, levels=1, **kw)
-        t_plain += time.perf_counter() - t1
+        dt = time.perf_counter() - t1
+        t_plain += dt
         plain[k] = (inst.state(), rep, w["params"]["dof"])
         inst.close()
+        print(json.dumps({"compare_plain": k, "dof": w["params"]["dof"], "seconds": dt, "status": rep["status"],
+                          "outer": rep["outer_iters"], "cg": rep["cg_iters"]}), flush=True)
     ids = sorted(plain)
     insts = {i: make(i)[1] for i in ids}
     b = cp.Batch(ctx, max_instances=len(ids))
@@ -667,7 +670,7 @@ def main():
     ap.add_argument("--batched-window", type=float, default=20.0, help="seconds counted in the saturation run")
     ap.add_argument("--compare", type=int, metavar="N",
                     help="like-for-like run only: the first N config-4 requests, plain FP64 one at a time vs batched")
-    ap.add_argument("--compare-max-outer", type=int, default=300)
+    ap.add_argument("--compare-max-outer", type=int, default=100)
     ap.add_argument("--serve-rate", type=float, default=10.0, help="Poisson arrival rate of the served leg")
     ap.add_argument("--serve-window", type=float, default=20.0, help="seconds of arrivals in the served leg")
     ap.add_argument("--batched-probe", type=int, nargs=2, metavar=("N", "TRIPS"),

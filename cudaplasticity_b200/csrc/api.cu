@@ -217,8 +217,64 @@ void run_cg_loop(cp_instance* I, const cp::CgArgs<T>& a, cudaGraphExec_t g) {
     }
 }
 
+// FP64 CG, one launch per iteration (cg_fused.cu).
+void cg_fp64_fused(cp_instance* I, double eps, long long max_iter, int precond) {
+    const int n = I->n_nodes;
+    if (!I->f_r) {
+        I->f_r = I->alloc<double2>(n);
+        I->f_w = I->alloc<double2>(n);
+        I->f_p = I->alloc<double2>(n);
+        I->f_kp = I->alloc<double2>(n);
+        I->f_g = I->alloc<double2>(6 * (size_t)n);
+        I->f_partials = I->alloc<double>(6 * (size_t)I->max_blocks);
+    }
+    if (precond && !I->minv64) (void)I->cg_args<double>(1);  // allocates the block-Jacobi inverse
+    cp::FusedArgs a;
+    a.n = n;
+    a.sm_count = I->sms();
+    a.max_blocks = I->max_blocks;
+    a.slice_ptr = I->csr.slice_ptr;
+    a.scol = I->csr.scol;
+    a.val = I->csr.val64;
+    a.b = I->b;
+    a.mask = I->mask;
+    a.x = I->u;
+    a.r = I->f_r;
+    a.w = I->f_w;
+    a.p = I->f_p;
+    a.kp = I->f_kp;
+    a.gA = I->f_g;
+    a.gB = I->f_g + 3 * (size_t)n;
+    a.minv = precond ? I->minv64 : nullptr;
+    a.precond = precond;
+    a.sc = I->sc;
+    a.partials = I->f_partials;
+    if (I->use_graph && !I->gf[precond]) I->gf[precond] = cp::fused_build_while_graph(a, I->body_iters, I->s());
+    cp::fused_launch_start(a, eps * eps, max_iter, I->s());
+    I->launches += 2;
+    if (I->use_graph) {
+        CP_CUDA(cudaGraphLaunch(I->gf[precond], I->s()));
+        CP_CUDA(cudaMemcpyAsync(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost, I->s()));
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+        const long long trips = std::max<long long>(1, (I->sc_h->iter + I->body_iters - 1) / I->body_iters);
+        I->launches += trips * (I->body_iters + 1);
+        return;
+    }
+    for (;;) {
+        for (int it = 0; it < I->body_iters; ++it) cp::fused_launch_iteration(a, it & 1, I->s());
+        I->launches += I->body_iters;
+        CP_CUDA(cudaMemcpyAsync(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost, I->s()));
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+        if (I->sc_h->converged || I->sc_h->status) return;
+    }
+}
+
 // Reference-semantics FP64 CG from the current u.
 void cg_fp64(cp_instance* I, double eps, long long max_iter, int precond = 0) {
+    if (I->fused_fp64) {
+        cg_fp64_fused(I, eps, max_iter, precond);
+        return;
+    }
     auto a = I->cg_args<double>(precond);
     if (I->use_graph && !I->g64[precond]) I->g64[precond] = cp::cg_build_while_graph<double>(a, I->body_iters, I->s());
     cp::cg_launch_init<double>(a, I->csr.val64, true, eps * eps, max_iter, 0, -1.0, I->s());
@@ -358,6 +414,7 @@ CP_API int cp_instance_create(cp_context* ctx, const cp_mesh_view* mv, const cp_
     if (!I) return CP_ERR_NOMEM;
     I->ctx = ctx;
     if (const char* g = std::getenv("CUPLAST_NO_GRAPH")) I->use_graph = !(g[0] == '1');
+    if (const char* g = std::getenv("CUPLAST_FP64_CG")) I->fused_fp64 = std::strcmp(g, "classic") != 0;
     int rc = guarded(ctx, [&] {
         CP_CHECK(mv->node_count > 0 && mv->node_xy, CP_ERR_INVALID, "mesh: no nodes");
         CP_CHECK(mv->count3 >= 0 && mv->count4 >= 0 && mv->count3 + mv->count4 > 0, CP_ERR_INVALID,
@@ -462,6 +519,7 @@ CP_API int cp_instance_destroy(cp_instance* I) {
     for (int k = 0; k < 2; ++k) {
         if (I->g64[k]) cudaGraphExecDestroy(I->g64[k]);
         if (I->g32[k]) cudaGraphExecDestroy(I->g32[k]);
+        if (I->gf[k]) cudaGraphExecDestroy(I->gf[k]);
     }
     for (void* p : I->allocs) cudaFreeAsync(p, I->ctx->stream);
     if (I->sc_h) cudaFreeHost(I->sc_h);

@@ -103,9 +103,9 @@ struct BState {
     int phase, status, level, levels_done;
     int outer_it, outer_total, parity, res_kind;  // res_kind: 0 first residual of a solve, 1 replacement
     unsigned int ticket;
-    int pad;
+    int stalls;  // consecutive FP64 residual replacements without a 2x reduction
     long long iter, lin_iters, cg_total, fp64_spmv;
-    double rr, gamma, alpha, beta, rr_ref, eps2_inner, bb, res64;
+    double rr, gamma, alpha, beta, rr_ref, eps2_inner, bb, res64, res_last;
     double eps, rel_err, w_prev, omega, cg_rel_res;
     unsigned long long t_first, t_done;  // %globaltimer, ns
 };
@@ -318,10 +318,21 @@ __device__ void tile_res(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh
         const double bb = S->bb;
         S->res64 = res64;
         S->cg_rel_res = bb > 0.0 ? sqrt(res64 / bb) : 0.0;
+        // FP32 limit: on very ill-conditioned systems (kappa * eps32 >~ 1) the
+        // recursive FP32 residual keeps falling while the FP64 residual no
+        // longer does. Two replacements in a row without halving the FP64
+        // residual norm end the linear solve with the best x so far (the
+        // secant iteration goes on) instead of iterating to the cap.
+        if (first) {
+            S->stalls = 0;
+        } else {
+            S->stalls = res64 < 0.25 * S->res_last ? 0 : S->stalls + 1;
+        }
+        S->res_last = res64;
         if (!(rr == rr) || !(bb == bb) || !(res64 == res64)) {
             finish(S, c, CP_ERR_BREAKDOWN);
-        } else if (res64 <= S->eps * S->eps * bb || rr == 0.0 || S->lin_iters >= d.max_cg) {
-            set_phase(S, c, PH_UPD);  // the linear solve meets its tolerance (or its cap)
+        } else if (res64 <= S->eps * S->eps * bb || rr == 0.0 || S->lin_iters >= d.max_cg || S->stalls >= 2) {
+            set_phase(S, c, PH_UPD);  // the linear solve meets its tolerance (or its cap, or stalls)
         } else {
             S->rr = rr;
             S->rr_ref = rr;
@@ -387,7 +398,11 @@ __device__ void tile_w(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, 
         const double den = t[1] + beta * (t[3] + t[4]) + beta * beta * t[5];
         const double alpha = g / den;
         if (!(den > 0.0) || !(g > 0.0) || !(alpha == alpha)) {
-            finish(S, c, CP_ERR_BREAKDOWN);
+            // at the start of a solve the FP32 system is not positive
+            // definite: a breakdown; after a replacement only the FP32 step
+            // degenerated, and the solve ends with the x it has
+            if (S->res_kind == 0) finish(S, c, CP_ERR_BREAKDOWN);
+            else set_phase(S, c, PH_UPD);
         } else {
             S->gamma = g;
             S->alpha = alpha;

@@ -50,6 +50,29 @@ struct CgArgs {
     double* partials = nullptr;     // >= 3 * max_blocks doubles
 };
 
+// The single-launch FP64 iteration of cg_fused.cu.
+struct FusedArgs {
+    int n = 0;
+    int sm_count = 148;
+    int max_blocks = 0;              // capacity of partials (blocks, 6 sums each)
+    const int* slice_ptr = nullptr;
+    const int* scol = nullptr;
+    const double* val = nullptr;
+    const double2* b = nullptr;
+    const uchar2* mask = nullptr;
+    double2* x = nullptr;
+    double2 *r = nullptr, *w = nullptr, *p = nullptr, *kp = nullptr;
+    double2 *gA = nullptr, *gB = nullptr;  // per node: u, M w, M kp (by parity)
+    double4* minv = nullptr;
+    int precond = 0;
+    CgScalars* sc = nullptr;
+    double* partials = nullptr;
+};
+
+void fused_launch_start(const FusedArgs& a, double eps2, long long max_iter, cudaStream_t s);
+void fused_launch_iteration(const FusedArgs& a, int parity, cudaStream_t s);
+cudaGraphExec_t fused_build_while_graph(const FusedArgs& a, int body_iters, cudaStream_t s);
+
 template <typename T>
 void cg_launch_init(const CgArgs<T>& a, const void* valA, bool valA_is_fp64, double eps2, long long max_iter,
                     int relative_to_r0, double outer_eps2, cudaStream_t s);

@@ -1,0 +1,331 @@
+// FP64 masked (P)CG of one instance with one launch per iteration.
+//
+// Same solve as ConjGradCuda::solve (src/ConjGradCuda.cu:185-231) and as the
+// two-kernel loop of cg.cu: r0 = m.(b - K x0), stop when (r, r) / (b, b) <=
+// eps^2, the caller's x carries the last iterate. The iteration is arranged
+// so that both inner products are taken together (Chronopoulos-Gear): with
+// M the 2x2 block-Jacobi inverse (the Dirichlet mask without
+// preconditioning), u = M r, w = K u, p the direction and kp = K p,
+//   p' = u + beta p, kp' = w + beta kp, x += alpha p', r' = m.(r - alpha kp'),
+//   u' = u - alpha (M w + beta M kp), w' = K u',
+//   gamma' = (r', u'), beta' = gamma' / gamma,
+//   alpha' = gamma' / (K p'', p''), (K p'', p'') = (w', u')
+//            + beta' ((w', p') + (kp', u')) + beta'^2 (kp', p').
+// K u' needs the neighbours' new u; each thread recomputes it from the
+// neighbours' u, M w, M kp, kept in one 48-byte record per node and
+// double-buffered by iteration parity, so an iteration is one kernel and one
+// deterministic cross-block reduction (last block, index order). The
+// scalars stay on the device; the loop runs in a CUDA graph with a WHILE
+// node, as in cg.cu.
+#include <mutex>
+#include <unordered_map>
+
+#include "cg.h"
+#include "common.cuh"
+#include "internal.h"
+
+namespace cp {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kSums = 6;
+
+__device__ __forceinline__ double2 mvec(const double4& m, double2 v) {
+    return make_double2(m.x * v.x + m.y * v.y, m.z * v.x + m.w * v.y);
+}
+
+__device__ __forceinline__ double2 apply_m(const FusedArgs& a, int n, double2 v) {
+    if (a.precond) return mvec(a.minv[n], v);
+    const uchar2 m = a.mask[n];
+    return make_double2(m.x ? v.x : 0.0, m.y ? v.y : 0.0);
+}
+
+__device__ __forceinline__ double2 load_lo(const double* val, long long b) {
+    return __ldg(reinterpret_cast<const double2*>(val + 4 * b));
+}
+__device__ __forceinline__ double2 load_hi(const double* val, long long b) {
+    return __ldg(reinterpret_cast<const double2*>(val + 4 * b) + 1);
+}
+
+#define CPF_SLICE_LOOP                                                                          \
+    const int lane = threadIdx.x & 31;                                                          \
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;                              \
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;                                           \
+    for (int sl = warp; sl < (a.n + 31) / 32; sl += nwarps)
+
+// Block sums of up to kSums values into partials[kSums * block]; true in the
+// last block to arrive, which then holds the totals in out (thread 0).
+__device__ __forceinline__ bool reduce_sums(const FusedArgs& a, double* v, int k, double* out, double* sh,
+                                            bool* last) {
+    for (int i = 0; i < k; i += 2) {
+        const double2 s = block_sum2(v[i], i + 1 < k ? v[i + 1] : 0.0, sh);
+        if (threadIdx.x == 0) {
+            a.partials[kSums * blockIdx.x + i] = s.x;
+            if (i + 1 < k) a.partials[kSums * blockIdx.x + i + 1] = s.y;
+        }
+    }
+    if (!last_block_arrive(&a.sc->ticket, last)) return false;
+    double t[kSums];
+    for (int i = 0; i < k; ++i) t[i] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+        const volatile double* p = a.partials + kSums * b;
+        for (int i = 0; i < k; ++i) t[i] += p[i];
+    }
+    for (int i = 0; i < k; i += 2) {
+        const double2 s = block_sum2(t[i], i + 1 < k ? t[i + 1] : 0.0, sh);
+        out[i] = s.x;
+        if (i + 1 < k) out[i + 1] = s.y;
+    }
+    return true;
+}
+
+// r = m.(b - K x), block-Jacobi inverse, u = M r, p = kp = 0, the parity-0
+// record (u, -, 0); sums (r, r), (b, b).
+__global__ void __launch_bounds__(kThreads) k_f_init(FusedArgs a, double eps2, long long max_iter) {
+    __shared__ double sh[2 * kThreads / 32];
+    __shared__ bool last;
+    double v[2] = {0.0, 0.0};
+    CPF_SLICE_LOOP {
+        const int n = 32 * sl + lane;
+        if (n >= a.n) continue;
+        const int base = a.slice_ptr[sl], wd = (a.slice_ptr[sl + 1] - base) >> 5;
+        double k0 = 0.0, k1 = 0.0;
+        for (int k = 0; k < wd; ++k) {
+            const long long bi = base + 32LL * k + lane;
+            const int col = __ldg(a.scol + bi);
+            const double2 lo = load_lo(a.val, bi), hi = load_hi(a.val, bi);
+            const double2 xc = a.x[col];
+            k0 += lo.x * xc.x + lo.y * xc.y;
+            k1 += hi.x * xc.x + hi.y * xc.y;
+        }
+        const double2 bb = a.b[n];
+        const uchar2 m = a.mask[n];
+        const double2 r = make_double2(m.x ? bb.x - k0 : 0.0, m.y ? bb.y - k1 : 0.0);
+        a.r[n] = r;
+        if (a.precond) {
+            const double2 lo = load_lo(a.val, base + lane), hi = load_hi(a.val, base + lane);
+            double i00 = 0, i01 = 0, i10 = 0, i11 = 0;
+            if (m.x && m.y) {
+                const double det = lo.x * hi.y - lo.y * hi.x;
+                i00 = hi.y / det; i01 = -lo.y / det; i10 = -hi.x / det; i11 = lo.x / det;
+            } else if (m.x) {
+                i00 = 1.0 / lo.x;
+            } else if (m.y) {
+                i11 = 1.0 / hi.y;
+            }
+            a.minv[n] = make_double4(i00, i01, i10, i11);
+        }
+        const double2 u = apply_m(a, n, r);
+        const double2 z = make_double2(0.0, 0.0);
+        a.p[n] = z;
+        a.kp[n] = z;
+        a.gA[3 * (size_t)n] = u;
+        a.gA[3 * (size_t)n + 2] = z;
+        v[0] += r.x * r.x + r.y * r.y;
+        v[1] += bb.x * bb.x + bb.y * bb.y;
+    }
+    double t[kSums];
+    if (!reduce_sums(a, v, 2, t, sh, &last)) return;
+    if (threadIdx.x == 0) {
+        CgScalars* sc = a.sc;
+        const double rr = t[0], bb = t[1];
+        sc->rr = rr;
+        sc->bb = bb;
+        sc->res64 = rr;
+        sc->normB_inv = bb > 0.0 ? 1.0 / bb : 0.0;
+        sc->eps2 = eps2;
+        sc->iter = 0;
+        sc->max_iter = max_iter;
+        sc->status = 0;
+        sc->lin_done = 0;
+        sc->alpha = sc->beta = 0.0;
+        sc->converged = (rr == 0.0 || rr * sc->normB_inv <= eps2) ? 1 : 0;
+        if (!(rr == rr) || !(bb == bb)) sc->status = CP_ERR_BREAKDOWN;
+        sc->ticket = 0;
+    }
+}
+
+// w = K u (u from the parity-0 records), M w into the record; gamma = (r, u),
+// delta = (w, u): the first step.
+__global__ void __launch_bounds__(kThreads) k_f_w(FusedArgs a) {
+    __shared__ double sh[2 * kThreads / 32];
+    __shared__ bool last;
+    CgScalars* sc = a.sc;
+    if (sc->converged || sc->status) return;
+    double v[2] = {0.0, 0.0};
+    CPF_SLICE_LOOP {
+        const int n = 32 * sl + lane;
+        if (n >= a.n) continue;
+        const int base = a.slice_ptr[sl], wd = (a.slice_ptr[sl + 1] - base) >> 5;
+        double k0 = 0.0, k1 = 0.0;
+        for (int k = 0; k < wd; ++k) {
+            const long long bi = base + 32LL * k + lane;
+            const int col = __ldg(a.scol + bi);
+            const double2 lo = load_lo(a.val, bi), hi = load_hi(a.val, bi);
+            const double2 uc = a.gA[3 * (size_t)col];
+            k0 += lo.x * uc.x + lo.y * uc.y;
+            k1 += hi.x * uc.x + hi.y * uc.y;
+        }
+        const double2 w = make_double2(k0, k1);
+        a.w[n] = w;
+        a.gA[3 * (size_t)n + 1] = apply_m(a, n, w);
+        const double2 u = a.gA[3 * (size_t)n], r = a.r[n];
+        v[0] += r.x * u.x + r.y * u.y;
+        v[1] += w.x * u.x + w.y * u.y;
+    }
+    double t[kSums];
+    if (!reduce_sums(a, v, 2, t, sh, &last)) return;
+    if (threadIdx.x == 0) {
+        const double g = t[0], d = t[1];
+        sc->rho = g;
+        sc->alpha = g / d;
+        sc->beta = 0.0;
+        if (!(d > 0.0) || !(sc->alpha == sc->alpha)) sc->status = CP_ERR_BREAKDOWN;
+        sc->ticket = 0;
+    }
+}
+
+// One iteration (see the file comment); parity selects the record buffers.
+__global__ void __launch_bounds__(kThreads) k_f_iter(FusedArgs a, int parity) {
+    __shared__ double sh[2 * kThreads / 32];
+    __shared__ bool last;
+    CgScalars* sc = a.sc;
+    if (sc->converged || sc->status) return;
+    const double2* __restrict__ go = parity ? a.gB : a.gA;
+    double2* __restrict__ gn = parity ? a.gA : a.gB;
+    const double al = sc->alpha, bt = sc->beta;
+    double v[kSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    CPF_SLICE_LOOP {
+        const int n = 32 * sl + lane;
+        if (n >= a.n) continue;
+        const int base = a.slice_ptr[sl], wd = (a.slice_ptr[sl + 1] - base) >> 5;
+        const double2 u0 = __ldg(go + 3 * (size_t)n), mw0 = __ldg(go + 3 * (size_t)n + 1),
+                      mk0 = __ldg(go + 3 * (size_t)n + 2);
+        const double2 pn = a.p[n], wn = a.w[n], kn = a.kp[n];
+        const uchar2 m = a.mask[n];
+        const double2 p = make_double2(u0.x + bt * pn.x, u0.y + bt * pn.y);
+        const double2 kp = make_double2(wn.x + bt * kn.x, wn.y + bt * kn.y);
+        const double2 u = make_double2(u0.x - al * (mw0.x + bt * mk0.x), u0.y - al * (mw0.y + bt * mk0.y));
+        double2 x = a.x[n];
+        x.x += al * p.x;
+        x.y += al * p.y;
+        double2 r = a.r[n];
+        if (m.x) r.x -= al * kp.x;
+        if (m.y) r.y -= al * kp.y;
+        double k0 = 0.0, k1 = 0.0;
+#pragma unroll 3
+        for (int k = 0; k < wd; ++k) {
+            const long long bi = base + 32LL * k + lane;
+            const int col = __ldg(a.scol + bi);
+            const double2 lo = load_lo(a.val, bi), hi = load_hi(a.val, bi);
+            const double2 uc = __ldg(go + 3 * (size_t)col), mwc = __ldg(go + 3 * (size_t)col + 1),
+                          mkc = __ldg(go + 3 * (size_t)col + 2);
+            const double ux = uc.x - al * (mwc.x + bt * mkc.x), uy = uc.y - al * (mwc.y + bt * mkc.y);
+            k0 += lo.x * ux + lo.y * uy;
+            k1 += hi.x * ux + hi.y * uy;
+        }
+        const double2 w = make_double2(k0, k1);
+        a.p[n] = p;
+        a.kp[n] = kp;
+        a.x[n] = x;
+        a.r[n] = r;
+        a.w[n] = w;
+        gn[3 * (size_t)n] = u;
+        gn[3 * (size_t)n + 1] = apply_m(a, n, w);
+        gn[3 * (size_t)n + 2] = apply_m(a, n, kp);
+        v[0] += r.x * u.x + r.y * u.y;
+        v[1] += w.x * u.x + w.y * u.y;
+        v[2] += r.x * r.x + r.y * r.y;
+        v[3] += (w.x * p.x + w.y * p.y) + (kp.x * u.x + kp.y * u.y);
+        v[4] += kp.x * p.x + kp.y * p.y;
+    }
+    double t[kSums];
+    if (!reduce_sums(a, v, 5, t, sh, &last)) return;
+    if (threadIdx.x == 0) {
+        const double g = t[0], rn = t[2];
+        const double beta = g / sc->rho;
+        const double den = t[1] + beta * t[3] + beta * beta * t[4];
+        sc->iter += 1;
+        sc->rr = rn;
+        sc->beta = beta;
+        sc->alpha = g / den;
+        sc->rho = g;
+        if (rn * sc->normB_inv <= sc->eps2) sc->converged = 1;
+        else if (sc->iter >= sc->max_iter) sc->status = CP_ERR_NOT_CONVERGED;
+        else if (!(den > 0.0) || !(g > 0.0)) sc->status = CP_ERR_BREAKDOWN;
+        if (!(rn == rn)) sc->status = CP_ERR_BREAKDOWN;
+        sc->ticket = 0;
+    }
+}
+
+__global__ void k_f_condition(const CgScalars* sc, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, (sc->converged || sc->status) ? 0u : 1u);
+}
+
+template <typename K>
+int fused_grid(K kernel, int n, int sm_count) {
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> cache;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find((const void*)kernel);
+        if (it != cache.end()) per_sm = it->second;
+    }
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        std::lock_guard<std::mutex> lock(mu);
+        cache[(const void*)kernel] = per_sm;
+    }
+    long long g = (n + kThreads - 1) / kThreads;
+    const long long cap = (long long)sm_count * per_sm;
+    if (g > cap) g = cap;
+    return g < 1 ? 1 : (int)g;
+}
+
+}  // namespace
+
+void fused_launch_start(const FusedArgs& a, double eps2, long long max_iter, cudaStream_t s) {
+    const int g1 = fused_grid(k_f_init, a.n, a.sm_count), g2 = fused_grid(k_f_w, a.n, a.sm_count);
+    CP_CHECK(g1 <= a.max_blocks && g2 <= a.max_blocks, CP_ERR_INVALID, "partials buffer too small");
+    k_f_init<<<g1, kThreads, 0, s>>>(a, eps2, max_iter);
+    k_f_w<<<g2, kThreads, 0, s>>>(a);
+    CP_CUDA(cudaGetLastError());
+}
+
+void fused_launch_iteration(const FusedArgs& a, int parity, cudaStream_t s) {
+    const int g = fused_grid(k_f_iter, a.n, a.sm_count);
+    CP_CHECK(g <= a.max_blocks, CP_ERR_INVALID, "partials buffer too small");
+    k_f_iter<<<g, kThreads, 0, s>>>(a, parity);
+    CP_CUDA(cudaGetLastError());
+}
+
+// "while (!converged) { body_iters x iteration }" as a graph with a WHILE
+// node; body_iters must be even (record parity).
+cudaGraphExec_t fused_build_while_graph(const FusedArgs& a, int body_iters, cudaStream_t s) {
+    cudaGraph_t g;
+    CP_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    CP_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CP_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CP_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    for (int it = 0; it < body_iters; ++it) fused_launch_iteration(a, it & 1, s);
+    k_f_condition<<<1, 1, 0, s>>>(a.sc, h);
+    cudaGraph_t captured = nullptr;
+    CP_CUDA(cudaStreamEndCapture(s, &captured));
+    cudaGraphExec_t exec;
+    CP_CUDA(cudaGraphInstantiate(&exec, g, 0));
+    CP_CUDA(cudaGraphDestroy(g));
+    return exec;
+}
+
+}  // namespace cp

@@ -45,6 +45,11 @@ struct cp_instance {
     bool use_graph = true;  // CG loop as a CUDA graph with a device-side WHILE condition
     bool loads_set = false;
     bool in_batch = false;  // owned by a cp_batch until harvested: no other call may touch it
+    // single-launch FP64 CG (cg_fused.cu), allocated on first use
+    bool fused_fp64 = true;  // false (CUPLAST_FP64_CG=classic): the two-kernel loop of cg.cu
+    double2 *f_r = nullptr, *f_w = nullptr, *f_p = nullptr, *f_kp = nullptr, *f_g = nullptr;
+    double* f_partials = nullptr;
+    cudaGraphExec_t gf[2] = {nullptr, nullptr};  // [precond]
     long long launches = 0;  // kernels launched (graph nodes included)
     int last_assembly = -1;  // precision of the last assembly
     size_t bytes = 0;
