@@ -1,7 +1,7 @@
 """Benchmark: converged plastic solves per second on one B200 (per GPU, replicas).
 
-Workload (configuration "plain method, small", the reference's CPU-runnable
-case): plane-stress 200 x 200 mm plate with a centred 20 mm hole, O-grid of 64
+Workload (the plain method on the small plate, which the reference's CPU path
+runs): plane-stress 200 x 200 mm plate with a centred 20 mm hole, O-grid of 64
 circumferential x 64 radial quads (4160 nodes, 8320 DOF), E = 210 GPa, nu = 0.3,
 bilinear hardening sigma_y = 250 MPa, E_t = 2 GPa; 200 MPa traction on the top
 edge in 10 equal increments; bottom edge fixed in y, bottom-left node fixed;
@@ -9,16 +9,17 @@ CG tolerance 1e-10, outer (secant) tolerance 1e-6. Quads on the O-grid nodes:
 the reference has no triangle element. Synthetic, seeded-free (deterministic).
 
 One step = one complete solve (all 10 load levels to convergence). The product
-arm runs the FP64 drop-in path (Aitken-relaxed secant iteration, block-Jacobi
+arm runs the FP64 drop-in path (one launch per CG iteration; Aitken-relaxed
+secant iteration, block-Jacobi
 PCG with the linear tolerance following the outer error; same fixed point as
 the reference). ``--impl reference`` runs the reference implementation's own
 CPU path (oracle/_ref/cpref, built from its sources) on the same job with all
 host cores.
 
 Beside the headline, the line carries the batched and served forms on the
-seeded config-4 / config-5 request streams (cudaplasticity_b200/workload.py):
+seeded request streams of cudaplasticity_b200/workload.py:
   batched  closed-loop saturation throughput of the batched mixed-precision
-           engine: a batch of 512 resident instances of the config-4 stream
+           engine: a batch of 512 resident instances of the batch stream
            (DOF log-uniform in [2k, 200k], plates and rings, 5-segment
            diagrams), refilled from the stream as solves finish, converged
            solves counted over a fixed window; the SpMV sweep over all 512
@@ -26,7 +27,7 @@ seeded config-4 / config-5 request streams (cudaplasticity_b200/workload.py):
   plain    the plain FP64 drop-in, one request at a time, on a seeded sample
            of the requests the batched window completed (same solver
            options), and the mixed-precision results' error against it;
-  served   the solve service (cp_server) under Poisson arrivals of config-5
+  served   the solve service (cp_server) under Poisson arrivals of the served stream
            requests (DOF log-uniform in [2k, 500k], 5-30 load increments),
            host buffers in and results out: solves/s and p50/p99 latency.
 
@@ -46,12 +47,12 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = dict(workload="config1_hole_plate_ogrid64x64_q4", plate_mm=200, hole_radius_mm=20, n_circ=64, n_rad=64,
+WORKLOAD = dict(workload="hole_plate_ogrid64x64_q4_8320dof", plate_mm=200, hole_radius_mm=20, n_circ=64, n_rad=64,
                 nodes=4160, dof=8320, elements=4096, E_mpa=210000, nu=0.3, sigma_y=250, E_t=2000, traction_mpa=200,
                 increments=10, cg_tol=1e-10, outer_tol=1e-6)
 SOLVE_KW = dict(cg_tol=1e-10, outer_tol=1e-6, max_outer=2000, levels=10, aitken=1, adaptive_cg=1, precond=1,
                 max_cg=2_000_000)
-METRIC = "converged solves/s (config-1 plate, FP64, <=1e-6 outer / 1e-10 CG)"
+METRIC = "converged solves/s (200 mm plate, 20 mm hole, 64x64 O-grid, 8320 DOF, FP64, <=1e-6 outer / 1e-10 CG)"
 
 
 def build_problem():
@@ -173,7 +174,7 @@ def run_reference_arm(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": WORKLOAD,
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": info["cores"], "kind": info["kind"],
-                             "sample": "full config-1 solve (10 levels) per step, reference CPU path, all host cores"},
+                             "sample": "full 8320-DOF hole-plate solve (10 levels) per step, reference CPU path, all host cores"},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "detail": {"outer_iters": info["outer"], "cg_iters": info["cg"]}}
     print(json.dumps(line), flush=True)
@@ -196,7 +197,7 @@ BATCH_KW = dict(cg_tol=1e-10, outer_tol=1e-6, max_outer=2000, max_cg=5_000_000, 
 
 
 def batched_leg(ctx, window_s=20.0, warm_s=3.0, slots=512, pool_size=768, seed=20261203):
-    """The batched engine on the config-4 stream.
+    """The batched engine on the batch stream (512 seeded instances, DOF 2k-200k).
 
     saturation: closed loop, a batch of `slots` resident instances refilled
         from the stream as solves finish; converged solves per second over a
@@ -264,7 +265,7 @@ def batched_leg(ctx, window_s=20.0, warm_s=3.0, slots=512, pool_size=768, seed=2
     }
 
     return {
-        "workload": "config-4 stream: seeded instances (base seed %d), DOF log-uniform [2k, 200k], plates / rings, "
+        "workload": "batch stream: seeded instances (base seed %d), DOF log-uniform [2k, 200k], plates / rings, "
                     "5-segment piecewise diagrams, 1 load level, CG 1e-10, outer 1e-6; batched = mixed precision, "
                     "plain = FP64 drop-in one request at a time, same solver options" % seed,
         "saturation": saturation,
@@ -273,7 +274,7 @@ def batched_leg(ctx, window_s=20.0, warm_s=3.0, slots=512, pool_size=768, seed=2
 
 def compare_leg(ctx, n_requests, max_outer=100, seed=20261203):
     """Like for like: the plain FP64 drop-in solves the first n requests of
-    the config-4 stream one at a time; the batched mixed-precision engine
+    the batch stream (DOF 2k-200k) one at a time; the batched mixed-precision engine
     then solves exactly the same requests (fresh instances) to completion.
     Same solver options and caps for both, wall clock for both, and the error
     of each mixed-precision result against its FP64 result. Requests that hit
@@ -334,7 +335,7 @@ def compare_leg(ctx, n_requests, max_outer=100, seed=20261203):
         insts[i].close()
     b.close()
     fixed = {
-        "workload": "first %d requests of the config-4 stream (base seed %d), outer cap %d, CG 1e-10, outer 1e-6"
+        "workload": "first %d requests of the batch stream (DOF 2k-200k, base seed %d), outer cap %d, CG 1e-10, outer 1e-6"
                     % (n_requests, seed, max_outer),
         "requests": len(ids), "dof": [plain[i][2] for i in ids],
         "capped": [i for i in ids if plain[i][1]["status"] != 0],
@@ -349,7 +350,8 @@ def compare_leg(ctx, n_requests, max_outer=100, seed=20261203):
 
 
 def served_leg(rate_hz=10.0, submit_s=20.0, drain_s=25.0, seed=20270101):
-    """The solve service under Poisson arrivals of config-5 requests."""
+    """The solve service under Poisson arrivals of served-stream requests
+    (DOF 2k-500k, 5-30 load increments)."""
     import random
 
     import numpy as np
@@ -398,7 +400,7 @@ def served_leg(rate_hz=10.0, submit_s=20.0, drain_s=25.0, seed=20270101):
     srv.close()
     n = len(lat)
     return {
-        "workload": "config-5 stream: Poisson arrivals, DOF log-uniform [2k, 500k], 5-30 load increments, "
+        "workload": "served stream: Poisson arrivals, DOF log-uniform [2k, 500k], 5-30 load increments, "
                     "mixed precision, CG 1e-10, outer 1e-6",
         "rate_hz": rate_hz, "submitted": len(ids), "completed": n,
         "solves_per_s": n / last_done if last_done > 0 else 0.0,
@@ -502,7 +504,7 @@ def run_product_arm(args):
     accuracy = {k: rel(k) for k in ("uv", "sig_i", "eps_p_i")}
 
     # roofline of the dominant kernel (the SpMV P of the CG), live CUDA events:
-    # on this workload, and on the 2.1M-DOF configuration-2 mesh ("CG GB/s")
+    # on this workload, and on the 2.1M-DOF 1024x1024 O-grid plate ("CG GB/s")
     peak, peak_kind = measured_peak_hbm()
     import ctypes
 
@@ -533,7 +535,7 @@ def run_product_arm(args):
     mp, mu, bp, bu = rows["fp64"]
     cg_large = {k: {"spmv_gbs": b / (m * 1e-3) / 1e9, "update_gbs": c / (n * 1e-3) / 1e9, "ms_spmv": m,
                     "ms_update": n, "us_per_cg_iter": 1e3 * (m + n)} for k, (m, n, b, c) in rows.items()}
-    roofline = {"bound": "hbm", "kernel": "k_cg_p<double> (SpMV+dot) on the 2.1M-DOF config-2 mesh",
+    roofline = {"bound": "hbm", "kernel": "k_cg_p<double> (SpMV+dot) on the 2.1M-DOF 1024x1024 O-grid plate",
                 "achieved": bp / (mp * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                 "frac": bp / (mp * 1e-3) / 1e9 / peak, "traffic": 402.7e6,
                 "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one k_cg_p<double> launch (ncu capture)",
@@ -543,7 +545,7 @@ def run_product_arm(args):
     if rank == 0 and world == 1 and not args.skip_cpu:
         c = cpu_baseline_run()
         cpu = {"value": 1.0 / c["seconds"], "unit": "solves/s", "cores": c["cores"], "kind": c["kind"],
-               "sample": "one full config-1 solve (10 levels, CG 1e-10, outer 1e-6), reference CPU path, "
+               "sample": "one full 8320-DOF hole-plate solve (10 levels, CG 1e-10, outer 1e-6), reference CPU path, "
                          f"{c['outer']} outer / {c['cg']} CG iterations"}
 
     batched = served = roof_batched = None
@@ -580,7 +582,7 @@ CG_ONLY_KW = dict(cg_tol=1e-12, outer_tol=1e-9, max_outer=50, max_cg=5_000_000, 
 
 def cg_kernel_roofline(ctx, n=512, warm_trips=3, trips=10, seed=20261203):
     """Live roofline of the batched CG iteration kernel (k_batch_cg, ITER
-    phase): n resident config-4 instances with tight, non-adaptive linear
+    phase): n resident batch-stream instances with tight, non-adaptive linear
     solves, so every launch after the warm-up is a CG iteration of every
     instance; CUDA-event time per iteration of the whole batch and the
     algorithmic bytes one iteration must move."""
@@ -629,7 +631,7 @@ def cg_kernel_roofline(ctx, n=512, warm_trips=3, trips=10, seed=20261203):
 
 
 def batched_probe(n, trips):
-    """A fixed slice of batched CG work for profilers: n resident config-4
+    """A fixed slice of batched CG work for profilers: n resident batch-stream
     instances with tight, non-adaptive linear solves (every launch after the
     first trips is a CG iteration), `trips` graph trips; prints the time."""
     import cudaplasticity_b200 as cp
@@ -665,16 +667,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU-baseline leg")
-    ap.add_argument("--skip-batched", action="store_true", help="omit the batched (config-4 stream) leg")
-    ap.add_argument("--skip-served", action="store_true", help="omit the served (config-5 stream) leg")
+    ap.add_argument("--skip-batched", action="store_true", help="omit the batched (batch stream, DOF 2k-200k) leg")
+    ap.add_argument("--skip-served", action="store_true", help="omit the served (served stream, DOF 2k-500k) leg")
     ap.add_argument("--batched-window", type=float, default=20.0, help="seconds counted in the saturation run")
     ap.add_argument("--compare", type=int, metavar="N",
-                    help="like-for-like run only: the first N config-4 requests, plain FP64 one at a time vs batched")
+                    help="like-for-like run only: the first N batch-stream requests, plain FP64 one at a time vs batched")
     ap.add_argument("--compare-max-outer", type=int, default=100)
     ap.add_argument("--serve-rate", type=float, default=10.0, help="Poisson arrival rate of the served leg")
     ap.add_argument("--serve-window", type=float, default=20.0, help="seconds of arrivals in the served leg")
     ap.add_argument("--batched-probe", type=int, nargs=2, metavar=("N", "TRIPS"),
-                    help="profiling aid: N resident config-4 instances, TRIPS graph trips, then exit")
+                    help="profiling aid: N resident batch-stream instances, TRIPS graph trips, then exit")
     args = ap.parse_args()
     if args.batched_probe:
         batched_probe(*args.batched_probe)

@@ -53,21 +53,21 @@ SCENARIOS = {
                        lines=[f"diagram linear {E304} 170 19300", f"material {E304} {NU304} 1"] + _PT_LOADS),
     "hole12_strain": dict(mesh=_hole12, reference=True,
                           lines=[f"diagram linear {E304} 170 19300", f"material {E304} {NU304} 1", "plane strain"] + _PT_LOADS),
-    # configuration-1 style O-grid (16 circumferential x 8 radial), bilinear
+    # hole-plate O-grid (16 circumferential x 8 radial), bilinear
     # sy = 250, Et = 2 GPa, top traction 200 MPa in 10 increments
     "ogrid16_bilin": dict(mesh=lambda: _ogrid(4, 8), reference=True, levels=10,
                           lines=["diagram linear 210000 250 2000", "material 210000 0.3 1"] + _OGRID_LOADS),
-    # configuration-2 style hardening sy (1 + ep/e0)^n, 4 increments to 220 MPa
+    # Hollomon hardening sy (1 + ep/e0)^n, 4 increments to 220 MPa
     "ogrid16_hollomon": dict(mesh=lambda: _ogrid(4, 8), reference=True, levels=4,
                              lines=["diagram hollomon 210000 250 0.002 0.2", "material 210000 0.3 1",
                                     "force 2 0 220 0", "fixborderhor 0", "fixpoint -100 -100"]),
-    # configuration-4 style ring under internal pressure, piecewise diagram
+    # ring under internal pressure, piecewise diagram (as in the request streams)
     "ring_pw": dict(mesh=_ring, reference=True, lines_fn=lambda m: [piecewise_lines(210000.0, 300.0), "material 210000 0.3 1"] + _ring_lines(m)),
     # solverTest (src/Main.cpp:14-38): elastic 4x4 patch
     "rect_elastic": dict(mesh=lambda: meshgen.rect(-1.0, 1.0, -1.0, 1.0, 4, 4), reference=True, mode="elastic",
                          lines=[f"diagram linear {E304} 170000000 {E304}", f"material {E304} {NU304 * 1e-6!r} 1",
                                 "displ 2 0 0 0 1", "force 0 1 0 0"]),
-    # CST extension (no reference counterpart): configuration-1 style split
+    # CST extension (no reference counterpart): the hole-plate O-grid split
     "ogrid16_t3": dict(mesh=lambda: meshgen.split_t3(_ogrid(4, 8)), reference=False, levels=10,
                        lines=["diagram linear 210000 250 2000", "material 210000 0.3 1"] + _OGRID_LOADS),
 }
