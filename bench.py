@@ -417,6 +417,7 @@ def run_product_arm(args):
     import numpy as np
 
     import cudaplasticity_b200 as cp
+    from cudaplasticity_b200.ranks import max_over_ranks, replica_throughput
 
     rank, world, local = dist_env()
     dist = None
@@ -456,14 +457,8 @@ def run_product_arm(args):
             times.append(rep["seconds"])
             reps.append(rep)
         barrier()
-    total = sum(times)
-    if dist is not None:
-        import torch
-
-        t = torch.tensor([total], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
-    value = world * len(times) / total
+    total = max_over_ranks(sum(times), dist, device)
+    value = replica_throughput(world, len(times), total)
 
     # end to end through the public C ABI with host buffers: mesh upload and
     # set-up, loads H2D, solve, every result field D2H, teardown
@@ -481,14 +476,8 @@ def run_product_arm(args):
         d2h = sum(v.nbytes for v in st.values())
         if k > 0:
             e2e_times.append(dt)
-    e2e_total = sum(e2e_times)
-    if dist is not None:
-        import torch
-
-        t = torch.tensor([e2e_total], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * len(e2e_times) / e2e_total
+    e2e_total = max_over_ranks(sum(e2e_times), dist, device)
+    e2e_value = replica_throughput(world, len(e2e_times), e2e_total)
 
     # accuracy of the timed configuration against a tight FP64 solve
     state = inst.state()
