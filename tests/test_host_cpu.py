@@ -135,3 +135,46 @@ def test_inp_loader_rejects_bad_files(tmp_path):
     with pytest.raises(cp.CuplastError) as e:
         cp.Mesh.load(q8)
     assert e.value.status == _capi.CP_ERR_UNSUPPORTED
+
+
+def test_batch_and_server_entry_points_validate_arguments_without_a_device():
+    """The batch and server C entry points reject missing handles and bad
+    options before touching a device; creating a server without a GPU fails
+    with CP_ERR_NO_DEVICE and leaves nothing running."""
+    import ctypes
+
+    L = _capi.lib()
+    inv = _capi.CP_ERR_INVALID
+    bo = _capi.cp_batch_opts()
+    L.cp_batch_opts_default(ctypes.byref(bo))
+    assert (bo.max_instances, bo.cg_per_trip, bo.elem_per_trip, bo.max_width) == (1024, 16, 3, 16)
+    out = _capi.c_p()
+    assert L.cp_batch_create(None, ctypes.byref(bo), ctypes.byref(out)) == inv
+    assert L.cp_batch_add(None, None, None, None) == inv
+    assert L.cp_batch_launch(None, _capi.CP_BATCH_RUN_ALL, 0) == inv
+    assert L.cp_batch_wait(None, None, None) == inv
+    assert L.cp_batch_run(None, _capi.CP_BATCH_RUN_ALL, 0, None, None) == inv
+    n = ctypes.c_int()
+    assert L.cp_batch_harvest(None, 1, None, None, None, ctypes.byref(n)) == inv
+    assert L.cp_batch_interrupt(None) == inv
+    assert L.cp_batch_set_tile(None, 0, 4) == inv
+    assert L.cp_batch_get_tile(None, 0, ctypes.byref(n)) == inv
+    assert L.cp_batch_autotune(None, None) == inv
+    assert L.cp_batch_stats(None, None, None, None) == inv
+    assert L.cp_batch_progress(None, 0, None, None, None) == inv
+    ms = ctypes.c_double()
+    assert L.cp_batch_last_run_ms(None, ctypes.byref(ms)) == inv
+    so = _capi.cp_server_opts()
+    L.cp_server_opts_default(ctypes.byref(so))
+    assert so.max_inflight == 1024 and 0.0 < so.hbm_reserve < 1.0 and so.batch.max_instances == 1024
+    srv = _capi.c_p()
+    assert L.cp_server_create(ctypes.byref(so), ctypes.byref(srv)) == _capi.CP_ERR_NO_DEVICE
+    assert not srv.value
+    so.max_inflight = 0
+    assert L.cp_server_create(ctypes.byref(so), ctypes.byref(srv)) == inv
+    rid = ctypes.c_longlong()
+    assert L.cp_server_submit(None, None, None, None, None, None, None, ctypes.byref(rid)) == inv
+    assert L.cp_server_wait(None, 1, 0.0, None, None, None) == inv
+    assert L.cp_server_get_stats(None, None) == inv
+    assert L.cp_server_destroy(None) == inv
+    assert L.cp_secant_update_noalloc(None, None, 0, None, 0, None, None, None, None, None, None, None) == inv
