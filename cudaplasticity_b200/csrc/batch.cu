@@ -1133,9 +1133,16 @@ CP_API int cp_batch_add(cp_batch* b, cp_instance* I, const cp_solve_opts* opts, 
         d.u_full = I->u_full;
         d.mask = I->mask;
         {
+            // the batch's own vectors, allocated once per instance (an
+            // instance may be added again after it was harvested)
             const size_t nn = (size_t)I->n_nodes;
-            float2* v = I->alloc<float2>(4 * nn);
-            float4* g = I->alloc<float4>(4 * nn);
+            if (!I->bt_vec) {
+                I->bt_vec = I->alloc<float2>(4 * nn);
+                I->bt_rec = I->alloc<float4>(4 * nn);
+                I->bt_part = I->alloc<double>(kPart * (size_t)std::max(d.n_slices, d.n_groups));
+            }
+            float2* v = I->bt_vec;
+            float4* g = I->bt_rec;
             CP_CUDA(cudaMemsetAsync(v, 0, sizeof(float2) * 4 * nn, I->s()));
             CP_CUDA(cudaMemsetAsync(g, 0, sizeof(float4) * 4 * nn, I->s()));
             d.r = v; d.w = v + nn; d.kp = v + 2 * nn; d.p = v + 3 * nn;
@@ -1144,7 +1151,7 @@ CP_API int cp_batch_add(cp_batch* b, cp_instance* I, const cp_solve_opts* opts, 
         d.minv = I->minv32;
         d.st = I->st;
         d.mat = I->mat;
-        d.part = I->alloc<double>(kPart * (size_t)std::max(d.n_slices, d.n_groups));
+        d.part = I->bt_part;
         d.cg_tol = o.cg_tol;
         d.outer_tol = o.outer_tol;
         d.inner_tol = o.inner_tol;

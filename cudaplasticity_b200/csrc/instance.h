@@ -50,6 +50,10 @@ struct cp_instance {
     double2 *f_r = nullptr, *f_w = nullptr, *f_p = nullptr, *f_kp = nullptr, *f_g = nullptr;
     double* f_partials = nullptr;
     cudaGraphExec_t gf[2] = {nullptr, nullptr};  // [precond]
+    // batched engine (batch.cu): FP32 CG vectors, neighbour records, partial sums
+    float2* bt_vec = nullptr;
+    float4* bt_rec = nullptr;
+    double* bt_part = nullptr;
     long long launches = 0;  // kernels launched (graph nodes included)
     int last_assembly = -1;  // precision of the last assembly
     size_t bytes = 0;

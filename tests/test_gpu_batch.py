@@ -247,3 +247,24 @@ def test_autotuner_keeps_results(ctx):
         b.close()
     for i in ids:
         assert np.array_equal(results[0][i]["uv"], results[1][i]["uv"]), i
+
+
+def test_instance_can_join_again_after_harvest(ctx):
+    """A harvested instance can be reset and added again (its batch buffers
+    are reused); the second solve repeats the first bit for bit."""
+    inst, kw = workload_instance(ctx, 3, dof_min=600, dof_max=6000)
+    w = workload.instance(3, dof_min=600, dof_max=6000)
+    b = cp.Batch(ctx, max_instances=2)
+    runs = []
+    for _ in range(2):
+        inst.reset_state()
+        inst.set_loads(w["rp"], w["mask"], w["uv"])
+        b.add(inst, **kw)
+        (got, rep), = run_all(b).values()
+        assert got is inst
+        runs.append((inst.state(), rep))
+    for k in cp.FIELDS + ["uv"]:
+        assert np.array_equal(runs[0][0][k], runs[1][0][k]), k
+    assert runs[0][1]["cg_iters"] == runs[1][1]["cg_iters"]
+    inst.close()
+    b.close()
