@@ -97,21 +97,21 @@ class Mesh:
             raise CuplastError(st)
 
     @classmethod
-    def rect(cls, x1, x2, y1, y2, n1, n2):
+    def rect(cls, x1, x2, y1, y2, n1, n2, order=1):
         m = cls()
-        m._check(C.lib().cpx_mesh_gen_rect(m._h, x1, x2, y1, y2, n1, n2))
+        m._check(C.lib().cpx_mesh_gen_rect(m._h, x1, x2, y1, y2, n1, n2, order))
         return m
 
     @classmethod
-    def rect_with_hole(cls, x1, x2, y1, y2, hole_rad, n1, n2, rad_n=0):
+    def rect_with_hole(cls, x1, x2, y1, y2, hole_rad, n1, n2, rad_n=0, order=1):
         m = cls()
-        m._check(C.lib().cpx_mesh_gen_rect_with_hole(m._h, x1, x2, y1, y2, hole_rad, n1, n2, rad_n))
+        m._check(C.lib().cpx_mesh_gen_rect_with_hole(m._h, x1, x2, y1, y2, hole_rad, n1, n2, rad_n, order))
         return m
 
     @classmethod
-    def ring(cls, a, b, n_phi, n_r):
+    def ring(cls, a, b, n_phi, n_r, order=1):
         m = cls()
-        m._check(C.lib().cpx_mesh_gen_ring(m._h, a, b, n_phi, n_r))
+        m._check(C.lib().cpx_mesh_gen_ring(m._h, a, b, n_phi, n_r, order))
         return m
 
     @classmethod
@@ -139,24 +139,36 @@ class Mesh:
         return self
 
     def counts(self):
-        v = [ctypes.c_int() for _ in range(5)]
+        """(nodes, triangles, quads, borders, border nodes in total)."""
+        v = [ctypes.c_int() for _ in range(6)]
         self._check(C.lib().cpx_mesh_counts(self._h, *[ctypes.byref(x) for x in v]))
-        return tuple(x.value for x in v)
+        return tuple(x.value for x in v[:5])
+
+    def count8(self):
+        """8-node elements (meshes generated with order=2 or read from S8R blocks)."""
+        v = ctypes.c_int()
+        self._check(C.lib().cpx_mesh_counts(self._h, None, None, None, None, None, ctypes.byref(v)))
+        return v.value
 
     def arrays(self):
         n, c3, c4, nb, bt = self.counts()
+        c8 = self.count8()
         xy = np.zeros(2 * n)
         e3 = np.zeros(max(3 * c3, 1), np.int32)
         e4 = np.zeros(max(4 * c4, 1), np.int32)
+        e8 = np.zeros(max(8 * c8, 1), np.int32)
         bl = np.zeros(max(nb, 1), np.int32)
         bn = np.zeros(max(bt, 1), np.int32)
-        self._check(C.lib().cpx_mesh_get(self._h, _dp(xy), _ip(e3), _ip(e4), _ip(bl), _ip(bn)))
+        self._check(C.lib().cpx_mesh_get(self._h, _dp(xy), _ip(e3), _ip(e4), _ip(bl), _ip(bn), _ip(e8)))
         borders, off = [], 0
         for L in bl[:nb]:
             borders.append(bn[off:off + L].copy())
             off += L
-        return dict(node_xy=xy.reshape(-1, 2), elem3=e3[:3 * c3].reshape(-1, 3), elem4=e4[:4 * c4].reshape(-1, 4),
-                    borders=borders)
+        out = dict(node_xy=xy.reshape(-1, 2), elem3=e3[:3 * c3].reshape(-1, 3), elem4=e4[:4 * c4].reshape(-1, 4),
+                   borders=borders)
+        if c8:
+            out["elem8"] = e8[:8 * c8].reshape(-1, 8)
+        return out
 
     def max_index_diff(self):
         v = ctypes.c_int()

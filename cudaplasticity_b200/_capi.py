@@ -131,15 +131,15 @@ _SIGS = {
     # host helpers
     "cpx_mesh_create": (c_int, [ctypes.POINTER(c_p)]),
     "cpx_mesh_destroy": (c_int, [c_p]),
-    "cpx_mesh_gen_rect": (c_int, [c_p, c_double, c_double, c_double, c_double, c_int, c_int]),
+    "cpx_mesh_gen_rect": (c_int, [c_p, c_double, c_double, c_double, c_double, c_int, c_int, c_int]),
     "cpx_mesh_gen_rect_with_hole": (c_int, [c_p, c_double, c_double, c_double, c_double, c_double, c_int, c_int,
-                                            c_int]),
-    "cpx_mesh_gen_ring": (c_int, [c_p, c_double, c_double, c_int, c_int]),
+                                            c_int, c_int]),
+    "cpx_mesh_gen_ring": (c_int, [c_p, c_double, c_double, c_int, c_int, c_int]),
     "cpx_mesh_split_t3": (c_int, [c_p]),
     "cpx_mesh_load_inp": (c_int, [c_p, ctypes.c_char_p]),
     "cpx_mesh_set": (c_int, [c_p, c_int, P_double, c_int, P_int, c_int, P_int, c_int, P_int, P_int]),
-    "cpx_mesh_counts": (c_int, [c_p, P_int, P_int, P_int, P_int, P_int]),
-    "cpx_mesh_get": (c_int, [c_p, P_double, P_int, P_int, P_int, P_int]),
+    "cpx_mesh_counts": (c_int, [c_p, P_int, P_int, P_int, P_int, P_int, P_int]),
+    "cpx_mesh_get": (c_int, [c_p, P_double, P_int, P_int, P_int, P_int, P_int]),
     "cpx_mesh_max_index_diff": (c_int, [c_p, P_int]),
     "cpx_loads_create": (c_int, [ctypes.POINTER(c_p)]),
     "cpx_loads_destroy": (c_int, [c_p]),

@@ -165,7 +165,42 @@ void buildConditions(const Mesh& mesh, const LoadConditions& cond, double h, dou
         if (id < 0 || id >= mesh.bordersCount) throw std::out_of_range("force on a border that does not exist");
         const int* border = mesh.borders[id];
         for (int i = 1; i < mesh.borderLength[id]; ++i) {
-            if (mesh.secOrdNodes[border[i]]) throw std::invalid_argument("quadratic borders (Q8) are not supported");
+            if (mesh.secOrdNodes[border[i]]) {
+                // quadratic edge (corner, mid-side, corner): consistent nodal
+                // loads 1/3, 4/3, 1/3 of the half-lengths' weights
+                // (src/PlasticitySolver.cu:823-866)
+                ++i;
+                if (i >= mesh.borderLength[id]) throw std::out_of_range("border ends on a mid-side node");
+                vec2 n1 = mesh.node[border[i - 2]], n2 = mesh.node[border[i - 1]], n3 = mesh.node[border[i]];
+                double hx1 = 0.5 * (n1.x - n2.x), hy1 = 0.5 * (n1.y - n2.y);
+                double hx2 = 0.5 * (n2.x - n3.x), hy2 = 0.5 * (n2.y - n3.y);
+                double dl1 = std::sqrt(hx1 * hx1 + hy1 * hy1), dl2 = std::sqrt(hx2 * hx2 + hy2 * hy2);
+                vec2 f1 = force.forceFunc(n1), f2 = force.forceFunc(n2), f3 = force.forceFunc(n3);
+                if (force.normOrient) {
+                    vec2 t1 = (n2 - n1).normalize();
+                    vec2 m1 = vec2(t1.y, -t1.x).normalize();
+                    vec2 t2 = (n3 - n2).normalize();
+                    vec2 m2 = vec2(t2.y, -t2.x).normalize();
+                    f1 = m1 * f1.x + t1 * f1.y;
+                    f2 = 0.5 * ((m1 + m2) * f2.x + (t1 + t2) * f2.y);
+                    f3 = m2 * f3.x + t2 * f3.y;
+                }
+                double R[6] = {f1.x / 3., f1.y / 3., f2.x * 4. / 3., f2.y * 4. / 3., f3.x / 3., f3.y / 3.};
+                R[0] *= h * dl1 * 2.;
+                R[1] *= h * dl1 * 2.;
+                R[2] *= h * (dl1 + dl2);
+                R[3] *= h * (dl1 + dl2);
+                R[4] *= h * dl2 * 2.;
+                R[5] *= h * dl2 * 2.;
+                const int gi = 2 * border[i - 2], gj = 2 * border[i - 1], gk = 2 * border[i];
+                rp[gi] += R[0];
+                rp[gi + 1] += R[1];
+                rp[gj] += R[2];
+                rp[gj + 1] += R[3];
+                rp[gk] += R[4];
+                rp[gk + 1] += R[5];
+                continue;
+            }
             vec2 n1 = mesh.node[border[i - 1]], n2 = mesh.node[border[i]];
             double hd1 = 0.5 * (n1.x - n2.x), hd2 = 0.5 * (n1.y - n2.y);
             double dl = std::sqrt(hd1 * hd1 + hd2 * hd2);
@@ -195,6 +230,19 @@ void buildConditions(const Mesh& mesh, const LoadConditions& cond, double h, dou
                 vec2 R = cond.R(mesh.node[nd]);
                 rp[2 * nd] += coef * R.x;
                 rp[2 * nd + 1] += coef * R.y;
+            }
+        }
+        // 8-node elements: -1/12 of the load to each corner, 1/3 to each
+        // mid-side node (src/PlasticitySolver.cu:911-927)
+        for (int e = 0; e < mesh.count8; ++e) {
+            double space = mesh.elemSpace8(e);
+            double c1 = -rho * h * space / 12., c2 = rho * h * space / 3.;
+            for (int i = 8 * e; i < 8 * (e + 1); ++i) {
+                int nd = mesh.elem8[i];
+                vec2 R = cond.R(mesh.node[nd]);
+                const double c = i < 8 * e + 4 ? c1 : c2;
+                rp[2 * nd] += c * R.x;
+                rp[2 * nd + 1] += c * R.y;
             }
         }
         for (int e = 0; e < mesh.count3; ++e) {

@@ -43,18 +43,18 @@ CP_API int cpx_mesh_destroy(cpx_mesh* m) {
     delete m;
     return CP_OK;
 }
-CP_API int cpx_mesh_gen_rect(cpx_mesh* m, double x1, double x2, double y1, double y2, int n1, int n2) {
-    if (!m || n1 <= 0 || n2 <= 0) return CP_ERR_INVALID;
-    return guard([&] { m->m.genRectangle(x1, x2, y1, y2, n1, n2); });
+CP_API int cpx_mesh_gen_rect(cpx_mesh* m, double x1, double x2, double y1, double y2, int n1, int n2, int order) {
+    if (!m || n1 <= 0 || n2 <= 0 || (order != 1 && order != 2)) return CP_ERR_INVALID;
+    return guard([&] { m->m.genRectangle(x1, x2, y1, y2, n1, n2, order); });
 }
 CP_API int cpx_mesh_gen_rect_with_hole(cpx_mesh* m, double x1, double x2, double y1, double y2, double r, int n1,
-                                       int n2, int rad_n) {
-    if (!m || n1 <= 0 || n2 <= 0 || !(r > 0)) return CP_ERR_INVALID;
-    return guard([&] { m->m.genRectWithHole(x1, x2, y1, y2, r, n1, n2, 1, rad_n); });
+                                       int n2, int rad_n, int order) {
+    if (!m || n1 <= 0 || n2 <= 0 || !(r > 0) || (order != 1 && order != 2)) return CP_ERR_INVALID;
+    return guard([&] { m->m.genRectWithHole(x1, x2, y1, y2, r, n1, n2, order, rad_n); });
 }
-CP_API int cpx_mesh_gen_ring(cpx_mesh* m, double a, double b, int n_phi, int n_r) {
-    if (!m || n_phi < 3 || n_r <= 0 || !(b > a) || !(a > 0)) return CP_ERR_INVALID;
-    return guard([&] { m->m.genRing(a, b, n_phi, n_r); });
+CP_API int cpx_mesh_gen_ring(cpx_mesh* m, double a, double b, int n_phi, int n_r, int order) {
+    if (!m || n_phi < 3 || n_r <= 0 || !(b > a) || !(a > 0) || (order != 1 && order != 2)) return CP_ERR_INVALID;
+    return guard([&] { m->m.genRing(a, b, n_phi, n_r, order); });
 }
 CP_API int cpx_mesh_load_inp(cpx_mesh* m, const char* path) {
     if (!m || !path) return CP_ERR_INVALID;
@@ -77,8 +77,9 @@ CP_API int cpx_mesh_set(cpx_mesh* m, int nodes, const double* xy, int c3, const 
         m->m.assign(nodes, xy, c3, e3, c4, e4, borders);
     });
 }
-CP_API int cpx_mesh_counts(const cpx_mesh* m, int* nodes, int* c3, int* c4, int* nb, int* bt) {
+CP_API int cpx_mesh_counts(const cpx_mesh* m, int* nodes, int* c3, int* c4, int* nb, int* bt, int* c8) {
     if (!m) return CP_ERR_INVALID;
+    if (c8) *c8 = m->m.count8;
     if (nodes) *nodes = m->m.nodeCount;
     if (c3) *c3 = m->m.count3;
     if (c4) *c4 = m->m.count4;
@@ -90,9 +91,11 @@ CP_API int cpx_mesh_counts(const cpx_mesh* m, int* nodes, int* c3, int* c4, int*
     }
     return CP_OK;
 }
-CP_API int cpx_mesh_get(const cpx_mesh* m, double* xy, int* e3, int* e4, int* bl, int* bn) {
+CP_API int cpx_mesh_get(const cpx_mesh* m, double* xy, int* e3, int* e4, int* bl, int* bn, int* e8) {
     if (!m) return CP_ERR_INVALID;
     const cuplast::Mesh& M = m->m;
+    if (e8)
+        for (int i = 0; i < 8 * M.count8; ++i) e8[i] = M.elem8[i];
     if (xy)
         for (int i = 0; i < M.nodeCount; ++i) {
             xy[2 * i] = M.node[i].x;

@@ -95,7 +95,11 @@ void Mesh::assign(int nodes, const double* xy, int c3, const int* e3, int c4, co
 }
 
 void Mesh::genRectangle(double x1, double x2, double y1, double y2, size_t N1, size_t N2, int order) {
-    if (order != 1) throw std::invalid_argument("second-order (Q8) meshes are not supported");
+    if (order != 1 && order != 2) throw std::out_of_range("element order must be 1 or 2");
+    if (order == 2) {
+        N1 *= 2;
+        N2 *= 2;
+    }
     clear();
     nodeCount = (int)((N1 + 1) * (N2 + 1));
     count4 = (int)(N1 * N2);
@@ -131,16 +135,23 @@ void Mesh::genRectangle(double x1, double x2, double y1, double y2, size_t N1, s
         borders[3][N1 - i] = (int)((N1 - i) * (N2 + 1));
     }
     fillPos();
+    if (order == 2) remapOrder((int)N2);
 }
 
 void Mesh::genRectWithHole(double x1, double x2, double y1, double y2, double holeRad, size_t N1, size_t N2,
                            int order, int radNOverride) {
-    if (order != 1) throw std::invalid_argument("second-order (Q8) meshes are not supported");
+    if (order != 1 && order != 2) throw std::out_of_range("element order must be 1 or 2");
     clear();
     int borderN = (int)((N1 + N2) * 2);
     int radN = (int)((N1 + N2) / 4);
     radN = (int)std::round(double(radN) * (x2 - x1 + y2 - y1 - 4. * holeRad) * 2. / (x2 - x1 + y2 - y1));
     if (radNOverride > 0) radN = radNOverride;
+    if (order == 2) {
+        N1 *= 2;
+        N2 *= 2;
+        borderN *= 2;
+        radN *= 2;
+    }
     nodeCount = borderN * (radN + 1);
     node = new vec2[nodeCount];
     secOrdNodes = new bool[nodeCount];
@@ -212,10 +223,15 @@ void Mesh::genRectWithHole(double x1, double x2, double y1, double y2, double ho
     }
     fillPos();
     renumerateRing(borderN);
+    if (order == 2) remapOrder(radN);
 }
 
 void Mesh::genRing(double a, double b, size_t N_phi, size_t N_r, int order) {
-    if (order != 1) throw std::invalid_argument("second-order (Q8) meshes are not supported");
+    if (order != 1 && order != 2) throw std::out_of_range("element order must be 1 or 2");
+    if (order == 2) {
+        N_phi *= 2;
+        N_r *= 2;
+    }
     clear();
     nodeCount = (int)((N_r + 1) * N_phi);
     node = new vec2[nodeCount];
@@ -258,6 +274,69 @@ void Mesh::genRing(double a, double b, size_t N_phi, size_t N_r, int order) {
     }
     fillPos();
     renumerateRing((int)N_phi);
+    if (order == 2) remapOrder((int)N_r);
+}
+
+// Mesh::remapOrder (src/Mesh.cu:443-505): the quads form rows of `width`;
+// every 2 x 2 block of them (rows i, i+1 and columns j, j+1, i and j even)
+// becomes one 8-node element -- corners from the block's outer corners,
+// mid-side nodes from the middles of its outer edges -- the node at the
+// block's centre disappears and the remaining nodes keep their order.
+void Mesh::remapOrder(int width) {
+    count8 = count4 / 4;
+    delete[] elem8;
+    elem8 = new int[8 * (size_t)count8 + 1];
+    std::vector<char> keep(nodeCount, 1);
+    const int rows = count4 / width;
+    auto q = [&](int i, int j, int k) { return elem4[4 * ((size_t)i * width + j) + k]; };
+    for (int i = 0; i < rows; i += 2)
+        for (int j = 0; j < width; j += 2) {
+            int* e = elem8 + 8 * ((size_t)i * width / 4 + j / 2);
+            e[0] = q(i + 1, j + 1, 0);
+            e[1] = q(i, j + 1, 1);
+            e[2] = q(i, j, 2);
+            e[3] = q(i + 1, j, 3);
+            e[4] = q(i + 1, j + 1, 1);
+            e[5] = q(i, j + 1, 2);
+            e[6] = q(i, j, 3);
+            e[7] = q(i + 1, j, 0);
+            keep[q(i, j, 0)] = 0;
+        }
+    std::vector<int> renum(nodeCount, -1);
+    int kept = 0;
+    for (int n = 0; n < nodeCount; ++n)
+        if (keep[n]) renum[n] = kept++;
+    for (size_t i = 0; i < 8 * (size_t)count8; ++i) elem8[i] = renum[elem8[i]];
+    for (int b = 0; b < bordersCount; ++b)
+        for (int k = 0; k < borderLength[b]; ++k) borders[b][k] = renum[borders[b][k]];
+    vec2* nodes = new vec2[kept ? kept : 1];
+    for (int n = 0; n < nodeCount; ++n)
+        if (keep[n]) nodes[renum[n]] = node[n];
+    delete[] node;
+    node = nodes;
+    nodeCount = kept;
+    delete[] secOrdNodes;
+    secOrdNodes = new bool[nodeCount ? nodeCount : 1];
+    std::fill(secOrdNodes, secOrdNodes + nodeCount, false);
+    for (int e = 0; e < count8; ++e)
+        for (int k = 4; k < 8; ++k) secOrdNodes[elem8[8 * e + k]] = true;
+    delete[] elem4;
+    elem4 = new int[1];
+    count4 = 0;
+    fillPos();
+}
+
+// Mesh::elemSpace8 (src/Mesh.cuh:269-278): the area of the polygon through
+// the corners and mid-side nodes, same operation order.
+double Mesh::elemSpace8(int e) const {
+    double s1 = 0., s2 = 0.;
+    for (int i = 8 * e; i < 8 * e + 3; ++i) {
+        s1 += node[elem8[i]].x * node[elem8[i + 4]].y + node[elem8[i + 4]].x * node[elem8[i + 1]].y;
+        s2 += node[elem8[i]].y * node[elem8[i + 4]].x + node[elem8[i + 4]].y * node[elem8[i + 1]].x;
+    }
+    s1 += node[elem8[8 * e + 3]].x * node[elem8[8 * e + 7]].y + node[elem8[8 * e + 7]].x * node[elem8[8 * e]].y;
+    s2 += node[elem8[8 * e + 3]].y * node[elem8[8 * e + 7]].x + node[elem8[8 * e + 7]].y * node[elem8[8 * e]].x;
+    return std::fabs(s1 - s2) * 0.5;
 }
 
 void Mesh::renumerateRing(int borderN) {
@@ -308,6 +387,9 @@ int Mesh::findMaxIndexDiff() const {
     for (int e = 0; e < count4; ++e)
         for (int i = 4 * e; i < 4 * (e + 1); ++i)
             for (int j = i + 1; j < 4 * (e + 1); ++j) mx = std::max(mx, std::abs(elem4[i] - elem4[j]));
+    for (int e = 0; e < count8; ++e)
+        for (int i = 8 * e; i < 8 * (e + 1); ++i)
+            for (int j = i + 1; j < 8 * (e + 1); ++j) mx = std::max(mx, std::abs(elem8[i] - elem8[j]));
     return mx;
 }
 
@@ -350,8 +432,8 @@ double Mesh::elemSpace4(int e) const {
 //  * every MPC section brings one reference node in the *NODE list, so the
 //    mesh has (node lines - MPC sections) nodes and node lines with a larger
 //    id are dropped.
-// Quadratic (S8R) elements are counted and rejected: this library has no
-// 8-node element.
+// Quadratic (S8R) elements are read into elem8, and their mid-side nodes
+// (local 4..7) marked as second-order nodes.
 namespace {
 
 bool is_data(const std::string& l) { return !l.empty() && l[0] != '*'; }
@@ -373,8 +455,7 @@ bool Mesh::loadFromFile(const std::string& fileName) {
     for (std::string l; std::getline(file, l);) lines.push_back(l);
 
     std::vector<std::pair<int, vec2>> nodeLines;
-    std::vector<int> e3, e4;
-    int c8 = 0;
+    std::vector<int> e3, e4, e8;
     std::vector<std::vector<int>> borderLists;
     size_t at = 0;
     auto next = [&](std::string& l) {
@@ -409,12 +490,8 @@ bool Mesh::loadFromFile(const std::string& fileName) {
                 const bool t8 = line.compare(i, 3, "S8R") == 0;
                 if (!(t3 || t4 || t8)) continue;
                 const int nn = t3 ? 3 : (t4 ? 4 : 8);
-                std::vector<int>& dst = t3 ? e3 : e4;
+                std::vector<int>& dst = t3 ? e3 : (t4 ? e4 : e8);
                 block(line, [&](const std::string& l) {
-                    if (t8) {
-                        ++c8;
-                        return;
-                    }
                     std::istringstream ss(blank_commas(l));
                     int id = 0;
                     ss >> id;
@@ -441,7 +518,6 @@ bool Mesh::loadFromFile(const std::string& fileName) {
             }
         }
     }
-    if (c8 > 0) throw std::invalid_argument("quadratic (S8R) elements are not supported");
     const int nodes = (int)nodeLines.size() - (int)borderLists.size();
     if (nodes <= 0) throw std::out_of_range("mesh file has no nodes");
     std::vector<double> xy(2 * (size_t)nodes, 0.0);
@@ -450,7 +526,18 @@ bool Mesh::loadFromFile(const std::string& fileName) {
             xy[2 * (size_t)nl.first] = nl.second.x;
             xy[2 * (size_t)nl.first + 1] = nl.second.y;
         }
+    for (const std::vector<int>* ev : {&e3, &e4, &e8})
+        for (int v : *ev)
+            if (v < 0 || v >= nodes) throw std::out_of_range("element references a node that does not exist");
     assign(nodes, xy.data(), (int)(e3.size() / 3), e3.data(), (int)(e4.size() / 4), e4.data(), borderLists);
+    if (!e8.empty()) {
+        count8 = (int)(e8.size() / 8);
+        delete[] elem8;
+        elem8 = dup(e8.data(), e8.size());
+        for (int e = 0; e < count8; ++e)
+            for (int k = 4; k < 8; ++k) secOrdNodes[elem8[8 * e + k]] = true;
+        fillPos();
+    }
     return true;
 }
 

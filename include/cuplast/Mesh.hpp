@@ -47,6 +47,9 @@ public:
     void genRing(double a, double b, size_t N_phi, size_t N_r, int order = 1);
     // src/Mesh.cu:332-380
     void renumerateRing(int borderN);
+    // src/Mesh.cu:443-505: quads in rows of `width` -> 8-node elements
+    // (what the generators do for order = 2)
+    void remapOrder(int width);
     // Extension: every quad (n1,n2,n3,n4) becomes (n1,n2,n3), (n1,n3,n4).
     void splitToTriangles();
     // src/Mesh.cu:417-440
@@ -54,11 +57,11 @@ public:
 
     double elemSpace3(int e) const;
     double elemSpace4(int e) const;
+    double elemSpace8(int e) const;
 
-    // src/Mesh.cu:725-937: a mesh from an .inp file (nodes, S3/S4 element
-    // blocks, *MPC border blocks); true when loaded. Throws
-    // std::out_of_range on a bad file, std::invalid_argument for quadratic
-    // (S8R) elements.
+    // src/Mesh.cu:725-937: a mesh from an .inp file (nodes, S3/S4/S8R
+    // element blocks, *MPC border blocks); true when loaded. Throws
+    // std::out_of_range on a bad file.
     bool loadFromFile(const std::string& fileName);
 
     // Replaces the arrays (takes copies).

@@ -19,24 +19,29 @@ typedef struct cpx_loads cpx_loads;
 
 CP_API int cpx_mesh_create(cpx_mesh** out);
 CP_API int cpx_mesh_destroy(cpx_mesh* m);
+/* The generators take the reference's element order: 1 (4-node quads) or 2
+ * (8-node quads: Mesh::remapOrder, src/Mesh.cu:443-505). The device solver
+ * takes order-1 meshes; order-2 meshes serve the host side (load building,
+ * I/O) and the C++ classes. */
 /* Mesh::genRectangle (src/Mesh.cu:17-110) */
-CP_API int cpx_mesh_gen_rect(cpx_mesh* m, double x1, double x2, double y1, double y2, int n1, int n2);
+CP_API int cpx_mesh_gen_rect(cpx_mesh* m, double x1, double x2, double y1, double y2, int n1, int n2, int order);
 /* Mesh::genRectWithHole (src/Mesh.cu:112-246); rad_n > 0 overrides the reference's radial count */
 CP_API int cpx_mesh_gen_rect_with_hole(cpx_mesh* m, double x1, double x2, double y1, double y2, double hole_rad,
-                                       int n1, int n2, int rad_n);
+                                       int n1, int n2, int rad_n, int order);
 /* Mesh::genRing (src/Mesh.cu:249-329) */
-CP_API int cpx_mesh_gen_ring(cpx_mesh* m, double a, double b, int n_phi, int n_r);
+CP_API int cpx_mesh_gen_ring(cpx_mesh* m, double a, double b, int n_phi, int n_r, int order);
 /* Mesh::loadFromFile (src/Mesh.cu:725-937): an .inp file with *NODE, *ELEMENT
- * (TYPE=S3, S4) and *MPC border blocks. CP_ERR_INVALID for a bad file,
- * CP_ERR_UNSUPPORTED for quadratic (S8R) elements. */
+ * (TYPE=S3, S4, S8R) and *MPC border blocks. CP_ERR_INVALID for a bad file. */
 CP_API int cpx_mesh_load_inp(cpx_mesh* m, const char* path);
 /* every quad (n1,n2,n3,n4) -> triangles (n1,n2,n3), (n1,n3,n4) (extension) */
 CP_API int cpx_mesh_split_t3(cpx_mesh* m);
 CP_API int cpx_mesh_set(cpx_mesh* m, int node_count, const double* xy, int count3, const int* elem3, int count4,
                         const int* elem4, int n_borders, const int* border_len, const int* border_nodes);
 CP_API int cpx_mesh_counts(const cpx_mesh* m, int* node_count, int* count3, int* count4, int* n_borders,
-                           int* border_total);
-CP_API int cpx_mesh_get(const cpx_mesh* m, double* xy, int* elem3, int* elem4, int* border_len, int* border_nodes);
+                           int* border_total, int* count8);
+/* elem8: 8 * count8 node indices, corners 0..3 then mid-side nodes 4..7 */
+CP_API int cpx_mesh_get(const cpx_mesh* m, double* xy, int* elem3, int* elem4, int* border_len, int* border_nodes,
+                        int* elem8);
 CP_API int cpx_mesh_max_index_diff(const cpx_mesh* m, int* out);
 
 CP_API int cpx_loads_create(cpx_loads** out);

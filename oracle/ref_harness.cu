@@ -14,7 +14,7 @@
  *
  * Usage: cpref <job.txt> <out.bin>
  * Job lines (one per line, '#' comments):
- *   mode mesh|csr|solve|phases|elastic
+ *   mode mesh|csr|loads|solve|phases|elastic   (loads: initConditions only)
  *   mesh hole x1 x2 y1 y2 R N1 N2 order      (Mesh::genRectWithHole, src/Mesh.cu:112)
  *   mesh ring a b Nphi Nr order              (Mesh::genRing, src/Mesh.cu:249)
  *   mesh rect x1 x2 y1 y2 N1 N2 order        (Mesh::genRectangle, src/Mesh.cu:17)
@@ -364,6 +364,11 @@ int main(int argc, char** argv) {
     if (j.dumpCsr) dumpCsr(out, spK, ps.mesh.nodeCount);
     cpbin_put(out, "rp", 'd', N, rpFull.data());
     cpbin_put(out, "mask", 'b', N, mask.data());
+    if (j.mode == "loads") {
+        cpbin_put(out, "uv", 'd', N, uvFull.data());
+        fclose(out);
+        return 0;
+    }
 
     std::vector<int> outerPerLevel, cgPerLevel;
     std::vector<double> errPerLevel;

@@ -57,7 +57,9 @@ def scenario_fixtures(workdir):
 
 def mesh_fixtures():
     specs = ["hole -3 3 -2 2 0.5 48 32 1", "hole -3 3 -2 2 0.5 12 8 1", "hole -100 100 -100 100 20 16 16 1",
-             "ring 50 120 32 8 1", "ring 0.1 0.2 40 5 1", "rect -1 1 -1 1 4 4 1", "rect -3 3 -2 2 6 4 1"]
+             "ring 50 120 32 8 1", "ring 0.1 0.2 40 5 1", "rect -1 1 -1 1 4 4 1", "rect -3 3 -2 2 6 4 1",
+             # 8-node (order 2) meshes: Mesh::remapOrder
+             "hole -3 3 -2 2 0.5 12 8 2", "ring 50 120 16 4 2", "rect -3 3 -2 2 6 4 2"]
     out = {}
     for s in specs:
         r = oracle.run_reference(["mode mesh", "mesh " + s])
@@ -65,9 +67,11 @@ def mesh_fixtures():
         for L in r["border_len"]:
             borders.append(r["border_nodes"][off:off + L])
             off += L
-        m = dict(node_xy=r["node_xy"].reshape(-1, 2), elem3=r["elem3"], elem4=r["elem4"], borders=borders)
+        m = dict(node_xy=r["node_xy"].reshape(-1, 2), elem3=r["elem3"], elem4=r["elem4"], borders=borders,
+                 elem8=r["elem8"], sec_ord=r["sec_ord"])
         out[s] = dict(digest=scenarios.mesh_digest(m), nodes=int(len(r["node_xy"]) // 2),
-                      count4=int(len(r["elem4"]) // 4), max_index_diff=int(r["max_index_diff"][0]))
+                      count4=int(len(r["elem4"]) // 4), max_index_diff=int(r["max_index_diff"][0]),
+                      **({"count8": int(len(r["elem8"]) // 8)} if len(r["elem8"]) else {}))
     with open(os.path.join(OUT, "ref_meshes.json"), "w") as f:
         json.dump(out, f, indent=1)
 
@@ -94,6 +98,28 @@ def shipped_fixtures():
             tables[name] = [[float(w) for w in line.split()] for line in f if line.strip()]
     with open(os.path.join(OUT, "ref_tables.json"), "w") as f:
         json.dump(tables, f, indent=1)
+
+
+# Load building on 8-node meshes (quadratic edges, 8-node body forces):
+# name -> (reference mesh spec, job lines)
+Q8_LOADS = {
+    "hole_q8": ("hole -3 3 -2 2 0.5 12 8 2",
+                ["material 193000 0.29 1", "force 1 170 0 0", "force 3 -170 0 0", "fixvertaxis 0", "fixhoraxis 0"]),
+    "ring_q8": ("ring 50 120 16 4 2",
+                ["material 210000 0.3 1", "force 0 200 0 1", "fixborderhor 1", "gravity 9.81 0 -1"]),
+    "rect_q8": ("rect -3 3 -2 2 6 4 2",
+                ["material 210000 0.3 2", "force 0 0 -50 0", "displ 2 0 0 0 0", "gravity 2.5 1 0"]),
+}
+
+
+def q8_load_fixtures():
+    out = {}
+    for name, (spec, lines) in Q8_LOADS.items():
+        r = oracle.run_reference(["mode loads", "mesh " + spec] + lines)
+        for k in ("rp", "mask", "uv"):
+            out[f"{name}_{k}"] = r[k]
+    np.savez_compressed(os.path.join(OUT, "q8_loads.npz"), **out)
+    print("q8 loads", list(Q8_LOADS))
 
 
 def write_inp_files():
@@ -159,6 +185,12 @@ def inp_fixtures():
 if __name__ == "__main__":
     import tempfile
 
+    if "--meshes" in sys.argv:  # only the generator and load-building pins
+        if not oracle.have_reference():
+            oracle.build(with_reference=True)
+        mesh_fixtures()
+        q8_load_fixtures()
+        sys.exit(0)
     if "--inp" in sys.argv:  # only the .inp loader pins
         if not oracle.have_reference():
             oracle.build(with_reference=True)
@@ -170,5 +202,6 @@ if __name__ == "__main__":
     with tempfile.TemporaryDirectory() as d:
         scenario_fixtures(d)
     mesh_fixtures()
+    q8_load_fixtures()
     shipped_fixtures()
     inp_fixtures()

@@ -90,4 +90,9 @@ def mesh_digest(m):
         h.update(np.ascontiguousarray(np.asarray(m[k], dtype=np.float64 if k == "node_xy" else np.int32)).tobytes())
     for b in m["borders"]:
         h.update(np.asarray(b, dtype=np.int32).tobytes())
+    e8 = np.asarray(m.get("elem8", ()), dtype=np.int32)
+    if e8.size:  # 8-node meshes only: the digests of 4-node meshes are unchanged
+        h.update(b"elem8")
+        h.update(np.ascontiguousarray(e8).tobytes())
+        h.update(np.ascontiguousarray(np.asarray(m["sec_ord"], dtype=np.uint8)).tobytes())
     return h.hexdigest()

@@ -44,7 +44,12 @@ def test_version_and_status_strings():
 
 def _digest_of(m):
     a = m.arrays()
-    return scenarios.mesh_digest(dict(node_xy=a["node_xy"], elem3=a["elem3"], elem4=a["elem4"], borders=a["borders"]))
+    d = dict(node_xy=a["node_xy"], elem3=a["elem3"], elem4=a["elem4"], borders=a["borders"])
+    if "elem8" in a:  # second-order nodes: the mid-side nodes of the 8-node elements
+        sec = np.zeros(len(a["node_xy"]), np.uint8)
+        sec[a["elem8"][:, 4:].ravel()] = 1
+        d.update(elem8=a["elem8"], sec_ord=sec)
+    return scenarios.mesh_digest(d)
 
 
 def test_product_mesh_generators_match_reference(golden_dir):
@@ -57,6 +62,10 @@ def test_product_mesh_generators_match_reference(golden_dir):
         "ring 0.1 0.2 40 5 1": lambda: cp.Mesh.ring(0.1, 0.2, 40, 5),
         "rect -1 1 -1 1 4 4 1": lambda: cp.Mesh.rect(-1, 1, -1, 1, 4, 4),
         "rect -3 3 -2 2 6 4 1": lambda: cp.Mesh.rect(-3, 3, -2, 2, 6, 4),
+        # 8-node meshes (Mesh::remapOrder)
+        "hole -3 3 -2 2 0.5 12 8 2": lambda: cp.Mesh.rect_with_hole(-3, 3, -2, 2, 0.5, 12, 8, order=2),
+        "ring 50 120 16 4 2": lambda: cp.Mesh.ring(50, 120, 16, 4, order=2),
+        "rect -3 3 -2 2 6 4 2": lambda: cp.Mesh.rect(-3, 3, -2, 2, 6, 4, order=2),
     }
     for spec, mk in makers.items():
         m = mk()
@@ -132,9 +141,14 @@ def test_inp_loader_rejects_bad_files(tmp_path):
     q8 = tmp_path / "q8.inp"
     q8.write_text("*NODE\n" + "".join(f"{i + 1}, {i % 3}.0, {i // 3}.0\n" for i in range(9)) +
                   "**\n*ELEMENT, TYPE=S8R\n1, 1, 3, 9, 7, 2, 6, 8, 4\n")
+    m = cp.Mesh.load(q8)  # read into elem8, as the reference's reader does
+    assert m.count8() == 1
+    assert list(m.arrays()["elem8"][0]) == [0, 2, 8, 6, 1, 5, 7, 3]
+    bad = tmp_path / "bad.inp"
+    bad.write_text("*NODE\n1, 0.0, 0.0\n2, 1.0, 0.0\n**\n*ELEMENT, TYPE=S3\n1, 1, 2, 9\n")
     with pytest.raises(cp.CuplastError) as e:
-        cp.Mesh.load(q8)
-    assert e.value.status == _capi.CP_ERR_UNSUPPORTED
+        cp.Mesh.load(bad)  # a node that does not exist
+    assert e.value.status == _capi.CP_ERR_INVALID
 
 
 def test_batch_and_server_entry_points_validate_arguments_without_a_device():
@@ -178,3 +192,35 @@ def test_batch_and_server_entry_points_validate_arguments_without_a_device():
     assert L.cp_server_get_stats(None, None) == inv
     assert L.cp_server_destroy(None) == inv
     assert L.cp_secant_update_noalloc(None, None, 0, None, 0, None, None, None, None, None, None, None) == inv
+
+
+@pytest.mark.parametrize("name", ["hole_q8", "ring_q8", "rect_q8"])
+def test_q8_loads_match_reference(name, golden_dir):
+    """initConditions on 8-node meshes (src/PlasticitySolver.cu:819-927):
+    consistent quadratic-edge loads (1/3, 4/3, 1/3 weights, normal pressure
+    on curved edges), 8-node body forces (-1/12 per corner, 1/3 per mid-side
+    node), Dirichlet masks and prescribed values, against the reference's own
+    load builder on the same order-2 meshes. Bit for bit, up to the
+    summation order of shared nodes (1e-14 of the largest load)."""
+    import sys
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import Q8_LOADS
+
+    g = dict(np.load(os.path.join(golden_dir, "q8_loads.npz")))
+    spec, lines = Q8_LOADS[name]
+    w = spec.split()
+    f = [float(x) for x in w[1:]]
+    if w[0] == "hole":
+        mesh = cp.Mesh.rect_with_hole(*f[:5], int(f[5]), int(f[6]), order=int(f[7]))
+    elif w[0] == "ring":
+        mesh = cp.Mesh.ring(f[0], f[1], int(f[2]), int(f[3]), order=int(f[4]))
+    else:
+        mesh = cp.Mesh.rect(*f[:4], int(f[4]), int(f[5]), order=int(f[6]))
+    assert mesh.count8() > 0
+    job = product_runner.parse(lines)
+    rp, mask, uv = product_runner.loads_of(job).build(mesh, h=job["h"], rho=1.0)
+    ref = g[f"{name}_rp"]
+    assert np.max(np.abs(rp - ref)) <= 1e-14 * np.max(np.abs(ref))
+    assert np.array_equal(mask, g[f"{name}_mask"])
+    assert np.array_equal(uv, g[f"{name}_uv"])
