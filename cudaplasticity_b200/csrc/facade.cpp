@@ -354,7 +354,9 @@ void PlasticitySolver::ensureInstance() {
     v.elem3 = mesh_.elem3;
     v.count4 = mesh_.count4;
     v.elem4 = mesh_.elem4;
-    if (mesh_.count8) throw std::invalid_argument("second-order (Q8) elements are not supported");
+    if (mesh_.count8)
+        throw std::invalid_argument("PlasticitySolver: the device path has no 8-node (Q8) element yet; the mesh, I/O "
+                                    "and load building support them");
     cp_material mc = m_.toC(pc_ == stress ? CP_PLANE_STRESS : CP_PLANE_STRAIN);
     check(cp_instance_create(ctx_, &v, &mc, &inst_));
     std::vector<double> rp, uv;
@@ -474,6 +476,9 @@ void PlasticitySolver::saveAsVtk(const std::string& fileName) {
 
 SparseSLAE::SparseSLAE(Mesh& mesh, int dim_, int device) : dim(dim_) {
     if (dim_ != 2) throw std::invalid_argument("SparseSLAE: only dim = 2 (2D displacements) is supported");
+    if (mesh.count8)
+        throw std::invalid_argument("SparseSLAE: the device path has no 8-node (Q8) element yet; the mesh, I/O and "
+                                    "load building support them");
     cp_context* ctx = nullptr;
     cp_instance* inst = nullptr;
     auto fail = [&](int st) {
