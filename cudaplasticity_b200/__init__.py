@@ -122,16 +122,18 @@ class Mesh:
         return m
 
     @classmethod
-    def from_arrays(cls, node_xy, elem3=None, elem4=None, borders=()):
+    def from_arrays(cls, node_xy, elem3=None, elem4=None, borders=(), elem8=None):
         m = cls()
         xy = np.ascontiguousarray(node_xy, dtype=np.float64).ravel()
         e3 = np.ascontiguousarray(elem3 if elem3 is not None else np.zeros(0), dtype=np.int32).ravel()
         e4 = np.ascontiguousarray(elem4 if elem4 is not None else np.zeros(0), dtype=np.int32).ravel()
+        e8 = np.ascontiguousarray(elem8 if elem8 is not None else np.zeros(0), dtype=np.int32).ravel()
         bl = np.array([len(b) for b in borders], dtype=np.int32)
         bn = np.ascontiguousarray(np.concatenate([np.asarray(b, np.int32) for b in borders]) if len(borders)
                                   else np.zeros(1, np.int32), dtype=np.int32)
         m._check(C.lib().cpx_mesh_set(m._h, xy.size // 2, _dp(xy), e3.size // 3, _ip(e3), e4.size // 4, _ip(e4),
-                                      len(borders), _ip(bl) if len(bl) else None, _ip(bn)))
+                                      len(borders), _ip(bl) if len(bl) else None, _ip(bn), e8.size // 8,
+                                      _ip(e8) if e8.size else None))
         return m
 
     def split_t3(self):
@@ -281,9 +283,10 @@ def mesh_view(arrays):
     xy = np.ascontiguousarray(arrays["node_xy"], dtype=np.float64).ravel()
     e3 = np.ascontiguousarray(arrays.get("elem3", np.zeros(0)), dtype=np.int32).ravel()
     e4 = np.ascontiguousarray(arrays.get("elem4", np.zeros(0)), dtype=np.int32).ravel()
+    e8 = np.ascontiguousarray(arrays.get("elem8", np.zeros(0)), dtype=np.int32).ravel()
     v = C.cp_mesh_view(xy.size // 2, _dp(xy), e3.size // 3, _ip(e3) if e3.size else None, e4.size // 4,
-                       _ip(e4) if e4.size else None)
-    return v, (xy, e3, e4)
+                       _ip(e4) if e4.size else None, e8.size // 8, _ip(e8) if e8.size else None)
+    return v, (xy, e3, e4, e8)
 
 
 def solve_opts(**kw):
@@ -302,9 +305,10 @@ class Instance:
         self._h = C.c_p()
         v, keep = mesh_view(mesh_arrays)
         self.n_nodes = v.node_count
-        self.n_elem = v.count3 + v.count4
+        self.n_elem = v.count3 + v.count4 + v.count8
         self.count3 = v.count3
         self.count4 = v.count4
+        self.count8 = v.count8
         ctx.check(C.lib().cp_instance_create(ctx._h, ctypes.byref(v), ctypes.byref(mat), ctypes.byref(self._h)))
         ctx._deps.add(self)
         del keep
@@ -373,7 +377,7 @@ class Instance:
         return dict(rows=rows, cols=cols, adj_pos=adj_pos, adj=adj[:nadj], k_data=vals)
 
     def slot_map(self):
-        ns = 9 * self.count3 + 16 * self.count4
+        ns = 9 * self.count3 + 16 * self.count4 + 64 * self.count8
         s = np.zeros(max(ns, 1), np.int32)
         self.ctx.check(C.lib().cp_get_slot_map(self._h, _ip(s)))
         return s[:ns]
@@ -500,11 +504,11 @@ class _Handed(Instance):
     server's streams: it is freed before the server (Server.close frees the
     ones still open)."""
 
-    def __init__(self, server, handle, n_nodes, n_elem, count3, count4):
+    def __init__(self, server, handle, n_nodes, n_elem, count3, count4, count8=0):
         self.ctx = server.ctx
         self._server = server
         self._h = handle
-        self.n_nodes, self.n_elem, self.count3, self.count4 = n_nodes, n_elem, count3, count4
+        self.n_nodes, self.n_elem, self.count3, self.count4, self.count8 = n_nodes, n_elem, count3, count4, count8
 
 
 _LIVE_SERVERS = weakref.WeakSet()
@@ -564,7 +568,7 @@ class Server:
                                       ctypes.byref(o), ctypes.byref(rid))
         if st != C.CP_OK:
             raise CuplastError(st)
-        self._meta[rid.value] = (v.node_count, v.count3 + v.count4, v.count3, v.count4)
+        self._meta[rid.value] = (v.node_count, v.count3 + v.count4 + v.count8, v.count3, v.count4, v.count8)
         del keep
         return rid.value
 

@@ -42,7 +42,7 @@ class cp_material(ctypes.Structure):
 
 class cp_mesh_view(ctypes.Structure):
     _fields_ = [("node_count", c_int), ("node_xy", P_double), ("count3", c_int), ("elem3", P_int),
-                ("count4", c_int), ("elem4", P_int)]
+                ("count4", c_int), ("elem4", P_int), ("count8", c_int), ("elem8", P_int)]
 
 
 class cp_solve_opts(ctypes.Structure):
@@ -137,7 +137,7 @@ _SIGS = {
     "cpx_mesh_gen_ring": (c_int, [c_p, c_double, c_double, c_int, c_int, c_int]),
     "cpx_mesh_split_t3": (c_int, [c_p]),
     "cpx_mesh_load_inp": (c_int, [c_p, ctypes.c_char_p]),
-    "cpx_mesh_set": (c_int, [c_p, c_int, P_double, c_int, P_int, c_int, P_int, c_int, P_int, P_int]),
+    "cpx_mesh_set": (c_int, [c_p, c_int, P_double, c_int, P_int, c_int, P_int, c_int, P_int, P_int, c_int, P_int]),
     "cpx_mesh_counts": (c_int, [c_p, P_int, P_int, P_int, P_int, P_int, P_int]),
     "cpx_mesh_get": (c_int, [c_p, P_double, P_int, P_int, P_int, P_int, P_int]),
     "cpx_mesh_max_index_diff": (c_int, [c_p, P_int]),

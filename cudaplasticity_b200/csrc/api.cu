@@ -390,14 +390,15 @@ CP_API int cp_context_synchronize(cp_context* ctx) {
 }
 
 CP_API int cp_instance_footprint(const cp_mesh_view* m, int precision, size_t* bytes) {
-    if (!m || !bytes || m->node_count <= 0 || m->count3 < 0 || m->count4 < 0) return CP_ERR_INVALID;
-    const size_t n = (size_t)m->node_count, ne = (size_t)m->count3 + (size_t)m->count4;
-    const size_t incs = 3 * (size_t)m->count3 + 4 * (size_t)m->count4;
+    if (!m || !bytes || m->node_count <= 0 || m->count3 < 0 || m->count4 < 0 || m->count8 < 0) return CP_ERR_INVALID;
+    const size_t n = (size_t)m->node_count, ne = (size_t)m->count3 + (size_t)m->count4 + (size_t)m->count8;
+    const size_t incs = 3 * (size_t)m->count3 + 4 * (size_t)m->count4 + 8 * (size_t)m->count8;
     // upper bound of the neighbour count: the reference's link capacity
-    const size_t nadj = 2 * (size_t)m->count3 + 3 * (size_t)m->count4;
+    const size_t nadj = 2 * (size_t)m->count3 + 3 * (size_t)m->count4 + 7 * (size_t)m->count8;
     const size_t nadj_est = std::min(nadj, incs * 3);
     const size_t nnz = 4 * (nadj_est + n);
-    size_t b = n * 16 + ne * 16 + incs * 8 + (2 * n + 2) * 4 + nadj_est * 4;  // mesh + structure
+    size_t b = n * 16 + ne * 16 + (size_t)m->count8 * 16 + incs * (m->count8 ? 12 : 8) + (2 * n + 2) * 4 +
+               nadj_est * 4;                                                   // mesh + structure
     b += nnz * 8;                                                              // K (FP64)
     b += n * (16 * 8 + 2);                                                     // u, b, b_full, u_full, r, z, z, q, mask
     b += ne * 18 * 8;                                                          // element state
@@ -417,41 +418,53 @@ CP_API int cp_instance_create(cp_context* ctx, const cp_mesh_view* mv, const cp_
     if (const char* g = std::getenv("CUPLAST_FP64_CG")) I->fused_fp64 = std::strcmp(g, "classic") != 0;
     int rc = guarded(ctx, [&] {
         CP_CHECK(mv->node_count > 0 && mv->node_xy, CP_ERR_INVALID, "mesh: no nodes");
-        CP_CHECK(mv->count3 >= 0 && mv->count4 >= 0 && mv->count3 + mv->count4 > 0, CP_ERR_INVALID,
-                 "mesh: no elements");
+        CP_CHECK(mv->count3 >= 0 && mv->count4 >= 0 && mv->count8 >= 0 &&
+                     (long long)mv->count3 + mv->count4 + mv->count8 > 0,
+                 CP_ERR_INVALID, "mesh: no elements");
         CP_CHECK(mv->count3 == 0 || mv->elem3, CP_ERR_INVALID, "mesh: elem3 missing");
         CP_CHECK(mv->count4 == 0 || mv->elem4, CP_ERR_INVALID, "mesh: elem4 missing");
-        CP_CHECK((long long)mv->count3 + mv->count4 < (1LL << 29), CP_ERR_UNSUPPORTED, "mesh: too many elements");
+        CP_CHECK(mv->count8 == 0 || mv->elem8, CP_ERR_INVALID, "mesh: elem8 missing");
+        CP_CHECK((long long)mv->count3 + mv->count4 + mv->count8 < (1LL << 28), CP_ERR_UNSUPPORTED,
+                 "mesh: too many elements");
         validate_material(*mat);
         CP_CUDA(cudaSetDevice(ctx->device));
         I->mat_host = *mat;
         I->mat = to_dev(*mat);
         I->n_nodes = mv->node_count;
-        I->n_elem = mv->count3 + mv->count4;
+        I->n_elem = mv->count3 + mv->count4 + mv->count8;
         cudaStream_t s = I->s();
         // mesh upload (the reference's meshToGPU, src/Mesh.cu:678-717)
         I->mesh.n_nodes = mv->node_count;
         I->mesh.c3 = mv->count3;
         I->mesh.c4 = mv->count4;
+        I->mesh.c8 = mv->count8;
         I->mesh.xy = I->alloc<double2>(I->n_nodes);
         std::vector<int4> e3((size_t)mv->count3), e4((size_t)mv->count4);
         for (int e = 0; e < mv->count3; ++e)
             e3[e] = make_int4(mv->elem3[3 * e], mv->elem3[3 * e + 1], mv->elem3[3 * e + 2], -1);
         for (int e = 0; e < mv->count4; ++e)
             e4[e] = make_int4(mv->elem4[4 * e], mv->elem4[4 * e + 1], mv->elem4[4 * e + 2], mv->elem4[4 * e + 3]);
+        std::vector<int4> e8(2 * (size_t)mv->count8);
+        for (size_t q = 0; q < e8.size(); ++q)
+            e8[q] = make_int4(mv->elem8[4 * q], mv->elem8[4 * q + 1], mv->elem8[4 * q + 2], mv->elem8[4 * q + 3]);
         I->mesh.e3 = I->alloc<int4>(e3.size());
         I->mesh.e4 = I->alloc<int4>(e4.size());
+        I->mesh.e8 = I->alloc<int4>(e8.size());
         CP_CUDA(cudaMemcpyAsync(I->mesh.xy, mv->node_xy, sizeof(double2) * I->n_nodes, cudaMemcpyHostToDevice, s));
         if (!e3.empty()) CP_CUDA(cudaMemcpyAsync(I->mesh.e3, e3.data(), sizeof(int4) * e3.size(), cudaMemcpyHostToDevice, s));
         if (!e4.empty()) CP_CUDA(cudaMemcpyAsync(I->mesh.e4, e4.data(), sizeof(int4) * e4.size(), cudaMemcpyHostToDevice, s));
+        if (!e8.empty()) CP_CUDA(cudaMemcpyAsync(I->mesh.e8, e8.data(), sizeof(int4) * e8.size(), cudaMemcpyHostToDevice, s));
         // sparsity structure + slot map on the device
         cp::setup_csr(I->mesh, I->csr, s, I->sms());
         I->allocs.push_back(I->csr.inc_pos);
         I->allocs.push_back(I->csr.adj_pos);
         I->allocs.push_back(I->csr.inc);
         I->allocs.push_back(I->csr.inc_k);
+        if (I->csr.inc_k8) I->allocs.push_back(I->csr.inc_k8);
         I->allocs.push_back(I->csr.adj);
-        I->bytes += (size_t)(2 * (I->n_nodes + 1)) * 4 + (3ull * mv->count3 + 4ull * mv->count4) * 8 + I->csr.nadj * 4;
+        I->bytes += (size_t)(2 * (I->n_nodes + 1)) * 4 +
+                    (3ull * mv->count3 + 4ull * mv->count4 + 8ull * mv->count8) * (mv->count8 ? 12 : 8) +
+                    I->csr.nadj * 4;
         CP_CHECK(I->csr.nnz < (1LL << 31), CP_ERR_UNSUPPORTED, "matrix too large for 32-bit CSR offsets");
         I->allocs.push_back(I->csr.slice_ptr);
         I->allocs.push_back(I->csr.scol);
@@ -815,7 +828,7 @@ CP_API int cp_get_slot_map(cp_instance* I, int* slots) {
     if (!I || !slots) return CP_ERR_INVALID;
     return guarded(I->ctx, [&] {
         cudaStream_t s = I->s();
-        const size_t ns = 9 * (size_t)I->mesh.c3 + 16 * (size_t)I->mesh.c4;
+        const size_t ns = 9 * (size_t)I->mesh.c3 + 16 * (size_t)I->mesh.c4 + 64 * (size_t)I->mesh.c8;
         int* d = nullptr;
         CP_CUDA(cudaMallocAsync(&d, sizeof(int) * std::max<size_t>(ns, 1), s));
         cp::csr_slot_map(I->mesh, I->csr, d, s);

@@ -79,6 +79,7 @@ struct BDesc {
     const int* inc_pos;
     const int* inc;
     const uint32_t* inc_k;
+    const uint32_t* inc_k8;
     double* val64;
     float* val32;
     double2* x;
@@ -596,6 +597,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_probe(const BDesc* __restric
 // slice's blocks accumulated in the warp's shared-memory region (each lane
 // only touches its own node's blocks; element order) and written once,
 // coalesced. Same arithmetic as the single-instance assembly.
+template <bool Q8>
 __global__ void __launch_bounds__(kThreads) k_batch_asm(const BDesc* __restrict__ D, BState* SS,
                                                         const int4* __restrict__ tiles, BCtl* c, int max_width) {
     extern __shared__ double sacc[];
@@ -623,9 +625,9 @@ __global__ void __launch_bounds__(kThreads) k_batch_asm(const BDesc* __restrict_
                 double* nb = acc + 4 * lane;
                 for (int q = d.inc_pos[n]; q < d.inc_pos[n + 1]; ++q) {
                     const int code = d.inc[q];
-                    const int e = code >> 2, i = code & 3;
+                    const int e = code >> 3, i = code & 7;
                     const Dmat dm = form_d(d.mat.plane, d.st.E_c[e], d.st.nu_c[e]);
-                    element_rows(d.m, e, i, d.inc_k[q], dm, d.mat.h, nb);
+                    element_rows<Q8>(d.m, e, i, d.inc_k[q], Q8 && d.inc_k8 ? d.inc_k8[q] : 0u, dm, d.mat.h, nb);
                 }
             }
             __syncwarp();
@@ -649,6 +651,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_asm(const BDesc* __restrict_
 
 // --------------------------------------------------- element phases --
 
+template <bool Q8>
 __global__ void __launch_bounds__(kThreads) k_batch_elem(const BDesc* __restrict__ D, BState* SS,
                                                          const int4* __restrict__ tiles, BCtl* c) {
     __shared__ double sh[2 * kWarps];
@@ -665,7 +668,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_elem(const BDesc* __restrict
         const int ph = tile_phase(S, &shp);
         if (ph != PH_LEVEL && ph != PH_UPD && ph != PH_RELAX && ph != PH_PLASTIC) continue;
         const BDesc& d = D[tl.x];
-        const int ne = d.m.c3 + d.m.c4;
+        const int ne = d.m.c3 + d.m.c4 + d.m.c8;
         const int g0 = tl.y * tl.z, g1 = min(g0 + tl.z, d.n_groups);
         if (ph == PH_LEVEL) {
             // k_set_level and the Aitken history reset of cp_solve
@@ -704,7 +707,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_elem(const BDesc* __restrict
             for (int g = g0 + w; g < g1; g += kWarps) {
                 const int e = 32 * g + lane;
                 double s_num = 0.0, s_den = 0.0, s_an = 0.0, s_ad = 0.0;
-                if (e < ne) update_element(d.m, d.mat, d.x, d.st, e, d.aitken, s_num, s_den, s_an, s_ad);
+                if (e < ne) update_element<Q8>(d.m, d.mat, d.x, d.st, e, d.aitken, s_num, s_den, s_an, s_ad);
                 s_num = warp_sum(s_num);
                 s_den = warp_sum(s_den);
                 s_an = warp_sum(s_an);
@@ -816,7 +819,8 @@ struct cp_batch {
     double* d_psums = nullptr;           // autotuner probe sums (one per block)
     size_t asm_smem = 0;
     bool running = false;
-    bool use_graph = true;  // false (CUPLAST_NO_GRAPH=1): trips launched kernel by kernel, for profilers
+    bool use_graph = true;
+    bool q8 = false;  // an 8-node instance joined: element kernels with the 8-node element  // false (CUPLAST_NO_GRAPH=1): trips launched kernel by kernel, for profilers
     int last_tiles = 0;
     long long trips = 0, launches = 0, runs = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // bracket each run on the batch's stream
@@ -930,12 +934,31 @@ void interleave_tiles(cp_batch* b, int n) {
     std::memcpy(b->h_tiles, out.data(), sizeof(int4) * (size_t)n);
 }
 
+// Grids of the element and assembly kernels: as many blocks as fit on the
+// GPU. Q8 selects the instantiations with the 8-node element, used from the
+// first 8-node instance on (they need more registers).
+template <bool Q8>
+void element_grids(cp_batch* b) {
+    int per_sm = 0;
+    CP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_elem<Q8>, kThreads, 0));
+    b->grid_elem = b->ctx->sm_count * std::max(1, std::min(per_sm, 8));
+    CP_CUDA(cudaFuncSetAttribute(k_batch_asm<Q8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->asm_smem));
+    CP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_asm<Q8>, kThreads, b->asm_smem));
+    b->grid_asm = b->ctx->sm_count * std::max(1, per_sm);
+}
+
 // One trip: element phases, assembly, CG launches.
 void launch_body(cp_batch* b, cudaStream_t s) {
-    for (int k = 0; k < b->o.elem_per_trip; ++k)
-        k_batch_elem<<<b->grid_elem, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
-    k_batch_asm<<<b->grid_asm, kThreads, b->asm_smem, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl,
-                                                           b->o.max_width);
+    for (int k = 0; k < b->o.elem_per_trip; ++k) {
+        if (b->q8) k_batch_elem<true><<<b->grid_elem, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
+        else k_batch_elem<false><<<b->grid_elem, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
+    }
+    if (b->q8)
+        k_batch_asm<true><<<b->grid_asm, kThreads, b->asm_smem, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl,
+                                                                     b->o.max_width);
+    else
+        k_batch_asm<false><<<b->grid_asm, kThreads, b->asm_smem, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl,
+                                                                      b->o.max_width);
     for (int k = 0; k < b->o.cg_per_trip; ++k)
         k_batch_cg<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
 }
@@ -1046,12 +1069,8 @@ CP_API int cp_batch_create(cp_context* ctx, const cp_batch_opts* opts, cp_batch*
         CP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cg, kThreads, 0));
         if (o.cg_blocks_per_sm > 0) per_sm = std::min(per_sm, o.cg_blocks_per_sm);
         b->grid_cg = ctx->sm_count * std::max(1, per_sm);
-        CP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_elem, kThreads, 0));
-        b->grid_elem = ctx->sm_count * std::max(1, std::min(per_sm, 8));
         b->asm_smem = (size_t)kWarps * 128 * o.max_width * sizeof(double);
-        CP_CUDA(cudaFuncSetAttribute(k_batch_asm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->asm_smem));
-        CP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_asm, kThreads, b->asm_smem));
-        b->grid_asm = ctx->sm_count * std::max(1, per_sm);
+        element_grids<false>(b);
         CP_CUDA(cudaEventCreate(&b->ev0));
         CP_CUDA(cudaEventCreate(&b->ev1));
         CP_CUDA(cudaMalloc(&b->d_sink, sizeof(float2) * (size_t)b->grid_cg * kThreads));
@@ -1115,6 +1134,16 @@ CP_API int cp_batch_add(cp_batch* b, cp_instance* I, const cp_solve_opts* opts, 
             }
         CP_CHECK(sl >= 0, CP_ERR_BUSY, "no free batch slot");
         CP_CUDA(cudaSetDevice(b->ctx->device));
+        if (I->mesh.c8 && !b->q8) {
+            // the first 8-node instance: switch to the kernels that have the
+            // 8-node element, and capture the trip again with them
+            b->q8 = true;
+            element_grids<true>(b);
+            if (b->graph) {
+                cudaGraphExecDestroy(b->graph);
+                b->graph = nullptr;
+            }
+        }
         instance_prepare_mixed(I, o.precond);
         BDesc d{};
         d.m = I->mesh;
@@ -1125,6 +1154,7 @@ CP_API int cp_batch_add(cp_batch* b, cp_instance* I, const cp_solve_opts* opts, 
         d.inc_pos = I->csr.inc_pos;
         d.inc = I->csr.inc;
         d.inc_k = I->csr.inc_k;
+        d.inc_k8 = I->csr.inc_k8;
         d.val64 = I->csr.val64;
         d.val32 = I->csr.val32;
         d.x = I->u;

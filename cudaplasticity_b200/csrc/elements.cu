@@ -23,7 +23,7 @@ constexpr int kAsmThreads = 128;  // = 4 slices of 32 nodes
 // one contiguous range of values in the sliced layout, accumulated in shared
 // memory (each thread only touches its own node's blocks: no atomics, and the
 // summation order is the element order) and written out coalesced, once.
-template <bool W64, bool W32>
+template <bool W64, bool W32, bool Q8>
 __global__ void __launch_bounds__(kAsmThreads) k_assemble(DevMesh m, DevCsr csr, MaterialDev M, const double* E_c,
                                                           const double* nu_c) {
     extern __shared__ double sacc[];
@@ -39,9 +39,9 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(DevMesh m, DevCsr csr,
             double* nb = sacc + 4 * (csr.slice_ptr[n >> 5] - B0 + (n & 31));
             for (int q = csr.inc_pos[n]; q < csr.inc_pos[n + 1]; ++q) {
                 const int code = csr.inc[q];
-                const int e = code >> 2, i = code & 3;
+                const int e = code >> 3, i = code & 7;
                 const Dmat d = form_d(M.plane, E_c[e], nu_c[e]);
-                element_rows(m, e, i, csr.inc_k[q], d, M.h, nb);
+                element_rows<Q8>(m, e, i, csr.inc_k[q], Q8 ? csr.inc_k8[q] : 0u, d, M.h, nb);
             }
         }
         __syncthreads();
@@ -65,14 +65,15 @@ constexpr int kElemThreads = 256;
 // last assembly, stress intensity, secant update, and the two exit-norm sums
 // (reduced deterministically by the last block). With Aitken on, the raw
 // secant target psi is stored as a residual and the relax kernel moves psi.
+template <bool Q8>
 __global__ void __launch_bounds__(kElemThreads) k_update(DevMesh m, MaterialDev M, const double2* __restrict__ u,
                                                          ElemState st, OuterScalars* sc, double* partials, int aitken) {
     __shared__ double sh[2 * kElemThreads / 32];
     __shared__ bool last;
-    const int ne = m.c3 + m.c4;
+    const int ne = m.c3 + m.c4 + m.c8;
     double s_num = 0.0, s_den = 0.0, s_an = 0.0, s_ad = 0.0;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x)
-        update_element(m, M, u, st, e, aitken, s_num, s_den, s_an, s_ad);
+        update_element<Q8>(m, M, u, st, e, aitken, s_num, s_den, s_an, s_ad);
     double2 a = block_sum2(s_num, s_den, sh);
     double2 b = aitken ? block_sum2(s_an, s_ad, sh) : make_double2(0.0, 0.0);
     if (threadIdx.x == 0) {
@@ -106,7 +107,7 @@ namespace {
 // psi_{k+1} = psi_k + w_k r_k, w_k = -w_{k-1} (r_{k-1}, r_k - r_{k-1}) / |r_k - r_{k-1}|^2.
 // The fixed point (r = 0) is the reference's.
 __global__ void k_aitken(DevMesh m, MaterialDev M, ElemState st, const OuterScalars* sc, double w) {
-    const int ne = m.c3 + m.c4;
+    const int ne = m.c3 + m.c4 + m.c8;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x)
         relax_element(M, st, e, w);
 }
@@ -120,6 +121,21 @@ __global__ void k_plastic(int ne, MaterialDev M, ElemState st) {
 
 }  // namespace
 
+template <bool Q8>
+void assemble_as(const DevMesh& m, const DevCsr& csr, const MaterialDev& mat, const double* E_c, const double* nu_c,
+                 bool want64, bool want32, int grid, size_t smem, cudaStream_t s) {
+    if (want64 && want32) {
+        CP_CUDA(cudaFuncSetAttribute(k_assemble<true, true, Q8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_assemble<true, true, Q8><<<grid, kAsmThreads, smem, s>>>(m, csr, mat, E_c, nu_c);
+    } else if (want64) {
+        CP_CUDA(cudaFuncSetAttribute(k_assemble<true, false, Q8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_assemble<true, false, Q8><<<grid, kAsmThreads, smem, s>>>(m, csr, mat, E_c, nu_c);
+    } else {
+        CP_CUDA(cudaFuncSetAttribute(k_assemble<false, true, Q8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_assemble<false, true, Q8><<<grid, kAsmThreads, smem, s>>>(m, csr, mat, E_c, nu_c);
+    }
+}
+
 void launch_assemble(const DevMesh& m, const DevCsr& csr, const MaterialDev& mat, const double* E_c,
                      const double* nu_c, bool want64, bool want32, cudaStream_t s, int sm_count) {
     const int ntiles = (m.n_nodes + kAsmThreads - 1) / kAsmThreads;
@@ -127,16 +143,10 @@ void launch_assemble(const DevMesh& m, const DevCsr& csr, const MaterialDev& mat
     CP_CHECK(smem <= 200 * 1024, CP_ERR_UNSUPPORTED, "node degree too large for the assembly tile");
     int grid = ntiles < sm_count * 8 ? ntiles : sm_count * 8;
     if (grid < 1) grid = 1;
-    if (want64 && want32) {
-        CP_CUDA(cudaFuncSetAttribute(k_assemble<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_assemble<true, true><<<grid, kAsmThreads, smem, s>>>(m, csr, mat, E_c, nu_c);
-    } else if (want64) {
-        CP_CUDA(cudaFuncSetAttribute(k_assemble<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_assemble<true, false><<<grid, kAsmThreads, smem, s>>>(m, csr, mat, E_c, nu_c);
-    } else {
-        CP_CUDA(cudaFuncSetAttribute(k_assemble<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_assemble<false, true><<<grid, kAsmThreads, smem, s>>>(m, csr, mat, E_c, nu_c);
-    }
+    if (m.c8)
+        assemble_as<true>(m, csr, mat, E_c, nu_c, want64, want32, grid, smem, s);
+    else
+        assemble_as<false>(m, csr, mat, E_c, nu_c, want64, want32, grid, smem, s);
     CP_CUDA(cudaGetLastError());
 }
 
@@ -148,20 +158,23 @@ int update_grid(int ne, int sm_count) {
 
 void launch_update(const DevMesh& m, const MaterialDev& mat, const double2* u, ElemState& st, OuterScalars* sc,
                    double* partials, int aitken, cudaStream_t s, int sm_count) {
-    const int ne = m.c3 + m.c4;
-    k_update<<<update_grid(ne, sm_count), kElemThreads, 0, s>>>(m, mat, u, st, sc, partials, aitken);
+    const int ne = m.c3 + m.c4 + m.c8;
+    if (m.c8)
+        k_update<true><<<update_grid(ne, sm_count), kElemThreads, 0, s>>>(m, mat, u, st, sc, partials, aitken);
+    else
+        k_update<false><<<update_grid(ne, sm_count), kElemThreads, 0, s>>>(m, mat, u, st, sc, partials, aitken);
     CP_CUDA(cudaGetLastError());
 }
 
 void launch_aitken_relax(const DevMesh& m, const MaterialDev& mat, ElemState& st, const OuterScalars* sc, double w,
                          cudaStream_t s, int sm_count) {
-    const int ne = m.c3 + m.c4;
+    const int ne = m.c3 + m.c4 + m.c8;
     k_aitken<<<update_grid(ne, sm_count), kElemThreads, 0, s>>>(m, mat, st, sc, w);
     CP_CUDA(cudaGetLastError());
 }
 
 void launch_plastic(const DevMesh& m, const MaterialDev& mat, ElemState& st, cudaStream_t s, int sm_count) {
-    const int ne = m.c3 + m.c4;
+    const int ne = m.c3 + m.c4 + m.c8;
     k_plastic<<<update_grid(ne, sm_count), kElemThreads, 0, s>>>(ne, mat, st);
     CP_CUDA(cudaGetLastError());
 }
@@ -249,7 +262,7 @@ extern "C" CP_API int cp_secant_update_noalloc(void* stream, const cp_material* 
     es.table_s = d_fields + 8 * ne;
     es.psi = d_psi; es.E_c = d_E_c; es.nu_c = d_nu_c;
     const int grid = (count4 + cp::kElemThreads - 1) / cp::kElemThreads;  // <= kNoAllocMaxBlocks
-    cp::k_update<<<grid, cp::kElemThreads, 0, s>>>(m, M, reinterpret_cast<const double2*>(d_uv), es, sc, partials, 0);
+    cp::k_update<false><<<grid, cp::kElemThreads, 0, s>>>(m, M, reinterpret_cast<const double2*>(d_uv), es, sc, partials, 0);
     if (cudaGetLastError() != cudaSuccess) return CP_ERR_CUDA;
     double host_err = 0.0;
     if (cudaMemcpyAsync(&host_err, &sc->rel_err, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)

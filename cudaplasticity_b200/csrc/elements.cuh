@@ -59,6 +59,45 @@ __device__ __forceinline__ double q4_grad(const double* x, const double* y, doub
     return det;
 }
 
+// calcB8 (src/PlasticitySolver.cu:67-134) at (r, s): gradients and detJ of the
+// 8-node serendipity quad. Local nodes: corners (1,1), (-1,1), (-1,-1), (1,-1),
+// then the mid-sides of the edges s = 1, r = -1, s = -1, r = 1. Corner shape
+// functions (1 + r ri)(1 + s si)(r ri + s si - 1)/4, mid-side ones
+// (1 - r^2)(1 + s si)/2 and (1 + r ri)(1 - s^2)/2, differentiated in factored
+// form. The 3x3 Gauss rule uses sqrt(3/5), 5/9 and 8/9 to full precision.
+__device__ __forceinline__ double q8_grad(const double* x, const double* y, double r, double s, double* bx,
+                                          double* by) {
+    double dr[8], ds[8];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double ri = (k == 0 || k == 3) ? 1. : -1., si = k < 2 ? 1. : -1.;
+        dr[k] = 0.25 * ri * (1. + s * si) * (2. * r * ri + s * si);
+        ds[k] = 0.25 * si * (1. + r * ri) * (r * ri + 2. * s * si);
+    }
+    dr[4] = -r * (1. + s);        ds[4] = 0.5 * (1. - r * r);     // s = 1
+    dr[5] = -0.5 * (1. - s * s);  ds[5] = -s * (1. - r);          // r = -1
+    dr[6] = -r * (1. - s);        ds[6] = -0.5 * (1. - r * r);    // s = -1
+    dr[7] = 0.5 * (1. - s * s);   ds[7] = -s * (1. + r);          // r = 1
+    double xr = 0., yr = 0., xs = 0., ys = 0.;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        xr += dr[k] * x[k]; yr += dr[k] * y[k];
+        xs += ds[k] * x[k]; ys += ds[k] * y[k];
+    }
+    const double det = xr * ys - yr * xs;
+    const double inv = 1. / det;
+    const double rx = ys * inv, sx = -yr * inv, ry = -xs * inv, sy = xr * inv;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        bx[k] = dr[k] * rx + ds[k] * sx;
+        by[k] = dr[k] * ry + ds[k] * sy;
+    }
+    return det;
+}
+
+__device__ __forceinline__ double q8_point(int g) { return g == 0 ? -0.7745966692414834 : (g == 1 ? 0.0 : 0.7745966692414834); }
+__device__ __forceinline__ double q8_weight(int g) { return g == 1 ? 8.0 / 9.0 : 5.0 / 9.0; }
+
 // CST gradients (no reference counterpart: calcB3 is only declared,
 // src/PlasticitySolver.cu:21-23). Returns the signed area.
 __device__ __forceinline__ double t3_grad(const double* x, const double* y, double* bx, double* by) {
@@ -97,8 +136,10 @@ __device__ __forceinline__ int nth(const int4& v, int j) {
 
 // Row-block (i, all j) of element e's stiffness, scaled by h, added into the
 // owning node's 2x2 blocks through the slot bytes kk (block index k of local
-// node j); block k of the node starts at nb + 128 k (sliced layout, 32 nodes
-// x 4 values per block row).
+// node j; kk8 for local nodes 4..7 of an 8-node element); block k of the node
+// starts at nb + 128 k (sliced layout, 32 nodes x 4 values per block row).
+// Q8 = false compiles the 8-node branch out (it needs about 50 registers
+// more), for meshes without 8-node elements.
 __device__ __forceinline__ void add_scaled(double* b, const double* blk, double h) {
     b[0] = __dadd_rn(b[0], __dmul_rn(blk[0], h));
     b[1] = __dadd_rn(b[1], __dmul_rn(blk[1], h));
@@ -106,8 +147,42 @@ __device__ __forceinline__ void add_scaled(double* b, const double* blk, double 
     b[3] = __dadd_rn(b[3], __dmul_rn(blk[3], h));
 }
 
-__device__ __forceinline__ void element_rows(const DevMesh& m, int e, int i, uint32_t kk, const Dmat& d, double h,
-                                             double* nb) {
+template <bool Q8>
+__device__ __forceinline__ void element_rows(const DevMesh& m, int e, int i, uint32_t kk, uint32_t kk8, const Dmat& d,
+                                             double h, double* nb) {
+    if (Q8 && e >= m.c3 + m.c4) {
+        // formKe8 (src/PlasticitySolver.cu:189-224), one Gauss point at a
+        // time: each point's block h (B_i^T D B_j) w detJ goes straight into
+        // the node's accumulator (the mirrored thread adds the transposed
+        // values in the same order, so K stays bitwise symmetric)
+        const int le = e - m.c3 - m.c4;
+        const int4 c = m.e8[2 * le], md = m.e8[2 * le + 1];
+        double x[8], y[8];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const double2 p = m.xy[nth(c, a)], q = m.xy[nth(md, a)];
+            x[a] = p.x; y[a] = p.y;
+            x[4 + a] = q.x; y[4 + a] = q.y;
+        }
+        for (int g = 0; g < 9; ++g) {
+            double bx[8], by[8];
+            const int gi = g / 3, gj = g - 3 * gi;
+            const double det = q8_grad(x, y, q8_point(gi), q8_point(gj), bx, by);
+            const double w = q8_weight(gi) * q8_weight(gj) * det;
+            double bxi = bx[0], byi = by[0];
+#pragma unroll
+            for (int a = 1; a < 8; ++a)
+                if (i == a) { bxi = bx[a]; byi = by[a]; }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                double blk[4] = {0.0, 0.0, 0.0, 0.0};
+                add_block(blk, bxi, byi, bx[j], by[j], d, w);
+                const uint32_t k = j < 4 ? (kk >> (8 * j)) & 0xffu : (kk8 >> (8 * (j - 4))) & 0xffu;
+                add_scaled(nb + 128 * (int)k, blk, h);
+            }
+        }
+        return;
+    }
     double x[4], y[4];
     if (e < m.c3) {
         int4 el = m.e3[e];
@@ -194,12 +269,13 @@ __device__ double diagram_f(const MaterialDev& M, double eps) {
 }
 
 
-// strain4 + plastStress (src/PlasticitySolver.cu:1517-1549, 1590-1610) for
+// strain4 / strain8 + plastStress (src/PlasticitySolver.cu:1517-1610) for
 // element e: element-mean strain, stress from the C of the last assembly,
 // stress intensity, diagram value and the secant target psi. Adds the exit
 // norm terms (sig_i - table_s)^2, table_s^2 to num / den. Without Aitken psi,
 // E_c, nu_c move to the secant target; with Aitken the target is stored as a
-// residual and the Aitken sums are added to an / ad.
+// residual and the Aitken sums are added to an / ad. Q8 as for element_rows.
+template <bool Q8>
 __device__ __forceinline__ void update_element(const DevMesh& m, const MaterialDev& M, const double2* __restrict__ u,
                                                const ElemState& st, int e, int aitken, double& s_num, double& s_den,
                                                double& s_an, double& s_ad) {
@@ -217,6 +293,35 @@ __device__ __forceinline__ void update_element(const DevMesh& m, const MaterialD
         ex = uu[0] * bx[0] + uu[1] * bx[1] + uu[2] * bx[2];
         ey = vv[0] * by[0] + vv[1] * by[1] + vv[2] * by[2];
         g = uu[0] * by[0] + uu[1] * by[1] + uu[2] * by[2] + vv[0] * bx[0] + vv[1] * bx[1] + vv[2] * bx[2];
+    } else if (Q8 && e >= m.c3 + m.c4) {
+        // strain8 (src/PlasticitySolver.cu:1551-1588): the Gauss-weighted
+        // mean over the reference square, (1/4) sum w_i w_j eps(r_i, s_j)
+        const int le = e - m.c3 - m.c4;
+        const int4 c = m.e8[2 * le], md = m.e8[2 * le + 1];
+        double x[8], y[8], uu[8], vv[8];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int n0 = nth(c, a), n1 = nth(md, a);
+            const double2 p = m.xy[n0], q = m.xy[n1], w0 = u[n0], w1 = u[n1];
+            x[a] = p.x; y[a] = p.y; uu[a] = w0.x; vv[a] = w0.y;
+            x[4 + a] = q.x; y[4 + a] = q.y; uu[4 + a] = w1.x; vv[4 + a] = w1.y;
+        }
+        ex = 0.0; ey = 0.0; g = 0.0;
+        for (int gp = 0; gp < 9; ++gp) {
+            double bx[8], by[8];
+            const int gi = gp / 3, gj = gp - 3 * gi;
+            q8_grad(x, y, q8_point(gi), q8_point(gj), bx, by);
+            double exl = 0.0, eyl = 0.0, gl = 0.0;
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                exl += uu[a] * bx[a];
+                eyl += vv[a] * by[a];
+                gl += uu[a] * by[a] + vv[a] * bx[a];
+            }
+            const double w = q8_weight(gi) * q8_weight(gj);
+            ex += exl * w; ey += eyl * w; g += gl * w;
+        }
+        ex *= 0.25; ey *= 0.25; g *= 0.25;
     } else {
         int4 el = m.e4[e - m.c3];
         double x[4], y[4], uu[4], vv[4];

@@ -354,9 +354,8 @@ void PlasticitySolver::ensureInstance() {
     v.elem3 = mesh_.elem3;
     v.count4 = mesh_.count4;
     v.elem4 = mesh_.elem4;
-    if (mesh_.count8)
-        throw std::invalid_argument("PlasticitySolver: the device path has no 8-node (Q8) element yet; the mesh, I/O "
-                                    "and load building support them");
+    v.count8 = mesh_.count8;
+    v.elem8 = mesh_.elem8;
     cp_material mc = m_.toC(pc_ == stress ? CP_PLANE_STRESS : CP_PLANE_STRAIN);
     check(cp_instance_create(ctx_, &v, &mc, &inst_));
     std::vector<double> rp, uv;
@@ -403,10 +402,18 @@ std::vector<double> PlasticitySolver::field(const std::string& name) const {
 double PlasticitySolver::getSxx0() const { return field("sxx")[0]; }
 double PlasticitySolver::getExx0() const { return field("exx")[0]; }
 
+// deformEnergy (src/PlasticitySolver.cuh:415-445): elements on the plastic
+// branch integrate the diagram, except 8-node ones, for which the reference
+// always takes the secant energy eps_i sig_i / 2.
 double PlasticitySolver::deformEnergy() {
     std::vector<double> sI = field("sig_i"), eI = field("eps_i");
     double energy = 0.;
+    const int q8 = mesh_.count3 + mesh_.count4;
     for (int e = 0; e < mesh_.elemCount(); ++e) {
+        if (e >= q8) {
+            energy += eI[e] * sI[e] * 0.5 * (m_.h * mesh_.elemSpace8(e - q8));
+            continue;
+        }
         double vol = m_.h * (e < mesh_.count3 ? mesh_.elemSpace3(e) : mesh_.elemSpace4(e - mesh_.count3));
         if (sI[e] > m_.sigmaT) {
             double ET = m_.sigmaT / m_.E;
@@ -432,7 +439,7 @@ void PlasticitySolver::saveAsVtk(const std::string& fileName) {
     f << "# vtk DataFile Version 2.0\nSolution\nASCII\nDATASET POLYDATA\n";
     f << "POINTS " << mesh_.nodeCount << " float\n";
     for (int i = 0; i < mesh_.nodeCount; ++i) f << mesh_.node[i].x << " " << mesh_.node[i].y << " " << 0 << "\n";
-    f << "POLYGONS " << ne << " " << 4 * mesh_.count3 + 5 * mesh_.count4;
+    f << "POLYGONS " << ne << " " << 4 * mesh_.count3 + 5 * mesh_.count4 + 9 * mesh_.count8;
     for (int i = 0; i < mesh_.count3; ++i) {
         f << "\n3 ";
         for (int j = 3 * i; j < 3 * (i + 1); ++j) f << mesh_.elem3[j] << " ";
@@ -440,6 +447,11 @@ void PlasticitySolver::saveAsVtk(const std::string& fileName) {
     for (int i = 0; i < mesh_.count4; ++i) {
         f << "\n4 ";
         for (int j = 4 * i; j < 4 * (i + 1); ++j) f << mesh_.elem4[j] << " ";
+    }
+    // an 8-node element as the polygon corner, mid-side, corner, ...
+    for (int i = 0; i < mesh_.count8; ++i) {
+        f << "\n8 ";
+        for (int j = 8 * i; j < 8 * i + 4; ++j) f << mesh_.elem8[j] << " " << mesh_.elem8[j + 4] << " ";
     }
     f << "\nCELL_DATA " << ne << "\nSCALARS ElementID int 1\nLOOKUP_TABLE default\n";
     for (int i = 0; i < ne; ++i) f << i << "\n";
@@ -476,9 +488,6 @@ void PlasticitySolver::saveAsVtk(const std::string& fileName) {
 
 SparseSLAE::SparseSLAE(Mesh& mesh, int dim_, int device) : dim(dim_) {
     if (dim_ != 2) throw std::invalid_argument("SparseSLAE: only dim = 2 (2D displacements) is supported");
-    if (mesh.count8)
-        throw std::invalid_argument("SparseSLAE: the device path has no 8-node (Q8) element yet; the mesh, I/O and "
-                                    "load building support them");
     cp_context* ctx = nullptr;
     cp_instance* inst = nullptr;
     auto fail = [&](int st) {
@@ -495,7 +504,8 @@ SparseSLAE::SparseSLAE(Mesh& mesh, int dim_, int device) : dim(dim_) {
         xy[2 * i] = mesh.node[i].x;
         xy[2 * i + 1] = mesh.node[i].y;
     }
-    cp_mesh_view v{mesh.nodeCount, xy.data(), mesh.count3, mesh.elem3, mesh.count4, mesh.elem4};
+    cp_mesh_view v{mesh.nodeCount, xy.data(), mesh.count3, mesh.elem3, mesh.count4, mesh.elem4, mesh.count8,
+                   mesh.elem8};
     cp_material mat{};
     mat.E = 1.0;
     mat.nu = 0.3;

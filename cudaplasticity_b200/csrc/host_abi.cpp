@@ -65,8 +65,8 @@ CP_API int cpx_mesh_split_t3(cpx_mesh* m) {
     return guard([&] { m->m.splitToTriangles(); });
 }
 CP_API int cpx_mesh_set(cpx_mesh* m, int nodes, const double* xy, int c3, const int* e3, int c4, const int* e4,
-                        int nb, const int* bl, const int* bn) {
-    if (!m || nodes <= 0 || !xy || c3 < 0 || c4 < 0 || nb < 0) return CP_ERR_INVALID;
+                        int nb, const int* bl, const int* bn, int c8, const int* e8) {
+    if (!m || nodes <= 0 || !xy || c3 < 0 || c4 < 0 || nb < 0 || c8 < 0 || (c8 && !e8)) return CP_ERR_INVALID;
     return guard([&] {
         std::vector<std::vector<int>> borders(nb);
         int off = 0;
@@ -74,7 +74,7 @@ CP_API int cpx_mesh_set(cpx_mesh* m, int nodes, const double* xy, int c3, const 
             borders[b].assign(bn + off, bn + off + bl[b]);
             off += bl[b];
         }
-        m->m.assign(nodes, xy, c3, e3, c4, e4, borders);
+        m->m.assign(nodes, xy, c3, e3, c4, e4, borders, c8, e8);
     });
 }
 CP_API int cpx_mesh_counts(const cpx_mesh* m, int* nodes, int* c3, int* c4, int* nb, int* bt, int* c8) {

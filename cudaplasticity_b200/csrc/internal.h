@@ -30,11 +30,14 @@ struct Error {
     } while (0)
 
 // ------------------------------------------------------------- device data --
+// Elements are numbered triangles first, then 4-node quads, then 8-node quads
+// (the reference's element order, elemPos, src/Mesh.cuh:60).
 struct DevMesh {
-    int n_nodes = 0, c3 = 0, c4 = 0;
+    int n_nodes = 0, c3 = 0, c4 = 0, c8 = 0;
     double2* xy = nullptr;
     int4* e3 = nullptr;  // (n1, n2, n3, -1)
     int4* e4 = nullptr;
+    int4* e8 = nullptr;  // two per element: the corners, then the mid-sides
 };
 
 // Node-blocked CSR in the reference's layout: node n owns rows 2n and 2n+1,
@@ -46,8 +49,9 @@ struct DevCsr {
     int* adj_pos = nullptr;   // n+1
     int* adj = nullptr;       // nadj
     int* inc_pos = nullptr;   // n+1, incidences of node n (element order)
-    int* inc = nullptr;       // (global element id << 2) | local node index
+    int* inc = nullptr;       // (global element id << 3) | local node index
     uint32_t* inc_k = nullptr;  // packed block index (byte j) of local node j in node n's row
+    uint32_t* inc_k8 = nullptr;  // 8-node meshes: the same for local nodes 4..7 (byte j - 4)
     // Values live in a sliced layout for the SpMV (the reference-ordered CSR
     // above is exported on demand): nodes in slices of 32, slice s padded to
     // width w_s = max(deg + 1) over its nodes; block k (2x2: K00 K01 K10 K11)

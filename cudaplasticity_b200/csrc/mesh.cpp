@@ -70,7 +70,7 @@ Mesh& Mesh::operator=(const Mesh& o) {
 Mesh::~Mesh() { clear(); }
 
 void Mesh::assign(int nodes, const double* xy, int c3, const int* e3, int c4, const int* e4,
-                  const std::vector<std::vector<int>>& borderLists) {
+                  const std::vector<std::vector<int>>& borderLists, int c8, const int* e8) {
     clear();
     nodeCount = nodes;
     node = new vec2[nodes ? nodes : 1];
@@ -83,7 +83,13 @@ void Mesh::assign(int nodes, const double* xy, int c3, const int* e3, int c4, co
     count4 = c4;
     elem3 = dup(e3, 3 * (size_t)c3);
     elem4 = dup(e4, 4 * (size_t)c4);
-    elem8 = new int[1];
+    count8 = e8 ? c8 : 0;
+    elem8 = dup(e8, 8 * (size_t)count8);
+    for (int e = 0; e < count8; ++e)
+        for (int k = 4; k < 8; ++k) {
+            const int nd = elem8[8 * (size_t)e + k];
+            if (nd >= 0 && nd < nodes) secOrdNodes[nd] = true;
+        }
     bordersCount = (int)borderLists.size();
     borderLength = new int[bordersCount ? bordersCount : 1];
     borders = new int*[bordersCount ? bordersCount : 1];

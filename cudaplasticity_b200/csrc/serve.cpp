@@ -37,9 +37,9 @@ using Clock = std::chrono::steady_clock;
 
 struct Request {
     long long id = 0;
-    int nn = 0, c3 = 0, c4 = 0;
+    int nn = 0, c3 = 0, c4 = 0, c8 = 0;
     std::vector<double> xy, rp, uv;
-    std::vector<int> e3, e4;
+    std::vector<int> e3, e4, e8;
     std::vector<unsigned char> mask;
     bool has_uv = false;
     cp_material mat{};
@@ -114,6 +114,8 @@ int setup(cp_server* s, const ReqP& r) {
     v.elem3 = r->c3 ? r->e3.data() : nullptr;
     v.count4 = r->c4;
     v.elem4 = r->c4 ? r->e4.data() : nullptr;
+    v.count8 = r->c8;
+    v.elem8 = r->c8 ? r->e8.data() : nullptr;
     cp_instance* I = nullptr;
     int st = cp_instance_create(s->ctx_setup, &v, &r->mat, &I);
     if (st != CP_OK) return st;
@@ -359,8 +361,9 @@ CP_API int cp_server_submit(cp_server* s, const cp_mesh_view* mv, const cp_mater
                             const unsigned char* mask, const double* uv, const cp_solve_opts* opts, long long* id) {
     if (!s || !mv || !mat || !rp || !mask || !opts || !id) return CP_ERR_INVALID;
     if (opts->precision != CP_PREC_MIXED) return CP_ERR_UNSUPPORTED;
-    if (mv->node_count <= 0 || !mv->node_xy || mv->count3 < 0 || mv->count4 < 0 || mv->count3 + mv->count4 <= 0 ||
-        (mv->count3 && !mv->elem3) || (mv->count4 && !mv->elem4))
+    if (mv->node_count <= 0 || !mv->node_xy || mv->count3 < 0 || mv->count4 < 0 || mv->count8 < 0 ||
+        (long long)mv->count3 + mv->count4 + mv->count8 <= 0 || (mv->count3 && !mv->elem3) ||
+        (mv->count4 && !mv->elem4) || (mv->count8 && !mv->elem8))
         return CP_ERR_INVALID;
     auto r = std::make_shared<Request>();
     const size_t n2 = 2 * (size_t)mv->node_count;
@@ -368,9 +371,11 @@ CP_API int cp_server_submit(cp_server* s, const cp_mesh_view* mv, const cp_mater
         r->nn = mv->node_count;
         r->c3 = mv->count3;
         r->c4 = mv->count4;
+        r->c8 = mv->count8;
         r->xy.assign(mv->node_xy, mv->node_xy + n2);
         if (mv->count3) r->e3.assign(mv->elem3, mv->elem3 + 3 * (size_t)mv->count3);
         if (mv->count4) r->e4.assign(mv->elem4, mv->elem4 + 4 * (size_t)mv->count4);
+        if (mv->count8) r->e8.assign(mv->elem8, mv->elem8 + 8 * (size_t)mv->count8);
         r->rp.assign(rp, rp + n2);
         r->mask.assign(mask, mask + n2);
         if (uv) {

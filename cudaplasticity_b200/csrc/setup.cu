@@ -3,9 +3,9 @@
 // The reference builds SparseSLAE(Mesh&, 2) on the host (src/SparseSLAE.h:60-196,
 // and CudaSparseSLAE::constructorByCPU, src/CudaSparseSLAE.cuh:303-458): per node,
 // the distinct other nodes of its elements in first-occurrence order over the
-// traversal "triangles, then quads; element order; own local index i; local
-// j != i". Here the same order comes out of a per-node walk over its incident
-// elements sorted by element id:
+// traversal "triangles, then 4-node quads, then 8-node quads; element order;
+// own local index i; local j != i". Here the same order comes out of a
+// per-node walk over its incident elements sorted by element id:
 //   1. count incidences per node           (integer atomics, counts only)
 //   2. exclusive scan -> inc_pos, cap_pos  (cap = sum of (nen - 1), the
 //                                            reference's linkCounts)
@@ -28,29 +28,44 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
-__device__ __forceinline__ int elem_nen(int e, int c3) { return e < c3 ? 3 : 4; }
-
-__device__ __forceinline__ int4 elem_nodes(const DevMesh& m, int e) {
-    return e < m.c3 ? m.e3[e] : m.e4[e - m.c3];
-}
+__device__ __forceinline__ int elem_nen(const DevMesh& m, int e) { return e < m.c3 ? 3 : (e < m.c3 + m.c4 ? 4 : 8); }
 
 __device__ __forceinline__ int nth(const int4& v, int j) {
     return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w));
 }
 
+// Local node j (0 .. nen-1) of element e.
+__device__ __forceinline__ int elem_node(const DevMesh& m, int e, int j) {
+    if (e < m.c3) return nth(m.e3[e], j);
+    if (e < m.c3 + m.c4) return nth(m.e4[e - m.c3], j);
+    return nth(m.e8[2 * (e - m.c3 - m.c4) + (j >> 2)], j & 3);
+}
+
+__device__ __forceinline__ long long incidence_count(const DevMesh& m) {
+    return 3LL * m.c3 + 4LL * m.c4 + 8LL * m.c8;
+}
+
+// Incidence t (element order, then local index) -> element and local index.
+__device__ __forceinline__ void incidence(const DevMesh& m, long long t, int& e, int& i) {
+    if (t < 3LL * m.c3) { e = (int)(t / 3); i = (int)(t % 3); return; }
+    t -= 3LL * m.c3;
+    if (t < 4LL * m.c4) { e = m.c3 + (int)(t / 4); i = (int)(t % 4); return; }
+    t -= 4LL * m.c4;
+    e = m.c3 + m.c4 + (int)(t / 8);
+    i = (int)(t % 8);
+}
+
 __global__ void k_count(DevMesh m, int* inc_cnt, int* cap_cnt, int* err) {
-    const long long total = 3LL * m.c3 + 4LL * m.c4;
+    const long long total = incidence_count(m);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         int e, i;
-        if (t < 3LL * m.c3) { e = (int)(t / 3); i = (int)(t % 3); }
-        else { long long u = t - 3LL * m.c3; e = m.c3 + (int)(u / 4); i = (int)(u % 4); }
-        int4 el = elem_nodes(m, e);
-        int nen = elem_nen(e, m.c3);
-        int n = nth(el, i);
+        incidence(m, t, e, i);
+        const int nen = elem_nen(m, e);
+        const int n = elem_node(m, e, i);
         if (n < 0 || n >= m.n_nodes) { atomicExch(err, 1); continue; }
         for (int j = 0; j < nen; ++j)
-            if (j != i && nth(el, j) == n) atomicExch(err, 2);  // degenerate element
+            if (j != i && elem_node(m, e, j) == n) atomicExch(err, 2);  // degenerate element
         atomicAdd(&inc_cnt[n], 1);
         atomicAdd(&cap_cnt[n], nen - 1);
     }
@@ -144,21 +159,20 @@ void exclusive_scan(const int* in, int* out /* n+1 */, int n, int* scratch /* ti
 }
 
 __global__ void k_fill(DevMesh m, const int* inc_pos, int* cursor, int* inc) {
-    const long long total = 3LL * m.c3 + 4LL * m.c4;
+    const long long total = incidence_count(m);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         int e, i;
-        if (t < 3LL * m.c3) { e = (int)(t / 3); i = (int)(t % 3); }
-        else { long long u = t - 3LL * m.c3; e = m.c3 + (int)(u / 4); i = (int)(u % 4); }
-        int n = nth(elem_nodes(m, e), i);
+        incidence(m, t, e, i);
+        const int n = elem_node(m, e, i);
         if (n < 0 || n >= m.n_nodes) continue;
         int slot = inc_pos[n] + atomicAdd(&cursor[n], 1);
-        inc[slot] = (e << 2) | i;
+        inc[slot] = (e << 3) | i;
     }
 }
 
 __global__ void k_adjacency(DevMesh m, const int* inc_pos, int* inc, const int* cap_pos, int* links, int* adj_cnt,
-                            uint32_t* inc_k, int* max_deg, int* err) {
+                            uint32_t* inc_k, uint32_t* inc_k8, int* max_deg, int* err) {
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < m.n_nodes; n += gridDim.x * blockDim.x) {
         const int b = inc_pos[n], cnt = inc_pos[n + 1] - b;
         if (cnt > kMaxInc) { atomicExch(err, 3); adj_cnt[n] = 0; continue; }
@@ -171,14 +185,13 @@ __global__ void k_adjacency(DevMesh m, const int* inc_pos, int* inc, const int* 
         int* L = links + cap_pos[n];
         int s = 0;
         for (int q = b; q < b + cnt; ++q) {
-            const int e = inc[q] >> 2, i = inc[q] & 3;
-            const int4 el = elem_nodes(m, e);
-            const int nen = elem_nen(e, m.c3);
-            uint32_t packed = 0;
+            const int e = inc[q] >> 3, i = inc[q] & 7;
+            const int nen = elem_nen(m, e);
+            uint32_t packed = 0, packed8 = 0;
             for (int j = 0; j < nen; ++j) {
                 uint32_t k = 0;
                 if (j != i) {
-                    const int mj = nth(el, j);
+                    const int mj = elem_node(m, e, j);
                     int pos = -1;
                     for (int t = 0; t < s; ++t)
                         if (L[t] == mj) { pos = t; break; }
@@ -186,9 +199,11 @@ __global__ void k_adjacency(DevMesh m, const int* inc_pos, int* inc, const int* 
                     k = (uint32_t)(pos + 1);
                 }
                 if (k > 255u) { atomicExch(err, 4); k = 255u; }
-                packed |= k << (8 * j);
+                if (j < 4) packed |= k << (8 * j);
+                else packed8 |= k << (8 * (j - 4));
             }
             inc_k[q] = packed;
+            if (inc_k8) inc_k8[q] = packed8;
         }
         adj_cnt[n] = s;
         atomicMax(max_deg, s);
@@ -223,14 +238,17 @@ __global__ void k_rows_cols(int n_nodes, const int* adj_pos, const int* adj, int
     }
 }
 
-__global__ void k_slot_map(DevMesh m, const int* inc_pos, const int* inc, const uint32_t* inc_k, const int* adj_pos,
-                           int* slots) {
+__global__ void k_slot_map(DevMesh m, const int* inc_pos, const int* inc, const uint32_t* inc_k,
+                           const uint32_t* inc_k8, const int* adj_pos, int* slots) {
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < m.n_nodes; n += gridDim.x * blockDim.x) {
         const int base = 4 * (adj_pos[n] + n);
         for (int q = inc_pos[n]; q < inc_pos[n + 1]; ++q) {
-            const int e = inc[q] >> 2, i = inc[q] & 3, nen = elem_nen(e, m.c3);
-            const long long off = e < m.c3 ? 9LL * e : 9LL * m.c3 + 16LL * (e - m.c3);
-            for (int j = 0; j < nen; ++j) slots[off + i * nen + j] = base + 2 * (int)((inc_k[q] >> (8 * j)) & 0xffu);
+            const int e = inc[q] >> 3, i = inc[q] & 7, nen = elem_nen(m, e);
+            const long long off = e < m.c3 ? 9LL * e
+                                : e < m.c3 + m.c4 ? 9LL * m.c3 + 16LL * (e - m.c3)
+                                                  : 9LL * m.c3 + 16LL * m.c4 + 64LL * (e - m.c3 - m.c4);
+            const uint64_t kk = (uint64_t)inc_k[q] | (nen == 8 ? (uint64_t)inc_k8[q] << 32 : 0);
+            for (int j = 0; j < nen; ++j) slots[off + i * nen + j] = base + 2 * (int)((kk >> (8 * j)) & 0xffu);
         }
     }
 }
@@ -293,12 +311,14 @@ void setup_csr(DevMesh& m, DevCsr& csr, cudaStream_t s, int sm_count) {
     int* cursor = cap_pos + (n + 1);
     int* tiles = cursor + (n + 1);
     int* flags = tiles + 2 * (ntiles + 1);  // [0] error, [1] max degree
-    const long long incs = 3LL * m.c3 + 4LL * m.c4;
+    const long long incs = 3LL * m.c3 + 4LL * m.c4 + 8LL * m.c8;
     CP_CHECK(incs < (1LL << 31), CP_ERR_UNSUPPORTED, "mesh too large for 32-bit incidence offsets");
+    CP_CHECK((long long)m.c3 + m.c4 + m.c8 < (1LL << 28), CP_ERR_UNSUPPORTED, "mesh: too many elements");
     CP_CUDA(cudaMallocAsync(&csr.inc_pos, (n + 1) * sizeof(int), s));
     CP_CUDA(cudaMallocAsync(&csr.adj_pos, (n + 1) * sizeof(int), s));
     CP_CUDA(cudaMallocAsync(&csr.inc, (incs + 1) * sizeof(int), s));
     CP_CUDA(cudaMallocAsync(&csr.inc_k, (incs + 1) * sizeof(uint32_t), s));
+    if (m.c8) CP_CUDA(cudaMallocAsync(&csr.inc_k8, (incs + 1) * sizeof(uint32_t), s));
     const int grid = sm_count * 8;
     k_count<<<grid, 256, 0, s>>>(m, inc_cnt, cap_cnt, flags);
     exclusive_scan(inc_cnt, csr.inc_pos, n, tiles, s);
@@ -316,8 +336,8 @@ void setup_csr(DevMesh& m, DevCsr& csr, cudaStream_t s, int sm_count) {
     int* links = nullptr;
     CP_CUDA(cudaMallocAsync(&links, ((size_t)cap_total + 1) * sizeof(int), s));
     int* adj_cnt = cursor;  // reuse
-    k_adjacency<<<(n + 127) / 128, 128, 0, s>>>(m, csr.inc_pos, csr.inc, cap_pos, links, adj_cnt, csr.inc_k, flags + 1,
-                                                flags);
+    k_adjacency<<<(n + 127) / 128, 128, 0, s>>>(m, csr.inc_pos, csr.inc, cap_pos, links, adj_cnt, csr.inc_k,
+                                                csr.inc_k8, flags + 1, flags);
     exclusive_scan(adj_cnt, csr.adj_pos, n, tiles, s);
     int nadj = 0, maxdeg = 0;
     CP_CUDA(cudaMemcpyAsync(&nadj, csr.adj_pos + n, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -361,7 +381,8 @@ void csr_rows_cols(const DevMesh& m, const DevCsr& csr, int* rows, int* cols, cu
 }
 
 void csr_slot_map(const DevMesh& m, const DevCsr& csr, int* slots, cudaStream_t s) {
-    k_slot_map<<<(m.n_nodes + 255) / 256, 256, 0, s>>>(m, csr.inc_pos, csr.inc, csr.inc_k, csr.adj_pos, slots);
+    k_slot_map<<<(m.n_nodes + 255) / 256, 256, 0, s>>>(m, csr.inc_pos, csr.inc, csr.inc_k, csr.inc_k8, csr.adj_pos,
+                                                        slots);
 }
 
 }  // namespace cp

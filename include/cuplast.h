@@ -72,7 +72,9 @@ typedef struct {
     double pw_eps[CP_MAX_PW], pw_sig[CP_MAX_PW];
 } cp_material;
 
-/* A mesh as the public arrays of class Mesh (src/Mesh.cuh:42-66). */
+/* A mesh as the public arrays of class Mesh (src/Mesh.cuh:42-66). Elements
+ * are numbered triangles, then 4-node quads, then 8-node quads; per-element
+ * fields follow that order. */
 typedef struct {
     int node_count;
     const double* node_xy;  /* 2 * node_count */
@@ -80,6 +82,9 @@ typedef struct {
     const int* elem3;       /* 3 * count3 */
     int count4;
     const int* elem4;       /* 4 * count4 */
+    int count8;
+    const int* elem8;       /* 8 * count8: corners, then the mid-sides of edges 1-2, 2-3, 3-4, 4-1
+                               (Mesh::remapOrder, src/Mesh.cu:443-503) */
 } cp_mesh_view;
 
 typedef struct {

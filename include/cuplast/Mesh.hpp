@@ -64,9 +64,10 @@ public:
     // std::out_of_range on a bad file.
     bool loadFromFile(const std::string& fileName);
 
-    // Replaces the arrays (takes copies).
+    // Replaces the arrays (takes copies). The mid-side nodes of 8-node
+    // elements become second-order nodes (secOrdNodes).
     void assign(int nodes, const double* xy, int c3, const int* e3, int c4, const int* e4,
-                const std::vector<std::vector<int>>& borderLists);
+                const std::vector<std::vector<int>>& borderLists, int c8 = 0, const int* e8 = nullptr);
 
 private:
     void clear();

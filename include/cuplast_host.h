@@ -35,8 +35,11 @@ CP_API int cpx_mesh_gen_ring(cpx_mesh* m, double a, double b, int n_phi, int n_r
 CP_API int cpx_mesh_load_inp(cpx_mesh* m, const char* path);
 /* every quad (n1,n2,n3,n4) -> triangles (n1,n2,n3), (n1,n3,n4) (extension) */
 CP_API int cpx_mesh_split_t3(cpx_mesh* m);
+/* Mesh from arrays; elem8 (8 * count8, may be NULL when count8 = 0) marks its
+ * mid-side nodes as second-order nodes, as the reference's generators do. */
 CP_API int cpx_mesh_set(cpx_mesh* m, int node_count, const double* xy, int count3, const int* elem3, int count4,
-                        const int* elem4, int n_borders, const int* border_len, const int* border_nodes);
+                        const int* elem4, int n_borders, const int* border_len, const int* border_nodes, int count8,
+                        const int* elem8);
 CP_API int cpx_mesh_counts(const cpx_mesh* m, int* node_count, int* count3, int* count4, int* n_borders,
                            int* border_total, int* count8);
 /* elem8: 8 * count8 node indices, corners 0..3 then mid-side nodes 4..7 */

@@ -85,8 +85,9 @@ def run_reference(lines, threads=None, workdir=None, binary=None):
         return cpbin.read(out)
 
 
-def write_mesh(path, node_xy, elem3=(), elem4=(), borders=()):
-    """Writes a mesh in the layout the harness and the restatement read."""
+def write_mesh(path, node_xy, elem3=(), elem4=(), borders=(), elem8=()):
+    """Writes a mesh in the layout the harness and the restatement read. The
+    mid-side nodes of 8-node elements are the mesh's second-order nodes."""
     import numpy as np
 
     bl = [len(b) for b in borders]
@@ -97,7 +98,7 @@ def write_mesh(path, node_xy, elem3=(), elem4=(), borders=()):
             "node_xy": np.asarray(node_xy, dtype=np.float64).ravel(),
             "elem3": np.asarray(elem3, dtype=np.int32).ravel(),
             "elem4": np.asarray(elem4, dtype=np.int32).ravel(),
-            "elem8": np.zeros(0, np.int32),
+            "elem8": np.asarray(elem8, dtype=np.int32).ravel(),
             "border_len": np.asarray(bl, dtype=np.int32),
             "border_nodes": bn,
         },

@@ -4,7 +4,7 @@
  * never part of it. Each function names the reference code it restates
  * (paths relative to the reference project root).
  *
- * Scope: T3 (extension; the reference only declares it) and Q4 elements,
+ * Scope: T3 (extension; the reference only declares it), Q4 and Q8 elements,
  * plane stress/strain, the reference's CSR ordering, masked unpreconditioned
  * CG, the secant (variable elastic parameters) update with the reference's
  * linear/power diagrams plus the injected Hollomon and piecewise-linear
@@ -21,7 +21,12 @@
  *    would divide 0/0);
  *  - body forces are evaluated at the element's node (the reference indexes the
  *    node array with the DOF index, src/PlasticitySolver.cu:937-940, which only
- *    gives the same value for constant fields such as gravity).
+ *    gives the same value for constant fields such as gravity);
+ *  - the Q8 Gauss rule uses sqrt(0.6), 5/9 and 8/9 to full precision (the
+ *    reference writes them with 15 decimals, src/PlasticitySolver.cu:70,190),
+ *    a difference of about 1e-15 relative; the shape-function derivatives are
+ *    the standard serendipity ones in factored form rather than the
+ *    reference's expanded polynomials (same values up to rounding).
  */
 #include "cuplast_oracle.h"
 
@@ -82,9 +87,11 @@ typedef struct {
 typedef struct {
     int n_nodes;
     double* xy;
-    int c3, c4;
+    int c3, c4, c8;
     int* e3;
     int* e4;
+    int* e8;
+    unsigned char* sec;   /* second-order (mid-side) nodes: Mesh::secOrdNodes */
     int n_borders;
     int* border_len;
     int** borders;
@@ -177,13 +184,14 @@ static int parse_job(const char* path, job_t* j) {
 
 static int load_mesh(const char* path, mesh_t* m) {
     cpbin_file f;
-    const cpbin_rec *xy, *e3, *e4, *bl, *bn;
-    int b, off = 0;
+    const cpbin_rec *xy, *e3, *e4, *e8, *bl, *bn;
+    int b, off = 0, e, i;
     memset(m, 0, sizeof *m);
     if (cpbin_read(path, &f) != 0) return -1;
     xy = cpbin_get(&f, "node_xy");
     e3 = cpbin_get(&f, "elem3");
     e4 = cpbin_get(&f, "elem4");
+    e8 = cpbin_get(&f, "elem8");
     bl = cpbin_get(&f, "border_len");
     bn = cpbin_get(&f, "border_nodes");
     if (!xy) { cpbin_free(&f); return -2; }
@@ -196,6 +204,13 @@ static int load_mesh(const char* path, mesh_t* m) {
     m->e4 = (int*)malloc(sizeof(int) * (4 * (size_t)m->c4 + 1));
     if (m->c3) memcpy(m->e3, e3->data, sizeof(int) * 3 * (size_t)m->c3);
     if (m->c4) memcpy(m->e4, e4->data, sizeof(int) * 4 * (size_t)m->c4);
+    m->c8 = e8 ? (int)(e8->count / 8) : 0;
+    m->e8 = (int*)malloc(sizeof(int) * (8 * (size_t)m->c8 + 1));
+    if (m->c8) memcpy(m->e8, e8->data, sizeof(int) * 8 * (size_t)m->c8);
+    /* the mid-side nodes of 8-node elements are the second-order nodes */
+    m->sec = (unsigned char*)calloc((size_t)m->n_nodes + 1, 1);
+    for (e = 0; e < m->c8; ++e)
+        for (i = 4; i < 8; ++i) m->sec[m->e8[8 * e + i]] = 1;
     m->n_borders = bl ? (int)bl->count : 0;
     m->border_len = (int*)malloc(sizeof(int) * (size_t)(m->n_borders + 1));
     m->borders = (int**)malloc(sizeof(int*) * (size_t)(m->n_borders + 1));
@@ -218,6 +233,8 @@ static void free_mesh(mesh_t* m) {
     free(m->xy);
     free(m->e3);
     free(m->e4);
+    free(m->e8);
+    free(m->sec);
 }
 
 /* ------------------------------------------------------------- diagrams -- */
@@ -269,8 +286,8 @@ static double diagram_f(const diagram_t* d, double eps) {
 
 /* SparseSLAE(Mesh&, dim=2), src/SparseSLAE.h:60-196: per node the distinct
  * other nodes of its elements in first-occurrence order over the traversal
- * elem3, then elem4 (element order, local i, local j != i). */
-int orc_csr_build(int n, int c3, const int* e3, int c4, const int* e4,
+ * elem3, then elem4, then elem8 (element order, local i, local j != i). */
+int orc_csr_build(int n, int c3, const int* e3, int c4, const int* e4, int c8, const int* e8,
                   int* rows, int* cols, int* adj_pos, int* adj, long long* nnz, long long* nadj) {
     int* cnt = (int*)calloc((size_t)n + 1, sizeof(int));
     int* cap_pos = (int*)calloc((size_t)n + 1, sizeof(int));
@@ -280,6 +297,7 @@ int orc_csr_build(int n, int c3, const int* e3, int c4, const int* e4,
     int e, i, jj, node;
     for (i = 0; i < 3 * c3; ++i) cnt[e3[i]] += 2;
     for (i = 0; i < 4 * c4; ++i) cnt[e4[i]] += 3;
+    for (i = 0; i < 8 * c8; ++i) cnt[e8[i]] += 7;
     for (node = 0; node < n; ++node) { cap_pos[node] = (int)total; total += cnt[node]; }
     cap_pos[n] = (int)total;
     links = (int*)malloc(sizeof(int) * (size_t)(total + 1));
@@ -300,6 +318,10 @@ int orc_csr_build(int n, int c3, const int* e3, int c4, const int* e4,
         for (i = 0; i < 4; ++i)
             for (jj = 0; jj < 4; ++jj)
                 if (i != jj) ADD_LINK(e4[4 * e + i], e4[4 * e + jj]);
+    for (e = 0; e < c8; ++e)
+        for (i = 0; i < 8; ++i)
+            for (jj = 0; jj < 8; ++jj)
+                if (i != jj) ADD_LINK(e8[8 * e + i], e8[8 * e + jj]);
 #undef ADD_LINK
     for (node = 0; node < n; ++node) tot_adj += ucnt[node];
     *nadj = tot_adj;
@@ -343,7 +365,7 @@ static int block_slot(const int* rows, const int* adj_pos, const int* adj, int n
     return -1;
 }
 
-int orc_slot_map(int n, int c3, const int* e3, int c4, const int* e4,
+int orc_slot_map(int n, int c3, const int* e3, int c4, const int* e4, int c8, const int* e8,
                  const int* rows, const int* adj_pos, const int* adj, int* slots) {
     int e, i, j;
     (void)n;
@@ -355,6 +377,11 @@ int orc_slot_map(int n, int c3, const int* e3, int c4, const int* e4,
         for (i = 0; i < 4; ++i)
             for (j = 0; j < 4; ++j)
                 slots[9 * c3 + 16 * e + 4 * i + j] = block_slot(rows, adj_pos, adj, e4[4 * e + i], e4[4 * e + j]);
+    for (e = 0; e < c8; ++e)
+        for (i = 0; i < 8; ++i)
+            for (j = 0; j < 8; ++j)
+                slots[9 * c3 + 16 * c4 + 64 * e + 8 * i + j] =
+                    block_slot(rows, adj_pos, adj, e8[8 * e + i], e8[8 * e + j]);
     return 0;
 }
 
@@ -401,6 +428,59 @@ static void calc_b3(const double* xy, const int* el, double B[2][3], double* are
     B[0][0] = (y2 - y3) * inv; B[0][1] = (y3 - y1) * inv; B[0][2] = (y1 - y2) * inv;
     B[1][0] = (x3 - x2) * inv; B[1][1] = (x1 - x3) * inv; B[1][2] = (x2 - x1) * inv;
     *area = 0.5 * twoA;
+}
+
+/* calcB8, src/PlasticitySolver.cu:67-134: 3x3 Gauss, point k = 3 i + j at
+ * (r_i, s_j). Local nodes: corners (1,1), (-1,1), (-1,-1), (1,-1), then the
+ * mid-sides of the edges s = 1, r = -1, s = -1, r = 1. Serendipity shape
+ * functions: corners N = (1 + r ri)(1 + s si)(r ri + s si - 1)/4, mid-sides
+ * N = (1 - r^2)(1 + s si)/2 or (1 + r ri)(1 - s^2)/2. */
+static const double q8_ri[8] = {1., -1., -1., 1., 0., -1., 0., 1.};
+static const double q8_si[8] = {1., 1., -1., -1., 1., 0., -1., 0.};
+static double q8_gp[3], q8_gw[3];
+
+static void q8_rule(void) {
+    q8_gp[0] = -sqrt(0.6); q8_gp[1] = 0.0; q8_gp[2] = sqrt(0.6);
+    q8_gw[0] = 5.0 / 9.0; q8_gw[1] = 8.0 / 9.0; q8_gw[2] = 5.0 / 9.0;
+}
+
+static void q8_dshape(double r, double s, double dr[8], double ds[8]) {
+    int k;
+    for (k = 0; k < 8; ++k) {
+        double ri = q8_ri[k], si = q8_si[k];
+        if (k < 4) {
+            dr[k] = 0.25 * ri * (1. + s * si) * (2. * r * ri + s * si);
+            ds[k] = 0.25 * si * (1. + r * ri) * (r * ri + 2. * s * si);
+        } else if (ri == 0.) {
+            dr[k] = -r * (1. + s * si);
+            ds[k] = 0.5 * si * (1. - r * r);
+        } else {
+            dr[k] = 0.5 * ri * (1. - s * s);
+            ds[k] = -s * (1. + r * ri);
+        }
+    }
+}
+
+static void calc_b8(const double* xy, const int* el, double B[9][2][8], double detJ[9]) {
+    int i, j, k;
+    for (i = 0; i < 3; ++i)
+        for (j = 0; j < 3; ++j) {
+            int q = 3 * i + j;
+            double dr[8], ds[8], xr = 0., yr = 0., xs = 0., ys = 0., inv, rx, sx, ry, sy;
+            q8_dshape(q8_gp[i], q8_gp[j], dr, ds);
+            for (k = 0; k < 8; ++k) {
+                double x = xy[2 * el[k]], y = xy[2 * el[k] + 1];
+                xr += dr[k] * x; yr += dr[k] * y;
+                xs += ds[k] * x; ys += ds[k] * y;
+            }
+            detJ[q] = xr * ys - yr * xs;
+            inv = 1. / detJ[q];
+            rx = ys * inv; sx = -yr * inv; ry = -xs * inv; sy = xr * inv;
+            for (k = 0; k < 8; ++k) {
+                B[q][0][k] = dr[k] * rx + ds[k] * sx;
+                B[q][1][k] = dr[k] * ry + ds[k] * sy;
+            }
+        }
 }
 
 /* formC_plainStress / formC_plainStrain, src/PlasticitySolver.cu:226-242. */
@@ -464,6 +544,7 @@ typedef struct {
     double* data;
     double* B4; double* detJ4;     /* [c4][4][2][4], [c4][4] */
     double* B3; double* area3;     /* [c3][2][3], [c3] */
+    double* B8; double* wJ8;       /* [c8][9][2][8], [c8][9] Gauss weight x detJ */
     double *rp, *uv;
     unsigned char* mask;
     double *exx, *eyy, *gam, *epsI, *sxx, *syy, *tau, *sigI, *tabS, *psi, *Ec, *nuc;
@@ -483,23 +564,36 @@ static void calc_bs(prob_t* p) {
 #pragma omp parallel for
     for (e = 0; e < m->c3; ++e)
         calc_b3(m->xy, m->e3 + 3 * e, (double(*)[3])(p->B3 + 6 * (size_t)e), p->area3 + e);
+#pragma omp parallel for
+    for (e = 0; e < m->c8; ++e) {
+        double* wJ = p->wJ8 + 9 * (size_t)e;
+        int q;
+        calc_b8(m->xy, m->e8 + 8 * e, (double(*)[2][8])(p->B8 + 144 * (size_t)e), wJ);
+        /* formKe8 (src/PlasticitySolver.cu:189-224) weights each point by
+         * w_i w_j detJ */
+        for (q = 0; q < 9; ++q) wJ[q] *= q8_gw[q / 3] * q8_gw[q % 3];
+    }
 }
 
-/* fillGlobalStiffness + distribKe4, src/PlasticitySolver.cu:711-746,786-810:
+/* fillGlobalStiffness + distribKe4/distribKe8, src/PlasticitySolver.cu:711-810:
  * Ke of every element added into CSR values through the slot map. */
 static void assemble(prob_t* p) {
     const mesh_t* m = &p->mesh;
     int e, i, j;
     memset(p->data, 0, sizeof(double) * (size_t)p->nnz);
     for (e = 0; e < p->E; ++e) {
-        int t3 = e < m->c3, nen = t3 ? 3 : 4, le = t3 ? e : e - m->c3;
-        const int* el = t3 ? m->e3 + 3 * le : m->e4 + 4 * le;
-        const int* sl = t3 ? p->slots + 9 * le : p->slots + 9 * (size_t)m->c3 + 16 * (size_t)le;
-        double C[9], Ke[36];
+        int kind = e < m->c3 ? 3 : e < m->c3 + m->c4 ? 4 : 8, nen = kind;
+        int le = kind == 3 ? e : kind == 4 ? e - m->c3 : e - m->c3 - m->c4;
+        const int* el = kind == 3 ? m->e3 + 3 * le : kind == 4 ? m->e4 + 4 * le : m->e8 + 8 * le;
+        const int* sl = kind == 3 ? p->slots + 9 * le
+                      : kind == 4 ? p->slots + 9 * (size_t)m->c3 + 16 * (size_t)le
+                                  : p->slots + 9 * (size_t)m->c3 + 16 * (size_t)m->c4 + 64 * (size_t)le;
+        double C[9], Ke[136];
         form_c(p->job.plane_strain, p->Ec[e], p->nuc[e], C);
         memcpy(p->Cst + 9 * (size_t)e, C, sizeof C);
-        if (t3) form_ke(3, 1, p->B3 + 6 * (size_t)le, p->area3 + le, C, p->job.h, Ke);
-        else form_ke(4, 4, p->B4 + 32 * (size_t)le, p->detJ4 + 4 * (size_t)le, C, p->job.h, Ke);
+        if (kind == 3) form_ke(3, 1, p->B3 + 6 * (size_t)le, p->area3 + le, C, p->job.h, Ke);
+        else if (kind == 4) form_ke(4, 4, p->B4 + 32 * (size_t)le, p->detJ4 + 4 * (size_t)le, C, p->job.h, Ke);
+        else form_ke(8, 9, p->B8 + 144 * (size_t)le, p->wJ8 + 9 * (size_t)le, C, p->job.h, Ke);
         for (i = 0; i < nen; ++i) {
             int ni = el[i], Li = p->rows[2 * ni + 1] - p->rows[2 * ni];
             for (j = 0; j < nen; ++j) {
@@ -533,8 +627,61 @@ static int find_node(const mesh_t* m, double x, double y) {
     return -1;
 }
 
+/* The quadratic-edge branch of initConditions, src/PlasticitySolver.cu:822-865:
+ * a border traction over corner a, mid-side c, corner d gives the consistent
+ * nodal forces f_a L1/3, f_c (4/3)(L1 + L2)/2, f_d L2/3 (L1 = |ac|, L2 = |cd|),
+ * times h. A normal/tangential traction turns with each half edge; the
+ * mid-side node takes the mean of the two frames. */
+static void quad_edge_force(prob_t* p, int b, int na, int nc, int nd) {
+    const mesh_t* m = &p->mesh;
+    const job_t* j = &p->job;
+    double xa = m->xy[2 * na], ya = m->xy[2 * na + 1], xc = m->xy[2 * nc], yc = m->xy[2 * nc + 1];
+    double xd = m->xy[2 * nd], yd = m->xy[2 * nd + 1];
+    double hx1 = 0.5 * (xa - xc), hy1 = 0.5 * (ya - yc), hx2 = 0.5 * (xc - xd), hy2 = 0.5 * (yc - yd);
+    double dl1 = sqrt(hx1 * hx1 + hy1 * hy1), dl2 = sqrt(hx2 * hx2 + hy2 * hy2);
+    double fx = j->force_v[b][0], fy = j->force_v[b][1];
+    double f1x = fx, f1y = fy, f2x = fx, f2y = fy, f3x = fx, f3y = fy, R[6];
+    int a;
+    if (j->force_norm[b]) {
+        double t1x = xc - xa, t1y = yc - ya, t2x = xd - xc, t2y = yd - yc, tn, n1x, n1y, n2x, n2y, nn;
+        tn = sqrt(t1x * t1x + t1y * t1y); t1x = t1x * (1. / tn); t1y = t1y * (1. / tn);
+        n1x = t1y; n1y = -t1x; nn = sqrt(n1x * n1x + n1y * n1y); n1x = n1x * (1. / nn); n1y = n1y * (1. / nn);
+        tn = sqrt(t2x * t2x + t2y * t2y); t2x = t2x * (1. / tn); t2y = t2y * (1. / tn);
+        n2x = t2y; n2y = -t2x; nn = sqrt(n2x * n2x + n2y * n2y); n2x = n2x * (1. / nn); n2y = n2y * (1. / nn);
+        f1x = n1x * fx + t1x * fy; f1y = n1y * fx + t1y * fy;
+        f2x = 0.5 * ((n1x + n2x) * fx + (t1x + t2x) * fy);
+        f2y = 0.5 * ((n1y + n2y) * fx + (t1y + t2y) * fy);
+        f3x = n2x * fx + t2x * fy; f3y = n2y * fx + t2y * fy;
+    }
+    R[0] = f1x / 3.; R[1] = f1y / 3.;
+    R[2] = f2x * 4. / 3.; R[3] = f2y * 4. / 3.;
+    R[4] = f3x / 3.; R[5] = f3y / 3.;
+    for (a = 0; a < 2; ++a) {
+        R[a] *= j->h * dl1 * 2.;
+        R[2 + a] *= j->h * (dl1 + dl2);
+        R[4 + a] *= j->h * dl2 * 2.;
+    }
+    p->rp[2 * na] += R[0]; p->rp[2 * na + 1] += R[1];
+    p->rp[2 * nc] += R[2]; p->rp[2 * nc + 1] += R[3];
+    p->rp[2 * nd] += R[4]; p->rp[2 * nd + 1] += R[5];
+}
+
+/* Mesh::elemSpace8 (src/Mesh.cuh:269-278): area of the polygon through the
+ * corners and mid-side nodes. */
+static double elem_space8(const mesh_t* m, const int* el) {
+    double s1 = 0., s2 = 0.;
+    int i;
+    for (i = 0; i < 3; ++i) {
+        s1 += m->xy[2 * el[i]] * m->xy[2 * el[i + 4] + 1] + m->xy[2 * el[i + 4]] * m->xy[2 * el[i + 1] + 1];
+        s2 += m->xy[2 * el[i] + 1] * m->xy[2 * el[i + 4]] + m->xy[2 * el[i + 4] + 1] * m->xy[2 * el[i + 1]];
+    }
+    s1 += m->xy[2 * el[3]] * m->xy[2 * el[7] + 1] + m->xy[2 * el[7]] * m->xy[2 * el[0] + 1];
+    s2 += m->xy[2 * el[3] + 1] * m->xy[2 * el[7]] + m->xy[2 * el[7] + 1] * m->xy[2 * el[0]];
+    return fabs(s1 - s2) * 0.5;
+}
+
 /* initConditions(SparseSLAE&), src/PlasticitySolver.cu:812-1005, for
- * constant-valued loads (linear border segments; T3/Q4 meshes). */
+ * constant-valued loads (linear and quadratic border segments). */
 static void init_conditions(prob_t* p) {
     const mesh_t* m = &p->mesh;
     const job_t* j = &p->job;
@@ -545,9 +692,15 @@ static void init_conditions(prob_t* p) {
         if (!j->force_set[b]) continue;
         bd = m->borders[b];
         for (i = 1; i < m->border_len[b]; ++i) {
-            double x1 = m->xy[2 * bd[i - 1]], y1 = m->xy[2 * bd[i - 1] + 1];
-            double x2 = m->xy[2 * bd[i]], y2 = m->xy[2 * bd[i] + 1];
-            double hd1 = 0.5 * (x1 - x2), hd2 = 0.5 * (y1 - y2);
+            double x1, y1, x2, y2, hd1, hd2;
+            if (m->sec[bd[i]] && i + 1 < m->border_len[b]) {
+                quad_edge_force(p, b, bd[i - 1], bd[i], bd[i + 1]);
+                ++i;
+                continue;
+            }
+            x1 = m->xy[2 * bd[i - 1]]; y1 = m->xy[2 * bd[i - 1] + 1];
+            x2 = m->xy[2 * bd[i]]; y2 = m->xy[2 * bd[i] + 1];
+            hd1 = 0.5 * (x1 - x2); hd2 = 0.5 * (y1 - y2);
             double dl = sqrt(hd1 * hd1 + hd2 * hd2);
             double f1x = j->force_v[b][0], f1y = j->force_v[b][1], f2x = f1x, f2y = f1y;
             double R[4];
@@ -585,6 +738,18 @@ static void init_conditions(prob_t* p) {
             for (i = 0; i < 4; ++i) {
                 p->rp[2 * el[i]] += coef * j->grav[0];
                 p->rp[2 * el[i] + 1] += coef * j->grav[1];
+            }
+        }
+        /* 8-node elements, src/PlasticitySolver.cu:911-929: -1/12 of the
+         * element's load to each corner, 1/3 to each mid-side node */
+        for (e = 0; e < m->c8; ++e) {
+            const int* el = m->e8 + 8 * e;
+            double space = elem_space8(m, el);
+            double coef1 = -p->job.rho * j->h * space / 12., coef2 = p->job.rho * j->h * space / 3.;
+            for (i = 0; i < 8; ++i) {
+                double c = i < 4 ? coef1 : coef2;
+                p->rp[2 * el[i]] += c * j->grav[0];
+                p->rp[2 * el[i] + 1] += c * j->grav[1];
             }
         }
     }
@@ -682,7 +847,7 @@ static long long cg_solve(prob_t* p, double* x, const double* b, double eps) {
     return it;
 }
 
-/* updateParameters, src/PlasticitySolver.cu:1249-1335 (Q4 part) plus the CST. */
+/* updateParameters, src/PlasticitySolver.cu:1249-1335 (Q4 and Q8) plus the CST. */
 static void update_parameters(prob_t* p) {
     const mesh_t* m = &p->mesh;
     const double E0 = p->job.E, nu0 = p->job.nu;
@@ -698,6 +863,26 @@ static void update_parameters(prob_t* p) {
             p->exx[e] = u1 * B[0] + u2 * B[1] + u3 * B[2];
             p->eyy[e] = v1 * B[3] + v2 * B[4] + v3 * B[5];
             p->gam[e] = u1 * B[3] + u2 * B[4] + u3 * B[5] + v1 * B[0] + v2 * B[1] + v3 * B[2];
+        } else if (e >= m->c3 + m->c4) {
+            /* src/PlasticitySolver.cu:1280-1305: Gauss-weighted mean over the
+             * reference square, (1/4) sum_ij w_i w_j eps(r_i, s_j) */
+            int le = e - m->c3 - m->c4, a, q;
+            const int* el = m->e8 + 8 * le;
+            double u[8], v[8], ex = 0., ey = 0., g = 0.;
+            for (a = 0; a < 8; ++a) { u[a] = p->uv[2 * el[a]]; v[a] = p->uv[2 * el[a] + 1]; }
+            for (q = 0; q < 9; ++q) {
+                const double* B = p->B8 + 144 * (size_t)le + 16 * q; /* B(r,c) = B[r*8+c] */
+                double exl = 0., eyl = 0., gl = 0., w = q8_gw[q / 3] * q8_gw[q % 3];
+                for (a = 0; a < 8; ++a) {
+                    exl += u[a] * B[a];
+                    eyl += v[a] * B[8 + a];
+                    gl += u[a] * B[8 + a] + v[a] * B[a];
+                }
+                ex += exl * w; ey += eyl * w; g += gl * w;
+            }
+            p->exx[e] = ex * 0.25;
+            p->eyy[e] = ey * 0.25;
+            p->gam[e] = g * 0.25;
         } else {
             int le = e - m->c3, k;
             const int* el = m->e4 + 4 * le;
@@ -758,7 +943,9 @@ static void plast_deform(prob_t* p) {
     }
 }
 
-/* deformEnergy, src/PlasticitySolver.cuh:415-445 (Q4 and CST elements) */
+/* deformEnergy, src/PlasticitySolver.cuh:415-445. Q4 and CST elements on the
+ * plastic branch integrate the diagram; Q8 elements always take the secant
+ * energy eps_i sig_i / 2 (the reference's Q8 loop has no plastic branch). */
 static double deform_energy(const prob_t* p) {
     const mesh_t* m = &p->mesh;
     const diagram_t* d = &p->job.dg;
@@ -766,6 +953,10 @@ static double deform_energy(const prob_t* p) {
     int e, i, k;
     for (e = 0; e < p->E; ++e) {
         double area, vol;
+        if (e >= m->c3 + m->c4) {
+            energy += p->epsI[e] * p->sigI[e] * 0.5 * (p->job.h * elem_space8(m, m->e8 + 8 * (e - m->c3 - m->c4)));
+            continue;
+        }
         if (e < m->c3) area = fabs(p->area3[e]);
         else {
             const int* el = m->e4 + 4 * (e - m->c3);
@@ -809,20 +1000,24 @@ int orc_run_job(const char* job_path, const char* out_path) {
     if (p->job.dg.kind == DG_NONE) { p->job.dg.kind = DG_LINEAR; p->job.dg.E = p->job.E; p->job.dg.sigmaT = 1e300; p->job.dg.K_T = p->job.E; }
     p->job.dg.E = p->job.E;
     N = p->N = 2 * p->mesh.n_nodes;
-    p->E = p->mesh.c3 + p->mesh.c4;
+    p->E = p->mesh.c3 + p->mesh.c4 + p->mesh.c8;
+    q8_rule();
     out = cpbin_open_write(out_path);
     if (!out) return 3;
 
-    orc_csr_build(p->mesh.n_nodes, p->mesh.c3, p->mesh.e3, p->mesh.c4, p->mesh.e4, NULL, NULL, NULL, NULL, &p->nnz, &p->nadj);
+    orc_csr_build(p->mesh.n_nodes, p->mesh.c3, p->mesh.e3, p->mesh.c4, p->mesh.e4, p->mesh.c8, p->mesh.e8, NULL, NULL,
+                  NULL, NULL, &p->nnz, &p->nadj);
     p->rows = (int*)malloc(sizeof(int) * (size_t)(N + 1));
     p->cols = (int*)malloc(sizeof(int) * (size_t)p->nnz);
     p->adj_pos = (int*)malloc(sizeof(int) * (size_t)(p->mesh.n_nodes + 1));
     p->adj = (int*)malloc(sizeof(int) * (size_t)(p->nadj + 1));
-    orc_csr_build(p->mesh.n_nodes, p->mesh.c3, p->mesh.e3, p->mesh.c4, p->mesh.e4, p->rows, p->cols, p->adj_pos, p->adj, &p->nnz, &p->nadj);
+    orc_csr_build(p->mesh.n_nodes, p->mesh.c3, p->mesh.e3, p->mesh.c4, p->mesh.e4, p->mesh.c8, p->mesh.e8, p->rows,
+                  p->cols, p->adj_pos, p->adj, &p->nnz, &p->nadj);
     if (!strcmp(p->job.mode, "csr") || p->job.dump_csr) {
-        size_t ns = 9 * (size_t)p->mesh.c3 + 16 * (size_t)p->mesh.c4;
+        size_t ns = 9 * (size_t)p->mesh.c3 + 16 * (size_t)p->mesh.c4 + 64 * (size_t)p->mesh.c8;
         int* sl = (int*)malloc(sizeof(int) * (ns + 1));
-        orc_slot_map(p->mesh.n_nodes, p->mesh.c3, p->mesh.e3, p->mesh.c4, p->mesh.e4, p->rows, p->adj_pos, p->adj, sl);
+        orc_slot_map(p->mesh.n_nodes, p->mesh.c3, p->mesh.e3, p->mesh.c4, p->mesh.e4, p->mesh.c8, p->mesh.e8, p->rows,
+                     p->adj_pos, p->adj, sl);
         cpbin_put(out, "rows", 'i', N + 1, p->rows);
         cpbin_put(out, "cols", 'i', p->nnz, p->cols);
         cpbin_put(out, "adj_pos", 'i', p->mesh.n_nodes + 1, p->adj_pos);
@@ -831,13 +1026,16 @@ int orc_run_job(const char* job_path, const char* out_path) {
         free(sl);
         if (!strcmp(p->job.mode, "csr")) goto done;
     }
-    p->slots = (int*)malloc(sizeof(int) * (9 * (size_t)p->mesh.c3 + 16 * (size_t)p->mesh.c4 + 1));
-    orc_slot_map(p->mesh.n_nodes, p->mesh.c3, p->mesh.e3, p->mesh.c4, p->mesh.e4, p->rows, p->adj_pos, p->adj, p->slots);
+    p->slots = (int*)malloc(sizeof(int) * (9 * (size_t)p->mesh.c3 + 16 * (size_t)p->mesh.c4 + 64 * (size_t)p->mesh.c8 + 1));
+    orc_slot_map(p->mesh.n_nodes, p->mesh.c3, p->mesh.e3, p->mesh.c4, p->mesh.e4, p->mesh.c8, p->mesh.e8, p->rows,
+                 p->adj_pos, p->adj, p->slots);
     p->data = dalloc((size_t)p->nnz);
     p->B4 = dalloc(32 * (size_t)p->mesh.c4);
     p->detJ4 = dalloc(4 * (size_t)p->mesh.c4);
     p->B3 = dalloc(6 * (size_t)p->mesh.c3);
     p->area3 = dalloc((size_t)p->mesh.c3);
+    p->B8 = dalloc(144 * (size_t)p->mesh.c8);
+    p->wJ8 = dalloc(9 * (size_t)p->mesh.c8);
     p->rp = dalloc((size_t)N); p->uv = dalloc((size_t)N);
     p->mask = (unsigned char*)calloc((size_t)N, 1);
     p->exx = dalloc(p->E); p->eyy = dalloc(p->E); p->gam = dalloc(p->E); p->epsI = dalloc(p->E);
@@ -916,6 +1114,7 @@ int orc_run_job(const char* job_path, const char* out_path) {
     }
     free(rp_full); free(uv_full); free(outer_lv); free(cg_lv); free(err_lv);
     free(p->slots); free(p->data); free(p->B4); free(p->detJ4); free(p->B3); free(p->area3);
+    free(p->B8); free(p->wJ8);
     free(p->rp); free(p->uv); free(p->mask);
     free(p->exx); free(p->eyy); free(p->gam); free(p->epsI); free(p->sxx); free(p->syy); free(p->tau);
     free(p->sigI); free(p->tabS); free(p->psi); free(p->Ec); free(p->nuc);

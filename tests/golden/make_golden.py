@@ -39,13 +39,14 @@ FIELDS = ["uv", "exx", "eyy", "gamma", "eps_i", "sxx", "syy", "tau", "sig_i", "t
           "exx_p", "eyy_p", "gamma_p", "eps_p_i"]
 
 
-def scenario_fixtures(workdir):
+def scenario_fixtures(workdir, only=None):
     for name, sc in scenarios.SCENARIOS.items():
-        if not sc.get("reference"):
+        if not sc.get("reference") or (only and name not in only):
             continue
         mesh_path = os.path.join(workdir, f"{name}.bin")
         m, lines = scenarios.scenario_lines(name, mesh_path, extra=["dump_k 1", "dump_csr 1"])
-        oracle.write_mesh(mesh_path, m["node_xy"], elem3=m["elem3"], elem4=m["elem4"], borders=m["borders"])
+        oracle.write_mesh(mesh_path, m["node_xy"], elem3=m["elem3"], elem4=m["elem4"], borders=m["borders"],
+                          elem8=m.get("elem8", ()))
         r = oracle.run_reference(lines, threads=1)
         arrays = {k: r[k] for k in ["rows", "cols", "adj_pos", "adj", "rp", "mask", "k_data"] + FIELDS}
         arrays.update(outer_per_level=r["outer_per_level"], cg_per_level=r["cg_per_level"],
@@ -190,6 +191,12 @@ if __name__ == "__main__":
             oracle.build(with_reference=True)
         mesh_fixtures()
         q8_load_fixtures()
+        sys.exit(0)
+    if "--scenarios" in sys.argv:  # only the named scenario fixtures
+        if not oracle.have_reference():
+            oracle.build(with_reference=True)
+        with tempfile.TemporaryDirectory() as d:
+            scenario_fixtures(d, only=sys.argv[sys.argv.index("--scenarios") + 1:])
         sys.exit(0)
     if "--inp" in sys.argv:  # only the .inp loader pins
         if not oracle.have_reference():

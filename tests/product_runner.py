@@ -92,7 +92,7 @@ def build_inputs(lines, mesh_arrays):
     """rp, mask, uv from the product's host-side load builder."""
     job = parse(lines)
     mesh = cp.Mesh.from_arrays(mesh_arrays["node_xy"], mesh_arrays.get("elem3"), mesh_arrays.get("elem4"),
-                               mesh_arrays["borders"])
+                               mesh_arrays["borders"], mesh_arrays.get("elem8"))
     return job, loads_of(job).build(mesh, h=job["h"], rho=1.0)
 
 

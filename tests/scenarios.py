@@ -4,7 +4,10 @@ harness syntax (material, diagram, loads). Units are those of the scenario
 (the configuration-style ones use mm and MPa).
 
 Scenarios with ``reference=True`` contain only what the reference supports
-(Q4, its BC types) and have golden fixtures made by running the reference.
+(Q4 and Q8 elements, its BC types) and have golden fixtures made by running
+the reference. The 8-node meshes come from the product's host generators,
+which are pinned to the reference's own (order 2, Mesh::remapOrder) by the
+digests in golden/ref_meshes.json.
 """
 import numpy as np
 
@@ -34,6 +37,19 @@ def _ogrid(n_c4, rad_n):
 
 def _ring():
     return meshgen.ring(50.0, 100.0, 32, 8)
+
+
+def _q8(make):
+    """An 8-node mesh from the host generators, with its second-order nodes."""
+    def build():
+        import cudaplasticity_b200 as cp
+
+        m = make(cp).arrays()
+        sec = np.zeros(len(m["node_xy"]), np.uint8)
+        sec[np.asarray(m["elem8"])[:, 4:].ravel()] = 1
+        m["sec_ord"] = sec
+        return m
+    return build
 
 
 _PT_LOADS = ["force 1 170 0 0", "force 3 -170 0 0", "fixvertaxis 0", "fixhoraxis 0"]
@@ -67,6 +83,20 @@ SCENARIOS = {
     "rect_elastic": dict(mesh=lambda: meshgen.rect(-1.0, 1.0, -1.0, 1.0, 4, 4), reference=True, mode="elastic",
                          lines=[f"diagram linear {E304} 170000000 {E304}", f"material {E304} {NU304 * 1e-6!r} 1",
                                 "displ 2 0 0 0 1", "force 0 1 0 0"]),
+    # 8-node elements (Q8, 3x3 Gauss points): the plasticityTest plate ...
+    "hole12_q8_pow": dict(mesh=_q8(lambda cp: cp.Mesh.rect_with_hole(-3.0, 3.0, -2.0, 2.0, 0.5, 12, 8, order=2)),
+                          reference=True,
+                          lines=[f"diagram power {E304} 170 1930 0.015", f"material {E304} {NU304} 1"] + _PT_LOADS),
+    # ... the O-grid with a bilinear diagram in 5 increments and gravity ...
+    "ogrid8_q8_bilin": dict(mesh=_q8(lambda cp: cp.Mesh.rect_with_hole(-100.0, 100.0, -100.0, 100.0, 20.0, 2, 2,
+                                                                        rad_n=4, order=2)),
+                            reference=True, levels=5,
+                            lines=["diagram linear 210000 250 2000", "material 210000 0.3 1", "gravity 9.81 0 -1"]
+                            + _OGRID_LOADS),
+    # ... and the ring under internal pressure (quadratic edges turned with
+    # the curved border), piecewise diagram
+    "ring_q8_pw": dict(mesh=_q8(lambda cp: cp.Mesh.ring(50.0, 100.0, 16, 4, order=2)), reference=True,
+                       lines_fn=lambda m: [piecewise_lines(210000.0, 300.0), "material 210000 0.3 1"] + _ring_lines(m)),
     # CST extension (no reference counterpart): the hole-plate O-grid split
     "ogrid16_t3": dict(mesh=lambda: meshgen.split_t3(_ogrid(4, 8)), reference=False, levels=10,
                        lines=["diagram linear 210000 250 2000", "material 210000 0.3 1"] + _OGRID_LOADS),

@@ -88,6 +88,41 @@ def test_batch_matches_fp64_reference(names, ctx, golden_dir, workdir):
     b.close()
 
 
+def test_batch_with_8_node_instances(ctx, golden_dir, workdir):
+    """8-node (Q8) instances next to a 4-node one: the batch switches to the
+    kernels with the 8-node element when the first joins; every instance
+    within 1e-8 of its FP64 golden state, and the 4-node instance bit-identical
+    to its run in a batch without 8-node instances."""
+    names = ("hole12_q8_pow", "ring_q8_pw", "hole12_pow")
+    b0 = cp.Batch(ctx, max_instances=2, max_width=24)
+    inst, kw = scenario_instance(ctx, "hole12_pow", workdir)
+    b0.add(inst, **kw)
+    (inst0, _), = run_all(b0).values()
+    q4_alone = inst0.state()
+    inst0.close()
+    b0.close()
+    b = cp.Batch(ctx, max_instances=4, max_width=24)
+    insts = {}
+    for n in names:
+        inst, kw = scenario_instance(ctx, n, workdir)
+        b.add(inst, **kw)
+        insts[n] = inst
+    res = run_all(b)
+    for n in names:
+        inst, rep = res[id(insts[n])]
+        assert rep["status"] == 0, (n, rep)
+        g = dict(np.load(os.path.join(golden_dir, f"{n}.npz")))
+        st = inst.state()
+        for k in ["uv", "sig_i", "eps_p_i"]:
+            assert field_error(k, st, g) <= MIXED_TOL, (n, k, field_error(k, st, g))
+        assert np.array_equal(yielded(st, 1e-9), yielded(g, 1e-9)), n
+        if n == "hole12_pow":
+            for k in cp.FIELDS + ["uv"]:
+                assert np.array_equal(st[k], q4_alone[k]), k
+        inst.close()
+    b.close()
+
+
 def test_batch_agrees_with_single_instance_mixed_solve(ctx, workdir):
     """Same algorithm as cp_solve in mixed precision: the batched result of an
     instance agrees with the single-instance solve to the mixed bar."""

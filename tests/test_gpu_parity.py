@@ -69,10 +69,11 @@ def test_converged_state_matches_reference(name, ctx, golden_dir, workdir):
 
 
 def test_slot_map_matches_oracle(ctx, workdir):
-    for name in ["hole12_pow", "ogrid16_t3", "ring_pw"]:
+    for name in ["hole12_pow", "ogrid16_t3", "ring_pw", "ogrid8_q8_bilin"]:
         m, lines = scenario(name, workdir)
         path = os.path.join(workdir, f"{name}.bin")
-        oracle.write_mesh(path, m["node_xy"], elem3=m["elem3"], elem4=m["elem4"], borders=m["borders"])
+        oracle.write_mesh(path, m["node_xy"], elem3=m["elem3"], elem4=m["elem4"], borders=m["borders"],
+                          elem8=m.get("elem8", ()))
         o = oracle.run_oracle(["mode csr", f"mesh file {path}", "material 1 0.3 1"])
         r = product_runner.run(ctx, lines, m, want_k=True, max_outer=1, outer_tol=1e300)
         assert np.array_equal(r["slots"], o["slots"]), name
@@ -105,7 +106,7 @@ def test_aitken_and_adaptive_cg_reach_the_same_fixed_point(name, ctx, golden_dir
     assert fast["report"]["outer_iters"] < plain["report"]["outer_iters"]
 
 
-@pytest.mark.parametrize("name", ["hole12_pow", "ogrid16_bilin", "ogrid16_hollomon"])
+@pytest.mark.parametrize("name", ["hole12_pow", "ogrid16_bilin", "ogrid16_hollomon", "ogrid8_q8_bilin"])
 def test_mixed_precision_within_1e8_of_fp64_reference(name, ctx, golden_dir, workdir):
     """FP32 matrix values and inner CG, FP64 defect correction / u / dot-product
     reductions / secant update: error stated against the FP64 golden state."""

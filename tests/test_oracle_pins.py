@@ -18,7 +18,8 @@ REF_SCEN = [n for n, s in scenarios.SCENARIOS.items() if s.get("reference")]
 def run_scenario(name, workdir, extra=()):
     path = os.path.join(workdir, f"{name}.bin")
     m, lines = scenarios.scenario_lines(name, path, extra=extra)
-    oracle.write_mesh(path, m["node_xy"], elem3=m["elem3"], elem4=m["elem4"], borders=m["borders"])
+    oracle.write_mesh(path, m["node_xy"], elem3=m["elem3"], elem4=m["elem4"], borders=m["borders"],
+                      elem8=m.get("elem8", ()))
     return m, oracle.run_oracle(lines)
 
 
@@ -31,9 +32,14 @@ def test_oracle_matches_reference_fixture(name, golden_dir, workdir):
     for k in ["rows", "cols", "adj_pos", "adj", "mask"]:
         assert np.array_equal(r[k], g[k]), k
     # the right-hand side and the first assembly are computed in the same
-    # operation order as the reference's single-threaded run: bit-exact too
+    # operation order as the reference's single-threaded run: bit-exact too.
+    # 8-node elements: the oracle's Gauss constants carry full precision where
+    # the reference writes 15 decimals, so their values agree to ~1e-15.
     assert np.array_equal(r["rp"], g["rp"])
-    assert np.array_equal(r["k_data"], g["k_data"])
+    if "elem8" in m:
+        assert np.max(np.abs(r["k_data"] - g["k_data"])) <= 1e-14 * np.max(np.abs(g["k_data"]))
+    else:
+        assert np.array_equal(r["k_data"], g["k_data"])
     # converged FP64 state under tight tolerances: 1e-10 relative L2
     for k in FIELDS:
         assert field_error(k, r, g) <= 1e-10, (k, field_error(k, r, g))
@@ -106,6 +112,59 @@ def test_oracle_energy_tables(table, diag, S, golden_dir, workdir):
                            f"force 1 {S} 0 0", f"force 3 {-S} 0 0", "fixvertaxis 0", "fixhoraxis 0"])
     got = float(r["energy"][0])
     assert float(f"{got:.6g}") == pytest.approx(expected, rel=1e-12), (got, expected)
+
+
+@pytest.mark.parametrize("table,diag,S", [
+    ("aitken_plast2pow", f"diagram power {scenarios.E304 * 1e6} 170e6 {scenarios.E304 * 1e4} 0.015", 170e6),
+    ("aitken_plast2", f"diagram linear {scenarios.E304 * 1e6} 170e6 {scenarios.E304 * 1e5}", 170e6),
+    ("aitken_elast2", f"diagram power {scenarios.E304 * 1e6} 170e6 {scenarios.E304 * 1e4} 0.015", 1e6),
+])
+def test_oracle_energy_tables_q8(table, diag, S, golden_dir, workdir):
+    """The same energy tables for 8-node elements (energyConvTest with order 2,
+    src/Main.cpp:110-175): the 2880-element Q8 plate. For Q8 elements the
+    reference's deformEnergy takes the secant energy on both branches."""
+    import cudaplasticity_b200 as cp
+
+    tables = json.load(open(os.path.join(golden_dir, "ref_tables.json")))
+    expected = [e for n, e in tables[table] if n == 2880][0]
+    m = cp.Mesh.rect_with_hole(-3, 3, -2, 2, 0.5, 36, 24, order=2).arrays()
+    assert m["elem8"].shape[0] == 2880 and m["elem4"].shape[0] == 0
+    path = os.path.join(workdir, "m8.bin")
+    oracle.write_mesh(path, m["node_xy"], borders=m["borders"], elem8=m["elem8"])
+    r = oracle.run_oracle(["mode solve", f"mesh file {path}", diag, f"material {scenarios.E304 * 1e6} 0.29 1",
+                           f"force 1 {S} 0 0", f"force 3 {-S} 0 0", "fixvertaxis 0", "fixhoraxis 0"])
+    got = float(r["energy"][0])
+    assert float(f"{got:.6g}") == pytest.approx(expected, rel=1e-12), (got, expected)
+
+
+@pytest.mark.parametrize("name", ["hole_q8", "ring_q8", "rect_q8"])
+def test_oracle_q8_loads(name, golden_dir, workdir):
+    """The oracle's load builder on 8-node meshes (quadratic edges, 8-node
+    body forces) against the reference's initConditions on the same meshes."""
+    import sys
+
+    import cudaplasticity_b200 as cp
+
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)) + "/golden")
+    from make_golden import Q8_LOADS
+
+    g = dict(np.load(os.path.join(golden_dir, "q8_loads.npz")))
+    spec, lines = Q8_LOADS[name]
+    w = spec.split()
+    f = [float(x) for x in w[1:]]
+    if w[0] == "hole":
+        mesh = cp.Mesh.rect_with_hole(*f[:5], int(f[5]), int(f[6]), order=int(f[7]))
+    elif w[0] == "ring":
+        mesh = cp.Mesh.ring(f[0], f[1], int(f[2]), int(f[3]), order=int(f[4]))
+    else:
+        mesh = cp.Mesh.rect(*f[:4], int(f[4]), int(f[5]), order=int(f[6]))
+    m = mesh.arrays()
+    path = os.path.join(workdir, "l8.bin")
+    oracle.write_mesh(path, m["node_xy"], borders=m["borders"], elem8=m["elem8"])
+    r = oracle.run_oracle(["mode elastic", f"mesh file {path}", "cg_eps 1e-3"] + lines)
+    ref = g[f"{name}_rp"]
+    assert np.max(np.abs(r["rp"] - ref)) <= 1e-14 * np.max(np.abs(ref))
+    assert np.array_equal(r["mask"].astype(bool), g[f"{name}_mask"].astype(bool))
 
 
 def test_oracle_diagram_reproduction(golden_dir, workdir):
