@@ -20,6 +20,7 @@ CP_ERR_UNSUPPORTED = 7
 CP_ERR_BUSY = 8
 CP_ERR_NO_DEVICE = 9
 CP_ERR_CANCELLED = 10
+CP_ERR_TIMEOUT = 11
 
 CP_PLANE_STRESS, CP_PLANE_STRAIN = 0, 1
 CP_DIAGRAM_ELASTIC, CP_DIAGRAM_LINEAR, CP_DIAGRAM_POWER, CP_DIAGRAM_HOLLOMON, CP_DIAGRAM_PIECEWISE = range(5)

@@ -249,6 +249,29 @@ void cg_fp64_fused(cp_instance* I, double eps, long long max_iter, int precond) 
     a.precond = precond;
     a.sc = I->sc;
     a.partials = I->f_partials;
+    if (I->cluster_fp64) {
+        if (!I->cluster_planned) {
+            I->cluster_plan = cp::cluster_cg_plan(a, I->csr.max_width);
+            I->cluster_planned = 1;
+        }
+        if (I->cluster_plan.ctas > 0) {
+            // one cluster holds the whole solve
+            cp::cluster_cg_launch(a, I->cluster_plan, eps * eps, max_iter, I->s());
+            I->launches += 1;
+            CP_CUDA(cudaMemcpyAsync(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost, I->s()));
+            CP_CUDA(cudaStreamSynchronize(I->s()));
+            return;
+        }
+    }
+    if (I->persistent_fp64 && cp::fused_persistent_fits(a)) {
+        // one cooperative launch for the whole solve
+        cp::fused_launch_persistent(a, eps * eps, max_iter, I->s());
+        I->launches += 1;
+        CP_CUDA(cudaMemcpyAsync(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost, I->s()));
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+        if (I->sc_h->status == CP_ERR_TIMEOUT) throw Error{CP_ERR_TIMEOUT, "persistent CG: grid barrier timed out"};
+        return;
+    }
     if (I->use_graph && !I->gf[precond]) I->gf[precond] = cp::fused_build_while_graph(a, I->body_iters, I->s());
     cp::fused_launch_start(a, eps * eps, max_iter, I->s());
     I->launches += 2;
@@ -335,6 +358,7 @@ CP_API const char* cp_status_string(int s) {
     case CP_ERR_BUSY: return "busy";
     case CP_ERR_NO_DEVICE: return "no CUDA device";
     case CP_ERR_CANCELLED: return "cancelled";
+    case CP_ERR_TIMEOUT: return "a bounded device-side wait gave up";
     default: return "unknown status";
     }
 }
@@ -415,7 +439,15 @@ CP_API int cp_instance_create(cp_context* ctx, const cp_mesh_view* mv, const cp_
     if (!I) return CP_ERR_NOMEM;
     I->ctx = ctx;
     if (const char* g = std::getenv("CUPLAST_NO_GRAPH")) I->use_graph = !(g[0] == '1');
-    if (const char* g = std::getenv("CUPLAST_FP64_CG")) I->fused_fp64 = std::strcmp(g, "classic") != 0;
+    // FP64 CG form: one thread-block cluster when the instance fits (default),
+    // else one launch per iteration in a graph; CUPLAST_FP64_CG=fused keeps
+    // the graph loop, =persistent makes it one cooperative launch, =classic
+    // selects the two-kernel loop of cg.cu.
+    if (const char* g = std::getenv("CUPLAST_FP64_CG")) {
+        I->fused_fp64 = std::strcmp(g, "classic") != 0;
+        I->persistent_fp64 = std::strcmp(g, "persistent") == 0;
+        I->cluster_fp64 = std::strcmp(g, "cluster") == 0;
+    }
     int rc = guarded(ctx, [&] {
         CP_CHECK(mv->node_count > 0 && mv->node_xy, CP_ERR_INVALID, "mesh: no nodes");
         CP_CHECK(mv->count3 >= 0 && mv->count4 >= 0 && mv->count8 >= 0 &&

@@ -71,7 +71,22 @@ struct FusedArgs {
 
 void fused_launch_start(const FusedArgs& a, double eps2, long long max_iter, cudaStream_t s);
 void fused_launch_iteration(const FusedArgs& a, int parity, cudaStream_t s);
+// The whole solve (init, first step, iterations) as one cooperative launch;
+// only when its grid is that of the kernels above (fused_persistent_fits).
+bool fused_persistent_fits(const FusedArgs& a);
+void fused_launch_persistent(const FusedArgs& a, double eps2, long long max_iter, cudaStream_t s);
 cudaGraphExec_t fused_build_while_graph(const FusedArgs& a, int body_iters, cudaStream_t s);
+
+// The same solve inside one thread-block cluster (cg_cluster.cu), for
+// instances whose blocks of K and records fit the cluster's shared memory.
+struct ClusterPlan {
+    int ctas = 0;      // cluster size (0: does not fit)
+    int spc = 0;       // slices of 32 nodes per CTA (one warp each)
+    int wmax = 0;      // widest node row, in blocks
+    size_t smem = 0;   // dynamic shared memory per CTA
+};
+ClusterPlan cluster_cg_plan(const FusedArgs& a, int max_width);
+void cluster_cg_launch(const FusedArgs& a, const ClusterPlan& plan, double eps2, long long max_iter, cudaStream_t s);
 
 template <typename T>
 void cg_launch_init(const CgArgs<T>& a, const void* valA, bool valA_is_fp64, double eps2, long long max_iter,

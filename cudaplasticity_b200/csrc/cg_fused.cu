@@ -17,6 +17,7 @@
 // deterministic cross-block reduction (last block, index order). The
 // scalars stay on the device; the loop runs in a CUDA graph with a WHILE
 // node, as in cg.cu.
+#include <cstddef>
 #include <mutex>
 #include <unordered_map>
 
@@ -80,12 +81,19 @@ __device__ __forceinline__ bool reduce_sums(const FusedArgs& a, double* v, int k
     return true;
 }
 
+// Loads of vectors that other blocks write during the same launch. The
+// one-launch-per-iteration kernels (P = false) read them through the
+// read-only path; the persistent kernel (P = true) loads them at L2
+// (ld.global.cg), since an SM's L1 is not coherent with the other SMs' stores.
+template <bool P>
+__device__ __forceinline__ double2 ld_other(const double2* p) {
+    if (P) return __ldcg(p);
+    return __ldg(p);
+}
+
 // r = m.(b - K x), block-Jacobi inverse, u = M r, p = kp = 0, the parity-0
 // record (u, -, 0); sums (r, r), (b, b).
-__global__ void __launch_bounds__(kThreads) k_f_init(FusedArgs a, double eps2, long long max_iter) {
-    __shared__ double sh[2 * kThreads / 32];
-    __shared__ bool last;
-    double v[2] = {0.0, 0.0};
+__device__ __forceinline__ void init_body(const FusedArgs& a, double* v) {
     CPF_SLICE_LOOP {
         const int n = 32 * sl + lane;
         if (n >= a.n) continue;
@@ -125,35 +133,29 @@ __global__ void __launch_bounds__(kThreads) k_f_init(FusedArgs a, double eps2, l
         v[0] += r.x * r.x + r.y * r.y;
         v[1] += bb.x * bb.x + bb.y * bb.y;
     }
-    double t[kSums];
-    if (!reduce_sums(a, v, 2, t, sh, &last)) return;
-    if (threadIdx.x == 0) {
-        CgScalars* sc = a.sc;
-        const double rr = t[0], bb = t[1];
-        sc->rr = rr;
-        sc->bb = bb;
-        sc->res64 = rr;
-        sc->normB_inv = bb > 0.0 ? 1.0 / bb : 0.0;
-        sc->eps2 = eps2;
-        sc->iter = 0;
-        sc->max_iter = max_iter;
-        sc->status = 0;
-        sc->lin_done = 0;
-        sc->alpha = sc->beta = 0.0;
-        sc->converged = (rr == 0.0 || rr * sc->normB_inv <= eps2) ? 1 : 0;
-        if (!(rr == rr) || !(bb == bb)) sc->status = CP_ERR_BREAKDOWN;
-        sc->ticket = 0;
-    }
+}
+
+__device__ __forceinline__ void init_scalars(CgScalars* sc, const double* t, double eps2, long long max_iter) {
+    const double rr = t[0], bb = t[1];
+    sc->rr = rr;
+    sc->bb = bb;
+    sc->res64 = rr;
+    sc->normB_inv = bb > 0.0 ? 1.0 / bb : 0.0;
+    sc->eps2 = eps2;
+    sc->iter = 0;
+    sc->max_iter = max_iter;
+    sc->status = 0;
+    sc->lin_done = 0;
+    sc->alpha = sc->beta = 0.0;
+    sc->converged = (rr == 0.0 || rr * sc->normB_inv <= eps2) ? 1 : 0;
+    if (!(rr == rr) || !(bb == bb)) sc->status = CP_ERR_BREAKDOWN;
+    sc->ticket = 0;
 }
 
 // w = K u (u from the parity-0 records), M w into the record; gamma = (r, u),
 // delta = (w, u): the first step.
-__global__ void __launch_bounds__(kThreads) k_f_w(FusedArgs a) {
-    __shared__ double sh[2 * kThreads / 32];
-    __shared__ bool last;
-    CgScalars* sc = a.sc;
-    if (sc->converged || sc->status) return;
-    double v[2] = {0.0, 0.0};
+template <bool P>
+__device__ __forceinline__ void w_body(const FusedArgs& a, double* v) {
     CPF_SLICE_LOOP {
         const int n = 32 * sl + lane;
         if (n >= a.n) continue;
@@ -163,7 +165,7 @@ __global__ void __launch_bounds__(kThreads) k_f_w(FusedArgs a) {
             const long long bi = base + 32LL * k + lane;
             const int col = __ldg(a.scol + bi);
             const double2 lo = load_lo(a.val, bi), hi = load_hi(a.val, bi);
-            const double2 uc = a.gA[3 * (size_t)col];
+            const double2 uc = P ? __ldcg(a.gA + 3 * (size_t)col) : a.gA[3 * (size_t)col];
             k0 += lo.x * uc.x + lo.y * uc.y;
             k1 += hi.x * uc.x + hi.y * uc.y;
         }
@@ -174,34 +176,28 @@ __global__ void __launch_bounds__(kThreads) k_f_w(FusedArgs a) {
         v[0] += r.x * u.x + r.y * u.y;
         v[1] += w.x * u.x + w.y * u.y;
     }
-    double t[kSums];
-    if (!reduce_sums(a, v, 2, t, sh, &last)) return;
-    if (threadIdx.x == 0) {
-        const double g = t[0], d = t[1];
-        sc->rho = g;
-        sc->alpha = g / d;
-        sc->beta = 0.0;
-        if (!(d > 0.0) || !(sc->alpha == sc->alpha)) sc->status = CP_ERR_BREAKDOWN;
-        sc->ticket = 0;
-    }
+}
+
+__device__ __forceinline__ void w_scalars(CgScalars* sc, const double* t) {
+    const double g = t[0], d = t[1];
+    sc->rho = g;
+    sc->alpha = g / d;
+    sc->beta = 0.0;
+    if (!(d > 0.0) || !(sc->alpha == sc->alpha)) sc->status = CP_ERR_BREAKDOWN;
+    sc->ticket = 0;
 }
 
 // One iteration (see the file comment); parity selects the record buffers.
-__global__ void __launch_bounds__(kThreads) k_f_iter(FusedArgs a, int parity) {
-    __shared__ double sh[2 * kThreads / 32];
-    __shared__ bool last;
-    CgScalars* sc = a.sc;
-    if (sc->converged || sc->status) return;
+template <bool P>
+__device__ __forceinline__ void iter_body(const FusedArgs& a, int parity, double al, double bt, double* v) {
     const double2* __restrict__ go = parity ? a.gB : a.gA;
     double2* __restrict__ gn = parity ? a.gA : a.gB;
-    const double al = sc->alpha, bt = sc->beta;
-    double v[kSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     CPF_SLICE_LOOP {
         const int n = 32 * sl + lane;
         if (n >= a.n) continue;
         const int base = a.slice_ptr[sl], wd = (a.slice_ptr[sl + 1] - base) >> 5;
-        const double2 u0 = __ldg(go + 3 * (size_t)n), mw0 = __ldg(go + 3 * (size_t)n + 1),
-                      mk0 = __ldg(go + 3 * (size_t)n + 2);
+        const double2 u0 = ld_other<P>(go + 3 * (size_t)n), mw0 = ld_other<P>(go + 3 * (size_t)n + 1),
+                      mk0 = ld_other<P>(go + 3 * (size_t)n + 2);
         const double2 pn = a.p[n], wn = a.w[n], kn = a.kp[n];
         const uchar2 m = a.mask[n];
         const double2 p = make_double2(u0.x + bt * pn.x, u0.y + bt * pn.y);
@@ -219,8 +215,8 @@ __global__ void __launch_bounds__(kThreads) k_f_iter(FusedArgs a, int parity) {
             const long long bi = base + 32LL * k + lane;
             const int col = __ldg(a.scol + bi);
             const double2 lo = load_lo(a.val, bi), hi = load_hi(a.val, bi);
-            const double2 uc = __ldg(go + 3 * (size_t)col), mwc = __ldg(go + 3 * (size_t)col + 1),
-                          mkc = __ldg(go + 3 * (size_t)col + 2);
+            const double2 uc = ld_other<P>(go + 3 * (size_t)col), mwc = ld_other<P>(go + 3 * (size_t)col + 1),
+                          mkc = ld_other<P>(go + 3 * (size_t)col + 2);
             const double ux = uc.x - al * (mwc.x + bt * mkc.x), uy = uc.y - al * (mwc.y + bt * mkc.y);
             k0 += lo.x * ux + lo.y * uy;
             k1 += hi.x * ux + hi.y * uy;
@@ -240,22 +236,154 @@ __global__ void __launch_bounds__(kThreads) k_f_iter(FusedArgs a, int parity) {
         v[3] += (w.x * p.x + w.y * p.y) + (kp.x * u.x + kp.y * u.y);
         v[4] += kp.x * p.x + kp.y * p.y;
     }
+}
+
+__device__ __forceinline__ void iter_scalars(CgScalars* sc, const double* t) {
+    const double g = t[0], rn = t[2];
+    const double beta = g / sc->rho;
+    const double den = t[1] + beta * t[3] + beta * beta * t[4];
+    sc->iter += 1;
+    sc->rr = rn;
+    sc->beta = beta;
+    sc->alpha = g / den;
+    sc->rho = g;
+    if (rn * sc->normB_inv <= sc->eps2) sc->converged = 1;
+    else if (sc->iter >= sc->max_iter) sc->status = CP_ERR_NOT_CONVERGED;
+    else if (!(den > 0.0) || !(g > 0.0)) sc->status = CP_ERR_BREAKDOWN;
+    if (!(rn == rn)) sc->status = CP_ERR_BREAKDOWN;
+    sc->ticket = 0;
+}
+
+__global__ void __launch_bounds__(kThreads) k_f_init(FusedArgs a, double eps2, long long max_iter) {
+    __shared__ double sh[2 * kThreads / 32];
+    __shared__ bool last;
+    double v[2] = {0.0, 0.0};
+    init_body(a, v);
+    double t[kSums];
+    if (!reduce_sums(a, v, 2, t, sh, &last)) return;
+    if (threadIdx.x == 0) init_scalars(a.sc, t, eps2, max_iter);
+}
+
+__global__ void __launch_bounds__(kThreads) k_f_w(FusedArgs a) {
+    __shared__ double sh[2 * kThreads / 32];
+    __shared__ bool last;
+    CgScalars* sc = a.sc;
+    if (sc->converged || sc->status) return;
+    double v[2] = {0.0, 0.0};
+    w_body<false>(a, v);
+    double t[kSums];
+    if (!reduce_sums(a, v, 2, t, sh, &last)) return;
+    if (threadIdx.x == 0) w_scalars(sc, t);
+}
+
+__global__ void __launch_bounds__(kThreads) k_f_iter(FusedArgs a, int parity) {
+    __shared__ double sh[2 * kThreads / 32];
+    __shared__ bool last;
+    CgScalars* sc = a.sc;
+    if (sc->converged || sc->status) return;
+    double v[kSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    iter_body<false>(a, parity, sc->alpha, sc->beta, v);
     double t[kSums];
     if (!reduce_sums(a, v, 5, t, sh, &last)) return;
+    if (threadIdx.x == 0) iter_scalars(sc, t);
+}
+
+// ---------------------------------------------------- persistent form --
+//
+// The whole linear solve in one cooperative launch: init, the first step and
+// every iteration run back to back, separated by a grid barrier. The block
+// that arrives last at a step (the reduction's last block) computes the
+// scalars and releases the others by advancing sc->gen; the arithmetic, the
+// block partition and the summation order are those of the kernels above, so
+// the results are the same bit for bit. Co-residency of all blocks comes from
+// the cooperative launch. Every wait is bounded in time: a block that gives up
+// sets CP_ERR_TIMEOUT and returns, and so does every other waiting block.
+
+constexpr unsigned long long kBarrierNs = 2000000000ull;  // 2 s; one step takes microseconds
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// The last block of a step (thread 0): publish the scalars it has just
+// written, then release the step.
+__device__ __forceinline__ void grid_release(CgScalars* sc) {
+    __threadfence();
+    atomicAdd(&sc->gen, 1u);
+}
+
+// Waits until step `target` is released. Thread 0 polls and then reads the
+// step's outcome once for the whole block (another block's time-out may
+// change sc->status at any moment, and every thread of a block must take the
+// same branch): true to go on, with alpha and beta in *view. Gives up after
+// kBarrierNs with CP_ERR_TIMEOUT set.
+struct StepView {
+    int go;
+    double alpha, beta;
+};
+
+__device__ __forceinline__ bool grid_wait(CgScalars* sc, unsigned int target, StepView* view) {
     if (threadIdx.x == 0) {
-        const double g = t[0], rn = t[2];
-        const double beta = g / sc->rho;
-        const double den = t[1] + beta * t[3] + beta * beta * t[4];
-        sc->iter += 1;
-        sc->rr = rn;
-        sc->beta = beta;
-        sc->alpha = g / den;
-        sc->rho = g;
-        if (rn * sc->normB_inv <= sc->eps2) sc->converged = 1;
-        else if (sc->iter >= sc->max_iter) sc->status = CP_ERR_NOT_CONVERGED;
-        else if (!(den > 0.0) || !(g > 0.0)) sc->status = CP_ERR_BREAKDOWN;
-        if (!(rn == rn)) sc->status = CP_ERR_BREAKDOWN;
-        sc->ticket = 0;
+        const volatile unsigned int* g = &sc->gen;
+        int ok = 1;
+        if (*g < target) {
+            const unsigned long long t0 = global_ns();
+            while (*g < target) {
+                if (global_ns() - t0 > kBarrierNs) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        if (!ok) atomicCAS(&sc->status, 0, CP_ERR_TIMEOUT);
+        __threadfence();
+        const volatile CgScalars* vs = sc;
+        view->go = ok && !vs->converged && !vs->status;
+        view->alpha = vs->alpha;
+        view->beta = vs->beta;
+    }
+    __syncthreads();
+    return view->go != 0;
+}
+
+__global__ void __launch_bounds__(kThreads) k_f_persistent(FusedArgs a, double eps2, long long max_iter) {
+    __shared__ double sh[2 * kThreads / 32];
+    __shared__ bool last;
+    __shared__ StepView view;
+    CgScalars* sc = a.sc;
+    unsigned int step = 0;
+    double t[kSums];
+    {
+        double v[2] = {0.0, 0.0};
+        init_body(a, v);
+        if (reduce_sums(a, v, 2, t, sh, &last) && threadIdx.x == 0) {
+            init_scalars(sc, t, eps2, max_iter);
+            grid_release(sc);
+        }
+        if (!grid_wait(sc, ++step, &view)) return;
+    }
+    {
+        double v[2] = {0.0, 0.0};
+        w_body<true>(a, v);
+        if (reduce_sums(a, v, 2, t, sh, &last) && threadIdx.x == 0) {
+            w_scalars(sc, t);
+            grid_release(sc);
+        }
+        if (!grid_wait(sc, ++step, &view)) return;
+    }
+    for (int it = 0;; ++it) {
+        double v[kSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        const double al = view.alpha, bt = view.beta;
+        __syncthreads();  // everyone has read the view before thread 0 overwrites it
+        iter_body<true>(a, it & 1, al, bt, v);
+        if (reduce_sums(a, v, 5, t, sh, &last) && threadIdx.x == 0) {
+            iter_scalars(sc, t);
+            grid_release(sc);
+        }
+        if (!grid_wait(sc, ++step, &view)) return;
     }
 }
 
@@ -293,6 +421,23 @@ void fused_launch_start(const FusedArgs& a, double eps2, long long max_iter, cud
     k_f_init<<<g1, kThreads, 0, s>>>(a, eps2, max_iter);
     k_f_w<<<g2, kThreads, 0, s>>>(a);
     CP_CUDA(cudaGetLastError());
+}
+
+bool fused_persistent_fits(const FusedArgs& a) {
+    const long long need = (a.n + kThreads - 1) / kThreads;
+    return need <= fused_grid(k_f_persistent, a.n, a.sm_count) && need <= fused_grid(k_f_iter, a.n, a.sm_count);
+}
+
+void fused_launch_persistent(const FusedArgs& a, double eps2, long long max_iter, cudaStream_t s) {
+    const int g = (a.n + kThreads - 1) / kThreads;  // the grid of k_f_init / k_f_w / k_f_iter when it fits
+    CP_CHECK(fused_persistent_fits(a) && g <= a.max_blocks, CP_ERR_INVALID, "persistent CG: grid does not fit");
+    // the reduction ticket and the barrier's release counter start at zero
+    static_assert(offsetof(CgScalars, gen) == offsetof(CgScalars, ticket) + sizeof(unsigned int),
+                  "ticket and gen must be adjacent");
+    CP_CUDA(cudaMemsetAsync(&a.sc->ticket, 0, 2 * sizeof(unsigned int), s));
+    FusedArgs args = a;
+    void* params[] = {&args, &eps2, &max_iter};
+    CP_CUDA(cudaLaunchCooperativeKernel((const void*)k_f_persistent, dim3(g), dim3(kThreads), params, 0, s));
 }
 
 void fused_launch_iteration(const FusedArgs& a, int parity, cudaStream_t s) {

@@ -46,7 +46,11 @@ struct cp_instance {
     bool loads_set = false;
     bool in_batch = false;  // owned by a cp_batch until harvested: no other call may touch it
     // single-launch FP64 CG (cg_fused.cu), allocated on first use
-    bool fused_fp64 = true;  // false (CUPLAST_FP64_CG=classic): the two-kernel loop of cg.cu
+    bool fused_fp64 = true;        // false (CUPLAST_FP64_CG=classic): the two-kernel loop of cg.cu
+    bool persistent_fp64 = false;  // CUPLAST_FP64_CG=persistent: one cooperative launch per linear solve
+    bool cluster_fp64 = true;      // one thread-block cluster when the instance fits (CUPLAST_FP64_CG other than cluster: off)
+    int cluster_planned = 0;       // cluster_plan below is computed (once per instance)
+    cp::ClusterPlan cluster_plan;
     double2 *f_r = nullptr, *f_w = nullptr, *f_p = nullptr, *f_kp = nullptr, *f_g = nullptr;
     double* f_partials = nullptr;
     cudaGraphExec_t gf[2] = {nullptr, nullptr};  // [precond]

@@ -88,6 +88,7 @@ struct CgScalars {
     int status;         // 0 running/ok, CP_ERR_BREAKDOWN, CP_ERR_NOT_CONVERGED
     int lin_done;       // init found the FP64 residual already below the caller's tolerance
     unsigned int ticket;
+    unsigned int gen;   // persistent CG: grid-barrier steps released so far
 };
 
 struct OuterScalars {

@@ -42,7 +42,8 @@ typedef enum {
     CP_ERR_UNSUPPORTED = 7,
     CP_ERR_BUSY = 8,
     CP_ERR_NO_DEVICE = 9,      /* no CUDA device visible */
-    CP_ERR_CANCELLED = 10
+    CP_ERR_CANCELLED = 10,
+    CP_ERR_TIMEOUT = 11        /* a bounded device-side wait gave up (grid barrier of the persistent CG) */
 } cp_status;
 
 typedef struct cp_context cp_context;

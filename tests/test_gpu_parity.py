@@ -118,6 +118,50 @@ def test_mixed_precision_within_1e8_of_fp64_reference(name, ctx, golden_dir, wor
     assert np.array_equal(yielded(r, 1e-9), yielded(g, 1e-9))
 
 
+@pytest.mark.parametrize("name", ["hole12_pow", "ogrid16_bilin", "hole12_q8_pow"])
+def test_persistent_cg_matches_graph_loop(name, ctx, golden_dir, workdir, monkeypatch):
+    """The FP64 CG as one cooperative launch per linear solve
+    (CUPLAST_FP64_CG=persistent, read at instance creation): same arithmetic,
+    block partition and summation order as the one-launch-per-iteration
+    graph loop, so the results agree bit for bit, with and without the
+    block-Jacobi preconditioner."""
+    m, lines = scenario(name, workdir)
+    for precond in (0, 1):
+        monkeypatch.setenv("CUPLAST_FP64_CG", "fused")
+        base = product_runner.run(ctx, lines, m, precond=precond)
+        monkeypatch.setenv("CUPLAST_FP64_CG", "persistent")
+        pers = product_runner.run(ctx, lines, m, precond=precond)
+        monkeypatch.delenv("CUPLAST_FP64_CG")
+        for k in cp.FIELDS + ["uv"]:
+            assert np.array_equal(pers[k], base[k]), (name, precond, k)
+        assert pers["report"]["cg_iters"] == base["report"]["cg_iters"]
+        assert pers["report"]["outer_iters"] == base["report"]["outer_iters"]
+    g = load_golden(golden_dir, name)
+    k, err, errs = worst(pers, g)
+    assert err <= FP64_TOL, (k, err, errs)
+
+
+@pytest.mark.parametrize("name", ["hole12_pow", "ogrid16_bilin", "hole12_q8_pow"])
+def test_cluster_cg_matches_reference(name, ctx, golden_dir, workdir, monkeypatch):
+    """The FP64 CG inside one thread-block cluster (the default where the
+    instance fits the cluster's shared memory): the converged state within
+    1e-10 of the reference's, as the other solvers, and the same number of
+    outer iterations as the grid-wide CG loop (CUPLAST_FP64_CG=fused, read at
+    instance creation) within a couple (the summation order differs)."""
+    m, lines = scenario(name, workdir)
+    monkeypatch.setenv("CUPLAST_FP64_CG", "fused")
+    base = product_runner.run(ctx, lines, m, precond=1)
+    monkeypatch.setenv("CUPLAST_FP64_CG", "cluster")
+    for precond in (0, 1):
+        r = product_runner.run(ctx, lines, m, precond=precond)
+        g = load_golden(golden_dir, name)
+        k, err, errs = worst(r, g)
+        assert err <= FP64_TOL, (name, precond, k, err, errs)
+        assert np.array_equal(yielded(r), yielded(g))
+    assert abs(r["report"]["outer_iters"] - base["report"]["outer_iters"]) <= 2
+    assert r["report"]["status"] == 0
+
+
 def test_cg_phase_reference_semantics(ctx, golden_dir, workdir):
     """One elastic solve through the phase entry points: assemble, CG from the
     current u, secant update; against the oracle's first outer iteration."""
