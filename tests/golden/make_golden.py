@@ -113,9 +113,24 @@ Q8_LOADS = {
 }
 
 
+# The remaining load and boundary-condition setters on 4-node meshes: point
+# forces, prescribed point displacements (fixPoint / setDisplPoint), whole
+# borders prescribed (setDisplacement without the mid-point options,
+# fixBorder), one-axis border fixes, plane strain, a thickness other than 1.
+MISC_LOADS = {
+    "rect_points": ("rect -2 2 -1 1 8 4 1",
+                    ["material 1000 0.25 1.5", "plane strain", "forcepoint 2 1 3 -4", "forcepoint 0 -1 0 -7.5",
+                     "displpoint -2 -1 0.01 -0.02", "fixpoint -2 1", "displ 1 0.05 0 0 0", "fixbordervert 3",
+                     "force 2 0 -10 0"]),
+    "ring_mixed": ("ring 50 120 24 6 1",
+                   ["material 210000 0.3 2", "force 0 150 20 1", "displ 1 0 0 0 0", "forcepoint 120 0 0 500",
+                    "gravity 9.81 1 1"]),
+}
+
+
 def q8_load_fixtures():
     out = {}
-    for name, (spec, lines) in Q8_LOADS.items():
+    for name, (spec, lines) in list(Q8_LOADS.items()) + list(MISC_LOADS.items()):
         r = oracle.run_reference(["mode loads", "mesh " + spec] + lines)
         for k in ("rp", "mask", "uv"):
             out[f"{name}_{k}"] = r[k]

@@ -194,21 +194,23 @@ def test_batch_and_server_entry_points_validate_arguments_without_a_device():
     assert L.cp_secant_update_noalloc(None, None, 0, None, 0, None, None, None, None, None, None, None) == inv
 
 
-@pytest.mark.parametrize("name", ["hole_q8", "ring_q8", "rect_q8"])
-def test_q8_loads_match_reference(name, golden_dir):
-    """initConditions on 8-node meshes (src/PlasticitySolver.cu:819-927):
+@pytest.mark.parametrize("name", ["hole_q8", "ring_q8", "rect_q8", "rect_points", "ring_mixed"])
+def test_q8_and_point_loads_match_reference(name, golden_dir):
+    """initConditions (src/PlasticitySolver.cu:812-1005) against the
+    reference's own load builder on the same meshes: on 8-node meshes the
     consistent quadratic-edge loads (1/3, 4/3, 1/3 weights, normal pressure
-    on curved edges), 8-node body forces (-1/12 per corner, 1/3 per mid-side
-    node), Dirichlet masks and prescribed values, against the reference's own
-    load builder on the same order-2 meshes. Bit for bit, up to the
-    summation order of shared nodes (1e-14 of the largest load)."""
+    on curved edges) and 8-node body forces (-1/12 per corner, 1/3 per
+    mid-side node); on 4-node meshes point forces, prescribed points, whole
+    prescribed borders, one-axis border fixes and a tangential traction
+    component. Dirichlet masks and prescribed values bit for bit, forces up
+    to the summation order of shared nodes (1e-14 of the largest load)."""
     import sys
 
     sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
-    from make_golden import Q8_LOADS
+    from make_golden import MISC_LOADS, Q8_LOADS
 
     g = dict(np.load(os.path.join(golden_dir, "q8_loads.npz")))
-    spec, lines = Q8_LOADS[name]
+    spec, lines = {**Q8_LOADS, **MISC_LOADS}[name]
     w = spec.split()
     f = [float(x) for x in w[1:]]
     if w[0] == "hole":
@@ -217,7 +219,7 @@ def test_q8_loads_match_reference(name, golden_dir):
         mesh = cp.Mesh.ring(f[0], f[1], int(f[2]), int(f[3]), order=int(f[4]))
     else:
         mesh = cp.Mesh.rect(*f[:4], int(f[4]), int(f[5]), order=int(f[6]))
-    assert mesh.count8() > 0
+    assert (mesh.count8() > 0) == (name in Q8_LOADS)
     job = product_runner.parse(lines)
     rp, mask, uv = product_runner.loads_of(job).build(mesh, h=job["h"], rho=1.0)
     ref = g[f"{name}_rp"]

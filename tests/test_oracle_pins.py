@@ -137,19 +137,20 @@ def test_oracle_energy_tables_q8(table, diag, S, golden_dir, workdir):
     assert float(f"{got:.6g}") == pytest.approx(expected, rel=1e-12), (got, expected)
 
 
-@pytest.mark.parametrize("name", ["hole_q8", "ring_q8", "rect_q8"])
+@pytest.mark.parametrize("name", ["hole_q8", "ring_q8", "rect_q8", "rect_points", "ring_mixed"])
 def test_oracle_q8_loads(name, golden_dir, workdir):
     """The oracle's load builder on 8-node meshes (quadratic edges, 8-node
-    body forces) against the reference's initConditions on the same meshes."""
+    body forces) and with the point and whole-border conditions, against the
+    reference's initConditions on the same meshes."""
     import sys
 
     import cudaplasticity_b200 as cp
 
     sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)) + "/golden")
-    from make_golden import Q8_LOADS
+    from make_golden import MISC_LOADS, Q8_LOADS
 
     g = dict(np.load(os.path.join(golden_dir, "q8_loads.npz")))
-    spec, lines = Q8_LOADS[name]
+    spec, lines = {**Q8_LOADS, **MISC_LOADS}[name]
     w = spec.split()
     f = [float(x) for x in w[1:]]
     if w[0] == "hole":
@@ -160,7 +161,7 @@ def test_oracle_q8_loads(name, golden_dir, workdir):
         mesh = cp.Mesh.rect(*f[:4], int(f[4]), int(f[5]), order=int(f[6]))
     m = mesh.arrays()
     path = os.path.join(workdir, "l8.bin")
-    oracle.write_mesh(path, m["node_xy"], borders=m["borders"], elem8=m["elem8"])
+    oracle.write_mesh(path, m["node_xy"], elem4=m["elem4"], borders=m["borders"], elem8=m.get("elem8", ()))
     r = oracle.run_oracle(["mode elastic", f"mesh file {path}", "cg_eps 1e-3"] + lines)
     ref = g[f"{name}_rp"]
     assert np.max(np.abs(r["rp"] - ref)) <= 1e-14 * np.max(np.abs(ref))
