@@ -16,7 +16,7 @@ import numpy as np
 
 from . import _capi as C
 from ._capi import (CP_DIAGRAM_ELASTIC, CP_DIAGRAM_HOLLOMON, CP_DIAGRAM_LINEAR, CP_DIAGRAM_PIECEWISE,  # noqa: F401
-                    CP_DIAGRAM_POWER, CP_PLANE_STRAIN, CP_PLANE_STRESS, CP_PREC_FP64, CP_PREC_MIXED)
+                    CP_DIAGRAM_POWER, CP_PLANE_STRAIN, CP_PLANE_STRESS, CP_PREC_FLOAT_BOOST, CP_PREC_FP64, CP_PREC_MIXED)
 
 FIELDS = ["exx", "eyy", "gamma", "eps_i", "sxx", "syy", "tau", "sig_i", "table_s", "psi", "E_c", "nu_c",
           "exx_p", "eyy_p", "gamma_p", "eps_p_i"]

@@ -24,7 +24,7 @@ CP_ERR_TIMEOUT = 11
 
 CP_PLANE_STRESS, CP_PLANE_STRAIN = 0, 1
 CP_DIAGRAM_ELASTIC, CP_DIAGRAM_LINEAR, CP_DIAGRAM_POWER, CP_DIAGRAM_HOLLOMON, CP_DIAGRAM_PIECEWISE = range(5)
-CP_PREC_FP64, CP_PREC_MIXED = 0, 1
+CP_PREC_FP64, CP_PREC_MIXED, CP_PREC_FLOAT_BOOST = 0, 1, 2
 CP_MAX_PW = 16
 
 c_int, c_double, c_ll, c_p = ctypes.c_int, ctypes.c_double, ctypes.c_longlong, ctypes.c_void_p

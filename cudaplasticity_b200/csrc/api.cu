@@ -426,7 +426,7 @@ CP_API int cp_instance_footprint(const cp_mesh_view* m, int precision, size_t* b
     b += nnz * 8;                                                              // K (FP64)
     b += n * (16 * 8 + 2);                                                     // u, b, b_full, u_full, r, z, z, q, mask
     b += ne * 18 * 8;                                                          // element state
-    if (precision == CP_PREC_MIXED) b += nnz * 4 + n * 8 * 4;
+    if (precision != CP_PREC_FP64) b += nnz * 4 + n * 8 * 4;
     b += 1 << 20;                                                              // scalars, partials, graphs
     *bytes = b;
     return CP_OK;
@@ -697,8 +697,12 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
     const cp_solve_opts o = *opts;
     if (!(o.cg_tol > 0) || !(o.outer_tol > 0) || o.max_outer <= 0 || o.levels <= 0 || o.max_cg <= 0)
         return CP_ERR_INVALID;
-    if (o.precision != CP_PREC_FP64 && o.precision != CP_PREC_MIXED) return CP_ERR_INVALID;
+    if (o.precision != CP_PREC_FP64 && o.precision != CP_PREC_MIXED && o.precision != CP_PREC_FLOAT_BOOST)
+        return CP_ERR_INVALID;
     if (o.precond != 0 && o.precond != 1) return CP_ERR_INVALID;
+    // floatBoost's first phase (solveCUDA_FD, src/PlasticitySolver.cu:660-679):
+    // CG 1e-4 and relErr 1e-4 in reduced precision
+    constexpr double kBoostTol = 1e-4;
     int rc = guarded(I->ctx, [&] {
         CP_CHECK(I->loads_set, CP_ERR_INVALID, "loads not set");
         cudaStream_t s = I->s();
@@ -715,12 +719,15 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
             I->launches += 2;
             double rel_err = 1.0, w_prev = 1.0;
             bool converged = false;
+            // floatBoost: the reduced-precision phase, then FP64 from its state
+            bool boost = o.precision == CP_PREC_FLOAT_BOOST;
+            int prec = boost ? CP_PREC_MIXED : o.precision;
             for (int it = 0; it < o.max_outer; ++it) {
                 // linear tolerance: tight once the secant iteration is close
-                double eps = o.cg_tol;
-                if (o.adaptive_cg && rel_err > 10.0 * o.outer_tol) eps = std::max(o.cg_tol, 1e-2 * rel_err);
-                assemble(I, o.precision);
-                if (o.precision == CP_PREC_FP64) {
+                double eps = boost ? std::max(o.cg_tol, kBoostTol) : o.cg_tol;
+                if (!boost && o.adaptive_cg && rel_err > 10.0 * o.outer_tol) eps = std::max(o.cg_tol, 1e-2 * rel_err);
+                assemble(I, prec);
+                if (prec == CP_PREC_FP64) {
                     cg_fp64(I, eps, o.max_cg, o.precond ? 1 : 0);
                     R.cg_iters += I->sc_h->iter;
                     R.cg_rel_res = std::sqrt(I->sc_h->rr * I->sc_h->normB_inv);
@@ -745,6 +752,22 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
                     cp::launch_aitken_relax(I->mesh, I->mat, I->st, I->osc, w, s, I->sms());
                     I->launches += 1;
                     w_prev = w;
+                }
+                if (boost) {
+                    if (rel_err <= kBoostTol) {
+                        // switch to FP64 (copyFloatToDouble keeps u, E_c, nu_c;
+                        // the Aitken history starts afresh); the FP64 phase
+                        // gets its own max_outer and takes at least one step
+                        boost = false;
+                        prec = CP_PREC_FP64;
+                        w_prev = 1.0;
+                        int g2;
+                        grid1d(2LL * I->n_elem, I->sms(), g2);
+                        k_zero_double<<<g2, 256, 0, s>>>(I->st.res_prev, 2LL * I->n_elem);
+                        I->launches += 1;
+                        it = -1;
+                    }
+                    continue;
                 }
                 if (rel_err <= o.outer_tol && eps <= o.cg_tol) {
                     converged = true;

@@ -369,7 +369,7 @@ double PlasticitySolver::run(bool elastic) {
     check(cp_instance_reset_state(inst_));
     cp_solve_opts o;
     cp_solve_opts_default(&o);
-    o.precision = floatBoost ? CP_PREC_MIXED : CP_PREC_FP64;
+    o.precision = floatBoost && !elastic ? CP_PREC_FLOAT_BOOST : CP_PREC_FP64;
     o.cg_tol = cgTol;
     o.outer_tol = outerTol;
     o.max_outer = elastic ? 1 : maxOuter;

@@ -57,7 +57,11 @@ enum {
     CP_DIAGRAM_HOLLOMON = 3,  /* sigma = sigma_y (1 + eps_p / eps0)^n (new) */
     CP_DIAGRAM_PIECEWISE = 4  /* elastic to (pw_eps[0], pw_sig[0]), then piecewise linear (new) */
 };
-enum { CP_PREC_FP64 = 0, CP_PREC_MIXED = 1 };
+/* CP_PREC_FLOAT_BOOST: the reference's floatBoost (solveCUDA_FD,
+ * src/PlasticitySolver.cu:631-708): each load level first iterates in mixed
+ * precision with loose tolerances (CG and relErr 1e-4), then goes on in FP64
+ * from that state to the caller's tolerances (at least one FP64 step). */
+enum { CP_PREC_FP64 = 0, CP_PREC_MIXED = 1, CP_PREC_FLOAT_BOOST = 2 };
 #define CP_MAX_PW 16
 
 /* Material and hardening diagram (class Material, src/Material.cuh:9-40). */
@@ -89,7 +93,8 @@ typedef struct {
 } cp_mesh_view;
 
 typedef struct {
-    int precision;       /* CP_PREC_FP64: FP64 throughout; CP_PREC_MIXED: FP32 matrix + inner CG, FP64 defect correction */
+    int precision;       /* CP_PREC_FP64: FP64 throughout; CP_PREC_MIXED: FP32 matrix + inner CG, FP64 defect correction;
+                            CP_PREC_FLOAT_BOOST: mixed to 1e-4, then FP64 (the reference's floatBoost) */
     double cg_tol;       /* linear solve: stop when ||r|| / ||b|| <= cg_tol (reference: 1e-7) */
     double outer_tol;    /* secant iteration: stop when relErr <= outer_tol (reference: 1e-5) */
     int max_outer;       /* per load level (reference CPU path: 50) */

@@ -20,7 +20,9 @@ public:
     // public flags of the reference (src/PlasticitySolver.cuh:207-211)
     bool polarCoord = false;
     bool iterOutput = true;
-    bool floatBoost = false;  // here: FP32 matrix + inner CG inside FP64 defect correction
+    // the reference's two phases (solveCUDA_FD, src/PlasticitySolver.cu:631-708): reduced precision to
+    // relErr 1e-4 (here FP32 matrix and inner CG inside FP64 defect correction), then FP64
+    bool floatBoost = false;
 
     // Extensions: the reference hard-codes CG 1e-7, outer 1e-5 and (CPU) 50 iterations.
     double cgTol = 1e-7;
@@ -29,7 +31,7 @@ public:
     int levels = 1;          // load increments, each a deformation-theory solve warm-started from the last
     bool aitken = false;     // Aitken-relaxed secant iteration (same fixed point)
     bool adaptiveCg = false; // loose linear solves while the secant iteration is far from converged
-    double innerTol = 1e-4;  // floatBoost: FP32 inner solves' relative tolerance
+    double innerTol = 1e-4;  // floatBoost's first phase: FP32 inner solves' relative tolerance
     int device = 0;
 
     PlasticitySolver(const Material& material, Mesh& mesh, const LoadConditions& loadConditions);

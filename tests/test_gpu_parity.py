@@ -162,6 +162,22 @@ def test_cluster_cg_matches_reference(name, ctx, golden_dir, workdir, monkeypatc
     assert r["report"]["status"] == 0
 
 
+@pytest.mark.parametrize("name", ["hole12_pow", "ogrid16_bilin"])
+def test_float_boost_reaches_the_fp64_fixed_point(name, ctx, golden_dir, workdir):
+    """The reference's floatBoost scheme (CP_PREC_FLOAT_BOOST; solveCUDA_FD,
+    src/PlasticitySolver.cu:631-708): each level iterates in reduced
+    precision to relErr 1e-4, then in FP64 from there; the result meets the
+    FP64 bar against the reference's fixture, and the reduced-precision phase
+    did run (its defect-correction steps are counted in fp64_spmv)."""
+    g = load_golden(golden_dir, name)
+    m, lines = scenario(name, workdir)
+    r = product_runner.run(ctx, lines, m, precision=cp.CP_PREC_FLOAT_BOOST, precond=1)
+    k, err, errs = worst(r, g)
+    assert err <= FP64_TOL, (k, err, errs)
+    assert np.array_equal(yielded(r), yielded(g))
+    assert r["report"]["status"] == 0 and r["report"]["fp64_spmv"] > 0
+
+
 def test_cg_phase_reference_semantics(ctx, golden_dir, workdir):
     """One elastic solve through the phase entry points: assemble, CG from the
     current u, secant update; against the oracle's first outer iteration."""
