@@ -522,14 +522,17 @@ def _close_servers():
 
 class Server:
     """Solve service (cp_server): requests are submitted as they arrive and
-    solved with continuous batching on one GPU; wait() hands back each
-    request's results."""
+    solved on one GPU, mixed-precision ones with continuous batching, FP64
+    ones concurrently on fp64_lanes lanes; wait() hands back each request's
+    results."""
 
-    def __init__(self, device=0, hbm_reserve=0.05, max_bytes=0, max_inflight=1024, trip_quantum=0, **batch):
+    def __init__(self, device=0, hbm_reserve=0.05, max_bytes=0, max_inflight=1024, trip_quantum=0, fp64_lanes=8,
+                 **batch):
         o = C.cp_server_opts()
         C.lib().cp_server_opts_default(ctypes.byref(o))
         o.device, o.hbm_reserve, o.max_bytes = device, hbm_reserve, int(max_bytes)
         o.max_inflight, o.trip_quantum = max_inflight, int(trip_quantum)
+        o.fp64_lanes = fp64_lanes
         for k, v in batch.items():
             setattr(o.batch, k, v)
         self._h = C.c_p()
@@ -553,6 +556,8 @@ class Server:
         self.close()
 
     def submit(self, mesh_arrays, mat, rp, mask, uv=None, **solve_kw):
+        """cp_solve options as keywords; precision defaults to CP_PREC_MIXED
+        (the batch), CP_PREC_FP64 / CP_PREC_FLOAT_BOOST go to the lanes."""
         v, keep = mesh_view(mesh_arrays)
         rp = np.ascontiguousarray(rp, np.float64)
         mask = np.ascontiguousarray(mask, np.uint8)
@@ -561,7 +566,7 @@ class Server:
             uv = np.ascontiguousarray(uv, np.float64)
             uvp = _dp(uv)
         kw = dict(solve_kw)
-        kw["precision"] = CP_PREC_MIXED
+        kw.setdefault("precision", CP_PREC_MIXED)
         o = solve_opts(**kw)
         rid = ctypes.c_longlong()
         st = C.lib().cp_server_submit(self._h, ctypes.byref(v), ctypes.byref(mat), _dp(rp), _up(mask), uvp,

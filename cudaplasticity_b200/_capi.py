@@ -68,7 +68,7 @@ CP_BATCH_RUN_ALL, CP_BATCH_RUN_ANY_DONE = 0, 1
 
 class cp_server_opts(ctypes.Structure):
     _fields_ = [("device", c_int), ("hbm_reserve", c_double), ("max_bytes", ctypes.c_size_t),
-                ("max_inflight", c_int), ("trip_quantum", c_ll), ("batch", cp_batch_opts)]
+                ("max_inflight", c_int), ("trip_quantum", c_ll), ("batch", cp_batch_opts), ("fp64_lanes", c_int)]
 
 
 class cp_server_stats(ctypes.Structure):

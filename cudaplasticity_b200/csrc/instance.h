@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -45,6 +46,7 @@ struct cp_instance {
     bool use_graph = true;  // CG loop as a CUDA graph with a device-side WHILE condition
     bool loads_set = false;
     bool in_batch = false;  // owned by a cp_batch until harvested: no other call may touch it
+    std::atomic<int> cancel{0};  // set from another thread: cp_solve stops at its next outer iteration
     // single-launch FP64 CG (cg_fused.cu), allocated on first use
     bool fused_fp64 = true;        // false (CUPLAST_FP64_CG=classic): the two-kernel loop of cg.cu
     bool persistent_fp64 = false;  // CUPLAST_FP64_CG=persistent: one cooperative launch per linear solve

@@ -13,6 +13,11 @@
 //      once some are ready make the graph stop at its next trip boundary so
 //      that they join.
 // Submitters and waiters only touch the queues under the mutex.
+//
+// FP64 (and floatBoost) requests take the same admission path but are solved
+// by cp_solve, one request per lane thread; each lane has its own context
+// (stream), so the lanes' solves and the batch run concurrently. A small
+// request's CG occupies one 16-SM cluster, so several of them share the GPU.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -61,8 +66,12 @@ struct cp_server {
     cp_context* ctx_run = nullptr;
     cp_context* ctx_setup = nullptr;
     cp_batch* batch = nullptr;
+    std::vector<cp_context*> lane_ctx;    // one per FP64 lane
+    std::vector<std::thread> lanes;
+    std::deque<ReqP> lane_q;              // admitted FP64 requests, not yet on a lane
+    std::vector<ReqP> lane_cur;           // the request each lane is solving (or null)
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_lane;
     std::deque<ReqP> pending;
     std::unordered_map<long long, ReqP> by_id;         // submitted, not yet taken
     std::unordered_map<cp_instance*, ReqP> inflight;   // in the batch or set up, waiting to join
@@ -87,11 +96,18 @@ void stop_thread(cp_server* s) {
     {
         std::lock_guard<std::mutex> lock(s->mu);
         s->stop = true;
+        for (auto& r : s->lane_cur)  // the lanes' solves stop at their next outer iteration
+            if (r && r->inst) r->inst->cancel.store(1);
     }
     cp_batch_interrupt(s->batch);
     s->cv_work.notify_all();
+    s->cv_lane.notify_all();
     if (s->th.joinable()) s->th.join();
+    for (auto& t : s->lanes)
+        if (t.joinable()) t.join();
 }
+
+bool is_lane_request(const cp_solve_opts& o) { return o.precision != CP_PREC_MIXED; }
 
 void stop_all_at_exit() {
     std::lock_guard<std::mutex> lock(g_live_mu);
@@ -105,8 +121,11 @@ void complete(cp_server* s, const ReqP& r) {
     s->st.completed += 1;
 }
 
-// Builds the instance of a request on the set-up stream.
-int setup(cp_server* s, const ReqP& r) {
+// Builds the instance of a request on stream ctx (the set-up stream for the
+// batch, the lane's own for an FP64 request) into *out; the caller publishes
+// it in the request under the mutex.
+int setup(cp_context* ctx, const ReqP& r, cp_instance** out) {
+    *out = nullptr;
     cp_mesh_view v{};
     v.node_count = r->nn;
     v.node_xy = r->xy.data();
@@ -117,10 +136,10 @@ int setup(cp_server* s, const ReqP& r) {
     v.count8 = r->c8;
     v.elem8 = r->c8 ? r->e8.data() : nullptr;
     cp_instance* I = nullptr;
-    int st = cp_instance_create(s->ctx_setup, &v, &r->mat, &I);
+    int st = cp_instance_create(ctx, &v, &r->mat, &I);
     if (st != CP_OK) return st;
     st = cp_instance_set_loads(I, r->rp.data(), r->mask.data(), r->has_uv ? r->uv.data() : nullptr);
-    if (st == CP_OK) {
+    if (st == CP_OK && !is_lane_request(r->opts)) {
         try {
             cp::instance_prepare_mixed(I, r->opts.precond);
             if (cudaStreamSynchronize(I->s()) != cudaSuccess) st = CP_ERR_CUDA;
@@ -132,8 +151,49 @@ int setup(cp_server* s, const ReqP& r) {
         cp_instance_destroy(I);
         return st;
     }
-    r->inst = I;
+    *out = I;
     return CP_OK;
+}
+
+// One FP64 lane: takes admitted requests in order and solves each with
+// cp_solve on its own stream.
+void lane(cp_server* s, int k) {
+    cudaSetDevice(s->o.device);
+    for (;;) {
+        ReqP r;
+        {
+            std::unique_lock<std::mutex> lock(s->mu);
+            s->cv_lane.wait(lock, [&] { return s->stop || !s->lane_q.empty(); });
+            if (s->stop) return;
+            r = s->lane_q.front();
+            s->lane_q.pop_front();
+            s->lane_cur[k] = r;
+        }
+        cp_instance* inst = nullptr;
+        int rc = setup(s->lane_ctx[k], r, &inst);
+        cp_solve_report rep{};
+        if (rc == CP_OK) {
+            {
+                std::lock_guard<std::mutex> lock(s->mu);
+                r->inst = inst;
+                if (s->stop) inst->cancel.store(1);
+            }
+            const int st = cp_solve(inst, &r->opts, &rep);
+            if (st != CP_OK && rep.status == CP_OK) rep.status = st;
+        }
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->lane_cur[k] = nullptr;
+        s->inflight_bytes -= r->footprint;
+        if (rc != CP_OK) {
+            r->status = rc;
+        } else {
+            r->rep = rep;
+            if (rep.status == CP_ERR_CANCELLED) r->status = CP_ERR_CANCELLED;
+        }
+        complete(s, r);
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();  // memory and a slot are free again
+    }
 }
 
 void scheduler(cp_server* s) {
@@ -221,8 +281,10 @@ void scheduler(cp_server* s) {
                 size_t free_b = 0, total_b = 0;
                 cudaMemGetInfo(&free_b, &total_b);
                 size_t planned = 0;
-                while (!s->pending.empty() &&
-                       (int)(s->inflight.size() + take.size()) < s->o.max_inflight) {
+                int lane_busy = 0;
+                for (auto& r : s->lane_cur) lane_busy += r ? 1 : 0;
+                while (!s->pending.empty() && (int)(s->inflight.size() + s->lane_q.size() + lane_busy + take.size()) <
+                                                  s->o.max_inflight) {
                     const ReqP& r = s->pending.front();
                     if (free_b < reserve || r->footprint + planned > free_b - reserve) break;  // head of line waits
                     if (s->o.max_bytes && s->inflight_bytes + planned + r->footprint > s->o.max_bytes) break;
@@ -237,8 +299,16 @@ void scheduler(cp_server* s) {
                 if (s->inflight_bytes > s->st.peak_bytes) s->st.peak_bytes = s->inflight_bytes;
             }
             for (auto& r : take) {
-                const int rc = setup(s, r);
+                if (is_lane_request(r->opts)) {
+                    std::lock_guard<std::mutex> lock(s->mu);
+                    s->lane_q.push_back(r);
+                    s->cv_lane.notify_one();
+                    continue;
+                }
+                cp_instance* inst = nullptr;
+                const int rc = setup(s->ctx_setup, r, &inst);
                 std::lock_guard<std::mutex> lock(s->mu);
+                r->inst = inst;
                 if (rc == CP_OK) {
                     s->inflight[r->inst] = r;
                     ready.push_back(r);
@@ -270,6 +340,13 @@ void scheduler(cp_server* s) {
                     running = false;
                 }
                 for (auto& r : ready) r->status = CP_ERR_CANCELLED;
+                for (auto& r : s->lane_q) {
+                    s->inflight_bytes -= r->footprint;
+                    r->status = CP_ERR_CANCELLED;
+                    complete(s, r);
+                }
+                s->lane_q.clear();
+                s->cv_done.notify_all();
                 break;
             }
         }
@@ -288,6 +365,7 @@ CP_API void cp_server_opts_default(cp_server_opts* o) {
     o->max_inflight = 1024;
     o->trip_quantum = 0;
     cp_batch_opts_default(&o->batch);
+    o->fp64_lanes = 8;
 }
 
 CP_API int cp_server_create(const cp_server_opts* opts, cp_server** out) {
@@ -296,7 +374,9 @@ CP_API int cp_server_create(const cp_server_opts* opts, cp_server** out) {
     cp_server_opts o;
     cp_server_opts_default(&o);
     if (opts) o = *opts;
-    if (o.max_inflight <= 0 || !(o.hbm_reserve >= 0.0 && o.hbm_reserve < 1.0)) return CP_ERR_INVALID;
+    if (o.max_inflight <= 0 || !(o.hbm_reserve >= 0.0 && o.hbm_reserve < 1.0) || o.fp64_lanes < 0 ||
+        o.fp64_lanes > 64)
+        return CP_ERR_INVALID;
     if (o.max_inflight > o.batch.max_instances) o.max_inflight = o.batch.max_instances;
     cp_server* s = new (std::nothrow) cp_server();
     if (!s) return CP_ERR_NOMEM;
@@ -304,12 +384,19 @@ CP_API int cp_server_create(const cp_server_opts* opts, cp_server** out) {
     int rc = cp_context_create(o.device, &s->ctx_run);
     if (rc == CP_OK) rc = cp_context_create(o.device, &s->ctx_setup);
     if (rc == CP_OK) rc = cp_batch_create(s->ctx_run, &o.batch, &s->batch);
+    for (int k = 0; rc == CP_OK && k < o.fp64_lanes; ++k) {
+        cp_context* c = nullptr;
+        rc = cp_context_create(o.device, &c);
+        if (rc == CP_OK) s->lane_ctx.push_back(c);
+    }
+    s->lane_cur.assign(s->lane_ctx.size(), nullptr);
     if (rc == CP_OK) {
         size_t f = 0, t = 0;
         if (cudaMemGetInfo(&f, &t) != cudaSuccess) rc = CP_ERR_CUDA;
         s->total_mem = t;
     }
     if (rc != CP_OK) {
+        for (cp_context* c : s->lane_ctx) cp_context_destroy(c);
         if (s->batch) cp_batch_destroy(s->batch);
         if (s->ctx_setup) cp_context_destroy(s->ctx_setup);
         if (s->ctx_run) cp_context_destroy(s->ctx_run);
@@ -320,8 +407,19 @@ CP_API int cp_server_create(const cp_server_opts* opts, cp_server** out) {
         std::lock_guard<std::mutex> lock(g_live_mu);
         if (!g_atexit_registered) g_atexit_registered = std::atexit(stop_all_at_exit) == 0;
         s->th = std::thread(scheduler, s);
+        for (int k = 0; k < (int)s->lane_ctx.size(); ++k) s->lanes.emplace_back(lane, s, k);
         g_live.push_back(s);
     } catch (...) {
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            s->stop = true;
+        }
+        s->cv_work.notify_all();
+        s->cv_lane.notify_all();
+        if (s->th.joinable()) s->th.join();
+        for (auto& t : s->lanes)
+            if (t.joinable()) t.join();
+        for (cp_context* c : s->lane_ctx) cp_context_destroy(c);
         cp_batch_destroy(s->batch);
         cp_context_destroy(s->ctx_setup);
         cp_context_destroy(s->ctx_run);
@@ -351,6 +449,7 @@ CP_API int cp_server_destroy(cp_server* s) {
         }
     }
     s->cv_done.notify_all();
+    for (cp_context* c : s->lane_ctx) cp_context_destroy(c);
     cp_context_destroy(s->ctx_setup);
     cp_context_destroy(s->ctx_run);
     delete s;
@@ -360,7 +459,9 @@ CP_API int cp_server_destroy(cp_server* s) {
 CP_API int cp_server_submit(cp_server* s, const cp_mesh_view* mv, const cp_material* mat, const double* rp,
                             const unsigned char* mask, const double* uv, const cp_solve_opts* opts, long long* id) {
     if (!s || !mv || !mat || !rp || !mask || !opts || !id) return CP_ERR_INVALID;
-    if (opts->precision != CP_PREC_MIXED) return CP_ERR_UNSUPPORTED;
+    if (opts->precision != CP_PREC_MIXED && opts->precision != CP_PREC_FP64 && opts->precision != CP_PREC_FLOAT_BOOST)
+        return CP_ERR_INVALID;
+    if (is_lane_request(*opts) && s->o.fp64_lanes == 0) return CP_ERR_UNSUPPORTED;
     if (mv->node_count <= 0 || !mv->node_xy || mv->count3 < 0 || mv->count4 < 0 || mv->count8 < 0 ||
         (long long)mv->count3 + mv->count4 + mv->count8 <= 0 || (mv->count3 && !mv->elem3) ||
         (mv->count4 && !mv->elem4) || (mv->count8 && !mv->elem8))
@@ -387,7 +488,7 @@ CP_API int cp_server_submit(cp_server* s, const cp_mesh_view* mv, const cp_mater
     }
     r->mat = *mat;
     r->opts = *opts;
-    int rc = cp_instance_footprint(mv, CP_PREC_MIXED, &r->footprint);
+    int rc = cp_instance_footprint(mv, opts->precision, &r->footprint);
     if (rc != CP_OK) return rc;
     const size_t reserve = (size_t)(s->o.hbm_reserve * (double)s->total_mem);
     std::lock_guard<std::mutex> lock(s->mu);

@@ -299,6 +299,9 @@ typedef struct {
     int max_inflight;        /* requests on the device at once (<= batch slots) */
     long long trip_quantum;  /* graph trips per run before the scheduler looks again (<= 0: until one finishes) */
     cp_batch_opts batch;
+    int fp64_lanes;          /* CP_PREC_FP64 / CP_PREC_FLOAT_BOOST requests: each is solved by cp_solve on one of
+                                this many lane threads, each with its own stream, concurrently with the other
+                                lanes and the batch (0: such requests are refused) */
 } cp_server_opts;
 
 typedef struct {
@@ -314,9 +317,10 @@ CP_API int cp_server_create(const cp_server_opts* opts, cp_server** out);
 /* Stops the scheduler; requests not yet completed are cancelled
  * (CP_ERR_CANCELLED to their waiters); instances not yet taken are freed. */
 CP_API int cp_server_destroy(cp_server* s);
-/* Copies the request and returns at once; *id identifies it. opts->precision
- * must be CP_PREC_MIXED. A request larger than the whole admission limit is
- * rejected here with CP_ERR_NOMEM. */
+/* Copies the request and returns at once; *id identifies it. CP_PREC_MIXED
+ * requests join the batch; CP_PREC_FP64 and CP_PREC_FLOAT_BOOST ones go to the
+ * FP64 lanes (CP_ERR_UNSUPPORTED when there are none). A request larger than
+ * the whole admission limit is rejected here with CP_ERR_NOMEM. */
 CP_API int cp_server_submit(cp_server* s, const cp_mesh_view* mesh, const cp_material* mat, const double* rp,
                             const unsigned char* mask, const double* uv, const cp_solve_opts* opts, long long* id);
 /* Waits (timeout_s < 0: without limit) until request id completes; returns

@@ -3,7 +3,8 @@
 Requests arrive from a separate thread at random times while others are on
 the device (continuous batching); each result must be bit-identical to the
 same request solved alone, admission must respect the byte budget, and a
-request larger than the budget is rejected at submission."""
+request larger than the budget is rejected at submission. FP64 requests run
+on the service's lanes (cp_solve, several at once) and equal cp_solve alone."""
 import random
 import threading
 import time
@@ -111,6 +112,63 @@ def test_destroy_with_requests_in_flight_returns():
     srv = cp.Server(max_inflight=2)
     for w in ws:
         srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"], **KW)
+    t0 = time.time()
+    srv.close()
+    assert time.time() - t0 < 60.0
+
+
+FP64_KW = dict(cg_tol=1e-10, outer_tol=1e-7, max_outer=120, max_cg=2_000_000, precond=1, aitken=1, adaptive_cg=1)
+
+
+def alone_fp64(ctx, w):
+    inst = cp.Instance(ctx, w["mesh"], w["material"])
+    inst.set_loads(w["rp"], w["mask"], w["uv"])
+    rep = inst.solve(allow_not_converged=True, levels=w["levels"], **FP64_KW)
+    st = inst.state()
+    inst.close()
+    return st, rep
+
+
+def test_fp64_lanes_equal_cp_solve_alone_next_to_the_batch():
+    """FP64 requests are solved by cp_solve on the server's lanes, several at
+    once on their own streams, while mixed requests join the batch: every
+    FP64 result is bit-identical to the same request solved alone with
+    cp_solve, and every mixed one has the status it has alone."""
+    ws = [workload.instance(i, increments=(1, 3), **GEN) for i in range(60, 68)]
+    ctx = cp.Context(0)
+    kinds = ["fp64" if k % 4 != 3 else "mixed" for k in range(len(ws))]
+    ref = [alone_fp64(ctx, w) if kind == "fp64" else alone(ctx, w) for w, kind in zip(ws, kinds)]
+    srv = cp.Server(fp64_lanes=4)
+    try:
+        ids = []
+        for w, kind in zip(ws, kinds):
+            kw = dict(FP64_KW, precision=cp.CP_PREC_FP64) if kind == "fp64" else KW
+            ids.append(srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"], **kw))
+        for k, rid in enumerate(ids):
+            inst, rep, latency = srv.wait(rid, timeout=600.0)
+            assert rep["status"] == ref[k][1]["status"], (k, rep, ref[k][1])
+            if kinds[k] == "fp64":
+                st = inst.state()
+                for f in cp.FIELDS + ["uv"]:
+                    assert np.array_equal(st[f], ref[k][0][f]), (k, f)
+                assert rep["cg_iters"] == ref[k][1]["cg_iters"] and rep["outer_iters"] == ref[k][1]["outer_iters"]
+            assert latency > 0
+            inst.close()
+        assert srv.stats()["completed"] == len(ws)
+    finally:
+        srv.close()
+        ctx.close()
+
+
+def test_destroy_with_fp64_solves_in_flight_returns():
+    """Closing the server cancels the lanes' solves at their next outer
+    iteration and the requests still queued."""
+    ws = [workload.instance(i, **GEN) for i in range(70, 76)]
+    srv = cp.Server(fp64_lanes=2)
+    for w in ws:
+        srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"],
+                   precision=cp.CP_PREC_FP64, **FP64_KW)
+    time.sleep(0.5)
     t0 = time.time()
     srv.close()
     assert time.time() - t0 < 60.0

@@ -181,9 +181,13 @@ def test_batch_and_server_entry_points_validate_arguments_without_a_device():
     so = _capi.cp_server_opts()
     L.cp_server_opts_default(ctypes.byref(so))
     assert so.max_inflight == 1024 and 0.0 < so.hbm_reserve < 1.0 and so.batch.max_instances == 1024
+    assert so.fp64_lanes == 8
     srv = _capi.c_p()
     assert L.cp_server_create(ctypes.byref(so), ctypes.byref(srv)) == _capi.CP_ERR_NO_DEVICE
     assert not srv.value
+    so.fp64_lanes = -1
+    assert L.cp_server_create(ctypes.byref(so), ctypes.byref(srv)) == inv
+    so.fp64_lanes = 8
     so.max_inflight = 0
     assert L.cp_server_create(ctypes.byref(so), ctypes.byref(srv)) == inv
     rid = ctypes.c_longlong()
