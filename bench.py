@@ -194,6 +194,9 @@ def flush_l2(ctx_dev):
 
 BATCH_KW = dict(cg_tol=1e-10, outer_tol=1e-6, max_outer=2000, max_cg=5_000_000, precond=1, aitken=1, adaptive_cg=1,
                 inner_tol=1e-3)
+# the FP64 lanes of the solve service: the same tolerances in FP64
+FP64_SERVE_KW = dict(cg_tol=1e-10, outer_tol=1e-6, max_outer=2000, max_cg=5_000_000, precond=1, aitken=1,
+                     adaptive_cg=1)
 
 
 def batched_leg(ctx, window_s=20.0, warm_s=3.0, slots=512, pool_size=768, seed=20261203):
@@ -272,10 +275,11 @@ def batched_leg(ctx, window_s=20.0, warm_s=3.0, slots=512, pool_size=768, seed=2
     }
 
 
-def compare_leg(ctx, n_requests, max_outer=100, seed=20261203):
+def compare_leg(ctx, n_requests, max_outer=100, seed=20261203, lanes=8):
     """Like for like: the plain FP64 drop-in solves the first n requests of
     the batch stream (DOF 2k-200k) one at a time; the batched mixed-precision engine
-    then solves exactly the same requests (fresh instances) to completion.
+    then solves exactly the same requests (fresh instances) to completion, and
+    so does the solve service's FP64 lanes.
     Same solver options and caps for both, wall clock for both, and the error
     of each mixed-precision result against its FP64 result. Requests that hit
     the outer cap count as solved by both (same cap) and are listed."""
@@ -346,12 +350,33 @@ def compare_leg(ctx, n_requests, max_outer=100, seed=20261203):
         "speedup_vs_plain": t_plain / t_batch,
         "max_rel_err_mixed_vs_fp64": errs,
     }
+    # the same requests through the solve service's FP64 lanes (cp_solve,
+    # several at once): FP64 results, which must equal the plain ones
+    srv = cp.Server(fp64_lanes=lanes)
+    ws = {i: workload.instance(i, seed=seed) for i in ids}
+    t1 = time.perf_counter()
+    rids = {i: srv.submit(ws[i]["mesh"], ws[i]["material"], ws[i]["rp"], ws[i]["mask"], ws[i]["uv"], levels=1,
+                          precision=cp.CP_PREC_FP64, **{k: v for k, v in kw.items() if k != "inner_tol"})
+            for i in ids}
+    same, lane_status = True, set()
+    for i in ids:
+        inst, rep, _ = srv.wait(rids[i], timeout=-1.0)
+        lane_status.add(rep["status"])
+        st = inst.state()
+        same = same and all(np.array_equal(st[f], plain[i][0][f]) for f in ("uv", "sig_i", "eps_p_i"))
+        inst.close()
+    t_lanes = time.perf_counter() - t1
+    srv.close()
+    fixed["fp64_lanes"] = {"lanes": lanes, "seconds": t_lanes, "solves_per_s": len(ids) / t_lanes,
+                           "statuses": sorted(lane_status), "identical_to_plain": bool(same),
+                           "speedup_vs_plain": t_plain / t_lanes}
     return fixed
 
 
-def served_leg(rate_hz=10.0, submit_s=20.0, drain_s=25.0, seed=20270101):
+def served_leg(rate_hz=10.0, submit_s=20.0, drain_s=25.0, seed=20270101, precision="mixed"):
     """The solve service under Poisson arrivals of served-stream requests
-    (DOF 2k-500k, 5-30 load increments)."""
+    (DOF 2k-500k, 5-30 load increments); precision "mixed" sends them to the
+    batch, "fp64" to the FP64 lanes (cp_solve, several at once)."""
     import random
 
     import numpy as np
@@ -361,6 +386,7 @@ def served_leg(rate_hz=10.0, submit_s=20.0, drain_s=25.0, seed=20270101):
 
     rng = random.Random(seed)
     srv = cp.Server()
+    kw = dict(BATCH_KW) if precision == "mixed" else dict(FP64_SERVE_KW, precision=cp.CP_PREC_FP64)
     ids, t_sub, h2d = [], [], 0
     t0 = time.perf_counter()
     k = 0
@@ -370,7 +396,7 @@ def served_leg(rate_hz=10.0, submit_s=20.0, drain_s=25.0, seed=20270101):
         now = time.perf_counter() - t0
         if next_t > now:
             time.sleep(next_t - now)
-        ids.append(srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"], **BATCH_KW))
+        ids.append(srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"], **kw))
         t_sub.append(time.perf_counter() - t0)
         h2d += sum(w["mesh"][a].nbytes for a in ("node_xy", "elem4")) + w["rp"].nbytes + w["mask"].nbytes + w["uv"].nbytes
         k += 1
@@ -401,7 +427,7 @@ def served_leg(rate_hz=10.0, submit_s=20.0, drain_s=25.0, seed=20270101):
     n = len(lat)
     return {
         "workload": "served stream: Poisson arrivals, DOF log-uniform [2k, 500k], 5-30 load increments, "
-                    "mixed precision, CG 1e-10, outer 1e-6",
+                    f"{'mixed precision (batch)' if precision == 'mixed' else 'FP64 (lanes)'}, CG 1e-10, outer 1e-6",
         "rate_hz": rate_hz, "submitted": len(ids), "completed": n,
         "solves_per_s": n / last_done if last_done > 0 else 0.0,
         "p50_s": float(np.percentile(lat, 50)) if n else None,
@@ -542,7 +568,8 @@ def run_product_arm(args):
         batched = batched_leg(ctx, window_s=args.batched_window)
         roof_batched = cg_kernel_roofline(ctx)
     if rank == 0 and not args.skip_served:
-        served = served_leg(rate_hz=args.serve_rate, submit_s=args.serve_window, drain_s=args.serve_window + 5)
+        served = served_leg(rate_hz=args.serve_rate, submit_s=args.serve_window, drain_s=args.serve_window + 5,
+                            precision=args.serve_precision)
 
     launches = sum(r["kernel_launches"] for r in reps)
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -663,6 +690,8 @@ def main():
                     help="like-for-like run only: the first N batch-stream requests, plain FP64 one at a time vs batched")
     ap.add_argument("--compare-max-outer", type=int, default=100)
     ap.add_argument("--serve-rate", type=float, default=10.0, help="Poisson arrival rate of the served leg")
+    ap.add_argument("--serve-precision", default="mixed", choices=["mixed", "fp64"],
+                    help="served leg: mixed-precision batch or FP64 lanes")
     ap.add_argument("--serve-window", type=float, default=20.0, help="seconds of arrivals in the served leg")
     ap.add_argument("--batched-probe", type=int, nargs=2, metavar=("N", "TRIPS"),
                     help="profiling aid: N resident batch-stream instances, TRIPS graph trips, then exit")
