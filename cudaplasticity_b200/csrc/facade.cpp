@@ -402,6 +402,80 @@ std::vector<double> PlasticitySolver::field(const std::string& name) const {
 double PlasticitySolver::getSxx0() const { return field("sxx")[0]; }
 double PlasticitySolver::getExx0() const { return field("exx")[0]; }
 
+namespace {
+
+// Centre of 4-node element e: the mean of its corners, as the reference's
+// polar transforms and error norms take it (src/PlasticitySolver.cuh:169-200).
+vec2 centre4(const Mesh& m, int e) {
+    vec2 ec;
+    for (int i = e * 4; i < (e + 1) * 4; ++i) ec += m.node[m.elem4[i]];
+    ec /= 4;
+    return ec;
+}
+
+// A symmetric tensor (xx, yy, xy) in polar components about the origin at
+// point ec: _rr, _phiphi, _rphi of src/PlasticitySolver.cuh:169-200.
+struct Polar {
+    double rr, pp, rp;
+};
+Polar to_polar(vec2 ec, double x, double y, double xy) {
+    const double r = ec.norm();
+    const double c = ec.x / r, s = ec.y / r;
+    return {c * c * x + s * s * y + 2. * c * s * xy, s * s * x + c * c * y - 2. * c * s * xy,
+            c * s * (-x + y) + xy * (c * c - s * s)};
+}
+
+}  // namespace
+
+double PlasticitySolver::sigmaError(std::function<double(vec2)> s_x, std::function<double(vec2)> s_y,
+                                    std::function<double(vec2)> s_xy) const {
+    const std::vector<double> sxx = field("sxx"), syy = field("syy"), tau = field("tau");
+    double avrSxx = 0., avrSyy = 0., avrSxy = 0., vol = 0., maxSxx = 0., maxSyy = 0., maxSxy = 0.;
+    for (int e = 0; e < mesh_.count4; ++e) {
+        const int i = mesh_.count3 + e;
+        const double loc = mesh_.elemSpace4(e);
+        avrSxx += sxx[i] * loc;
+        avrSyy += syy[i] * loc;
+        avrSxy += tau[i] * loc;
+        vol += loc;
+        const vec2 ec = centre4(mesh_, e);
+        maxSxx = std::fmax(maxSxx, std::fabs(s_x(ec) - sxx[i]));
+        maxSyy = std::fmax(maxSyy, std::fabs(s_y(ec) - syy[i]));
+        maxSxy = std::fmax(maxSxy, std::fabs(s_xy(ec) - tau[i]));
+    }
+    maxSxx *= vol / avrSxx;
+    maxSyy *= vol / avrSyy;
+    maxSxy *= vol / avrSxy;
+    return std::fmax(std::fmax(maxSxx, maxSyy), maxSxy);
+}
+
+double PlasticitySolver::polarSigmaError(std::function<double(vec2)> s_r, std::function<double(vec2)> s_phi,
+                                         std::function<double(vec2)> s_rphi, double maxR) const {
+    const std::vector<double> sxx = field("sxx"), syy = field("syy"), tau = field("tau");
+    const double pi = 3.141592653589793;
+    double avrSrr = 0., avrSpp = 0., avrSrp = 0., vol = 0., maxSrr = 0., maxSpp = 0., maxSrp = 0.;
+    for (int e = 0; e < mesh_.count4; ++e) {
+        const int i = mesh_.count3 + e;
+        const vec2 ec = centre4(mesh_, e);
+        const vec2 r(std::sqrt(ec.x * ec.x + ec.y * ec.y), std::atan(ec.y / ec.x) + (ec.x < 0. ? pi : 0.));
+        if (r.x > maxR) continue;
+        const Polar p = to_polar(ec, sxx[i], syy[i], tau[i]);
+        const double loc = mesh_.elemSpace4(e);
+        avrSrr += std::fabs(p.rr) * loc;
+        avrSpp += std::fabs(p.pp) * loc;
+        avrSrp += std::fabs(p.rp) * loc;
+        vol += loc;
+        maxSrr = std::fmax(maxSrr, std::fabs(s_r(r) - p.rr));
+        maxSpp = std::fmax(maxSpp, std::fabs(s_phi(r) - p.pp));
+        maxSrp = std::fmax(maxSrp, std::fabs(s_rphi(r) - p.rp));
+    }
+    maxSrr *= vol / avrSrr;
+    maxSpp *= vol / avrSpp;
+    maxSrp *= vol / avrSrp;
+    if (iterOutput) std::cout << maxSrr << " " << maxSpp << " " << maxSrp << "\n";
+    return std::fmax(std::fmax(maxSrr, maxSpp), maxSrp);
+}
+
 // deformEnergy (src/PlasticitySolver.cuh:415-445): elements on the plastic
 // branch integrate the diagram, except 8-node ones, for which the reference
 // always takes the secant energy eps_i sig_i / 2.
@@ -456,26 +530,49 @@ void PlasticitySolver::saveAsVtk(const std::string& fileName) {
     f << "\nCELL_DATA " << ne << "\nSCALARS ElementID int 1\nLOOKUP_TABLE default\n";
     for (int i = 0; i < ne; ++i) f << i << "\n";
     f.precision(16);
-    std::vector<std::pair<const char*, const char*>> fields = {
-        {"Eps_xx", "exx"}, {"Eps_yy", "eyy"}, {"Gamma_xy", "gamma"}, {"Eps_intensity", "eps_i"}};
+    // (name, values): Cartesian components of every element, or with
+    // polarCoord the polar components of the 4-node elements about the
+    // origin. As in the reference (src/PlasticitySolver.cu:1820-1925) the
+    // polar strains are taken from the tensor shear gamma / 2 and written
+    // under the Gamma_ names.
+    std::vector<std::pair<std::string, std::vector<double>>> fields;
+    auto group = [&](const char* nx, const char* ny, const char* nxy, const char* fx, const char* fy,
+                     const char* fxy, double shear) {
+        const std::vector<double> x = field(fx), y = field(fy), xy = field(fxy);
+        if (!polarCoord) {
+            fields.emplace_back(nx, x);
+            fields.emplace_back(ny, y);
+            fields.emplace_back(nxy, xy);
+            return;
+        }
+        std::vector<double> rr(mesh_.count4), pp(mesh_.count4), rp(mesh_.count4);
+        for (int e = 0; e < mesh_.count4; ++e) {
+            const int i = mesh_.count3 + e;
+            const Polar p = to_polar(centre4(mesh_, e), x[i], y[i], xy[i] * shear);
+            rr[e] = p.rr;
+            pp[e] = p.pp;
+            rp[e] = p.rp;
+        }
+        std::string base(nxy);
+        fields.emplace_back(std::string(nx).substr(0, std::string(nx).size() - 2) + "rr", rr);
+        fields.emplace_back(std::string(ny).substr(0, std::string(ny).size() - 2) + "phiphi", pp);
+        fields.emplace_back(base.substr(0, base.size() - 2) + "rphi", rp);
+    };
+    group("Eps_xx", "Eps_yy", "Gamma_xy", "exx", "eyy", "gamma", 0.5);
+    fields.emplace_back("Eps_intensity", field("eps_i"));
     if (plastSolved_) {
-        for (auto p : std::vector<std::pair<const char*, const char*>>{{"Eps_p_xx", "exx_p"},
-                                                                        {"Eps_p_yy", "eyy_p"},
-                                                                        {"Gamma_p_xy", "gamma_p"},
-                                                                        {"Eps_p_intensity", "eps_p_i"},
-                                                                        {"Psi", "psi"},
-                                                                        {"E_c", "E_c"},
-                                                                        {"nu_c", "nu_c"}})
-            fields.push_back(p);
+        group("Eps_p_xx", "Eps_p_yy", "Gamma_p_xy", "exx_p", "eyy_p", "gamma_p", 0.5);
+        fields.emplace_back("Eps_p_intensity", field("eps_p_i"));
+        fields.emplace_back("Psi", field("psi"));
+        fields.emplace_back("E_c", field("E_c"));
+        fields.emplace_back("nu_c", field("nu_c"));
     }
-    for (auto p : std::vector<std::pair<const char*, const char*>>{
-             {"Sigma_xx", "sxx"}, {"Sigma_yy", "syy"}, {"Tau_xy", "tau"}, {"Sigma_intensity", "sig_i"}})
-        fields.push_back(p);
+    group("Sigma_xx", "Sigma_yy", "Tau_xy", "sxx", "syy", "tau", 1.0);
+    fields.emplace_back("Sigma_intensity", field("sig_i"));
     f << "FIELD FieldData " << fields.size();
     for (auto& p : fields) {
-        std::vector<double> v = field(p.second);
-        f << "\n" << p.first << " 1 " << ne << " float\n";
-        for (double x : v) f << x << " ";
+        f << "\n" << p.first << " 1 " << p.second.size() << " float\n";
+        for (double x : p.second) f << x << " ";
     }
     std::vector<double> uv = field("uv");
     f << "\nPOINT_DATA " << mesh_.nodeCount << "\nSCALARS NodeID int 1\nLOOKUP_TABLE my_table";

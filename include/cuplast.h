@@ -6,8 +6,8 @@
  *
  * The reference exposes this path only through C++ classes (no C ABI). Each
  * entry point below names the reference code it replaces; the C++ drop-in
- * classes with the reference's names (include/cuplast/*.hpp) are written on
- * top of these functions.
+ * classes with the reference's names (the headers in include/cuplast/) are
+ * written on top of these functions.
  *
  * Conventions: every function returns a cp_status (0 = CP_OK); on error the
  * context keeps a message (cp_context_last_error). All array arguments are

@@ -51,6 +51,17 @@ public:
     double getSxx0() const;
     double getExx0() const;
 
+    // Largest element-centre deviation from analytic stresses, each component
+    // scaled by the mean of that component over the area (4-node elements;
+    // src/PlasticitySolver.cuh:464-494).
+    double sigmaError(std::function<double(vec2)> s_x, std::function<double(vec2)> s_y,
+                      std::function<double(vec2)> s_xy) const;
+    // The same in polar components about the origin, for element centres
+    // within maxR; the analytic functions take (r, phi) as a vec2 (the Kirsch
+    // problem; src/PlasticitySolver.cuh:496-540).
+    double polarSigmaError(std::function<double(vec2)> s_r, std::function<double(vec2)> s_phi,
+                           std::function<double(vec2)> s_rphi, double maxR) const;
+
     // Host copy of a field ("uv", "exx", ... as in cp_get_field).
     std::vector<double> field(const std::string& name) const;
     const cp_solve_report& lastReport() const { return report_; }

@@ -9,7 +9,9 @@
 //   scenario_drivers solverTest <out.vtk>
 //   scenario_drivers plasticityTest <out.vtk>
 //   scenario_drivers energyConvTest <order> <power|linear|elastic>   (prints the energy)
+//   scenario_drivers kirschTest <segments> <out.vtk>                  (prints the error norms)
 //   scenario_drivers noDevice                                         (expects a clean error)
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <iostream>
@@ -92,6 +94,47 @@ int energyConvTest(int order, const std::string& kind) {
     return 0;
 }
 
+// kirschConvTest, src/Main.cpp:178-227, one mesh of its sequence: the
+// elastic plate with a hole against Kirsch's analytic stresses, through
+// polarSigmaError (and sigmaError with zero reference stresses, which gives
+// the scaled largest stress of each component). The linear solve is tightened
+// (cgTol, an extension member) so that the norms are those of the exact
+// discrete solution. Writes the polar-coordinate VTK.
+int kirschTest(int segments, const char* out) {
+    Material m;
+    m.E = E_304L;
+    m.nu = nu_304L;
+    m.h = 1.;
+    const double a = 0.5, S = 1e6;
+    LoadConditions lc;
+    lc.setForce(1, vec2(S, 0));
+    lc.setForce(3, vec2(-S, 0));
+    lc.fixVertAxis(0.);
+    lc.fixHorAxis(0.);
+    auto s_r = [&](vec2 r) {
+        return 0.5 * S * (1. - a * a / (r.x * r.x)) +
+               0.5 * S * (1. + 3. * std::pow(a, 4.) / std::pow(r.x, 4.) - 4. * a * a / (r.x * r.x)) * std::cos(2. * r.y);
+    };
+    auto s_phi = [&](vec2 r) {
+        return 0.5 * S * (1. + a * a / (r.x * r.x)) - 0.5 * S * (1. + 3. * std::pow(a, 4.) / std::pow(r.x, 4.)) * std::cos(2. * r.y);
+    };
+    auto tau = [&](vec2 r) {
+        return -0.5 * S * (1. - 3. * std::pow(a, 4.) / std::pow(r.x, 4.) + 2. * a * a / (r.x * r.x)) * std::sin(2. * r.y);
+    };
+    Mesh mesh;
+    mesh.genRectWithHole(-3., 3., -2., 2., a, segments, segments);
+    PlasticitySolver ps(m, mesh, lc);
+    ps.iterOutput = false;
+    ps.cgTol = 1e-13;
+    ps.solveElast();
+    auto zero = [](vec2) { return 0.0; };
+    std::printf("polar %.17g cartesian_zero %.17g\n", ps.polarSigmaError(s_r, s_phi, tau, 2.),
+                ps.sigmaError(zero, zero, zero));
+    ps.polarCoord = true;
+    ps.saveAsVtk(out);
+    return 0;
+}
+
 // Without a device the drop-in classes report the library's status as a
 // std::runtime_error (the reference has no error reporting at all).
 int noDevice() {
@@ -122,12 +165,13 @@ int main(int argc, char** argv) {
         if (what == "solverTest" && argc > 2) return solverTest(argv[2]);
         if (what == "plasticityTest" && argc > 2) return plasticityTest(argv[2]);
         if (what == "energyConvTest" && argc > 3) return energyConvTest(std::atoi(argv[2]), argv[3]);
+        if (what == "kirschTest" && argc > 3) return kirschTest(std::atoi(argv[2]), argv[3]);
         if (what == "noDevice") return noDevice();
     } catch (const std::exception& e) {
         std::fprintf(stderr, "%s: %s\n", what.c_str(), e.what());
         return 2;
     }
     std::fprintf(stderr, "usage: scenario_drivers solverTest|plasticityTest <out.vtk> | energyConvTest <order> "
-                         "<power|linear|elastic> | noDevice\n");
+                         "<power|linear|elastic> | kirschTest <segments> <out.vtk> | noDevice\n");
     return 64;
 }

@@ -98,3 +98,67 @@ def test_energy_conv_test_energies(drivers, golden_dir, order, kind, table):
     tables = json.load(open(os.path.join(golden_dir, "ref_tables.json")))
     expected = [e for n, e in tables[table] if n == 2880][0]
     assert _six_digits(got, expected), (got, expected)
+
+
+def _polar(c, x, y, xy):
+    """_rr, _phiphi, _rphi of src/PlasticitySolver.cuh:169-200 at centres c."""
+    r = np.sqrt(c[:, 0] ** 2 + c[:, 1] ** 2)
+    cs, sn = c[:, 0] / r, c[:, 1] / r
+    return (cs * cs * x + sn * sn * y + 2.0 * cs * sn * xy, sn * sn * x + cs * cs * y - 2.0 * cs * sn * xy,
+            cs * sn * (-x + y) + xy * (cs * cs - sn * sn))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("segments", [4, 8])
+def test_kirsch_error_norms_and_polar_vtk(drivers, segments, tmp_path):
+    """kirschConvTest (src/Main.cpp:178-227) through the drop-in classes:
+    polarSigmaError and sigmaError (src/PlasticitySolver.cuh:464-540) and the
+    polar-coordinate VTK, against the same formulas applied here (numpy) to
+    the oracle's solution of the same elastic problem."""
+    import meshgen
+    import oracle
+
+    out = str(tmp_path / "kirsch.vtk")
+    r = subprocess.run([drivers, "kirschTest", str(segments), out], capture_output=True, text=True, check=True,
+                       timeout=300)
+    w = r.stdout.split()
+    assert w[0] == "polar" and w[2] == "cartesian_zero"
+    polar_err, cart_err = float(w[1]), float(w[3])
+    m = meshgen.hole_plate(-3, 3, -2, 2, 0.5, segments, segments)
+    path = str(tmp_path / "m.bin")
+    oracle.write_mesh(path, m["node_xy"], elem4=m["elem4"], borders=m["borders"])
+    S, a, E, nu = 1e6, 0.5, 193e9, 0.29
+    o = oracle.run_oracle(["mode elastic", f"mesh file {path}", f"material {E} {nu} 1", "cg_eps 1e-13",
+                           f"force 1 {S} 0 0", f"force 3 {-S} 0 0", "fixvertaxis 0", "fixhoraxis 0"])
+    xy, e4 = np.asarray(m["node_xy"]), np.asarray(m["elem4"])
+    p = xy[e4]
+    c = (((p[:, 0] + p[:, 1]) + p[:, 2]) + p[:, 3]) / 4
+    x, y = p[:, :, 0], p[:, :, 1]
+    area = np.abs((x * np.roll(y, -1, axis=1)).sum(1) - (y * np.roll(x, -1, axis=1)).sum(1)) * 0.5
+    sxx, syy, tau = o["sxx"], o["syy"], o["tau"]
+    # polarSigmaError against Kirsch's solution, centres within r <= 2
+    rr, pp, rp = _polar(c, sxx, syy, tau)
+    rad = np.sqrt(c[:, 0] ** 2 + c[:, 1] ** 2)
+    phi = np.arctan(c[:, 1] / c[:, 0]) + np.where(c[:, 0] < 0, np.pi, 0.0)
+    s_r = 0.5 * S * (1 - a * a / rad ** 2) + 0.5 * S * (1 + 3 * a ** 4 / rad ** 4 - 4 * a * a / rad ** 2) * np.cos(2 * phi)
+    s_p = 0.5 * S * (1 + a * a / rad ** 2) - 0.5 * S * (1 + 3 * a ** 4 / rad ** 4) * np.cos(2 * phi)
+    s_rp = -0.5 * S * (1 - 3 * a ** 4 / rad ** 4 + 2 * a * a / rad ** 2) * np.sin(2 * phi)
+    k = rad <= 2.0
+    vol = area[k].sum()
+    expect_polar = max(np.abs(s_r - rr)[k].max() * vol / (np.abs(rr) * area)[k].sum(),
+                       np.abs(s_p - pp)[k].max() * vol / (np.abs(pp) * area)[k].sum(),
+                       np.abs(s_rp - rp)[k].max() * vol / (np.abs(rp) * area)[k].sum())
+    assert polar_err == pytest.approx(expect_polar, rel=1e-8)
+    # sigmaError with zero reference stresses: each component's largest
+    # magnitude over its area-weighted mean (signed, as in the reference)
+    vol = area.sum()
+    expect_cart = max(np.abs(v).max() * vol / (v * area).sum() for v in (sxx, syy, tau))
+    assert cart_err == pytest.approx(expect_cart, rel=1e-8)
+    # the polar-coordinate VTK: strains from the tensor shear gamma / 2
+    v = vtk.read_solution_vtk(out)["cell_fields"]
+    for name, ref in zip(("Sigma_rr", "Sigma_phiphi", "Tau_rphi"), (rr, pp, rp)):
+        assert rel_l2(v[name], ref) < 1e-8, name
+    err, epp, erp = _polar(c, o["exx"], o["eyy"], 0.5 * o["gamma"])
+    for name, ref in zip(("Eps_rr", "Eps_phiphi", "Gamma_rphi"), (err, epp, erp)):
+        assert rel_l2(v[name], ref) < 1e-8, name
+    assert "Sigma_xx" not in v
