@@ -136,6 +136,22 @@ class Mesh:
                                       _ip(e8) if e8.size else None))
         return m
 
+    def renum_by_direction(self, dx=1.0, dy=1.0):
+        """Mesh::renumByDirection: nodes renumbered by projection on (dx, dy)."""
+        self._check(C.lib().cpx_mesh_renum_by_direction(self._h, dx, dy))
+        return self
+
+    def smooth_ring(self, border_n):
+        self._check(C.lib().cpx_mesh_smooth_ring(self._h, border_n))
+        return self
+
+    def quality(self):
+        """aspect ratio and skew-angle sine per 4-node element, mean element area."""
+        c4 = self.counts()[2]
+        asp, skw, avr = np.zeros(max(c4, 1)), np.zeros(max(c4, 1)), ctypes.c_double()
+        self._check(C.lib().cpx_mesh_quality(self._h, _dp(asp), _dp(skw), ctypes.byref(avr)))
+        return dict(aspect=asp[:c4], skew_sin=skw[:c4], avr_elem_size=avr.value)
+
     def split_t3(self):
         self._check(C.lib().cpx_mesh_split_t3(self._h))
         return self

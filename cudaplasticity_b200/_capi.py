@@ -138,6 +138,9 @@ _SIGS = {
     "cpx_mesh_gen_ring": (c_int, [c_p, c_double, c_double, c_int, c_int, c_int]),
     "cpx_mesh_split_t3": (c_int, [c_p]),
     "cpx_mesh_load_inp": (c_int, [c_p, ctypes.c_char_p]),
+    "cpx_mesh_renum_by_direction": (c_int, [c_p, c_double, c_double]),
+    "cpx_mesh_smooth_ring": (c_int, [c_p, c_int]),
+    "cpx_mesh_quality": (c_int, [c_p, P_double, P_double, P_double]),
     "cpx_mesh_set": (c_int, [c_p, c_int, P_double, c_int, P_int, c_int, P_int, c_int, P_int, P_int, c_int, P_int]),
     "cpx_mesh_counts": (c_int, [c_p, P_int, P_int, P_int, P_int, P_int, P_int]),
     "cpx_mesh_get": (c_int, [c_p, P_double, P_int, P_int, P_int, P_int, P_int]),

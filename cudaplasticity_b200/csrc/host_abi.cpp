@@ -60,6 +60,24 @@ CP_API int cpx_mesh_load_inp(cpx_mesh* m, const char* path) {
     if (!m || !path) return CP_ERR_INVALID;
     return guard([&] { m->m.loadFromFile(path); });
 }
+CP_API int cpx_mesh_renum_by_direction(cpx_mesh* m, double dx, double dy) {
+    if (!m) return CP_ERR_INVALID;
+    return guard([&] { m->m.renumByDirection(cuplast::vec2(dx, dy)); });
+}
+CP_API int cpx_mesh_smooth_ring(cpx_mesh* m, int border_n) {
+    if (!m || border_n < 3 || m->m.nodeCount % border_n) return CP_ERR_INVALID;
+    return guard([&] { m->m.smoothRing(border_n); });
+}
+CP_API int cpx_mesh_quality(const cpx_mesh* m, double* aspect, double* skew_sin, double* avr_size) {
+    if (!m) return CP_ERR_INVALID;
+    return guard([&] {
+        for (int e = 0; e < m->m.count4; ++e) {
+            if (aspect) aspect[e] = m->m.aspectRatio(e);
+            if (skew_sin) skew_sin[e] = m->m.skewAngleSin(e);
+        }
+        if (avr_size) *avr_size = m->m.avrElemSize();
+    });
+}
 CP_API int cpx_mesh_split_t3(cpx_mesh* m) {
     if (!m) return CP_ERR_INVALID;
     return guard([&] { m->m.splitToTriangles(); });

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstring>
 #include <fstream>
+#include <iostream>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -40,6 +41,10 @@ void Mesh::clear() {
     bordersCount = 0;
     count3 = count4 = count8 = 0;
     nodeCount = 0;
+    analysed = false;
+    spaces.clear();
+    aspects.clear();
+    skewAngles.clear();
     fillPos();
 }
 
@@ -63,6 +68,10 @@ Mesh& Mesh::operator=(const Mesh& o) {
     borderLength = dup(o.borderLength, (size_t)bordersCount);
     borders = new int*[bordersCount ? bordersCount : 1];
     for (int b = 0; b < bordersCount; ++b) borders[b] = dup(o.borders[b], (size_t)borderLength[b]);
+    analysed = o.analysed;
+    spaces = o.spaces;
+    aspects = o.aspects;
+    skewAngles = o.skewAngles;
     fillPos();
     return *this;
 }
@@ -545,6 +554,197 @@ bool Mesh::loadFromFile(const std::string& fileName) {
         fillPos();
     }
     return true;
+}
+
+}  // namespace cuplast
+
+// ------------------------------------------------------------ mesh tooling --
+
+namespace cuplast {
+
+namespace {
+
+// Top-down merge sort of keys with their node indices, the order
+// renumByDirection numbers the nodes in (src/Mesh.cu:505-535): the halves are
+// split at n / 2 and merged taking the left key only when it is strictly
+// smaller, so equal keys come out right half first. Kept so that the new
+// numbering is the reference's, ties included.
+void merge_sort(double* key, int* idx, size_t n, double* kbuf, int* ibuf) {
+    if (n < 2) return;
+    const size_t half = n / 2;
+    merge_sort(key, idx, half, kbuf, ibuf);
+    merge_sort(key + half, idx + half, n - half, kbuf + half, ibuf + half);
+    size_t a = 0, b = half, o = 0;
+    while (a < half && b < n) {
+        if (key[a] < key[b]) {
+            kbuf[o] = key[a];
+            ibuf[o++] = idx[a++];
+        } else {
+            kbuf[o] = key[b];
+            ibuf[o++] = idx[b++];
+        }
+    }
+    while (a < half) {
+        kbuf[o] = key[a];
+        ibuf[o++] = idx[a++];
+    }
+    while (b < n) {
+        kbuf[o] = key[b];
+        ibuf[o++] = idx[b++];
+    }
+    std::memcpy(key, kbuf, n * sizeof(double));
+    std::memcpy(idx, ibuf, n * sizeof(int));
+}
+
+}  // namespace
+
+void Mesh::renumByDirection(vec2 direction) {
+    const size_t n = (size_t)nodeCount;
+    std::vector<double> key(n), kbuf(n);
+    std::vector<int> old(n), ibuf(n), now(n);
+    for (size_t i = 0; i < n; ++i) {
+        old[i] = (int)i;
+        key[i] = node[i] * direction;
+    }
+    merge_sort(key.data(), old.data(), n, kbuf.data(), ibuf.data());
+    for (size_t i = 0; i < n; ++i) now[old[i]] = (int)i;
+    // the reference leaves elem3 alone (its generators make no triangles);
+    // here triangles follow too
+    for (size_t i = 0; i < 3 * (size_t)count3; ++i) elem3[i] = now[elem3[i]];
+    for (size_t i = 0; i < 4 * (size_t)count4; ++i) elem4[i] = now[elem4[i]];
+    for (size_t i = 0; i < 8 * (size_t)count8; ++i) elem8[i] = now[elem8[i]];
+    for (int b = 0; b < bordersCount; ++b)
+        for (int j = 0; j < borderLength[b]; ++j) borders[b][j] = now[borders[b][j]];
+    std::vector<vec2> moved(n);
+    for (size_t i = 0; i < n; ++i) moved[now[i]] = node[i];
+    std::copy(moved.begin(), moved.end(), node);
+    for (size_t i = 0; i < n; ++i) secOrdNodes[i] = false;
+    for (int e = 0; e < count8; ++e)
+        for (int k = 4; k < 8; ++k) secOrdNodes[elem8[8 * (size_t)e + k]] = true;
+    analysed = false;
+}
+
+void Mesh::smoothRing(int borderN) {
+    const int radN = nodeCount / borderN;
+    for (int i = radN - 2; i > 0; --i)
+        for (int j = 1; j < borderN - 1; ++j) {
+            const vec2 outer = node[(i + 1) * borderN + j];
+            node[i * borderN + j] = outer - (outer - node[i * borderN + j]).normalize() * 2. * kPi * outer.norm() / borderN;
+        }
+}
+
+double Mesh::aspectRatio(int e) const {
+    const int b = 4 * e;
+    double minSide = (node[elem4[b]] - node[elem4[b + 1]]).norm(), maxSide = minSide;
+    for (int i = 0; i < 4; ++i) {
+        const double len = (node[elem4[b + (i + 1) % 4]] - node[elem4[b + i]]).norm();
+        if (len < minSide) minSide = len;
+        else if (len > maxSide) maxSide = len;
+    }
+    return maxSide / minSide;
+}
+
+double Mesh::skewAngleSin(int e) const {
+    const int b = 4 * e;
+    const vec2 v1 = (node[elem4[b]] + node[elem4[b + 1]] - node[elem4[b + 2]] - node[elem4[b + 3]]) * 0.5;
+    const vec2 v2 = (node[elem4[b + 1]] + node[elem4[b + 2]] - node[elem4[b + 3]] - node[elem4[b]]) * 0.5;
+    const double dot = v1 * v2;
+    return 1. - dot * dot / ((v1.x * v1.x + v1.y * v1.y) * (v2.x * v2.x + v2.y * v2.y));
+}
+
+double Mesh::avrElemSize() const {
+    double s = 0.;
+    for (int e = 0; e < count3; ++e) s += elemSpace3(e);
+    for (int e = 0; e < count4; ++e) s += elemSpace4(e);
+    for (int e = 0; e < count8; ++e) s += elemSpace8(e);
+    return s / elemCount();
+}
+
+void Mesh::printAnalysis() {
+    spaces.assign(count4, 0.);
+    aspects.assign(count4, 0.);
+    skewAngles.assign(count4, 0.);
+    double avrSpace = 0., minSpace = 1e300, maxSpace = 0., avrAspect = 0., minAspect = 1e300, maxAspect = 0.,
+           avrSkew = 0., minSkew = 1e300, maxSkew = 0.;
+    for (int e = 0; e < count4; ++e) {
+        const double space = elemSpace4(e), aspect = aspectRatio(e), skew = skewAngleSin(e);
+        spaces[e] = space;
+        aspects[e] = aspect;
+        skewAngles[e] = std::acos(skew);
+        avrSpace += space;
+        avrAspect += aspect;
+        avrSkew += skew;
+        maxSpace = std::max(maxSpace, space);
+        minSpace = std::min(minSpace, space);
+        maxAspect = std::max(maxAspect, aspect);
+        minAspect = std::min(minAspect, aspect);
+        maxSkew = std::max(maxSkew, skew);
+        minSkew = std::min(minSkew, skew);
+    }
+    avrAspect /= count4;
+    avrSpace /= count4;
+    avrSkew /= count4;
+    std::cout << "Mesh analysis:"
+              << "\nNodes max index difference in element: " << findMaxIndexDiff() << "\nSpace: avr = " << avrSpace
+              << ", min = " << minSpace << ", max = " << maxSpace << "\nAspect ratio " << 100. / avrAspect
+              << "%: avr = " << avrAspect << ", min = " << minAspect << ", max = " << maxAspect << "\nSkew angle sin "
+              << 100 * avrSkew << "%: avr = " << avrSkew << ", min = " << minSkew << ", max = " << maxSkew << "\n"
+              << std::endl;
+    analysed = true;
+}
+
+void Mesh::saveAsVtk(const std::string& fileName) const {
+    std::ofstream f(fileName);
+    f << "# vtk DataFile Version 2.0\nMesh\nASCII\nDATASET POLYDATA\n";
+    f << "POINTS " << nodeCount << " float\n";
+    for (int i = 0; i < nodeCount; ++i) f << node[i].x << " " << node[i].y << " " << 0 << "\n";
+    f << "POLYGONS " << elemCount() << " " << 4 * count3 + 5 * count4 + 9 * count8;
+    for (int i = 0; i < count3; ++i) {
+        f << "\n3 ";
+        for (int j = 3 * i; j < 3 * (i + 1); ++j) f << elem3[j] << " ";
+    }
+    for (int i = 0; i < count4; ++i) {
+        f << "\n4 ";
+        for (int j = 4 * i; j < 4 * (i + 1); ++j) f << elem4[j] << " ";
+    }
+    for (int i = 0; i < count8; ++i) {
+        f << "\n8 ";
+        for (int j = 8 * i; j < 8 * i + 4; ++j) f << elem8[j] << " " << elem8[j + 4] << " ";
+    }
+    f << "\nCELL_DATA " << elemCount() << "\nSCALARS ElementID int 1\nLOOKUP_TABLE default\n";
+    for (int i = 0; i < elemCount(); ++i) f << i << "\n";
+    if (analysed) {
+        const std::pair<const char*, const std::vector<double>*> q[3] = {
+            {"Element_space", &spaces}, {"Element_aspect_ratio", &aspects}, {"Element_skew_angle", &skewAngles}};
+        f << "FIELD FieldData 3";
+        for (auto& p : q) {
+            f << "\n" << p.first << " 1 " << p.second->size() << " float\n";
+            for (double v : *p.second) f << v << " ";
+        }
+    }
+    f << "\nPOINT_DATA " << nodeCount << "\nSCALARS NodeID int 1\nLOOKUP_TABLE my_table";
+    for (int i = 0; i < nodeCount; ++i) f << "\n" << i;
+}
+
+void Mesh::print() const {
+    std::cout << "Nodes\n" << nodeCount << "\n";
+    for (int i = 0; i < nodeCount; ++i) std::cout << i + 1 << " " << node[i].x << " " << node[i].y << "\n";
+    const int counts[3] = {count3, count4, count8}, nen[3] = {3, 4, 8};
+    const int* arrays[3] = {elem3, elem4, elem8};
+    for (int t = 0; t < 3; ++t) {
+        if (!counts[t]) continue;
+        std::cout << "\nElements (" << nen[t] << " nodes): " << counts[t] << "\n";
+        for (int i = 0; i < counts[t]; ++i) {
+            for (int j = nen[t] * i; j < nen[t] * (i + 1); ++j) std::cout << arrays[t][j] + 1 << " ";
+            std::cout << "\n";
+        }
+    }
+    std::cout << "\nBorders\n" << bordersCount;
+    for (int b = 0; b < bordersCount; ++b) {
+        std::cout << "\n" << borderLength[b] << ": ";
+        for (int j = 0; j < borderLength[b]; ++j) std::cout << borders[b][j] << " ";
+    }
+    std::cout << std::endl;
 }
 
 }  // namespace cuplast

@@ -30,6 +30,11 @@ public:
     int* borderLength = nullptr;
     int** borders = nullptr;
 
+    // quality of the 4-node elements, filled by printAnalysis (and then
+    // written by saveAsVtk)
+    bool analysed = false;
+    std::vector<double> spaces, aspects, skewAngles;
+
     Mesh() = default;
     Mesh(const Mesh& other);
     Mesh& operator=(const Mesh& other);
@@ -58,6 +63,30 @@ public:
     double elemSpace3(int e) const;
     double elemSpace4(int e) const;
     double elemSpace8(int e) const;
+
+    // Mesh tooling of the reference (host side):
+    // src/Mesh.cu:537-636: renumber the nodes by their projection on a
+    // direction (element, border and second-order node arrays follow)
+    void renumByDirection(vec2 direction = vec2(1., 1.));
+    // src/Mesh.cu:386-416: moves the inner rings of an O-grid with borderN
+    // columns so that each cell's radial side matches its ring's arc step
+    void smoothRing(int borderN);
+    // src/Mesh.cuh:279-317: largest over smallest side, 1 - cos^2 of the
+    // angle between the mid-lines (4-node element e), mean element area
+    double aspectRatio(int e) const;
+    double skewAngleSin(int e) const;
+    double avrElemSize() const;
+    // src/Mesh.cu:1032-1080: per-element area, aspect ratio and skew angle
+    // of the 4-node elements, with a summary on std::cout
+    void printAnalysis();
+    // src/Mesh.cu:939-990 and 992-1030: the mesh as VTK polygons; the arrays
+    // on std::cout
+    void saveAsVtk(const std::string& fileName) const;
+    void print() const;
+    // the reference's host/device copies; the solver instance holds the
+    // device copy here, so both do nothing
+    void meshToRAM() {}
+    void meshToGPU() {}
 
     // src/Mesh.cu:725-937: a mesh from an .inp file (nodes, S3/S4/S8R
     // element blocks, *MPC border blocks); true when loaded. Throws

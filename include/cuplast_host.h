@@ -33,6 +33,14 @@ CP_API int cpx_mesh_gen_ring(cpx_mesh* m, double a, double b, int n_phi, int n_r
 /* Mesh::loadFromFile (src/Mesh.cu:725-937): an .inp file with *NODE, *ELEMENT
  * (TYPE=S3, S4, S8R) and *MPC border blocks. CP_ERR_INVALID for a bad file. */
 CP_API int cpx_mesh_load_inp(cpx_mesh* m, const char* path);
+/* Mesh::renumByDirection (src/Mesh.cu:537-636): nodes renumbered by their
+ * projection on (dx, dy) */
+CP_API int cpx_mesh_renum_by_direction(cpx_mesh* m, double dx, double dy);
+/* Mesh::smoothRing (src/Mesh.cu:386-416) of an O-grid with border_n columns */
+CP_API int cpx_mesh_smooth_ring(cpx_mesh* m, int border_n);
+/* Mesh::aspectRatio / skewAngleSin per 4-node element (count4 each, either
+ * may be NULL) and Mesh::avrElemSize (src/Mesh.cuh:279-317) */
+CP_API int cpx_mesh_quality(const cpx_mesh* m, double* aspect, double* skew_sin, double* avr_size);
 /* every quad (n1,n2,n3,n4) -> triangles (n1,n2,n3), (n1,n3,n4) (extension) */
 CP_API int cpx_mesh_split_t3(cpx_mesh* m);
 /* Mesh from arrays; elem8 (8 * count8, may be NULL when count8 = 0) marks its

@@ -19,6 +19,7 @@
  *   mesh ring a b Nphi Nr order              (Mesh::genRing, src/Mesh.cu:249)
  *   mesh rect x1 x2 y1 y2 N1 N2 order        (Mesh::genRectangle, src/Mesh.cu:17)
  *   mesh file path.bin                       (arrays written by the test helpers)
+ *   renum dx dy | smooth_ring borderN        (Mesh::renumByDirection / smoothRing after the mesh is made)
  *   mesh inp path.inp                        (Mesh::loadFromFile, src/Mesh.cu:725)
  *   material E nu h
  *   diagram linear E sigmaT K_T              (Material::setLinearPlast)
@@ -95,6 +96,7 @@ static double piecewiseDiagram(double eps, double E, double, double, double, dou
 struct Job {
     std::string mode = "solve";
     std::vector<std::string> meshSpec;
+    std::vector<std::vector<std::string>> meshOps;  // renum dx dy | smooth_ring borderN, in order
     double E = 0, nu = 0.3, h = 1.0;
     bool haveMaterialLine = false;
     std::vector<std::string> diagram;
@@ -124,6 +126,7 @@ static Job parseJob(const char* path) {
         const std::string& k = w[0];
         if (k == "mode") j.mode = w[1];
         else if (k == "mesh") j.meshSpec.assign(w.begin() + 1, w.end());
+        else if (k == "renum" || k == "smooth_ring") j.meshOps.push_back(w);
         else if (k == "material") { j.E = atof(w[1].c_str()); j.nu = atof(w[2].c_str()); j.h = atof(w[3].c_str()); j.haveMaterialLine = true; }
         else if (k == "diagram") j.diagram.assign(w.begin() + 1, w.end());
         else if (k == "plane") j.planeStrain = (w[1] == "strain");
@@ -278,6 +281,11 @@ static void dumpMesh(FILE* f, Mesh& mesh) {
     for (int i = 0; i < mesh.nodeCount; ++i) so[i] = mesh.secOrdNodes[i] ? 1 : 0;
     cpbin_put(f, "sec_ord", 'b', so.size(), so.data());
     cpbin_put_i(f, "max_index_diff", mesh.findMaxIndexDiff());
+    std::vector<double> aspect(mesh.count4), skew(mesh.count4);
+    for (int e = 0; e < mesh.count4; ++e) { aspect[e] = mesh.aspectRatio(e); skew[e] = mesh.skewAngleSin(e); }
+    cpbin_put(f, "aspect", 'd', aspect.size(), aspect.data());
+    cpbin_put(f, "skew_sin", 'd', skew.size(), skew.data());
+    cpbin_put_d(f, "avr_elem_size", mesh.avrElemSize());
 }
 
 static void dumpCsr(FILE* f, SparseSLAE& sp, int nodeCount) {
@@ -314,6 +322,10 @@ int main(int argc, char** argv) {
 
     Mesh mesh;
     buildMesh(j, mesh);
+    for (const auto& op : j.meshOps) {
+        if (op[0] == "renum") mesh.renumByDirection(vec2(atof(op[1].c_str()), atof(op[2].c_str())));
+        else mesh.smoothRing(atoi(op[1].c_str()));
+    }
     FILE* out = cpbin_open_write(argv[2]);
     if (!out) return 3;
 

@@ -10,6 +10,7 @@
 //   scenario_drivers plasticityTest <out.vtk>
 //   scenario_drivers energyConvTest <order> <power|linear|elastic>   (prints the energy)
 //   scenario_drivers kirschTest <segments> <out.vtk>                  (prints the error norms)
+//   scenario_drivers meshVtk <out.vtk>                                (mesh tooling only: no device)
 //   scenario_drivers noDevice                                         (expects a clean error)
 #include <cmath>
 #include <cstdio>
@@ -135,6 +136,20 @@ int kirschTest(int segments, const char* out) {
     return 0;
 }
 
+// The mesh tooling as src/Main.cpp:229-246 (meshTransferTest) uses it: the
+// analysis, a copy, the mesh VTK. Host only.
+int meshVtk(const char* out) {
+    Mesh mesh;
+    mesh.genRectWithHole(-3., 3., -2., 2., 0.5, 12, 8);
+    mesh.renumByDirection();
+    mesh.printAnalysis();
+    Mesh copy(mesh);
+    copy.meshToRAM();
+    copy.saveAsVtk(out);
+    std::printf("avr %.17g max_index_diff %d\n", copy.avrElemSize(), copy.findMaxIndexDiff());
+    return 0;
+}
+
 // Without a device the drop-in classes report the library's status as a
 // std::runtime_error (the reference has no error reporting at all).
 int noDevice() {
@@ -166,12 +181,13 @@ int main(int argc, char** argv) {
         if (what == "plasticityTest" && argc > 2) return plasticityTest(argv[2]);
         if (what == "energyConvTest" && argc > 3) return energyConvTest(std::atoi(argv[2]), argv[3]);
         if (what == "kirschTest" && argc > 3) return kirschTest(std::atoi(argv[2]), argv[3]);
+        if (what == "meshVtk" && argc > 2) return meshVtk(argv[2]);
         if (what == "noDevice") return noDevice();
     } catch (const std::exception& e) {
         std::fprintf(stderr, "%s: %s\n", what.c_str(), e.what());
         return 2;
     }
     std::fprintf(stderr, "usage: scenario_drivers solverTest|plasticityTest <out.vtk> | energyConvTest <order> "
-                         "<power|linear|elastic> | kirschTest <segments> <out.vtk> | noDevice\n");
+                         "<power|linear|elastic> | kirschTest <segments> <out.vtk> | meshVtk <out.vtk> | noDevice\n");
     return 64;
 }

@@ -128,6 +128,32 @@ MISC_LOADS = {
 }
 
 
+# Mesh tooling: (reference mesh spec, operations applied after it)
+MESH_TOOLS = {
+    "hole_renum11": ("hole -3 3 -2 2 0.5 12 8 1", [("renum", 1.0, 1.0)]),
+    "ring_q8_renum": ("ring 50 120 16 4 2", [("renum", 0.3, -1.0)]),
+    "ogrid_smooth": ("hole -100 100 -100 100 20 8 8 1", [("smooth_ring", 32)]),
+    "rect_renum_ties": ("rect -3 3 -2 2 6 4 1", [("renum", 1.0, 0.0)]),
+}
+
+
+def mesh_tool_fixtures():
+    out = {}
+    for name, (spec, ops) in MESH_TOOLS.items():
+        r = oracle.run_reference(["mode mesh", "mesh " + spec] + [" ".join(str(x) for x in op) for op in ops])
+        off, borders = 0, []
+        for L in r["border_len"]:
+            borders.append(r["border_nodes"][off:off + L])
+            off += L
+        m = dict(node_xy=r["node_xy"].reshape(-1, 2), elem3=r["elem3"], elem4=r["elem4"], borders=borders,
+                 elem8=r["elem8"], sec_ord=r["sec_ord"])
+        out[f"{name}_digest"] = np.array(scenarios.mesh_digest(m))
+        for k in ("aspect", "skew_sin", "avr_elem_size"):
+            out[f"{name}_{k}"] = r[k]
+    np.savez_compressed(os.path.join(OUT, "ref_mesh_tools.npz"), **out)
+    print("mesh tools", list(MESH_TOOLS))
+
+
 def q8_load_fixtures():
     out = {}
     for name, (spec, lines) in list(Q8_LOADS.items()) + list(MISC_LOADS.items()):
@@ -206,6 +232,7 @@ if __name__ == "__main__":
             oracle.build(with_reference=True)
         mesh_fixtures()
         q8_load_fixtures()
+        mesh_tool_fixtures()
         sys.exit(0)
     if "--scenarios" in sys.argv:  # only the named scenario fixtures
         if not oracle.have_reference():
@@ -225,5 +252,6 @@ if __name__ == "__main__":
         scenario_fixtures(d)
     mesh_fixtures()
     q8_load_fixtures()
+    mesh_tool_fixtures()
     shipped_fixtures()
     inp_fixtures()

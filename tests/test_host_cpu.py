@@ -73,6 +73,40 @@ def test_product_mesh_generators_match_reference(golden_dir):
         assert m.max_index_diff() == ref[spec]["max_index_diff"], spec
 
 
+@pytest.mark.parametrize("name", ["hole_renum11", "ring_q8_renum", "ogrid_smooth", "rect_renum_ties"])
+def test_mesh_tooling_matches_reference(name, golden_dir):
+    """Mesh::renumByDirection (ties in the reference's merge order),
+    smoothRing, aspectRatio, skewAngleSin and avrElemSize of the drop-in Mesh
+    against the reference's own, on the meshes of its generators: the
+    renumbered / smoothed mesh bit for bit (digest), the quality figures bit
+    for bit."""
+    import sys
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import MESH_TOOLS
+
+    g = dict(np.load(os.path.join(golden_dir, "ref_mesh_tools.npz")))
+    spec, ops = MESH_TOOLS[name]
+    w = spec.split()
+    f = [float(x) for x in w[1:]]
+    if w[0] == "hole":
+        mesh = cp.Mesh.rect_with_hole(*f[:5], int(f[5]), int(f[6]), order=int(f[7]))
+    elif w[0] == "ring":
+        mesh = cp.Mesh.ring(f[0], f[1], int(f[2]), int(f[3]), order=int(f[4]))
+    else:
+        mesh = cp.Mesh.rect(*f[:4], int(f[4]), int(f[5]), order=int(f[6]))
+    for op in ops:
+        if op[0] == "renum":
+            mesh.renum_by_direction(op[1], op[2])
+        else:
+            mesh.smooth_ring(op[1])
+    assert _digest_of(mesh) == str(g[f"{name}_digest"])
+    q = mesh.quality()
+    assert np.array_equal(q["aspect"], g[f"{name}_aspect"])
+    assert np.array_equal(q["skew_sin"], g[f"{name}_skew_sin"])
+    assert q["avr_elem_size"] == float(g[f"{name}_avr_elem_size"][0])
+
+
 def test_product_ogrid_matches_test_generator():
     """The O-grid with a free radial count (benchmark meshes) and the T3 split."""
     a = cp.Mesh.rect_with_hole(-100, 100, -100, 100, 20, 16, 16, rad_n=64).arrays()
