@@ -576,7 +576,9 @@ def run_product_arm(args):
             "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(WORKLOAD, parallelism=f"replicas x{world}", l2="flushed (512 MB write) between steps",
-                           solver="FP64, Aitken secant, block-Jacobi PCG, adaptive CG tolerance"),
+                           solver="FP64, Aitken secant, block-Jacobi PCG, adaptive CG tolerance",
+                           cg_form=os.environ.get("CUPLAST_FP64_CG") or
+                           "one thread-block cluster per linear solve (on chip) where the instance fits"),
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches), "roofline": roofline, "roofline_this_workload": roof_small,
