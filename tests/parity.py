@@ -5,7 +5,7 @@ norm and the norm of the quantity that sets its natural scale (strain
 components by the strain intensity, stress components by the stress
 intensity, plastic strains by the total strain intensity), so that a field
 which is round-off noise in a scenario (e.g. a lateral strain at nu ~ 0) is
-judged against the scale of the solution rather than against itself.
+compared against the scale of the solution rather than against itself.
 """
 import numpy as np
 
