@@ -251,7 +251,7 @@ void cg_fp64_fused(cp_instance* I, double eps, long long max_iter, int precond) 
     a.partials = I->f_partials;
     if (I->cluster_fp64) {
         if (!I->cluster_planned) {
-            I->cluster_plan = cp::cluster_cg_plan(a, I->csr.max_width);
+            I->cluster_plan = cp::cluster_cg_plan(a, I->csr.max_width, I->cluster_variant);
             I->cluster_planned = 1;
         }
         if (I->cluster_plan.ctas > 0) {
@@ -446,7 +446,8 @@ CP_API int cp_instance_create(cp_context* ctx, const cp_mesh_view* mv, const cp_
     if (const char* g = std::getenv("CUPLAST_FP64_CG")) {
         I->fused_fp64 = std::strcmp(g, "classic") != 0;
         I->persistent_fp64 = std::strcmp(g, "persistent") == 0;
-        I->cluster_fp64 = std::strcmp(g, "cluster") == 0;
+        I->cluster_fp64 = std::strcmp(g, "cluster") == 0 || std::strcmp(g, "cluster2") == 0;
+        I->cluster_variant = std::strcmp(g, "cluster2") == 0 ? 2 : 1;
     }
     int rc = guarded(ctx, [&] {
         CP_CHECK(mv->node_count > 0 && mv->node_xy, CP_ERR_INVALID, "mesh: no nodes");

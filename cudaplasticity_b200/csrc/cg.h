@@ -84,8 +84,9 @@ struct ClusterPlan {
     int spc = 0;       // slices of 32 nodes per CTA (one warp each)
     int wmax = 0;      // widest node row, in blocks
     size_t smem = 0;   // dynamic shared memory per CTA
+    int variant = 1;   // 1: k_c_solve; 2: k_c_solve2 (opt-in second form)
 };
-ClusterPlan cluster_cg_plan(const FusedArgs& a, int max_width);
+ClusterPlan cluster_cg_plan(const FusedArgs& a, int max_width, int variant = 1);
 void cluster_cg_launch(const FusedArgs& a, const ClusterPlan& plan, double eps2, long long max_iter, cudaStream_t s);
 
 template <typename T>

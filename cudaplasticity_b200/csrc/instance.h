@@ -51,6 +51,7 @@ struct cp_instance {
     bool fused_fp64 = true;        // false (CUPLAST_FP64_CG=classic): the two-kernel loop of cg.cu
     bool persistent_fp64 = false;  // CUPLAST_FP64_CG=persistent: one cooperative launch per linear solve
     bool cluster_fp64 = true;      // one thread-block cluster when the instance fits (CUPLAST_FP64_CG other than cluster: off)
+    int cluster_variant = 1;       // 2: the second form (CUPLAST_FP64_CG=cluster2)
     int cluster_planned = 0;       // cluster_plan below is computed (once per instance)
     cp::ClusterPlan cluster_plan;
     double2 *f_r = nullptr, *f_w = nullptr, *f_p = nullptr, *f_kp = nullptr, *f_g = nullptr;
