@@ -572,8 +572,22 @@ def run_product_arm(args):
     for prec, name in ((cp.CP_PREC_FP64, "fp64"), (cp.CP_PREC_MIXED, "fp32")):
         binst.set_field("uv", np.zeros_like(brp))
         rows[name] = bench_cg(binst, prec, 0, 100)
+    # elements assembled per second (fillGlobalStiffness on the 1,048,576-element
+    # mesh, CUDA events around the launches) and DOF-iterations per second
+    throughput = {"assembly_mesh": "1024x1024 O-grid plate, 1,048,576 Q4, FP64 values"}
+    try:
+        ams, aby = ctypes.c_double(), ctypes.c_double()
+        binst.ctx.check(cp._capi.lib().cp_bench_assemble(binst._h, cp.CP_PREC_FP64, 10, ctypes.byref(ams),
+                                                          ctypes.byref(aby)))
+        big_nodes, big_elems = binst.sizes()[:2]
+        throughput.update(elements_assembled_per_s=big_elems / (ams.value * 1e-3), assembly_ms=ams.value,
+                          assembly_gbs=aby.value / (ams.value * 1e-3) / 1e9, assembly_bytes=aby.value)
+    except cp.CuplastError as exc:  # an auxiliary figure: report the failure, keep the line
+        big_nodes = binst.sizes()[0]
+        throughput["assembly_error"] = str(exc)
     binst.close()
     mp, mu, bp, bu = rows["fp64"]
+    throughput["dof_iterations_per_s_2M"] = 2 * big_nodes / ((mp + mu) * 1e-3)
     cg_large = {k: {"spmv_gbs": b / (m * 1e-3) / 1e9, "update_gbs": c / (n * 1e-3) / 1e9, "ms_spmv": m,
                     "ms_update": n, "us_per_cg_iter": 1e3 * (m + n)} for k, (m, n, b, c) in rows.items()}
     roofline = {"bound": "hbm", "kernel": "k_cg_p<double> (SpMV+dot) on the 2.1M-DOF 1024x1024 O-grid plate",
@@ -611,6 +625,8 @@ def run_product_arm(args):
             "cg_large_mesh": cg_large, "cpu_baseline": cpu, "clocks": clocks.summary(),
             "accuracy_vs_tight_fp64": accuracy, "batched": batched, "roofline_batched": roof_batched,
             "served": served,
+            "throughput": dict(throughput, dof_iterations_per_s_headline=2 * arrays["node_xy"].shape[0] *
+                               sum(r["cg_iters"] for r in reps) / sum(times)),
             "detail": {"outer_iters": reps[-1]["outer_iters"], "cg_iters": reps[-1]["cg_iters"],
                        "step_seconds": times}}
     if rank == 0:

@@ -851,6 +851,38 @@ CP_API int cp_bench_cg(cp_instance* I, int precision, int precond, int iters, do
     });
 }
 
+CP_API int cp_bench_assemble(cp_instance* I, int precision, int iters, double* ms, double* bytes) {
+    if (I && I->in_batch) return CP_ERR_BUSY;
+    if (!I || iters <= 0 || (precision != CP_PREC_FP64 && precision != CP_PREC_MIXED)) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        cudaStream_t s = I->s();
+        assemble(I, precision);  // warm, and allocates the FP32 values if asked
+        cudaEvent_t e0, e1;
+        CP_CUDA(cudaEventCreate(&e0));
+        CP_CUDA(cudaEventCreate(&e1));
+        CP_CUDA(cudaEventRecord(e0, s));
+        for (int it = 0; it < iters; ++it)
+            cp::launch_assemble(I->mesh, I->csr, I->mat, I->st.E_c, I->st.nu_c, true, precision == CP_PREC_MIXED, s,
+                                I->sms());
+        CP_CUDA(cudaEventRecord(e1, s));
+        CP_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        CP_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        I->launches += iters + 1;
+        const double incs = 3.0 * I->mesh.c3 + 4.0 * I->mesh.c4 + 8.0 * I->mesh.c8;
+        if (ms) *ms = t / iters;
+        // values written once (sliced layout, padding included); the
+        // connectivity (4 per node of an element) and E_c, nu_c (16 per
+        // element); per incidence its code and slot bytes (8, 12 with 8-node
+        // elements); the node coordinates once (16 per node)
+        if (bytes)
+            *bytes = 4.0 * I->csr.sell_blocks * (precision == CP_PREC_MIXED ? 12.0 : 8.0) + incs * 4.0 +
+                     16.0 * I->n_elem + incs * (I->mesh.c8 ? 12.0 : 8.0) + 16.0 * I->n_nodes;
+    });
+}
+
 CP_API int cp_get_csr(cp_instance* I, int* rows, int* cols, int* adj_pos, int* adj, double* values) {
     if (!I) return CP_ERR_INVALID;
     return guarded(I->ctx, [&] {

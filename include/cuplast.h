@@ -178,6 +178,13 @@ CP_API int cp_solve(cp_instance* inst, const cp_solve_opts* opts, cp_solve_repor
  * Jacobi). Leaves uv changed. */
 CP_API int cp_bench_cg(cp_instance* inst, int precision, int precond, int iters, double* ms_spmv, double* ms_update,
                        double* bytes_spmv, double* bytes_update);
+/* Measurement entry point: runs the assembly (fillGlobalStiffness) `iters`
+ * times as direct launches with CUDA events around each, from the current
+ * secant moduli. Outputs the mean duration in milliseconds and the
+ * algorithmic bytes one assembly moves: the values written (FP64, plus FP32
+ * for CP_PREC_MIXED), the connectivity, E_c and nu_c of every element, the
+ * incidence codes and slot bytes, and the node coordinates once. */
+CP_API int cp_bench_assemble(cp_instance* inst, int precision, int iters, double* ms, double* bytes);
 
 /* Allocation-free secant update (no counterpart in the reference). For
  * callers that cannot allocate device memory -- code running while a CUDA
