@@ -389,6 +389,28 @@ double PlasticitySolver::run(bool elastic) {
 
 double PlasticitySolver::solve() { return run(false); }
 double PlasticitySolver::solveElast() { return run(true); }
+double PlasticitySolver::solveElastCUDA() { return run(true); }
+
+namespace {
+// Sets a flag for one call and puts the caller's value back, also when the
+// call throws.
+struct FlagFor {
+    bool& flag;
+    bool saved;
+    FlagFor(bool& f, bool v) : flag(f), saved(f) { flag = v; }
+    ~FlagFor() { flag = saved; }
+};
+}  // namespace
+
+double PlasticitySolver::solveCUDA() {
+    FlagFor f(floatBoost, false);
+    return run(false);
+}
+
+double PlasticitySolver::solveCUDA_FD() {
+    FlagFor f(floatBoost, true);
+    return run(false);
+}
 
 std::vector<double> PlasticitySolver::field(const std::string& name) const {
     if (!inst_) throw std::logic_error("solve() first");

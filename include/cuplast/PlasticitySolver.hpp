@@ -44,6 +44,12 @@ public:
     // Both return seconds of device time, like the reference returns wall time.
     double solve();
     double solveElast();
+    // The reference's explicit device paths (src/PlasticitySolver.cuh:379-407):
+    // FP64, floatBoost's two phases, and the elastic solve. There is no CPU
+    // path (solveCPU / solveElastCPU): the library has no CPU fallback.
+    double solveCUDA();
+    double solveCUDA_FD();
+    double solveElastCUDA();
 
     double deformEnergy();                               // src/PlasticitySolver.cuh:415-445
     void saveDisplsToFile(const std::string& fileName);  // src/PlasticitySolver.cuh:448-458
