@@ -230,6 +230,14 @@ def test_batch_and_server_entry_points_validate_arguments_without_a_device():
     assert L.cp_server_get_stats(None, None) == inv
     assert L.cp_server_destroy(None) == inv
     assert L.cp_secant_update_noalloc(None, None, 0, None, 0, None, None, None, None, None, None, None) == inv
+    ms, by = ctypes.c_double(), ctypes.c_double()
+    assert L.cp_bench_assemble(None, 0, 1, ctypes.byref(ms), ctypes.byref(by)) == inv
+    # host-side mesh tooling validates its arguments
+    m = cp.Mesh.rect_with_hole(-3, 3, -2, 2, 0.5, 12, 8)
+    assert L.cpx_mesh_smooth_ring(m._h, 7) == inv  # node count not a multiple of the column count
+    assert L.cpx_mesh_smooth_ring(m._h, 2) == inv
+    assert L.cpx_mesh_renum_by_direction(None, 1.0, 1.0) == inv
+    assert L.cpx_mesh_quality(None, None, None, None) == inv
 
 
 @pytest.mark.parametrize("name", ["hole_q8", "ring_q8", "rect_q8", "rect_points", "ring_mixed"])
