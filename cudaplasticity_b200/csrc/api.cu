@@ -701,6 +701,7 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
     if (o.precision != CP_PREC_FP64 && o.precision != CP_PREC_MIXED && o.precision != CP_PREC_FLOAT_BOOST)
         return CP_ERR_INVALID;
     if (o.precond != 0 && o.precond != 1) return CP_ERR_INVALID;
+    if (o.adaptive_cg < 0 || o.adaptive_cg > 2) return CP_ERR_INVALID;
     // floatBoost's first phase (solveCUDA_FD, src/PlasticitySolver.cu:660-679):
     // CG 1e-4 and relErr 1e-4 in reduced precision
     constexpr double kBoostTol = 1e-4;
@@ -727,7 +728,8 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
                 CP_CHECK(!I->cancel.load(std::memory_order_relaxed), CP_ERR_CANCELLED, "solve cancelled");
                 // linear tolerance: tight once the secant iteration is close
                 double eps = boost ? std::max(o.cg_tol, kBoostTol) : o.cg_tol;
-                if (!boost && o.adaptive_cg && rel_err > 10.0 * o.outer_tol) eps = std::max(o.cg_tol, 1e-2 * rel_err);
+                if (!boost && o.adaptive_cg == 1 && rel_err > 10.0 * o.outer_tol) eps = std::max(o.cg_tol, 1e-2 * rel_err);
+                if (!boost && o.adaptive_cg == 2 && rel_err > o.outer_tol) eps = std::max(o.cg_tol, 1e-1 * rel_err);
                 assemble(I, prec);
                 if (prec == CP_PREC_FP64) {
                     cg_fp64(I, eps, o.max_cg, o.precond ? 1 : 0);

@@ -102,7 +102,10 @@ typedef struct {
     int levels;          /* load levels lambda_k = k / levels, k = 1..levels, each warm-started */
     int aitken;          /* 1: Aitken-relaxed secant iteration (same fixed point) */
     double inner_tol;    /* mixed precision: relative tolerance of each FP32 inner solve */
-    int adaptive_cg;     /* 1: linear tolerance follows the outer error (inexact early steps) */
+    int adaptive_cg;     /* linear tolerance follows the outer error (inexact early steps; the converged result
+                            meets the same criterion): 1: max(cg_tol, 1e-2 relErr) while relErr > 10 outer_tol;
+                            2: max(cg_tol, 1e-1 relErr) while relErr > outer_tol (fewer CG iterations, a few
+                            more outer ones; the batch treats it as 1) */
     int precond;         /* 0: unpreconditioned CG as the reference; 1: 2x2 block-Jacobi PCG (same solution) */
 } cp_solve_opts;
 
