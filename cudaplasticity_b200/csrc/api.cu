@@ -45,6 +45,37 @@ __global__ void k_reset_state(int ne, double E, double nu, cp::ElemState st) {
     }
 }
 
+// Level predictor: keeps the last level's u and psi in u_prev / psi_prev and,
+// with extrapolate, starts the next level from 2 (last) - (one before) on the
+// free DOFs (k_set_level then sets the prescribed ones), with psi >= 1 and
+// E_c, nu_c from psi as the secant update sets them.
+__global__ void k_predict(int n, int ne, const uchar2* mask, double2* u, double2* u_prev, double E, double nu,
+                          cp::ElemState st, double* psi_prev, int extrapolate) {
+    const int m = n > ne ? n : ne;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        if (i < n) {
+            const double2 c = u[i];
+            if (extrapolate) {
+                const double2 p = u_prev[i];
+                const uchar2 f = mask[i];
+                u[i] = make_double2(f.x ? 2.0 * c.x - p.x : c.x, f.y ? 2.0 * c.y - p.y : c.y);
+            }
+            u_prev[i] = c;
+        }
+        if (i < ne) {
+            const double c = st.psi[i];
+            if (extrapolate) {
+                double v = 2.0 * c - psi_prev[i];
+                if (!(v >= 1.0)) v = 1.0;
+                st.psi[i] = v;
+                st.E_c[i] = E / v;
+                st.nu_c[i] = 0.5 * (1. - (1. - 2. * nu) / v);
+            }
+            psi_prev[i] = c;
+        }
+    }
+}
+
 __global__ void k_zero_double(double* p, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         p[i] = 0.0;
@@ -701,7 +732,7 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
     if (o.precision != CP_PREC_FP64 && o.precision != CP_PREC_MIXED && o.precision != CP_PREC_FLOAT_BOOST)
         return CP_ERR_INVALID;
     if (o.precond != 0 && o.precond != 1) return CP_ERR_INVALID;
-    if (o.adaptive_cg < 0 || o.adaptive_cg > 2) return CP_ERR_INVALID;
+    if (o.adaptive_cg < 0 || o.adaptive_cg > 2 || o.predict < 0 || o.predict > 1) return CP_ERR_INVALID;
     // floatBoost's first phase (solveCUDA_FD, src/PlasticitySolver.cu:660-679):
     // CG 1e-4 and relErr 1e-4 in reduced precision
     constexpr double kBoostTol = 1e-4;
@@ -714,6 +745,17 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
         for (int lev = 1; lev <= o.levels; ++lev) {
             const double lam = (double)lev / o.levels;
             int g;
+            if (o.predict && lev >= 2) {
+                // level 2 records level 1; from level 3 on, extrapolate
+                if (!I->pred_u) {
+                    I->pred_u = I->alloc<double2>(I->n_nodes);
+                    I->pred_psi = I->alloc<double>(I->n_elem);
+                }
+                grid1d(std::max(I->n_nodes, I->n_elem), I->sms(), g);
+                k_predict<<<g, 256, 0, s>>>(I->n_nodes, I->n_elem, I->mask, I->u, I->pred_u, I->mat.E, I->mat.nu,
+                                            I->st, I->pred_psi, lev >= 3 ? 1 : 0);
+                I->launches += 1;
+            }
             grid1d(I->n_nodes, I->sms(), g);
             k_set_level<<<g, 256, 0, s>>>(I->n_nodes, lam, I->b_full, I->u_full, I->mask, I->b, I->u);
             grid1d(2LL * I->n_elem, I->sms(), g);

@@ -53,6 +53,8 @@ struct cp_instance {
     bool cluster_fp64 = true;      // one thread-block cluster when the instance fits (CUPLAST_FP64_CG other than cluster: off)
     int cluster_variant = 1;       // 2: the second form (CUPLAST_FP64_CG=cluster2)
     int cluster_planned = 0;       // cluster_plan below is computed (once per instance)
+    double2* pred_u = nullptr;     // level predictor (cp_solve_opts.predict): the last level's u and psi
+    double* pred_psi = nullptr;
     cp::ClusterPlan cluster_plan;
     double2 *f_r = nullptr, *f_w = nullptr, *f_p = nullptr, *f_kp = nullptr, *f_g = nullptr;
     double* f_partials = nullptr;

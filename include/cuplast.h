@@ -107,6 +107,9 @@ typedef struct {
                             2: max(cg_tol, 1e-1 relErr) while relErr > outer_tol (fewer CG iterations, a few
                             more outer ones; the batch treats it as 1) */
     int precond;         /* 0: unpreconditioned CG as the reference; 1: 2x2 block-Jacobi PCG (same solution) */
+    int predict;         /* 1: from the third load level on, start from the linear extrapolation of the last two
+                            levels' displacements and secant moduli (a predictor; each level still converges to
+                            the same criterion) */
 } cp_solve_opts;
 
 typedef struct {

@@ -162,6 +162,21 @@ def test_cluster_cg_matches_reference(name, ctx, golden_dir, workdir, monkeypatc
     assert r["report"]["status"] == 0
 
 
+@pytest.mark.parametrize("name", ["ogrid16_bilin", "ogrid16_hollomon", "ogrid8_q8_bilin"])
+def test_level_predictor_and_loose_adaptive_rule_reach_the_same_fixed_point(name, ctx, golden_dir, workdir):
+    """The level predictor (cp_solve_opts.predict: each level from the third
+    on starts from the linear extrapolation of the last two) and adaptive
+    rule 2 change the path, not the fixed point: the FP64 bar against the
+    reference's fixture, on scenarios with several load levels."""
+    g = load_golden(golden_dir, name)
+    m, lines = scenario(name, workdir)
+    r = product_runner.run(ctx, lines, m, aitken=1, adaptive_cg=2, predict=1, precond=1)
+    k, err, errs = worst(r, g)
+    assert err <= FP64_TOL, (k, err, errs)
+    assert np.array_equal(yielded(r), yielded(g))
+    assert r["report"]["levels_done"] == scenarios.SCENARIOS[name].get("levels", 1)
+
+
 @pytest.mark.parametrize("name", ["hole12_pow", "ogrid16_bilin"])
 def test_float_boost_reaches_the_fp64_fixed_point(name, ctx, golden_dir, workdir):
     """The reference's floatBoost scheme (CP_PREC_FLOAT_BOOST; solveCUDA_FD,
