@@ -97,6 +97,9 @@ struct BDesc {
     double cg_tol, outer_tol, inner_tol;
     long long max_cg;
     int max_outer, levels, aitken, adaptive, precond;
+    int predict;        // level predictor (cp_solve_opts.predict)
+    double2* pred_u;    // the last level's u and psi (predict only)
+    double* pred_psi;
 };
 
 // Mutable state of one instance.
@@ -187,9 +190,11 @@ __device__ __forceinline__ int tile_phase(const BState* S, int* sh) {
     return *sh;
 }
 
-// Linear tolerance of the next solve (cp_solve: inexact early steps with
-// the adaptive option, tight once the secant iteration is close).
+// Linear tolerance of the next solve, cp_solve's adaptive rules: 1 inexact
+// early steps, tight within 10x of the outer tolerance; 2 looser, tight once
+// the outer tolerance is met.
 __device__ __forceinline__ double next_eps(const BDesc& d, double rel_err) {
+    if (d.adaptive == 2) return rel_err > d.outer_tol ? fmax(d.cg_tol, 1e-1 * rel_err) : d.cg_tol;
     return (d.adaptive && rel_err > 10.0 * d.outer_tol) ? fmax(d.cg_tol, 1e-2 * rel_err) : d.cg_tol;
 }
 
@@ -671,8 +676,11 @@ __global__ void __launch_bounds__(kThreads) k_batch_elem(const BDesc* __restrict
         const int ne = d.m.c3 + d.m.c4 + d.m.c8;
         const int g0 = tl.y * tl.z, g1 = min(g0 + tl.z, d.n_groups);
         if (ph == PH_LEVEL) {
-            // k_set_level and the Aitken history reset of cp_solve
+            // k_set_level, the Aitken history reset and the level predictor
+            // (k_predict) of cp_solve
             const double lam = (double)S->level / d.levels;
+            const int lev = S->level;
+            const bool rec = d.predict && lev >= 2, extra = d.predict && lev >= 3;
             const int s1 = min(g0 + tl.z, d.n_slices);
             for (int sl = g0 + w; sl < s1; sl += kWarps) {
                 const int n = 32 * sl + lane;
@@ -681,6 +689,15 @@ __global__ void __launch_bounds__(kThreads) k_batch_elem(const BDesc* __restrict
                     d.b[n] = make_double2(lam * bf.x, lam * bf.y);
                     const uchar2 m = d.mask[n];
                     double2 uu = d.x[n];
+                    if (rec) {
+                        const double2 cur = uu;
+                        if (extra) {
+                            const double2 pv = d.pred_u[n];
+                            if (m.x) uu.x = 2.0 * cur.x - pv.x;
+                            if (m.y) uu.y = 2.0 * cur.y - pv.y;
+                        }
+                        d.pred_u[n] = cur;
+                    }
                     const double2 uf = d.u_full[n];
                     if (!m.x) uu.x = lam * uf.x;
                     if (!m.y) uu.y = lam * uf.y;
@@ -692,6 +709,17 @@ __global__ void __launch_bounds__(kThreads) k_batch_elem(const BDesc* __restrict
                 if (e < ne) {
                     d.st.res_prev[e] = 0.0;
                     d.st.res_cur[e] = 0.0;
+                    if (rec) {
+                        const double cur = d.st.psi[e];
+                        if (extra) {
+                            double v = 2.0 * cur - d.pred_psi[e];
+                            if (!(v >= 1.0)) v = 1.0;
+                            d.st.psi[e] = v;
+                            d.st.E_c[e] = d.mat.E / v;
+                            d.st.nu_c[e] = 0.5 * (1. - (1. - 2. * d.mat.nu) / v);
+                        }
+                        d.pred_psi[e] = cur;
+                    }
                 }
             }
             if (arrive(S, tl.w, &shf) && threadIdx.x == 0) {
@@ -1119,7 +1147,8 @@ CP_API int cp_batch_add(cp_batch* b, cp_instance* I, const cp_solve_opts* opts, 
     const cp_solve_opts o = *opts;
     if (o.precision != CP_PREC_MIXED) return CP_ERR_UNSUPPORTED;
     if (!(o.cg_tol > 0) || !(o.outer_tol > 0) || !(o.inner_tol > 0 && o.inner_tol < 1) || o.max_outer <= 0 ||
-        o.levels <= 0 || o.max_cg <= 0 || (o.precond & ~1))
+        o.levels <= 0 || o.max_cg <= 0 || (o.precond & ~1) || o.adaptive_cg < 0 || o.adaptive_cg > 2 ||
+        (o.predict & ~1))
         return CP_ERR_INVALID;
     return bguard(b, [&] {
         CP_CHECK(I->loads_set, CP_ERR_INVALID, "loads not set");
@@ -1189,7 +1218,16 @@ CP_API int cp_batch_add(cp_batch* b, cp_instance* I, const cp_solve_opts* opts, 
         d.max_outer = o.max_outer;
         d.levels = o.levels;
         d.aitken = o.aitken ? 1 : 0;
-        d.adaptive = o.adaptive_cg ? 1 : 0;
+        d.adaptive = o.adaptive_cg;
+        d.predict = o.predict ? 1 : 0;
+        if (d.predict) {
+            if (!I->pred_u) {
+                I->pred_u = I->alloc<double2>(I->n_nodes);
+                I->pred_psi = I->alloc<double>(I->n_elem);
+            }
+            d.pred_u = I->pred_u;
+            d.pred_psi = I->pred_psi;
+        }
         d.precond = o.precond;
         CP_CUDA(cudaStreamSynchronize(I->s()));  // buffers of the instance's own stream are ready
         BState S{};

@@ -105,7 +105,7 @@ typedef struct {
     int adaptive_cg;     /* linear tolerance follows the outer error (inexact early steps; the converged result
                             meets the same criterion): 1: max(cg_tol, 1e-2 relErr) while relErr > 10 outer_tol;
                             2: max(cg_tol, 1e-1 relErr) while relErr > outer_tol (fewer CG iterations, a few
-                            more outer ones; the batch treats it as 1) */
+                            more outer ones) */
     int precond;         /* 0: unpreconditioned CG as the reference; 1: 2x2 block-Jacobi PCG (same solution) */
     int predict;         /* 1: from the third load level on, start from the linear extrapolation of the last two
                             levels' displacements and secant moduli (a predictor; each level still converges to
