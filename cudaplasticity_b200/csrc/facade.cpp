@@ -375,7 +375,8 @@ double PlasticitySolver::run(bool elastic) {
     o.max_outer = elastic ? 1 : maxOuter;
     o.levels = elastic ? 1 : levels;
     o.aitken = aitken ? 1 : 0;
-    o.adaptive_cg = adaptiveCg ? 1 : 0;
+    o.adaptive_cg = adaptiveCg ? (adaptiveRule == 2 ? 2 : 1) : 0;
+    o.predict = predict ? 1 : 0;
     o.inner_tol = innerTol;
     if (elastic) o.outer_tol = 1e300;  // one linear solve + stress update (solveElast)
     int st = cp_solve(inst_, &o, &report_);

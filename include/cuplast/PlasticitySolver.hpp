@@ -31,6 +31,8 @@ public:
     int levels = 1;          // load increments, each a deformation-theory solve warm-started from the last
     bool aitken = false;     // Aitken-relaxed secant iteration (same fixed point)
     bool adaptiveCg = false; // loose linear solves while the secant iteration is far from converged
+    int adaptiveRule = 1;    // adaptiveCg: 1 tight within 10x of outerTol; 2 looser until outerTol (cp_solve_opts)
+    bool predict = false;    // levels from the third on start from the extrapolation of the last two
     double innerTol = 1e-4;  // floatBoost's first phase: FP32 inner solves' relative tolerance
     int device = 0;
 
