@@ -1,0 +1,86 @@
+"""One kernel at a time, on a fixed input, for profilers (ncu -k <kernel>).
+
+    python -m cudaplasticity_b200.kernel_cases <case> [--repeat R]
+
+Cases (each prints one JSON line with its host-side facts):
+
+* ``assemble``   -- k_assemble on the 1024x1024 O-grid plate (1,048,576 Q4,
+  2.1M DOF), R launches (cp_bench_assemble: CUDA events around them);
+* ``update``     -- k_update (strain, stress, secant update, exit norm) on the
+  same plate, R launches after one linear solve;
+* ``cg_cluster`` -- k_c_solve: one PCG solve of the 64x64 O-grid plate
+  (8320 DOF) from zero, the whole solve in one thread-block cluster;
+* ``cg_graph``   -- the same solve with one k_f_iter launch per iteration
+  (run with CUPLAST_FP64_CG=fused CUPLAST_NO_GRAPH=1 so that every launch is
+  visible to the profiler);
+* ``cg_large``   -- k_cg_p / k_cg_u on the 2.1M-DOF plate, R iterations
+  (cp_bench_cg).
+
+The inputs are the benchmark's (bilinear steel, top traction), built the
+same way; nothing here is timed for a report.
+"""
+import argparse
+import ctypes
+import json
+import sys
+
+import numpy as np
+
+from . import CP_PREC_FP64, Context, Instance, Loads, Mesh, material
+from . import _capi as C
+
+
+def _plate(n_circ4, rad_n):
+    mesh = Mesh.rect_with_hole(-100.0, 100.0, -100.0, 100.0, 20.0, n_circ4, n_circ4, rad_n=rad_n)
+    rp, mask, uv = Loads().set_force(2, 0.0, 200.0).fix_border_hor(0).fix_point(-100.0, -100.0).build(mesh)
+    mat = material(210000.0, 0.3, diagram="linear", sigma_t=250.0, k_t=2000.0)
+    return mesh, mat, rp, mask, uv
+
+
+def _instance(ctx, n_circ4, rad_n):
+    mesh, mat, rp, mask, uv = _plate(n_circ4, rad_n)
+    inst = Instance(ctx, mesh.arrays(), mat)
+    inst.set_loads(rp, mask, uv)
+    return inst
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("case", choices=["assemble", "update", "cg_cluster", "cg_graph", "cg_large"])
+    ap.add_argument("--repeat", type=int, default=3)
+    a = ap.parse_args(argv)
+    ctx = Context(0)
+    out = {"case": a.case}
+    if a.case in ("assemble", "update", "cg_large"):
+        inst = _instance(ctx, 256, 1024)
+        n_nodes, n_elem, nnz, _ = inst.sizes()
+        out.update(nodes=n_nodes, elements=n_elem, nnz=nnz)
+        if a.case == "assemble":
+            ms, by = ctypes.c_double(), ctypes.c_double()
+            ctx.check(C.lib().cp_bench_assemble(inst._h, CP_PREC_FP64, a.repeat, ctypes.byref(ms), ctypes.byref(by)))
+            out.update(ms_per_launch=ms.value, bytes_per_launch=by.value)
+        elif a.case == "update":
+            inst.assemble(CP_PREC_FP64)
+            it, _ = inst.cg_solve(1e-6)
+            out["cg_iters"] = it
+            out["rel_err"] = [inst.secant_update() for _ in range(a.repeat)]
+        else:
+            mp, mu, bp, bu = (ctypes.c_double() for _ in range(4))
+            inst.set_field("uv", np.zeros(2 * n_nodes))
+            ctx.check(C.lib().cp_bench_cg(inst._h, CP_PREC_FP64, 0, a.repeat, ctypes.byref(mp), ctypes.byref(mu),
+                                          ctypes.byref(bp), ctypes.byref(bu)))
+            out.update(ms_spmv=mp.value, ms_update=mu.value, bytes_spmv=bp.value, bytes_update=bu.value)
+        inst.close()
+    else:
+        inst = _instance(ctx, 16, 64)
+        inst.assemble(CP_PREC_FP64)
+        it, rel = inst.cg_solve(1e-10)
+        out.update(nodes=inst.sizes()[0], cg_iters=it, rel_res=rel)
+        inst.close()
+    ctx.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
