@@ -615,6 +615,67 @@ class Server:
         return {k: getattr(s, k) for k, _ in C.cp_server_stats._fields_}
 
 
+class Hierarchy:
+    """Aggregation multigrid hierarchy of a node graph (cpx_amg_build): level 0
+    has 2 DOFs per node, every coarser level 3 per aggregate (its rigid-body
+    modes). ``adj_pos`` / ``adj`` are the graph without the nodes themselves
+    (``Instance.csr()``'s), ``mask`` 1 per free DOF."""
+
+    def __init__(self, adj_pos, adj, xy, mask, min_coarse_dofs=400):
+        ap = np.ascontiguousarray(adj_pos, np.int32)
+        aj = np.ascontiguousarray(adj, np.int32)
+        if aj.size == 0:
+            aj = np.zeros(1, np.int32)
+        xy = np.ascontiguousarray(np.asarray(xy, np.float64).ravel())
+        mk = np.ascontiguousarray(mask, np.uint8)
+        n = ap.size - 1
+        if xy.size != 2 * n or mk.size != 2 * n:
+            raise ValueError("xy and mask need 2 values per node")
+        self._h = C.c_p()
+        Mesh._check(C.lib().cpx_amg_build(n, _ip(ap), _ip(aj), _dp(xy), _up(mk), min_coarse_dofs,
+                                          ctypes.byref(self._h)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            C.lib().cpx_amg_destroy(self._h)
+            self._h = None
+
+    def __len__(self):
+        n = ctypes.c_int()
+        Mesh._check(C.lib().cpx_amg_levels(self._h, ctypes.byref(n)))
+        return n.value
+
+    def sizes(self, level):
+        """(nodes, DOFs per node, blocks, aggregates of the next level)."""
+        out = [ctypes.c_int() for _ in range(4)]
+        Mesh._check(C.lib().cpx_amg_level_sizes(self._h, level, *(ctypes.byref(x) for x in out)))
+        return tuple(x.value for x in out)
+
+    def level(self, level):
+        """Graph, aggregates and prolongator blocks (nodes x dofs x 3) of a level."""
+        n, fb, nb, na = self.sizes(level)
+        ap, aj = np.zeros(n + 1, np.int32), np.zeros(max(nb - n, 1), np.int32)
+        agg, T = np.zeros(max(n, 1), np.int32), np.zeros(max(n * fb * 3, 1))
+        last = na == 0
+        Mesh._check(C.lib().cpx_amg_level_get(self._h, level, _ip(ap), _ip(aj), None if last else _ip(agg),
+                                              None if last else _dp(T)))
+        out = dict(nodes=n, dofs=fb, blocks=nb, aggregates=na, adj_pos=ap, adj=aj[:nb - n])
+        if not last:
+            out.update(agg=agg[:n], T=T[:n * fb * 3].reshape(n, fb, 3))
+        return out
+
+    def galerkin(self, level, fine_blocks):
+        """Blocks of level + 1's operator from level's (blocks x dofs x dofs)."""
+        n, fb, nb, na = self.sizes(level)
+        f = np.ascontiguousarray(fine_blocks, np.float64).reshape(-1)
+        if f.size != nb * fb * fb:
+            raise ValueError(f"expected {nb} blocks of {fb}x{fb}")
+        cb = self.sizes(level + 1)[2]
+        out = np.zeros(9 * cb)
+        Mesh._check(C.lib().cpx_amg_galerkin(self._h, level, _dp(f), _dp(out)))
+        return out.reshape(cb, 3, 3)
+
+
 def footprint(mesh_arrays, precision=CP_PREC_FP64):
     v, keep = mesh_view(mesh_arrays)
     out = ctypes.c_size_t()

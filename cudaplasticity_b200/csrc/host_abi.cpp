@@ -1,4 +1,5 @@
 // extern "C" wrappers of the host-side drop-in classes (include/cuplast_host.h).
+#include <algorithm>
 #include <exception>
 #include <new>
 #include <stdexcept>
@@ -6,12 +7,16 @@
 
 #include "../../include/cuplast/LoadConditions.hpp"
 #include "../../include/cuplast_host.h"
+#include "amg.h"
 
 struct cpx_mesh {
     cuplast::Mesh m;
 };
 struct cpx_loads {
     cuplast::LoadConditions l;
+};
+struct cpx_amg {
+    cp::amg::Hierarchy h;
 };
 
 namespace {
@@ -188,6 +193,58 @@ CP_API int cpx_loads_build(const cpx_mesh* m, const cpx_loads* l, double h, doub
         std::copy(k.begin(), k.end(), mask);
         std::copy(u.begin(), u.end(), uv);
     });
+}
+
+CP_API int cpx_amg_build(int node_count, const int* adj_pos, const int* adj, const double* xy,
+                         const unsigned char* mask, int min_coarse_dofs, cpx_amg** out) {
+    if (!out || node_count <= 0 || !adj_pos || !adj || !xy || !mask || min_coarse_dofs < 0) return CP_ERR_INVALID;
+    *out = nullptr;
+    for (int n = 0; n < node_count; ++n)
+        if (adj_pos[n + 1] < adj_pos[n]) return CP_ERR_INVALID;
+    for (int q = 0; q < adj_pos[node_count]; ++q)
+        if (adj[q] < 0 || adj[q] >= node_count) return CP_ERR_INVALID;
+    return guard([&] {
+        auto* p = new cpx_amg();
+        try {
+            p->h = cp::amg::build(node_count, adj_pos, adj, xy, mask, min_coarse_dofs);
+        } catch (...) {
+            delete p;
+            throw;
+        }
+        *out = p;
+    });
+}
+CP_API int cpx_amg_destroy(cpx_amg* h) {
+    delete h;
+    return CP_OK;
+}
+CP_API int cpx_amg_levels(const cpx_amg* h, int* n_levels) {
+    if (!h || !n_levels) return CP_ERR_INVALID;
+    *n_levels = (int)h->h.levels.size();
+    return CP_OK;
+}
+CP_API int cpx_amg_level_sizes(const cpx_amg* h, int level, int* node_count, int* dofs_per_node, int* n_blocks,
+                               int* n_aggregates) {
+    if (!h || level < 0 || level >= (int)h->h.levels.size()) return CP_ERR_INVALID;
+    const cp::amg::Level& L = h->h.levels[level];
+    if (node_count) *node_count = L.n_nodes;
+    if (dofs_per_node) *dofs_per_node = L.fb;
+    if (n_blocks) *n_blocks = L.n_nodes + L.adj_pos[L.n_nodes];
+    if (n_aggregates) *n_aggregates = L.n_aggs;
+    return CP_OK;
+}
+CP_API int cpx_amg_level_get(const cpx_amg* h, int level, int* adj_pos, int* adj, int* agg, double* T) {
+    if (!h || level < 0 || level >= (int)h->h.levels.size()) return CP_ERR_INVALID;
+    const cp::amg::Level& L = h->h.levels[level];
+    if (adj_pos) std::copy(L.adj_pos.begin(), L.adj_pos.end(), adj_pos);
+    if (adj) std::copy(L.adj.begin(), L.adj.end(), adj);
+    if (agg) std::copy(L.agg.begin(), L.agg.end(), agg);
+    if (T) std::copy(L.T.begin(), L.T.end(), T);
+    return CP_OK;
+}
+CP_API int cpx_amg_galerkin(const cpx_amg* h, int level, const double* fine, double* coarse) {
+    if (!h || !fine || !coarse || level < 0 || level + 1 >= (int)h->h.levels.size()) return CP_ERR_INVALID;
+    return guard([&] { cp::amg::galerkin(h->h, level, fine, coarse); });
 }
 
 }  // extern "C"

@@ -76,6 +76,33 @@ CP_API int cpx_loads_fix_dof(cpx_loads* l, int dof);
 CP_API int cpx_loads_build(const cpx_mesh* m, const cpx_loads* l, double h, double rho, double* rp,
                            unsigned char* mask, double* uv);
 
+/* Aggregation multigrid hierarchy of the node graph (host set-up; the
+ * solver keeps one per instance for the whole solve). adj_pos / adj: node
+ * graph without the node itself (cp_get_csr's adj_pos / adj); xy: 2 per
+ * node; mask: 2 per node, 1 = free DOF. Coarsening stops at
+ * min_coarse_dofs DOFs or when a level stops shrinking. Level 0 has 2 DOFs
+ * per node, coarser levels 3 (the rigid-body modes of an aggregate). */
+typedef struct cpx_amg cpx_amg;
+CP_API int cpx_amg_build(int node_count, const int* adj_pos, const int* adj, const double* xy,
+                         const unsigned char* mask, int min_coarse_dofs, cpx_amg** out);
+CP_API int cpx_amg_destroy(cpx_amg* h);
+CP_API int cpx_amg_levels(const cpx_amg* h, int* n_levels);
+/* Level l: its node count, DOFs per node and blocks (node count + graph
+ * edges: row n holds n itself, then its neighbours), and the aggregate count
+ * of the next level (0 on the coarsest). */
+CP_API int cpx_amg_level_sizes(const cpx_amg* h, int level, int* node_count, int* dofs_per_node, int* n_blocks,
+                               int* n_aggregates);
+/* Level l's graph (adj_pos: node_count + 1; adj: n_blocks - node_count), the
+ * aggregate of every node and the prolongator blocks (dofs_per_node x 3 per
+ * node, row-major). agg and T are left untouched on the coarsest level; any
+ * output may be NULL. */
+CP_API int cpx_amg_level_get(const cpx_amg* h, int level, int* adj_pos, int* adj, int* agg, double* T);
+/* Galerkin operator of level l + 1 from level l's blocks: fine holds
+ * dofs_per_node^2 values per block (row-major, blocks in row order: node n's
+ * row starts at block adj_pos[n] + n with the diagonal block), coarse
+ * receives 9 per block of level l + 1 in the same order. */
+CP_API int cpx_amg_galerkin(const cpx_amg* h, int level, const double* fine, double* coarse);
+
 #ifdef __cplusplus
 }
 #endif
