@@ -619,9 +619,10 @@ class Hierarchy:
     """Aggregation multigrid hierarchy of a node graph (cpx_amg_build): level 0
     has 2 DOFs per node, every coarser level 3 per aggregate (its rigid-body
     modes). ``adj_pos`` / ``adj`` are the graph without the nodes themselves
-    (``Instance.csr()``'s), ``mask`` 1 per free DOF."""
+    (``Instance.csr()``'s), ``mask`` 1 per free DOF; ``part_nodes`` > 0 cuts
+    level 0 into node ranges that no aggregate crosses, at any level."""
 
-    def __init__(self, adj_pos, adj, xy, mask, min_coarse_dofs=400):
+    def __init__(self, adj_pos, adj, xy, mask, min_coarse_dofs=400, part_nodes=0):
         ap = np.ascontiguousarray(adj_pos, np.int32)
         aj = np.ascontiguousarray(adj, np.int32)
         if aj.size == 0:
@@ -632,7 +633,7 @@ class Hierarchy:
         if xy.size != 2 * n or mk.size != 2 * n:
             raise ValueError("xy and mask need 2 values per node")
         self._h = C.c_p()
-        Mesh._check(C.lib().cpx_amg_build(n, _ip(ap), _ip(aj), _dp(xy), _up(mk), min_coarse_dofs,
+        Mesh._check(C.lib().cpx_amg_build(n, _ip(ap), _ip(aj), _dp(xy), _up(mk), min_coarse_dofs, part_nodes,
                                           ctypes.byref(self._h)))
 
     def __del__(self):
@@ -650,6 +651,14 @@ class Hierarchy:
         out = [ctypes.c_int() for _ in range(4)]
         Mesh._check(C.lib().cpx_amg_level_sizes(self._h, level, *(ctypes.byref(x) for x in out)))
         return tuple(x.value for x in out)
+
+    def parts(self, level):
+        """Partition bounds of a level (n_parts + 1 node indices)."""
+        np_ = ctypes.c_int()
+        Mesh._check(C.lib().cpx_amg_level_parts(self._h, level, ctypes.byref(np_), None))
+        out = np.zeros(np_.value + 1, np.int32)
+        Mesh._check(C.lib().cpx_amg_level_parts(self._h, level, None, _ip(out)))
+        return out
 
     def level(self, level):
         """Graph, aggregates and prolongator blocks (nodes x dofs x 3) of a level."""

@@ -162,7 +162,8 @@ _SIGS = {
     "cpx_loads_set_rotation": (c_int, [c_p, c_double, c_double, c_double]),
     "cpx_loads_fix_dof": (c_int, [c_p, c_int]),
     "cpx_loads_build": (c_int, [c_p, c_p, c_double, c_double, P_double, P_ubyte, P_double]),
-    "cpx_amg_build": (c_int, [c_int, P_int, P_int, P_double, P_ubyte, c_int, ctypes.POINTER(c_p)]),
+    "cpx_amg_build": (c_int, [c_int, P_int, P_int, P_double, P_ubyte, c_int, c_int, ctypes.POINTER(c_p)]),
+    "cpx_amg_level_parts": (c_int, [c_p, c_int, P_int, P_int]),
     "cpx_amg_destroy": (c_int, [c_p]),
     "cpx_amg_levels": (c_int, [c_p, P_int]),
     "cpx_amg_level_sizes": (c_int, [c_p, c_int, P_int, P_int, P_int, P_int]),

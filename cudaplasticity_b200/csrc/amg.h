@@ -11,7 +11,12 @@
 // rotation) as its degrees of freedom.
 //   - aggregation: greedy on the level's node graph (a node whose neighbours
 //     are all free starts an aggregate of itself and its neighbours; the rest
-//     join their first aggregated neighbour, or start a singleton);
+//     join their first aggregated neighbour, or start a singleton), never
+//     across partitions: level 0 may be cut into ranges of part_nodes nodes
+//     (the nodes one thread block owns on the device), and every aggregate
+//     belongs to its members' partition, so restriction and prolongation stay
+//     inside a block at every level; aggregates are numbered partition by
+//     partition;
 //   - tentative prolongator T_l: for each aggregate, the near-null-space rows
 //     of its members (at level 0 the rigid-body modes about the aggregate's
 //     centroid, with zero rows for prescribed DOFs; at coarser levels the R
@@ -30,6 +35,7 @@ struct Level {
     int n_nodes = 0;  // nodes of this level (level 0: mesh nodes; else aggregates of the level below)
     int fb = 2;       // DOFs per node (2 at level 0, 3 above)
     std::vector<int> adj_pos, adj;  // node graph: row n holds n, then adj[adj_pos[n] .. adj_pos[n+1])
+    std::vector<int> part_pos;      // partition p owns nodes [part_pos[p], part_pos[p+1])
     // to the next level (empty on the coarsest)
     int n_aggs = 0;
     std::vector<int> agg;           // aggregate of every node
@@ -48,11 +54,11 @@ struct Hierarchy {
 };
 
 // Builds the hierarchy. adj_pos / adj: the mesh node graph (node n's
-// neighbours, without n); xy: 2 per node; mask: 2 per node, 1 = free DOF.
-// Coarsening stops when a level has at most min_coarse_dofs DOFs or stops
-// shrinking.
+// neighbours, without n); xy: 2 per node; mask: 2 per node, 1 = free DOF;
+// part_nodes: nodes per level-0 partition (0: one partition). Coarsening
+// stops when a level has at most min_coarse_dofs DOFs or stops shrinking.
 Hierarchy build(int n_nodes, const int* adj_pos, const int* adj, const double* xy, const unsigned char* mask,
-                int min_coarse_dofs);
+                int min_coarse_dofs, int part_nodes = 0);
 
 // A_{l+1} from A_l (host restatement of the map the device applies):
 // fine: per block of level l, fb*fb values row-major, blocks in row order;

@@ -11,36 +11,55 @@ namespace amg {
 
 namespace {
 
-// Greedy aggregation of a node graph: pass 1 makes an aggregate of every
-// node whose neighbours are all still free (the node and its neighbours);
-// pass 2 puts each remaining node into the aggregate of its first aggregated
-// neighbour, or into a new singleton.
-int aggregate(int n, const std::vector<int>& adj_pos, const std::vector<int>& adj, std::vector<int>& agg) {
+// Greedy aggregation of a node graph inside each partition (nodes
+// [part_pos[p], part_pos[p+1]) form partition p; edges between partitions are
+// ignored): pass 1 makes an aggregate of every node whose neighbours are all
+// still free (the node and its neighbours); pass 2 puts each remaining node
+// into the aggregate of its first aggregated neighbour, or into a new
+// singleton. Aggregates are then numbered partition by partition, in order of
+// creation within a partition, and the next level's partition bounds are
+// returned in cpart.
+int aggregate(int n, const std::vector<int>& adj_pos, const std::vector<int>& adj, const std::vector<int>& part_pos,
+              std::vector<int>& agg, std::vector<int>& cpart) {
+    const int np = (int)part_pos.size() - 1;
+    std::vector<int> part_of(n);
+    for (int p = 0; p < np; ++p)
+        for (int i = part_pos[p]; i < part_pos[p + 1]; ++i) part_of[i] = p;
     agg.assign(n, -1);
     int na = 0;
     for (int i = 0; i < n; ++i) {
         if (agg[i] >= 0) continue;
         bool free_all = true;
         for (int q = adj_pos[i]; q < adj_pos[i + 1]; ++q)
-            if (agg[adj[q]] >= 0) {
+            if (part_of[adj[q]] == part_of[i] && agg[adj[q]] >= 0) {
                 free_all = false;
                 break;
             }
         if (!free_all) continue;
         agg[i] = na;
-        for (int q = adj_pos[i]; q < adj_pos[i + 1]; ++q) agg[adj[q]] = na;
+        for (int q = adj_pos[i]; q < adj_pos[i + 1]; ++q)
+            if (part_of[adj[q]] == part_of[i]) agg[adj[q]] = na;
         ++na;
     }
     for (int i = 0; i < n; ++i) {
         if (agg[i] >= 0) continue;
         int a = -1;
         for (int q = adj_pos[i]; q < adj_pos[i + 1]; ++q)
-            if (agg[adj[q]] >= 0) {
+            if (part_of[adj[q]] == part_of[i] && agg[adj[q]] >= 0) {
                 a = agg[adj[q]];
                 break;
             }
         agg[i] = a >= 0 ? a : na++;
     }
+    // partition of every aggregate (its members share one), then renumber
+    std::vector<int> apart(na), cnt(np + 1, 0);
+    for (int i = 0; i < n; ++i) apart[agg[i]] = part_of[i];
+    for (int a = 0; a < na; ++a) ++cnt[apart[a] + 1];
+    for (int p = 0; p < np; ++p) cnt[p + 1] += cnt[p];
+    cpart = cnt;
+    std::vector<int> renum(na);
+    for (int a = 0; a < na; ++a) renum[a] = cnt[apart[a]]++;
+    for (int i = 0; i < n; ++i) agg[i] = renum[agg[i]];
     return na;
 }
 
@@ -76,14 +95,21 @@ void mgs(std::vector<double>& B, int rows, double R[9]) {
 }  // namespace
 
 Hierarchy build(int n_nodes, const int* adj_pos, const int* adj, const double* xy, const unsigned char* mask,
-                int min_coarse_dofs) {
-    if (n_nodes <= 0 || !adj_pos || !adj || !xy || !mask) throw std::invalid_argument("amg: empty input");
+                int min_coarse_dofs, int part_nodes) {
+    if (n_nodes <= 0 || !adj_pos || !adj || !xy || !mask || part_nodes < 0)
+        throw std::invalid_argument("amg: empty input");
     Hierarchy h;
     Level L0;
     L0.n_nodes = n_nodes;
     L0.fb = 2;
     L0.adj_pos.assign(adj_pos, adj_pos + n_nodes + 1);
     L0.adj.assign(adj, adj + adj_pos[n_nodes]);
+    if (part_nodes == 0 || part_nodes >= n_nodes) {
+        L0.part_pos = {0, n_nodes};
+    } else {
+        for (int b = 0; b < n_nodes; b += part_nodes) L0.part_pos.push_back(b);
+        L0.part_pos.push_back(n_nodes);
+    }
     // level-0 near-null space: rigid-body modes, centred per aggregate below
     L0.nullspace.assign(6 * (size_t)n_nodes, 0.0);
     h.levels.push_back(std::move(L0));
@@ -93,8 +119,8 @@ Hierarchy build(int n_nodes, const int* adj_pos, const int* adj, const double* x
         F.block_pos.assign(F.n_nodes + 1, 0);
         for (int i = 0; i < F.n_nodes; ++i) F.block_pos[i + 1] = F.block_pos[i] + 1 + (F.adj_pos[i + 1] - F.adj_pos[i]);
         if (F.n_nodes * fb <= min_coarse_dofs) break;
-        std::vector<int> agg;
-        const int na = aggregate(F.n_nodes, F.adj_pos, F.adj, agg);
+        std::vector<int> agg, cpart;
+        const int na = aggregate(F.n_nodes, F.adj_pos, F.adj, F.part_pos, agg, cpart);
         if (na >= F.n_nodes) break;  // no longer shrinking
         F.agg = agg;
         F.n_aggs = na;
@@ -132,6 +158,7 @@ Hierarchy build(int n_nodes, const int* adj_pos, const int* adj, const double* x
         Level C;
         C.n_nodes = na;
         C.fb = 3;
+        C.part_pos = cpart;
         C.nullspace.assign(9 * (size_t)na, 0.0);
         for (int a = 0; a < na; ++a) {
             const int m0 = mpos[a], m1 = mpos[a + 1], rows = (m1 - m0) * fb;

@@ -196,8 +196,9 @@ CP_API int cpx_loads_build(const cpx_mesh* m, const cpx_loads* l, double h, doub
 }
 
 CP_API int cpx_amg_build(int node_count, const int* adj_pos, const int* adj, const double* xy,
-                         const unsigned char* mask, int min_coarse_dofs, cpx_amg** out) {
-    if (!out || node_count <= 0 || !adj_pos || !adj || !xy || !mask || min_coarse_dofs < 0) return CP_ERR_INVALID;
+                         const unsigned char* mask, int min_coarse_dofs, int part_nodes, cpx_amg** out) {
+    if (!out || node_count <= 0 || !adj_pos || !adj || !xy || !mask || min_coarse_dofs < 0 || part_nodes < 0)
+        return CP_ERR_INVALID;
     *out = nullptr;
     for (int n = 0; n < node_count; ++n)
         if (adj_pos[n + 1] < adj_pos[n]) return CP_ERR_INVALID;
@@ -206,7 +207,7 @@ CP_API int cpx_amg_build(int node_count, const int* adj_pos, const int* adj, con
     return guard([&] {
         auto* p = new cpx_amg();
         try {
-            p->h = cp::amg::build(node_count, adj_pos, adj, xy, mask, min_coarse_dofs);
+            p->h = cp::amg::build(node_count, adj_pos, adj, xy, mask, min_coarse_dofs, part_nodes);
         } catch (...) {
             delete p;
             throw;
@@ -231,6 +232,13 @@ CP_API int cpx_amg_level_sizes(const cpx_amg* h, int level, int* node_count, int
     if (dofs_per_node) *dofs_per_node = L.fb;
     if (n_blocks) *n_blocks = L.n_nodes + L.adj_pos[L.n_nodes];
     if (n_aggregates) *n_aggregates = L.n_aggs;
+    return CP_OK;
+}
+CP_API int cpx_amg_level_parts(const cpx_amg* h, int level, int* n_parts, int* part_pos) {
+    if (!h || level < 0 || level >= (int)h->h.levels.size()) return CP_ERR_INVALID;
+    const cp::amg::Level& L = h->h.levels[level];
+    if (n_parts) *n_parts = (int)L.part_pos.size() - 1;
+    if (part_pos) std::copy(L.part_pos.begin(), L.part_pos.end(), part_pos);
     return CP_OK;
 }
 CP_API int cpx_amg_level_get(const cpx_amg* h, int level, int* adj_pos, int* adj, int* agg, double* T) {

@@ -24,15 +24,19 @@ from cudaplasticity_b200 import CuplastError, Hierarchy
 # ------------------------------------------------------------ restatement --
 
 
-def aggregate(adj_pos, adj):
-    """Greedy aggregation: pass 1 takes a node and its neighbours when all are
-    free; pass 2 joins each remaining node to its first aggregated neighbour
-    or makes it a singleton."""
+def aggregate(adj_pos, adj, part_pos):
+    """Greedy aggregation inside each partition: pass 1 takes a node and its
+    neighbours when all are free; pass 2 joins each remaining node to its
+    first aggregated neighbour or makes it a singleton. Edges between
+    partitions are ignored; aggregates are renumbered partition by
+    partition."""
     n = len(adj_pos) - 1
+    part = np.searchsorted(part_pos, np.arange(n), side="right") - 1
     agg = -np.ones(n, np.int64)
     na = 0
     for i in range(n):
         nb = adj[adj_pos[i]:adj_pos[i + 1]]
+        nb = nb[part[nb] == part[i]]
         if agg[i] < 0 and np.all(agg[nb] < 0):
             agg[i] = na
             agg[nb] = na
@@ -41,13 +45,20 @@ def aggregate(adj_pos, adj):
         if agg[i] >= 0:
             continue
         nb = adj[adj_pos[i]:adj_pos[i + 1]]
+        nb = nb[part[nb] == part[i]]
         got = agg[nb][agg[nb] >= 0]
         if len(got):
             agg[i] = got[0]
         else:
             agg[i] = na
             na += 1
-    return agg, na
+    apart = np.zeros(na, np.int64)
+    apart[agg] = part
+    order = np.argsort(apart, kind="stable")
+    renum = np.empty(na, np.int64)
+    renum[order] = np.arange(na)
+    cpart = np.concatenate([[0], np.cumsum(np.bincount(apart, minlength=len(part_pos) - 1))])
+    return renum[agg], na, cpart
 
 
 def mgs(B):
@@ -68,17 +79,18 @@ def mgs(B):
     return B, R
 
 
-def restate(adj_pos, adj, xy, mask, min_coarse_dofs):
-    """Levels as dicts (graph, aggregates, prolongator blocks)."""
+def restate(adj_pos, adj, xy, mask, min_coarse_dofs, part_nodes=0):
+    """Levels as dicts (graph, partitions, aggregates, prolongator blocks)."""
     levels = []
     n, fb = len(adj_pos) - 1, 2
     ns = None
+    part_pos = np.array([0, n]) if part_nodes == 0 else np.append(np.arange(0, n, part_nodes), n)
     while True:
-        lev = dict(nodes=n, dofs=fb, adj_pos=np.asarray(adj_pos), adj=np.asarray(adj))
+        lev = dict(nodes=n, dofs=fb, adj_pos=np.asarray(adj_pos), adj=np.asarray(adj), parts=part_pos)
         levels.append(lev)
         if n * fb <= min_coarse_dofs:
             break
-        agg, na = aggregate(lev["adj_pos"], lev["adj"])
+        agg, na, cpart = aggregate(lev["adj_pos"], lev["adj"], part_pos)
         if na >= n:
             break
         if ns is None:  # rigid-body modes about each aggregate's centroid
@@ -108,7 +120,7 @@ def restate(adj_pos, adj, xy, mask, min_coarse_dofs):
         lev.update(agg=agg, aggregates=na, T=T)
         adj_pos = np.concatenate([[0], np.cumsum([len(x) for x in nb_c])])
         adj = np.array([b for x in nb_c for b in x], np.int64)
-        n, fb, ns = na, 3, ns_c
+        n, fb, ns, part_pos = na, 3, ns_c, cpart
     return levels
 
 
@@ -175,16 +187,17 @@ def t_matrix(lev):
 MESHES = ["hole12_pow", "ogrid16_bilin", "ring_pw", "hole12_q8_pow", "ogrid16_t3"]
 
 
-@pytest.mark.parametrize("name", MESHES)
-def test_hierarchy_matches_restatement(name, workdir):
+@pytest.mark.parametrize("name,part", [(m, 0) for m in MESHES] + [("ogrid16_bilin", 32), ("hole12_q8_pow", 64)])
+def test_hierarchy_matches_restatement(name, part, workdir):
     m, r = elastic_system(name, workdir)
     xy = np.asarray(m["node_xy"], np.float64).reshape(-1, 2)
-    h = Hierarchy(r["adj_pos"], r["adj"], xy, r["mask"], min_coarse_dofs=40)
-    ref = restate(r["adj_pos"], r["adj"], xy, r["mask"], 40)
+    h = Hierarchy(r["adj_pos"], r["adj"], xy, r["mask"], min_coarse_dofs=40, part_nodes=part)
+    ref = restate(r["adj_pos"], r["adj"], xy, r["mask"], 40, part)
     assert len(h) == len(ref) >= 2
     for lv in range(len(ref)):
         got, want = h.level(lv), ref[lv]
         assert got["nodes"] == want["nodes"] and got["dofs"] == want["dofs"]
+        assert np.array_equal(h.parts(lv), want["parts"])
         assert np.array_equal(got["adj_pos"], want["adj_pos"])
         assert np.array_equal(got["adj"], want["adj"])
         if "agg" in want:
@@ -193,6 +206,19 @@ def test_hierarchy_matches_restatement(name, workdir):
             assert np.max(np.abs(got["T"] - want["T"])) <= 1e-12
         else:
             assert got["aggregates"] == 0 and "agg" not in got
+
+
+def test_partitioned_aggregates_stay_inside(workdir):
+    m, r = elastic_system("ogrid16_bilin", workdir)
+    xy = np.asarray(m["node_xy"], np.float64).reshape(-1, 2)
+    h = Hierarchy(r["adj_pos"], r["adj"], xy, r["mask"], min_coarse_dofs=40, part_nodes=32)
+    assert len(h.parts(0)) - 1 == -(-len(xy) // 32)
+    for lv in range(len(h) - 1):
+        lev, pp, cp_ = h.level(lv), h.parts(lv), h.parts(lv + 1)
+        assert len(pp) == len(cp_)
+        for p in range(len(pp) - 1):
+            a = lev["agg"][pp[p]:pp[p + 1]]
+            assert a.min() >= cp_[p] and a.max() < cp_[p + 1]
 
 
 def test_prolongator_properties(workdir):
