@@ -673,6 +673,20 @@ class Hierarchy:
             out.update(agg=agg[:n], T=T[:n * fb * 3].reshape(n, fb, 3))
         return out
 
+    def device_maps(self, level, slice_ptr=None):
+        """Index arrays of the device kernels of a level (cpx_amg_device_maps):
+        rp, ci, mem_pos, mem, gal_pos and gal (entries x 4)."""
+        sp_ = None if slice_ptr is None else np.ascontiguousarray(slice_ptr, np.int32)
+        counts = np.zeros(6, np.int32)
+        spp = None if sp_ is None else _ip(sp_)
+        Mesh._check(C.lib().cpx_amg_device_maps(self._h, level, spp, _ip(counts), *([None] * 6)))
+        bufs = [np.zeros(max(int(c), 1), np.int32) for c in counts]
+        Mesh._check(C.lib().cpx_amg_device_maps(self._h, level, spp, _ip(counts), *(_ip(b) for b in bufs)))
+        names = ["rp", "ci", "mem_pos", "mem", "gal_pos", "gal"]
+        out = {k: b[:int(c)] for k, b, c in zip(names, bufs, counts)}
+        out["gal"] = out["gal"].reshape(-1, 4)
+        return out
+
     def galerkin(self, level, fine_blocks):
         """Blocks of level + 1's operator from level's (blocks x dofs x dofs)."""
         n, fb, nb, na = self.sizes(level)

@@ -60,6 +60,19 @@ struct Hierarchy {
 Hierarchy build(int n_nodes, const int* adj_pos, const int* adj, const double* xy, const unsigned char* mask,
                 int min_coarse_dofs, int part_nodes = 0);
 
+// The index arrays the device kernels of level l use (mg.cu):
+//   rp, ci   -- block CSR of level l >= 1 (diagonal block first in every row);
+//   mem_pos, mem -- members of every level l + 1 node (not on the coarsest);
+//   gal_pos, gal -- the Galerkin map with 4 ints per entry: the fine block's
+//      storage index (level 0: its position in the sliced layout given by
+//      slice_ptr, in blocks of 32 nodes, slice s of width w_s holding block k
+//      of node 32 s + t at slice_ptr[s] + 32 k + t; coarser levels: its block
+//      CSR position), its row node, its column node, 0.
+struct DeviceMaps {
+    std::vector<int> rp, ci, mem_pos, mem, gal_pos, gal;
+};
+DeviceMaps device_maps(const Hierarchy& h, int l, const int* slice_ptr);
+
 // A_{l+1} from A_l (host restatement of the map the device applies):
 // fine: per block of level l, fb*fb values row-major, blocks in row order;
 // coarse: the same for level l+1 (3x3 blocks).

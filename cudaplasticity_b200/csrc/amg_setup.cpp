@@ -209,6 +209,50 @@ Hierarchy build(int n_nodes, const int* adj_pos, const int* adj, const double* x
     return h;
 }
 
+DeviceMaps device_maps(const Hierarchy& h, int l, const int* slice_ptr) {
+    const Level& F = h.levels.at(l);
+    const int n = F.n_nodes, nb = F.block_pos[n];
+    DeviceMaps d;
+    if (l > 0) {
+        d.rp = F.block_pos;
+        d.ci.resize(nb);
+        for (int i = 0; i < n; ++i) {
+            int q = F.block_pos[i];
+            d.ci[q++] = i;
+            for (int r = F.adj_pos[i]; r < F.adj_pos[i + 1]; ++r) d.ci[q++] = F.adj[r];
+        }
+    }
+    if (F.agg.empty()) return d;  // the coarsest level
+    const int nn = F.n_aggs;
+    d.mem_pos.assign(nn + 1, 0);
+    d.mem.resize(n);
+    for (int i = 0; i < n; ++i) ++d.mem_pos[F.agg[i] + 1];
+    for (int a = 0; a < nn; ++a) d.mem_pos[a + 1] += d.mem_pos[a];
+    {
+        std::vector<int> cur(d.mem_pos.begin(), d.mem_pos.end() - 1);
+        for (int i = 0; i < n; ++i) d.mem[cur[F.agg[i]]++] = i;
+    }
+    std::vector<int> row_of(nb), col_of(nb), k_of(nb);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k <= F.adj_pos[i + 1] - F.adj_pos[i]; ++k) {
+            const int b = F.block_pos[i] + k;
+            row_of[b] = i;
+            col_of[b] = k == 0 ? i : F.adj[F.adj_pos[i] + k - 1];
+            k_of[b] = k;
+        }
+    if (l == 0 && !slice_ptr) throw std::invalid_argument("amg: level 0 needs the sliced layout");
+    d.gal_pos = F.gal_pos;
+    d.gal.resize(4 * F.gal_src.size());
+    for (size_t q = 0; q < F.gal_src.size(); ++q) {
+        const int b = F.gal_src[q], i = row_of[b];
+        d.gal[4 * q] = l == 0 ? slice_ptr[i >> 5] + 32 * k_of[b] + (i & 31) : b;
+        d.gal[4 * q + 1] = i;
+        d.gal[4 * q + 2] = col_of[b];
+        d.gal[4 * q + 3] = 0;
+    }
+    return d;
+}
+
 void galerkin(const Hierarchy& h, int l, const double* fine, double* coarse) {
     const Level& F = h.levels.at(l);
     const Level& C = h.levels.at(l + 1);

@@ -323,6 +323,48 @@ void cg_fp64_fused(cp_instance* I, double eps, long long max_iter, int precond) 
     }
 }
 
+// FP64 CG preconditioned by one aggregation-multigrid V-cycle (mg.cu), from
+// the current u: coarse operators from the current K, then the PCG loop.
+void cg_fp64_mg(cp_instance* I, double eps, long long max_iter) {
+    cp::mg_prepare(I);
+    cp::MgArgs a;
+    a.n = I->n_nodes;
+    a.sm_count = I->sms();
+    a.max_blocks = I->max_blocks;
+    a.slice_ptr = I->csr.slice_ptr;
+    a.scol = I->csr.scol;
+    a.val = I->csr.val64;
+    a.b = I->b;
+    a.mask = I->mask;
+    a.x = I->u;
+    a.r = I->r64;
+    a.q = I->q64;
+    a.p0 = I->z64a;
+    a.p1 = I->z64b;
+    a.sc = I->sc;
+    a.partials = I->partials;
+    const int body = std::max(2, I->body_iters + (I->body_iters & 1));
+    I->launches += cp::mg_launch_setup(I->mg, a, I->s());
+    if (I->use_graph && !I->gmg) I->gmg = cp::mg_build_while_graph(I->mg, a, body, I->s());
+    I->launches += cp::mg_launch_start(I->mg, a, eps * eps, max_iter, I->s());
+    const long long per_iter = 2LL * I->mg.L + 1;
+    if (I->use_graph) {
+        CP_CUDA(cudaGraphLaunch(I->gmg, I->s()));
+        CP_CUDA(cudaMemcpyAsync(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost, I->s()));
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+        const long long trips = std::max<long long>(1, (I->sc_h->iter + body - 1) / body);
+        I->launches += trips * (body * per_iter + 1);
+        return;
+    }
+    for (;;) {
+        for (int it = 0; it < body; ++it) cp::mg_launch_iteration(I->mg, a, it & 1, I->s());
+        I->launches += body * per_iter;
+        CP_CUDA(cudaMemcpyAsync(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost, I->s()));
+        CP_CUDA(cudaStreamSynchronize(I->s()));
+        if (I->sc_h->converged || I->sc_h->status) return;
+    }
+}
+
 // Reference-semantics FP64 CG from the current u.
 void cg_fp64(cp_instance* I, double eps, long long max_iter, int precond = 0) {
     if (I->fused_fp64) {
@@ -598,6 +640,7 @@ CP_API int cp_instance_destroy(cp_instance* I) {
         if (I->g32[k]) cudaGraphExecDestroy(I->g32[k]);
         if (I->gf[k]) cudaGraphExecDestroy(I->gf[k]);
     }
+    if (I->ctx) cp::mg_release(I);
     for (void* p : I->allocs) cudaFreeAsync(p, I->ctx->stream);
     if (I->sc_h) cudaFreeHost(I->sc_h);
     if (I->osc_h) cudaFreeHost(I->osc_h);
@@ -637,6 +680,7 @@ CP_API int cp_instance_set_loads(cp_instance* I, const double* rp, const unsigne
         k_set_level<<<g, 256, 0, s>>>(n, 1.0, I->b_full, I->u_full, I->mask, I->b, I->u);
         CP_CUDA(cudaGetLastError());
         CP_CUDA(cudaStreamSynchronize(s));
+        I->mask_host = m;
         I->loads_set = true;
     });
 }
@@ -731,7 +775,8 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
         return CP_ERR_INVALID;
     if (o.precision != CP_PREC_FP64 && o.precision != CP_PREC_MIXED && o.precision != CP_PREC_FLOAT_BOOST)
         return CP_ERR_INVALID;
-    if (o.precond != 0 && o.precond != 1) return CP_ERR_INVALID;
+    if (o.precond < 0 || o.precond > 2) return CP_ERR_INVALID;
+    if (o.precond == 2 && o.precision != CP_PREC_FP64) return CP_ERR_UNSUPPORTED;  // multigrid: FP64 only
     if (o.adaptive_cg < 0 || o.adaptive_cg > 2 || o.predict < 0 || o.predict > 1) return CP_ERR_INVALID;
     // floatBoost's first phase (solveCUDA_FD, src/PlasticitySolver.cu:660-679):
     // CG 1e-4 and relErr 1e-4 in reduced precision
@@ -774,7 +819,8 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
                 if (!boost && o.adaptive_cg == 2 && rel_err > o.outer_tol) eps = std::max(o.cg_tol, 1e-1 * rel_err);
                 assemble(I, prec);
                 if (prec == CP_PREC_FP64) {
-                    cg_fp64(I, eps, o.max_cg, o.precond ? 1 : 0);
+                    if (o.precond == 2) cg_fp64_mg(I, eps, o.max_cg);
+                    else cg_fp64(I, eps, o.max_cg, o.precond ? 1 : 0);
                     R.cg_iters += I->sc_h->iter;
                     R.cg_rel_res = std::sqrt(I->sc_h->rr * I->sc_h->normB_inv);
                     if (I->sc_h->status == CP_ERR_BREAKDOWN) throw Error{CP_ERR_BREAKDOWN, "CG broke down"};

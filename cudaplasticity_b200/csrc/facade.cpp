@@ -377,6 +377,7 @@ double PlasticitySolver::run(bool elastic) {
     o.aitken = aitken ? 1 : 0;
     o.adaptive_cg = adaptiveCg ? (adaptiveRule == 2 ? 2 : 1) : 0;
     o.predict = predict ? 1 : 0;
+    o.precond = precond;
     o.inner_tol = innerTol;
     if (elastic) o.outer_tol = 1e300;  // one linear solve + stress update (solveElast)
     int st = cp_solve(inst_, &o, &report_);

@@ -250,6 +250,20 @@ CP_API int cpx_amg_level_get(const cpx_amg* h, int level, int* adj_pos, int* adj
     if (T) std::copy(L.T.begin(), L.T.end(), T);
     return CP_OK;
 }
+CP_API int cpx_amg_device_maps(const cpx_amg* h, int level, const int* slice_ptr, int* counts, int* rp, int* ci,
+                               int* mem_pos, int* mem, int* gal_pos, int* gal) {
+    if (!h || !counts || level < 0 || level >= (int)h->h.levels.size() || (level == 0 && !slice_ptr))
+        return CP_ERR_INVALID;
+    return guard([&] {
+        const cp::amg::DeviceMaps d = cp::amg::device_maps(h->h, level, slice_ptr);
+        const std::vector<int>* v[6] = {&d.rp, &d.ci, &d.mem_pos, &d.mem, &d.gal_pos, &d.gal};
+        int* out[6] = {rp, ci, mem_pos, mem, gal_pos, gal};
+        for (int k = 0; k < 6; ++k) {
+            counts[k] = (int)v[k]->size();
+            if (out[k]) std::copy(v[k]->begin(), v[k]->end(), out[k]);
+        }
+    });
+}
 CP_API int cpx_amg_galerkin(const cpx_amg* h, int level, const double* fine, double* coarse) {
     if (!h || !fine || !coarse || level < 0 || level + 1 >= (int)h->h.levels.size()) return CP_ERR_INVALID;
     return guard([&] { cp::amg::galerkin(h->h, level, fine, coarse); });

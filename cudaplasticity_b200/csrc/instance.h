@@ -11,6 +11,7 @@
 
 #include "cg.h"
 #include "internal.h"
+#include "mg.h"
 
 struct cp_context {
     int device = 0;
@@ -63,6 +64,13 @@ struct cp_instance {
     float2* bt_vec = nullptr;
     float4* bt_rec = nullptr;
     double* bt_part = nullptr;
+    // aggregation-multigrid PCG (mg.cu, cp_solve_opts.precond 2), built on first use
+    std::vector<unsigned char> mask_host;  // the Dirichlet mask of the last cp_instance_set_loads
+    std::vector<unsigned char> mg_mask;    // the mask the hierarchy was built for
+    bool mg_ready = false;
+    cp::MgDev mg;
+    std::vector<void*> mg_allocs;
+    cudaGraphExec_t gmg = nullptr;
     long long launches = 0;  // kernels launched (graph nodes included)
     int last_assembly = -1;  // precision of the last assembly
     size_t bytes = 0;

@@ -106,7 +106,10 @@ typedef struct {
                             meets the same criterion): 1: max(cg_tol, 1e-2 relErr) while relErr > 10 outer_tol;
                             2: max(cg_tol, 1e-1 relErr) while relErr > outer_tol (fewer CG iterations, a few
                             more outer ones) */
-    int precond;         /* 0: unpreconditioned CG as the reference; 1: 2x2 block-Jacobi PCG (same solution) */
+    int precond;         /* 0: unpreconditioned CG as the reference; 1: 2x2 block-Jacobi PCG (same solution);
+                            2: PCG with one aggregation-multigrid V-cycle (CP_PREC_FP64 only, else
+                            CP_ERR_UNSUPPORTED; the hierarchy is built on first use and kept while the
+                            Dirichlet mask stays the same) */
     int predict;         /* 1: from the third load level on, start from the linear extrapolation of the last two
                             levels' displacements and secant moduli (a predictor; each level still converges to
                             the same criterion) */

@@ -33,6 +33,8 @@ public:
     bool adaptiveCg = false; // loose linear solves while the secant iteration is far from converged
     int adaptiveRule = 1;    // adaptiveCg: 1 tight within 10x of outerTol; 2 looser until outerTol (cp_solve_opts)
     bool predict = false;    // levels from the third on start from the extrapolation of the last two
+    int precond = 0;         // linear solver (cp_solve_opts): 0 CG as the reference, 1 2x2 block-Jacobi PCG,
+                             // 2 aggregation-multigrid PCG (FP64; not with floatBoost)
     double innerTol = 1e-4;  // floatBoost's first phase: FP32 inner solves' relative tolerance
     int device = 0;
 

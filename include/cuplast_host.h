@@ -107,6 +107,14 @@ CP_API int cpx_amg_level_get(const cpx_amg* h, int level, int* adj_pos, int* adj
  * row starts at block adj_pos[n] + n with the diagonal block), coarse
  * receives 9 per block of level l + 1 in the same order. */
 CP_API int cpx_amg_galerkin(const cpx_amg* h, int level, const double* fine, double* coarse);
+/* The index arrays the device kernels of level l read: counts[6] receives the
+ * lengths of rp, ci (block CSR of levels >= 1, diagonal block first), mem_pos,
+ * mem (members of every next-level node), gal_pos and gal (the Galerkin map,
+ * 4 ints per entry: the fine block's storage index -- at level 0 its position
+ * in the sliced layout slice_ptr describes -- its row node, its column node,
+ * 0). Arrays may be NULL (counts only); slice_ptr is needed at level 0. */
+CP_API int cpx_amg_device_maps(const cpx_amg* h, int level, const int* slice_ptr, int* counts, int* rp, int* ci,
+                               int* mem_pos, int* mem, int* gal_pos, int* gal);
 
 #ifdef __cplusplus
 }
