@@ -52,6 +52,7 @@ WORKLOAD = dict(workload="hole_plate_ogrid64x64_q4_8320dof", plate_mm=200, hole_
                 increments=10, cg_tol=1e-10, outer_tol=1e-6)
 SOLVE_KW = dict(cg_tol=1e-10, outer_tol=1e-6, max_outer=2000, levels=10, aitken=1, adaptive_cg=2, precond=1,
                 max_cg=2_000_000, predict=1)
+PRECOND_NAMES = {0: "unpreconditioned CG", 1: "block-Jacobi PCG", 2: "aggregation-multigrid V-cycle PCG"}
 METRIC = "converged solves/s (200 mm plate, 20 mm hole, 64x64 O-grid, 8320 DOF, FP64, <=1e-6 outer / 1e-10 CG)"
 
 
@@ -616,11 +617,13 @@ def run_product_arm(args):
             "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(WORKLOAD, parallelism=f"replicas x{world}", l2="flushed (512 MB write) between steps",
-                           solver="FP64, Aitken secant, block-Jacobi PCG, adaptive CG tolerance "
+                           solver=f"FP64, Aitken secant, {PRECOND_NAMES[SOLVE_KW['precond']]}, adaptive CG tolerance "
                                   "max(1e-10, 0.1 relErr) until relErr <= 1e-6, then 1e-10; levels from the "
                                   "third on start from the linear extrapolation of the last two",
-                           cg_form=os.environ.get("CUPLAST_FP64_CG") or
-                           "one thread-block cluster per linear solve (on chip) where the instance fits"),
+                           cg_form=("graph loop: P, U, then the V-cycle (restrict per level, dense coarsest "
+                                    "inverse, prolongation fused into post-smoothing), one kernel each"
+                                    if SOLVE_KW["precond"] == 2 else os.environ.get("CUPLAST_FP64_CG") or
+                                    "one thread-block cluster per linear solve (on chip) where the instance fits")),
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches), "roofline": roofline, "roofline_this_workload": roof_small,
@@ -741,7 +744,10 @@ def main():
     ap.add_argument("--serve-window", type=float, default=20.0, help="seconds of arrivals in the served leg")
     ap.add_argument("--batched-probe", type=int, nargs=2, metavar=("N", "TRIPS"),
                     help="profiling aid: N resident batch-stream instances, TRIPS graph trips, then exit")
+    ap.add_argument("--precond", type=int, default=SOLVE_KW["precond"], choices=[0, 1, 2],
+                    help="linear solver of the headline: 0 CG, 1 block-Jacobi PCG, 2 multigrid PCG")
     args = ap.parse_args()
+    SOLVE_KW["precond"] = args.precond
     if args.batched_probe:
         batched_probe(*args.batched_probe)
         return
