@@ -347,7 +347,7 @@ void cg_fp64_mg(cp_instance* I, double eps, long long max_iter) {
     I->launches += cp::mg_launch_setup(I->mg, a, I->s());
     if (I->use_graph && !I->gmg) I->gmg = cp::mg_build_while_graph(I->mg, a, body, I->s());
     I->launches += cp::mg_launch_start(I->mg, a, eps * eps, max_iter, I->s());
-    const long long per_iter = 2LL * I->mg.L + 1;
+    const long long per_iter = cp::mg_launches_per_iteration(I->mg);
     if (I->use_graph) {
         CP_CUDA(cudaGraphLaunch(I->gmg, I->s()));
         CP_CUDA(cudaMemcpyAsync(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost, I->s()));

@@ -12,14 +12,16 @@
 //       q = K p, (p, q) -> alpha
 //   U : x += alpha p, r -= m.alpha q, (r, r) -> converged?; pre-smoothing of
 //       level 0 from zero: y0 = w0 D0^-1 r
-//   R0: per level-1 node: residual of its members r - K y0, restricted by
-//       T0^T; pre-smoothing y1 = w1 D1^-1 b1
+//   R0: one block per level-0 node range: residuals r - K y0 restricted by
+//       T0^T into each level-1 node; pre-smoothing y1 = w1 D1^-1 b1
 //   R_l (l >= 1): the same one level down, on the 3x3 block CSR
 //   C : coarsest correction e = A_c^-1 b_c (dense inverse)
 //   S_l (l >= 1): prolongation fused into the post-smoothing sweep:
 //       y' = y + T e, z = y' + w D^-1 (b - A y'), A y' gathered from the
 //       neighbours' y and their aggregates' e
 //   S0: the same on level 0; (r, z) -> rho, beta
+// When level 1 is small, R_1 .. S_1 run in one block (k_mg_coarse_cycle), so
+// an iteration is five kernels: P, U, R0, the coarse cycle, S0.
 // Every kernel returns at once when the solve has converged or failed, so a
 // graph body of several iterations stops doing work after convergence. Each
 // value is produced by one thread in a fixed order and every cross-block sum
@@ -417,26 +419,34 @@ __global__ void __launch_bounds__(kThreads) k_mg_u(MgArgs a, MgLevel L0, const d
     }
 }
 
-// R0: per level-1 node, the level-0 residual r - K y0 of its members,
-// restricted; then level 1's pre-smoothing from zero (unless it is the
-// coarsest level).
-__global__ void __launch_bounds__(kSmall) k_mg_restrict0(MgArgs a, MgLevel L0, MgLevel L1, const double* lam,
-                                                         double omega, int coarsest) {
+// R0: per level-0 range of kMgPartNodes nodes (one block; no aggregate
+// crosses a range), each thread the residual r - K y0 of one node, restricted
+// by its prolongator block into shared memory; then per level-1 node of the
+// range, the sum over its members in member order, and level 1's
+// pre-smoothing from zero (unless it is the coarsest level).
+__global__ void __launch_bounds__(kMgPartNodes) k_mg_restrict0(MgArgs a, MgLevel L0, MgLevel L1, const double* lam,
+                                                               double omega, int coarsest) {
+    __shared__ double tr[kMgPartNodes][3];
     if (a.sc->converged || a.sc->status) return;
-    const double2* __restrict__ y0 = reinterpret_cast<const double2*>(L0.y);
+    const int i0 = blockIdx.x * kMgPartNodes, i = i0 + threadIdx.x;
+    if (i < a.n) {
+        const double2 ky = k_row(a, i, reinterpret_cast<const double2*>(L0.y));
+        const uchar2 m = a.mask[i];
+        const double2 ri = a.r[i];
+        const double rx = m.x ? ri.x - ky.x : 0.0, ry = m.y ? ri.y - ky.y : 0.0;
+        const double* t = L0.T + 6 * (size_t)i;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) tr[threadIdx.x][c] = t[c] * rx + t[3 + c] * ry;
+    }
+    __syncthreads();
     const double w1 = coarsest ? 0.0 : damping(lam, 1, omega);
-    for (int A = blockIdx.x * blockDim.x + threadIdx.x; A < L1.n; A += gridDim.x * blockDim.x) {
+    for (int A = L1.part_pos[blockIdx.x] + threadIdx.x; A < L1.part_pos[blockIdx.x + 1]; A += blockDim.x) {
         double c0 = 0.0, c1 = 0.0, c2 = 0.0;
         for (int q = L0.mem_pos[A]; q < L0.mem_pos[A + 1]; ++q) {
-            const int i = L0.mem[q];
-            const double2 ky = k_row(a, i, y0);
-            const uchar2 m = a.mask[i];
-            const double2 ri = a.r[i];
-            const double rx = m.x ? ri.x - ky.x : 0.0, ry = m.y ? ri.y - ky.y : 0.0;
-            const double* t = L0.T + 6 * (size_t)i;
-            c0 += t[0] * rx + t[3] * ry;
-            c1 += t[1] * rx + t[4] * ry;
-            c2 += t[2] * rx + t[5] * ry;
+            const double* u = tr[L0.mem[q] - i0];
+            c0 += u[0];
+            c1 += u[1];
+            c2 += u[2];
         }
         double* b = L1.b + 3 * (size_t)A;
         b[0] = c0;
@@ -451,76 +461,109 @@ __global__ void __launch_bounds__(kSmall) k_mg_restrict0(MgArgs a, MgLevel L0, M
     }
 }
 
-// R_l (l >= 1): the same from level l (F) to level l + 1 (C).
+// One node A of level l + 1 (C): the level-l (F) residual b - A y of its
+// members, restricted, and C's pre-smoothing (wc = 0 on the coarsest).
+__device__ __forceinline__ void restrict_node(const MgLevel& F, const MgLevel& C, int A, double wc, bool coarsest) {
+    double c[3] = {0.0, 0.0, 0.0};
+    for (int q = F.mem_pos[A]; q < F.mem_pos[A + 1]; ++q) {
+        const int i = F.mem[q];
+        double r[3] = {F.b[3 * (size_t)i], F.b[3 * (size_t)i + 1], F.b[3 * (size_t)i + 2]};
+        for (int p = F.rp[i]; p < F.rp[i + 1]; ++p) {
+            const double* Ab = F.val + 9 * (size_t)p;
+            const double* yj = F.y + 3 * (size_t)F.ci[p];
+            const double y0 = yj[0], y1 = yj[1], y2 = yj[2];
+#pragma unroll
+            for (int rr = 0; rr < 3; ++rr) r[rr] -= Ab[3 * rr] * y0 + Ab[3 * rr + 1] * y1 + Ab[3 * rr + 2] * y2;
+        }
+        const double* t = F.T + 9 * (size_t)i;
+#pragma unroll
+        for (int col = 0; col < 3; ++col) c[col] += t[col] * r[0] + t[3 + col] * r[1] + t[6 + col] * r[2];
+    }
+    double* b = C.b + 3 * (size_t)A;
+    b[0] = c[0];
+    b[1] = c[1];
+    b[2] = c[2];
+    if (!coarsest) {
+        const double* di = C.dinv + 9 * (size_t)A;
+        double* y = C.y + 3 * (size_t)A;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) y[r] = wc * (di[3 * r] * c[0] + di[3 * r + 1] * c[1] + di[3 * r + 2] * c[2]);
+    }
+}
+
+// Row r of the coarsest correction e = A_c^-1 b_c (column-major inverse).
+__device__ __forceinline__ void coarse_row(const MgLevel& C, int nc, const double* __restrict__ cinv, int r) {
+    double s = 0.0;
+    for (int c = 0; c < nc; ++c) s += cinv[(size_t)c * nc + r] * C.b[c];
+    C.z[r] = s;
+}
+
+// One node i of level l (F): z = y' + w D^-1 (b - A y'), y' = y + T e with e
+// the next level's (C) correction, gathered for every column of the row.
+__device__ __forceinline__ void smooth_node(const MgLevel& F, const MgLevel& C, int i, double w) {
+    double s[3] = {F.b[3 * (size_t)i], F.b[3 * (size_t)i + 1], F.b[3 * (size_t)i + 2]};
+    double yi[3] = {0.0, 0.0, 0.0};
+    for (int p = F.rp[i]; p < F.rp[i + 1]; ++p) {
+        double yj[3];
+        prolonged3(F, C, F.ci[p], yj);
+        const double* Ab = F.val + 9 * (size_t)p;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) s[r] -= Ab[3 * r] * yj[0] + Ab[3 * r + 1] * yj[1] + Ab[3 * r + 2] * yj[2];
+        if (p == F.rp[i]) {  // the diagonal block: column i itself
+            yi[0] = yj[0];
+            yi[1] = yj[1];
+            yi[2] = yj[2];
+        }
+    }
+    const double* di = F.dinv + 9 * (size_t)i;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+        F.z[3 * (size_t)i + r] = yi[r] + w * (di[3 * r] * s[0] + di[3 * r + 1] * s[1] + di[3 * r + 2] * s[2]);
+}
+
+// R_l (l >= 1), one thread per level-(l + 1) node.
 __global__ void __launch_bounds__(kSmall) k_mg_restrict(MgLevel F, MgLevel C, const double* lam, int lc,
                                                         double omega, int coarsest, const CgScalars* sc) {
     if (sc->converged || sc->status) return;
     const double wc = coarsest ? 0.0 : damping(lam, lc, omega);
-    for (int A = blockIdx.x * blockDim.x + threadIdx.x; A < C.n; A += gridDim.x * blockDim.x) {
-        double c[3] = {0.0, 0.0, 0.0};
-        for (int q = F.mem_pos[A]; q < F.mem_pos[A + 1]; ++q) {
-            const int i = F.mem[q];
-            double r[3] = {F.b[3 * (size_t)i], F.b[3 * (size_t)i + 1], F.b[3 * (size_t)i + 2]};
-            for (int p = F.rp[i]; p < F.rp[i + 1]; ++p) {
-                const double* Ab = F.val + 9 * (size_t)p;
-                const double* yj = F.y + 3 * (size_t)F.ci[p];
-                const double y0 = yj[0], y1 = yj[1], y2 = yj[2];
-#pragma unroll
-                for (int rr = 0; rr < 3; ++rr) r[rr] -= Ab[3 * rr] * y0 + Ab[3 * rr + 1] * y1 + Ab[3 * rr + 2] * y2;
-            }
-            const double* t = F.T + 9 * (size_t)i;
-#pragma unroll
-            for (int col = 0; col < 3; ++col) c[col] += t[col] * r[0] + t[3 + col] * r[1] + t[6 + col] * r[2];
-        }
-        double* b = C.b + 3 * (size_t)A;
-        b[0] = c[0];
-        b[1] = c[1];
-        b[2] = c[2];
-        if (!coarsest) {
-            const double* di = C.dinv + 9 * (size_t)A;
-            double* y = C.y + 3 * (size_t)A;
-#pragma unroll
-            for (int r = 0; r < 3; ++r) y[r] = wc * (di[3 * r] * c[0] + di[3 * r + 1] * c[1] + di[3 * r + 2] * c[2]);
-        }
-    }
+    for (int A = blockIdx.x * blockDim.x + threadIdx.x; A < C.n; A += gridDim.x * blockDim.x)
+        restrict_node(F, C, A, wc, coarsest != 0);
 }
 
-// C: e = A_c^-1 b_c (column-major inverse: the threads of a warp read
-// consecutive entries).
+// C: the coarsest correction (the threads of a warp read consecutive entries).
 __global__ void __launch_bounds__(kSmall) k_mg_coarse(MgLevel C, int nc, const double* __restrict__ cinv,
                                                       const CgScalars* sc) {
     if (sc->converged || sc->status) return;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nc; r += gridDim.x * blockDim.x) {
-        double s = 0.0;
-        for (int c = 0; c < nc; ++c) s += cinv[(size_t)c * nc + r] * C.b[c];
-        C.z[r] = s;
-    }
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nc; r += gridDim.x * blockDim.x) coarse_row(C, nc, cinv, r);
 }
 
-// S_l (l >= 1): z = y' + w D^-1 (b - A y'), y' = y + T e (e: level l + 1's z).
+// S_l (l >= 1), one thread per level-l node.
 __global__ void __launch_bounds__(kSmall) k_mg_smooth(MgLevel F, MgLevel C, const double* lam, int l, double omega,
                                                       const CgScalars* sc) {
     if (sc->converged || sc->status) return;
     const double w = damping(lam, l, omega);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.n; i += gridDim.x * blockDim.x) {
-        double s[3] = {F.b[3 * (size_t)i], F.b[3 * (size_t)i + 1], F.b[3 * (size_t)i + 2]};
-        double yi[3] = {0.0, 0.0, 0.0};
-        for (int p = F.rp[i]; p < F.rp[i + 1]; ++p) {
-            double yj[3];
-            prolonged3(F, C, F.ci[p], yj);
-            const double* Ab = F.val + 9 * (size_t)p;
-#pragma unroll
-            for (int r = 0; r < 3; ++r) s[r] -= Ab[3 * r] * yj[0] + Ab[3 * r + 1] * yj[1] + Ab[3 * r + 2] * yj[2];
-            if (p == F.rp[i]) {  // the diagonal block: column i itself
-                yi[0] = yj[0];
-                yi[1] = yj[1];
-                yi[2] = yj[2];
-            }
-        }
-        const double* di = F.dinv + 9 * (size_t)i;
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-            F.z[3 * (size_t)i + r] = yi[r] + w * (di[3 * r] * s[0] + di[3 * r + 1] * s[1] + di[3 * r + 2] * s[2]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.n; i += gridDim.x * blockDim.x) smooth_node(F, C, i, w);
+}
+
+// Levels 1 .. L-1 of the V-cycle in one block when level 1 is small: the
+// restrictions R_1 .. R_{L-2}, the coarsest correction and the sweeps
+// S_{L-2} .. S_1, separated by block barriers instead of kernel boundaries
+// (the same per-node arithmetic as the kernels above).
+__global__ void __launch_bounds__(1024) k_mg_coarse_cycle(MgDev m, const CgScalars* sc) {
+    if (sc->converged || sc->status) return;
+    const int L = m.L, tid = threadIdx.x, nt = blockDim.x;
+    for (int l = 1; l + 1 < L; ++l) {
+        const bool coarsest = l + 1 == L - 1;
+        const double wc = coarsest ? 0.0 : damping(m.lam, l + 1, m.omega);
+        for (int A = tid; A < m.lv[l + 1].n; A += nt) restrict_node(m.lv[l], m.lv[l + 1], A, wc, coarsest);
+        __syncthreads();
+    }
+    for (int r = tid; r < m.nc; r += nt) coarse_row(m.lv[L - 1], m.nc, m.cinv, r);
+    __syncthreads();
+    for (int l = L - 2; l >= 1; --l) {
+        const double w = damping(m.lam, l, m.omega);
+        for (int i = tid; i < m.lv[l].n; i += nt) smooth_node(m.lv[l], m.lv[l + 1], i, w);
+        __syncthreads();
     }
 }
 
@@ -584,23 +627,38 @@ int grid_small(long long n, int sms) {
     return (int)std::max<long long>(1, std::min<long long>(g, 8LL * sms));
 }
 
-// The V-cycle from U's y0 to S0's z: 2 L - 1 launches.
+// Level 1 at most this many nodes: levels 1 .. L-1 run in one block.
+constexpr int kMgOneBlockNodes = 4096;
+
+bool one_block_coarse(const MgDev& m) { return m.L >= 3 && m.lv[1].n <= kMgOneBlockNodes; }
+
+// The V-cycle from U's y0 to S0's z.
 int launch_vcycle(const MgDev& m, const MgArgs& a, cudaStream_t s) {
     const int L = m.L;
     const int sms = a.sm_count;
-    k_mg_restrict0<<<grid_small(m.lv[1].n, sms), kSmall, 0, s>>>(a, m.lv[0], m.lv[1], m.lam, m.omega, L == 2);
-    for (int l = 1; l + 1 < L; ++l)
-        k_mg_restrict<<<grid_small(m.lv[l + 1].n, sms), kSmall, 0, s>>>(m.lv[l], m.lv[l + 1], m.lam, l + 1, m.omega,
-                                                                        l + 1 == L - 1, a.sc);
-    k_mg_coarse<<<grid_small(m.nc, sms), kSmall, 0, s>>>(m.lv[L - 1], m.nc, m.cinv, a.sc);
-    for (int l = L - 2; l >= 1; --l)
-        k_mg_smooth<<<grid_small(m.lv[l].n, sms), kSmall, 0, s>>>(m.lv[l], m.lv[l + 1], m.lam, l, m.omega, a.sc);
+    const int parts = (a.n + kMgPartNodes - 1) / kMgPartNodes;
+    k_mg_restrict0<<<parts, kMgPartNodes, 0, s>>>(a, m.lv[0], m.lv[1], m.lam, m.omega, L == 2);
+    int launches = 1;
+    if (one_block_coarse(m)) {
+        k_mg_coarse_cycle<<<1, 1024, 0, s>>>(m, a.sc);
+        ++launches;
+    } else {
+        for (int l = 1; l + 1 < L; ++l)
+            k_mg_restrict<<<grid_small(m.lv[l + 1].n, sms), kSmall, 0, s>>>(m.lv[l], m.lv[l + 1], m.lam, l + 1,
+                                                                            m.omega, l + 1 == L - 1, a.sc);
+        k_mg_coarse<<<grid_small(m.nc, sms), kSmall, 0, s>>>(m.lv[L - 1], m.nc, m.cinv, a.sc);
+        for (int l = L - 2; l >= 1; --l)
+            k_mg_smooth<<<grid_small(m.lv[l].n, sms), kSmall, 0, s>>>(m.lv[l], m.lv[l + 1], m.lam, l, m.omega, a.sc);
+        launches += 2 * (L - 2) + 1;
+    }
     k_mg_smooth0<<<grid_nodes(a), kThreads, 0, s>>>(a, m.lv[0], m.lv[1], m.lam, m.omega);
     CP_CUDA(cudaGetLastError());
-    return 2 * L - 1;
+    return launches + 1;
 }
 
 }  // namespace
+
+int mg_launches_per_iteration(const MgDev& m) { return 2 + (one_block_coarse(m) ? 3 : 2 * m.L - 1); }
 
 int mg_launch_setup(const MgDev& m, const MgArgs& a, cudaStream_t s) {
     const int sms = a.sm_count;
@@ -736,6 +794,7 @@ void mg_prepare(cp_instance* I) {
         } else {
             D.rp = mg_upload(I, dm.rp);
             D.ci = mg_upload(I, dm.ci);
+            D.part_pos = mg_upload(I, F.part_pos);
             D.val = mg_alloc<double>(I, 9 * (size_t)D.nb);
             D.dinv = mg_alloc<double>(I, 9 * (size_t)D.n);
             D.b = mg_alloc<double>(I, 3 * (size_t)D.n);

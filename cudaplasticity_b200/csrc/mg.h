@@ -33,6 +33,7 @@ struct MgLevel {
     int* ci = nullptr;          // column node of every block
     double* val = nullptr;      // 9 per block, row-major
     double* dinv = nullptr;     // smoother: fb x fb inverse of the diagonal block per node
+    int* part_pos = nullptr;    // levels >= 1: the nodes of level-0 range p are part_pos[p] .. part_pos[p+1]
     // transfer to the next level (not on the coarsest)
     int* agg = nullptr;         // next-level node of every node
     double* T = nullptr;        // fb x 3 prolongator block per node, row-major
@@ -81,6 +82,8 @@ int mg_launch_setup(const MgDev& m, const MgArgs& a, cudaStream_t s);
 int mg_launch_start(const MgDev& m, const MgArgs& a, double eps2, long long max_iter, cudaStream_t s);
 // One PCG iteration (search direction, update, V-cycle).
 int mg_launch_iteration(const MgDev& m, const MgArgs& a, int parity, cudaStream_t s);
+// Kernels launched by one iteration.
+int mg_launches_per_iteration(const MgDev& m);
 // while (!converged) { body_iters iterations } as one graph (body_iters even).
 cudaGraphExec_t mg_build_while_graph(const MgDev& m, const MgArgs& a, int body_iters, cudaStream_t s);
 

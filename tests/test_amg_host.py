@@ -542,6 +542,14 @@ def test_device_kernels_emulated(workdir):
     slice_ptr, scol, val = sliced_layout(r["adj_pos"], r["adj"], blocks)
     h = Hierarchy(r["adj_pos"], r["adj"], xy, r["mask"], min_coarse_dofs=150, part_nodes=256)
     assert 3 <= len(h) <= 8 and 3 * h.sizes(len(h) - 1)[0] <= 160
+    # R0 runs one block per range of 256 level-0 nodes: every level-1 node of
+    # range p has its members inside the range
+    pp1 = h.parts(1)
+    mp0 = h.device_maps(0, slice_ptr)
+    assert len(pp1) - 1 == -(-len(xy) // 256)
+    for p_ in range(len(pp1) - 1):
+        mem = mp0["mem"][mp0["mem_pos"][pp1[p_]]:mp0["mem_pos"][pp1[p_ + 1]]]
+        assert mem.min() >= 256 * p_ and mem.max() < 256 * (p_ + 1)
     em = DeviceEmulation(h, slice_ptr, scol, val, r["mask"])
     em.setup()
     # the sliced gather reproduces the host Galerkin product
