@@ -620,7 +620,7 @@ class Hierarchy:
     has 2 DOFs per node, every coarser level 3 per aggregate (its rigid-body
     modes). ``adj_pos`` / ``adj`` are the graph without the nodes themselves
     (``Instance.csr()``'s), ``mask`` 1 per free DOF; ``part_nodes`` > 0 cuts
-    level 0 into node ranges that no aggregate crosses, at any level."""
+    level 0 into node ranges that no level-0 aggregate crosses."""
 
     def __init__(self, adj_pos, adj, xy, mask, min_coarse_dofs=400, part_nodes=0):
         ap = np.ascontiguousarray(adj_pos, np.int32)

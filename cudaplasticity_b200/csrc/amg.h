@@ -13,10 +13,10 @@
 //     are all free starts an aggregate of itself and its neighbours; the rest
 //     join their first aggregated neighbour, or start a singleton), never
 //     across partitions: level 0 may be cut into ranges of part_nodes nodes
-//     (the nodes one thread block owns on the device), and every aggregate
-//     belongs to its members' partition, so restriction and prolongation stay
-//     inside a block at every level; aggregates are numbered partition by
-//     partition;
+//     (the nodes one thread block restricts on the device), and every level-0
+//     aggregate belongs to its members' range; level-1 nodes are numbered
+//     range by range, and level 1's part_pos records where each range's
+//     aggregates lie; coarser levels aggregate without ranges;
 //   - tentative prolongator T_l: for each aggregate, the near-null-space rows
 //     of its members (at level 0 the rigid-body modes about the aggregate's
 //     centroid, with zero rows for prescribed DOFs; at coarser levels the R
@@ -35,7 +35,8 @@ struct Level {
     int n_nodes = 0;  // nodes of this level (level 0: mesh nodes; else aggregates of the level below)
     int fb = 2;       // DOFs per node (2 at level 0, 3 above)
     std::vector<int> adj_pos, adj;  // node graph: row n holds n, then adj[adj_pos[n] .. adj_pos[n+1])
-    std::vector<int> part_pos;      // partition p owns nodes [part_pos[p], part_pos[p+1])
+    std::vector<int> part_pos;      // level 0: range p owns nodes [part_pos[p], part_pos[p+1]); level 1: the
+                                    // aggregates of range p; coarser levels: one range
     // to the next level (empty on the coarsest)
     int n_aggs = 0;
     std::vector<int> agg;           // aggregate of every node

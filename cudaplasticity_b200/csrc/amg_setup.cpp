@@ -11,6 +11,8 @@ namespace amg {
 
 namespace {
 
+constexpr int kMinRange = 16;  // coarse levels: fewest nodes of a range aggregated on its own
+
 // Greedy aggregation of a node graph inside each partition (nodes
 // [part_pos[p], part_pos[p+1]) form partition p; edges between partitions are
 // ignored): pass 1 makes an aggregate of every node whose neighbours are all
@@ -119,8 +121,22 @@ Hierarchy build(int n_nodes, const int* adj_pos, const int* adj, const double* x
         F.block_pos.assign(F.n_nodes + 1, 0);
         for (int i = 0; i < F.n_nodes; ++i) F.block_pos[i + 1] = F.block_pos[i] + 1 + (F.adj_pos[i + 1] - F.adj_pos[i]);
         if (F.n_nodes * fb <= min_coarse_dofs) break;
+        // Level 0 aggregates inside its ranges. A coarser level aggregates
+        // inside the ranges it inherits, merged with their successors until
+        // each holds at least kMinRange nodes: small ranges keep the coarse
+        // aggregates small (gentle coarsening), merging keeps coarsening going.
+        const bool fine = h.levels.size() == 1;
+        std::vector<int> ranges = {0};
+        if (fine) {
+            ranges = F.part_pos;
+        } else {
+            for (size_t p = 1; p < F.part_pos.size(); ++p)
+                if (F.part_pos[p] - ranges.back() >= kMinRange || p + 1 == F.part_pos.size()) ranges.push_back(F.part_pos[p]);
+            if (ranges.size() > 2 && ranges[ranges.size() - 1] - ranges[ranges.size() - 2] < kMinRange)
+                ranges.erase(ranges.end() - 2);  // a short last range joins the one before
+        }
         std::vector<int> agg, cpart;
-        const int na = aggregate(F.n_nodes, F.adj_pos, F.adj, F.part_pos, agg, cpart);
+        const int na = aggregate(F.n_nodes, F.adj_pos, F.adj, ranges, agg, cpart);
         if (na >= F.n_nodes) break;  // no longer shrinking
         F.agg = agg;
         F.n_aggs = na;
@@ -133,7 +149,6 @@ Hierarchy build(int n_nodes, const int* adj_pos, const int* adj, const double* x
             for (int i = 0; i < F.n_nodes; ++i) mem[cur[agg[i]]++] = i;
         }
         // near-null-space rows of level 0: rigid-body modes about the centroid
-        const bool fine = h.levels.size() == 1;
         if (fine) {
             for (int a = 0; a < na; ++a) {
                 double cx = 0.0, cy = 0.0;

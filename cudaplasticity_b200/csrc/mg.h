@@ -20,7 +20,7 @@ struct cp_instance;
 
 namespace cp {
 
-constexpr int kMgMaxLevels = 8;
+constexpr int kMgMaxLevels = 10;
 constexpr int kMgMaxCoarse = 160;  // coarsest DOFs whose inversion runs in shared memory
 constexpr int kMgMinCoarse = 150;  // coarsening stops at this many DOFs
 constexpr int kMgPartNodes = 256;  // level-0 node ranges that no aggregate crosses

@@ -82,13 +82,14 @@ CP_API int cpx_loads_build(const cpx_mesh* m, const cpx_loads* l, double h, doub
  * node; mask: 2 per node, 1 = free DOF. Coarsening stops at
  * min_coarse_dofs DOFs or when a level stops shrinking. Level 0 has 2 DOFs
  * per node, coarser levels 3 (the rigid-body modes of an aggregate).
- * part_nodes > 0 cuts level 0 into ranges of that many nodes; no aggregate
- * crosses a range at any level (0: one range). */
+ * part_nodes > 0 cuts level 0 into ranges of that many nodes that no level-0
+ * aggregate crosses (0: one range); level 1's partition bounds then give the
+ * aggregates of each range, and coarser levels aggregate without ranges. */
 typedef struct cpx_amg cpx_amg;
 CP_API int cpx_amg_build(int node_count, const int* adj_pos, const int* adj, const double* xy,
                          const unsigned char* mask, int min_coarse_dofs, int part_nodes, cpx_amg** out);
 /* Partition bounds of level l: part_pos[p] .. part_pos[p + 1] are the nodes
- * of partition p (n_parts + 1 values). */
+ * of partition p (n_parts + 1 values; one partition from level 2 on). */
 CP_API int cpx_amg_level_parts(const cpx_amg* h, int level, int* n_parts, int* part_pos);
 CP_API int cpx_amg_destroy(cpx_amg* h);
 CP_API int cpx_amg_levels(const cpx_amg* h, int* n_levels);

@@ -79,6 +79,19 @@ def mgs(B):
     return B, R
 
 
+def merged_ranges(part_pos, min_range=16):
+    """A coarse level aggregates inside its inherited ranges, each merged with
+    its successors until it holds at least min_range nodes (a short last
+    range joins the one before)."""
+    out = [0]
+    for p in range(1, len(part_pos)):
+        if part_pos[p] - out[-1] >= min_range or p + 1 == len(part_pos):
+            out.append(part_pos[p])
+    if len(out) > 2 and out[-1] - out[-2] < min_range:
+        del out[-2]
+    return np.array(out)
+
+
 def restate(adj_pos, adj, xy, mask, min_coarse_dofs, part_nodes=0):
     """Levels as dicts (graph, partitions, aggregates, prolongator blocks)."""
     levels = []
@@ -90,7 +103,7 @@ def restate(adj_pos, adj, xy, mask, min_coarse_dofs, part_nodes=0):
         levels.append(lev)
         if n * fb <= min_coarse_dofs:
             break
-        agg, na, cpart = aggregate(lev["adj_pos"], lev["adj"], part_pos)
+        agg, na, cpart = aggregate(lev["adj_pos"], lev["adj"], part_pos if fb == 2 else merged_ranges(part_pos))
         if na >= n:
             break
         if ns is None:  # rigid-body modes about each aggregate's centroid
@@ -213,12 +226,18 @@ def test_partitioned_aggregates_stay_inside(workdir):
     xy = np.asarray(m["node_xy"], np.float64).reshape(-1, 2)
     h = Hierarchy(r["adj_pos"], r["adj"], xy, r["mask"], min_coarse_dofs=40, part_nodes=32)
     assert len(h.parts(0)) - 1 == -(-len(xy) // 32)
-    for lv in range(len(h) - 1):
-        lev, pp, cp_ = h.level(lv), h.parts(lv), h.parts(lv + 1)
-        assert len(pp) == len(cp_)
-        for p in range(len(pp) - 1):
-            a = lev["agg"][pp[p]:pp[p + 1]]
-            assert a.min() >= cp_[p] and a.max() < cp_[p + 1]
+    lev, pp, cp_ = h.level(0), h.parts(0), h.parts(1)
+    assert len(pp) == len(cp_)
+    for p in range(len(pp) - 1):
+        a = lev["agg"][pp[p]:pp[p + 1]]
+        assert a.min() >= cp_[p] and a.max() < cp_[p + 1]
+    for lv in range(1, len(h) - 1):
+        # coarser levels: no aggregate crosses the merged inherited ranges
+        lev, rg = h.level(lv), merged_ranges(h.parts(lv))
+        for p in range(len(rg) - 1):
+            a = lev["agg"][rg[p]:rg[p + 1]]
+            if p + 1 < len(rg) - 1:
+                assert a.max() < lev["agg"][rg[p + 1]]
 
 
 def test_prolongator_properties(workdir):
