@@ -745,9 +745,11 @@ def main():
     ap.add_argument("--batched-probe", type=int, nargs=2, metavar=("N", "TRIPS"),
                     help="profiling aid: N resident batch-stream instances, TRIPS graph trips, then exit")
     ap.add_argument("--precond", type=int, default=SOLVE_KW["precond"], choices=[0, 1, 2],
-                    help="linear solver of the headline: 0 CG, 1 block-Jacobi PCG, 2 multigrid PCG")
+                    help="linear solver of the headline and of the FP64 served arm: 0 CG, 1 block-Jacobi PCG, "
+                         "2 multigrid PCG")
     args = ap.parse_args()
     SOLVE_KW["precond"] = args.precond
+    FP64_SERVE_KW["precond"] = args.precond
     if args.batched_probe:
         batched_probe(*args.batched_probe)
         return

@@ -14,7 +14,12 @@ Cases (each prints one JSON line with its host-side facts):
   (run with CUPLAST_FP64_CG=fused CUPLAST_NO_GRAPH=1 so that every launch is
   visible to the profiler);
 * ``cg_large``   -- k_cg_p / k_cg_u on the 2.1M-DOF plate, R iterations
-  (cp_bench_cg).
+  (cp_bench_cg);
+* ``cg_mg``      -- the multigrid-preconditioned solve (cp_solve_opts.precond
+  2: set-up kernels, then k_mg_p / k_mg_u / k_mg_restrict0 /
+  k_mg_coarse_cycle / k_mg_smooth0 per iteration) of the 64x64 plate from
+  zero, R linear solves;
+* ``cg_mg_large`` -- the same on the 2.1M-DOF plate, one linear solve to 1e-6.
 
 The inputs are the benchmark's (bilinear steel, top traction), built the
 same way; nothing here is timed for a report.
@@ -46,12 +51,23 @@ def _instance(ctx, n_circ4, rad_n):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("case", choices=["assemble", "update", "cg_cluster", "cg_graph", "cg_large"])
+    ap.add_argument("case", choices=["assemble", "update", "cg_cluster", "cg_graph", "cg_large", "cg_mg", "cg_mg_large"])
     ap.add_argument("--repeat", type=int, default=3)
     a = ap.parse_args(argv)
     ctx = Context(0)
     out = {"case": a.case}
-    if a.case in ("assemble", "update", "cg_large"):
+    if a.case in ("cg_mg", "cg_mg_large"):
+        inst = _instance(ctx, 16, 64) if a.case == "cg_mg" else _instance(ctx, 256, 1024)
+        n_nodes = inst.sizes()[0]
+        reps = []
+        for _ in range(a.repeat if a.case == "cg_mg" else 1):
+            inst.set_field("uv", np.zeros(2 * n_nodes))
+            reps.append(inst.solve(cg_tol=1e-10 if a.case == "cg_mg" else 1e-6, outer_tol=1e300, max_outer=1,
+                                   levels=1, precond=2, max_cg=100000))
+        out.update(nodes=n_nodes, cg_iters=[r["cg_iters"] for r in reps], rel_res=reps[-1]["cg_rel_res"],
+                   seconds=[r["seconds"] for r in reps], launches=reps[-1]["kernel_launches"])
+        inst.close()
+    elif a.case in ("assemble", "update", "cg_large"):
         inst = _instance(ctx, 256, 1024)
         n_nodes, n_elem, nnz, _ = inst.sizes()
         out.update(nodes=n_nodes, elements=n_elem, nnz=nnz)
