@@ -530,6 +530,15 @@ def run_product_arm(args):
                                                       ctypes.byref(mu), ctypes.byref(bp), ctypes.byref(bu)))
         return mp.value, mu.value, bp.value, bu.value
 
+    def bench_mg(instance, iters):
+        """Per-part timings of the multigrid PCG (cp_bench_mg): P, U, R0, the
+        coarse levels, S0 per iteration and the per-outer-iteration set-up."""
+        ms, by = (ctypes.c_double * 6)(), (ctypes.c_double * 6)()
+        instance.ctx.check(cp._capi.lib().cp_bench_mg(instance._h, iters, ms, by))
+        names = ["P", "U", "R0", "coarse", "S0", "setup"]
+        return {k: {"ms": ms[i], "bytes": by[i], "gbs": by[i] / (ms[i] * 1e-3) / 1e9,
+                    "frac": by[i] / (ms[i] * 1e-3) / 1e9 / peak} for i, k in enumerate(names)}
+
     # this workload's own CG: each linear solve is one k_c_solve launch (the
     # whole CG inside one thread-block cluster, matrix and records in shared
     # memory). Time per CG iteration from one elastic PCG solve from zero
@@ -586,6 +595,13 @@ def run_product_arm(args):
     except cp.CuplastError as exc:  # an auxiliary figure: report the failure, keep the line
         big_nodes = binst.sizes()[0]
         throughput["assembly_error"] = str(exc)
+    mg_parts = None
+    if SOLVE_KW["precond"] == 2:
+        try:
+            binst.set_field("uv", np.zeros_like(brp))
+            mg_parts = {"plate_2.1M_dof": bench_mg(binst, 20)}
+        except cp.CuplastError as exc:  # an auxiliary figure: report the failure, keep the line
+            mg_parts = {"error": str(exc)}
     binst.close()
     mp, mu, bp, bu = rows["fp64"]
     throughput["dof_iterations_per_s_2M"] = 2 * big_nodes / ((mp + mu) * 1e-3)
@@ -627,7 +643,7 @@ def run_product_arm(args):
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches), "roofline": roofline, "roofline_this_workload": roof_small,
-            "cg_large_mesh": cg_large, "cpu_baseline": cpu, "clocks": clocks.summary(),
+            "cg_large_mesh": cg_large, "multigrid_parts": mg_parts, "cpu_baseline": cpu, "clocks": clocks.summary(),
             "accuracy_vs_tight_fp64": accuracy, "batched": batched, "roofline_batched": roof_batched,
             "served": served,
             "throughput": dict(throughput, dof_iterations_per_s_headline=2 * arrays["node_xy"].shape[0] *

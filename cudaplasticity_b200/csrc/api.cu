@@ -325,8 +325,7 @@ void cg_fp64_fused(cp_instance* I, double eps, long long max_iter, int precond) 
 
 // FP64 CG preconditioned by one aggregation-multigrid V-cycle (mg.cu), from
 // the current u: coarse operators from the current K, then the PCG loop.
-void cg_fp64_mg(cp_instance* I, double eps, long long max_iter) {
-    cp::mg_prepare(I);
+cp::MgArgs mg_args(cp_instance* I) {
     cp::MgArgs a;
     a.n = I->n_nodes;
     a.sm_count = I->sms();
@@ -343,6 +342,12 @@ void cg_fp64_mg(cp_instance* I, double eps, long long max_iter) {
     a.p1 = I->z64b;
     a.sc = I->sc;
     a.partials = I->partials;
+    return a;
+}
+
+void cg_fp64_mg(cp_instance* I, double eps, long long max_iter) {
+    cp::mg_prepare(I);
+    const cp::MgArgs a = mg_args(I);
     const int body = std::max(2, I->body_iters + (I->body_iters & 1));
     I->launches += cp::mg_launch_setup(I->mg, a, I->s());
     if (I->use_graph && !I->gmg) I->gmg = cp::mg_build_while_graph(I->mg, a, body, I->s());
@@ -885,6 +890,43 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
     if (rep) *rep = R;
     if (rc != CP_OK) return rc;
     return R.status;
+}
+
+CP_API int cp_bench_mg(cp_instance* I, int iters, double* ms, double* bytes) {
+    if (I && I->in_batch) return CP_ERR_BUSY;
+    if (!I || iters <= 0 || !ms) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        CP_CHECK(I->loads_set, CP_ERR_INVALID, "loads not set");
+        cudaStream_t s = I->s();
+        assemble(I, CP_PREC_FP64);
+        cp::mg_prepare(I);
+        const cp::MgArgs a = mg_args(I);
+        std::vector<cudaEvent_t> ev(6 * (size_t)iters + 2);
+        for (auto& e : ev) CP_CUDA(cudaEventCreate(&e));
+        CP_CUDA(cudaEventRecord(ev[0], s));
+        cp::mg_launch_setup(I->mg, a, s);
+        CP_CUDA(cudaEventRecord(ev[1], s));
+        // a tolerance no iteration reaches, so every kernel does its work
+        cp::mg_launch_start(I->mg, a, 0.0, (long long)iters + 8, s);
+        for (int it = 0; it < iters; ++it) cp::mg_launch_iteration(I->mg, a, it & 1, s, &ev[2 + 6 * (size_t)it]);
+        CP_CUDA(cudaEventSynchronize(ev.back()));
+        double t[5] = {0, 0, 0, 0, 0};
+        for (int it = 0; it < iters; ++it)
+            for (int k = 0; k < 5; ++k) {
+                float x = 0;
+                CP_CUDA(cudaEventElapsedTime(&x, ev[2 + 6 * (size_t)it + k], ev[2 + 6 * (size_t)it + k + 1]));
+                t[k] += x;
+            }
+        float su = 0;
+        CP_CUDA(cudaEventElapsedTime(&su, ev[0], ev[1]));
+        for (auto& e : ev) cudaEventDestroy(e);
+        CP_CUDA(cudaMemcpy(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost));
+        CP_CHECK(I->sc_h->status == 0 && I->sc_h->iter == iters, CP_ERR_BREAKDOWN,
+                 "multigrid bench: the iterations stopped early");
+        for (int k = 0; k < 5; ++k) ms[k] = t[k] / iters;
+        ms[5] = su;
+        if (bytes) cp::mg_algorithmic_bytes(I->mg, a, I->csr.nadj + I->n_nodes, bytes);
+    });
 }
 
 CP_API int cp_bench_cg(cp_instance* I, int precision, int precond, int iters, double* ms_p, double* ms_u,

@@ -632,12 +632,14 @@ constexpr int kMgOneBlockNodes = 4096;
 
 bool one_block_coarse(const MgDev& m) { return m.L >= 3 && m.lv[1].n <= kMgOneBlockNodes; }
 
-// The V-cycle from U's y0 to S0's z.
-int launch_vcycle(const MgDev& m, const MgArgs& a, cudaStream_t s) {
+// The V-cycle from U's y0 to S0's z, in three parts: R0, the coarse levels,
+// S0. `ev` (optional): events recorded after R0 and after the coarse levels.
+int launch_vcycle(const MgDev& m, const MgArgs& a, cudaStream_t s, cudaEvent_t* ev = nullptr) {
     const int L = m.L;
     const int sms = a.sm_count;
     const int parts = (a.n + kMgPartNodes - 1) / kMgPartNodes;
     k_mg_restrict0<<<parts, kMgPartNodes, 0, s>>>(a, m.lv[0], m.lv[1], m.lam, m.omega, L == 2);
+    if (ev) CP_CUDA(cudaEventRecord(ev[0], s));
     int launches = 1;
     if (one_block_coarse(m)) {
         k_mg_coarse_cycle<<<1, 1024, 0, s>>>(m, a.sc);
@@ -651,6 +653,7 @@ int launch_vcycle(const MgDev& m, const MgArgs& a, cudaStream_t s) {
             k_mg_smooth<<<grid_small(m.lv[l].n, sms), kSmall, 0, s>>>(m.lv[l], m.lv[l + 1], m.lam, l, m.omega, a.sc);
         launches += 2 * (L - 2) + 1;
     }
+    if (ev) CP_CUDA(cudaEventRecord(ev[1], s));
     k_mg_smooth0<<<grid_nodes(a), kThreads, 0, s>>>(a, m.lv[0], m.lv[1], m.lam, m.omega);
     CP_CUDA(cudaGetLastError());
     return launches + 1;
@@ -692,11 +695,41 @@ int mg_launch_start(const MgDev& m, const MgArgs& a, double eps2, long long max_
     return 1 + launch_vcycle(m, a, s);
 }
 
-int mg_launch_iteration(const MgDev& m, const MgArgs& a, int parity, cudaStream_t s) {
+int mg_launch_iteration(const MgDev& m, const MgArgs& a, int parity, cudaStream_t s, cudaEvent_t* ev) {
+    if (ev) CP_CUDA(cudaEventRecord(ev[0], s));
     k_mg_p<<<grid_nodes(a), kThreads, 0, s>>>(a, m.lv[0], parity);
+    if (ev) CP_CUDA(cudaEventRecord(ev[1], s));
     k_mg_u<<<grid_nodes(a), kThreads, 0, s>>>(a, m.lv[0], m.lam, m.omega, parity);
+    if (ev) CP_CUDA(cudaEventRecord(ev[2], s));
     CP_CUDA(cudaGetLastError());
-    return 2 + launch_vcycle(m, a, s);
+    const int n = 2 + launch_vcycle(m, a, s, ev ? ev + 3 : nullptr);
+    if (ev) CP_CUDA(cudaEventRecord(ev[5], s));
+    return n;
+}
+
+void mg_algorithmic_bytes(const MgDev& m, const MgArgs& a, long long blocks0, double* bytes) {
+    // FP64 values; a level-0 block is 32 bytes of values and a 4-byte column,
+    // a coarse block 72 bytes and a 4-byte column; vectors counted once each.
+    const double n = a.n, K0 = 36.0 * (double)blocks0, n1 = m.lv[1].n;
+    bytes[0] = K0 + 64 * n;                                // P: K, z, p; p', q
+    bytes[1] = 146 * n;                                    // U: p, q, x, r, mask, D0^-1; x, r, y0
+    bytes[2] = K0 + 90 * n + 124 * n1;                     // R0: K, y0, r, mask, T0, members; b1, y1, D1^-1
+    double c = 0.0;
+    for (int l = 1; l + 1 < m.L; ++l) {                    // restriction and sweep of every coarse level
+        const double nl = m.lv[l].n, bl = m.lv[l].nb;
+        c += 2 * 76 * bl + nl * (48 + 72 + 4 + 72 + 24 + 24) + 48.0 * m.lv[l + 1].n;
+    }
+    c += 8.0 * m.nc * m.nc + 16.0 * m.nc;                  // the coarsest inverse times b_c
+    bytes[3] = c;
+    bytes[4] = K0 + 134 * n + 24 * n1;                     // S0: K, y0, T0, agg, e1, r, mask, D0^-1; z
+    double su = K0 + 2 * n + 32 * n;                       // diag0: K, mask; D0^-1
+    for (int l = 0; l + 1 < m.L; ++l) {
+        const double fb = l == 0 ? 36.0 : 76.0, bl = m.lv[l].nb;
+        su += fb * bl + 16 * bl + 4.0 * (m.lv[l + 1].nb + 1) + 72.0 * m.lv[l + 1].nb;  // Galerkin: blocks, map; A_{l+1}
+        if (l + 1 < m.L - 1) su += 76.0 * m.lv[l + 1].nb + 72.0 * m.lv[l + 1].n;       // diag: A, D^-1
+    }
+    su += 2 * 8.0 * m.nc * m.nc;                           // the coarsest inverse, written once
+    bytes[5] = su;
 }
 
 cudaGraphExec_t mg_build_while_graph(const MgDev& m, const MgArgs& a, int body_iters, cudaStream_t s) {

@@ -80,8 +80,12 @@ struct MgArgs {
 int mg_launch_setup(const MgDev& m, const MgArgs& a, cudaStream_t s);
 // r = m.(b - K x), the first V-cycle and the scalars of a solve.
 int mg_launch_start(const MgDev& m, const MgArgs& a, double eps2, long long max_iter, cudaStream_t s);
-// One PCG iteration (search direction, update, V-cycle).
-int mg_launch_iteration(const MgDev& m, const MgArgs& a, int parity, cudaStream_t s);
+// One PCG iteration (search direction, update, V-cycle). `ev` (optional, 6
+// events): recorded before P and after P, U, R0, the coarse levels and S0.
+int mg_launch_iteration(const MgDev& m, const MgArgs& a, int parity, cudaStream_t s, cudaEvent_t* ev = nullptr);
+// Algorithmic bytes per launch of P, U, R0, the coarse levels (all of their
+// kernels), S0 and the per-outer-iteration set-up (all of its kernels).
+void mg_algorithmic_bytes(const MgDev& m, const MgArgs& a, long long blocks0, double* bytes);
 // Kernels launched by one iteration.
 int mg_launches_per_iteration(const MgDev& m);
 // while (!converged) { body_iters iterations } as one graph (body_iters even).

@@ -19,7 +19,9 @@ Cases (each prints one JSON line with its host-side facts):
   2: set-up kernels, then k_mg_p / k_mg_u / k_mg_restrict0 /
   k_mg_coarse_cycle / k_mg_smooth0 per iteration) of the 64x64 plate from
   zero, R linear solves;
-* ``cg_mg_large`` -- the same on the 2.1M-DOF plate, one linear solve to 1e-6.
+* ``cg_mg_large`` -- the same on the 2.1M-DOF plate, one linear solve to 1e-6;
+* ``mg_parts``   -- cp_bench_mg on the 2.1M-DOF plate: the set-up once, then
+  R iterations with CUDA events around P, U, R0, the coarse levels and S0.
 
 The inputs are the benchmark's (bilinear steel, top traction), built the
 same way; nothing here is timed for a report.
@@ -51,12 +53,20 @@ def _instance(ctx, n_circ4, rad_n):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("case", choices=["assemble", "update", "cg_cluster", "cg_graph", "cg_large", "cg_mg", "cg_mg_large"])
+    ap.add_argument("case", choices=["assemble", "update", "cg_cluster", "cg_graph", "cg_large", "cg_mg", "cg_mg_large", "mg_parts"])
     ap.add_argument("--repeat", type=int, default=3)
     a = ap.parse_args(argv)
     ctx = Context(0)
     out = {"case": a.case}
-    if a.case in ("cg_mg", "cg_mg_large"):
+    if a.case == "mg_parts":
+        inst = _instance(ctx, 256, 1024)
+        ms, by = (ctypes.c_double * 6)(), (ctypes.c_double * 6)()
+        inst.set_field("uv", np.zeros(2 * inst.sizes()[0]))
+        ctx.check(C.lib().cp_bench_mg(inst._h, a.repeat, ms, by))
+        out.update(nodes=inst.sizes()[0], parts=["P", "U", "R0", "coarse", "S0", "setup"], ms=list(ms),
+                   bytes=list(by))
+        inst.close()
+    elif a.case in ("cg_mg", "cg_mg_large"):
         inst = _instance(ctx, 16, 64) if a.case == "cg_mg" else _instance(ctx, 256, 1024)
         n_nodes = inst.sizes()[0]
         reps = []

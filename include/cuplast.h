@@ -194,6 +194,14 @@ CP_API int cp_bench_cg(cp_instance* inst, int precision, int precond, int iters,
  * for CP_PREC_MIXED), the connectivity, E_c and nu_c of every element, the
  * incidence codes and slot bytes, and the node coordinates once. */
 CP_API int cp_bench_assemble(cp_instance* inst, int precision, int iters, double* ms, double* bytes);
+/* Measurement entry point of the multigrid PCG (precond 2): assembles K from
+ * the current secant moduli, runs the per-outer-iteration set-up once and
+ * `iters` PCG iterations as direct launches, with CUDA events around each
+ * part. ms[0..4]: mean duration of P, U, R0, the coarse levels (all of their
+ * kernels) and S0 per iteration; ms[5]: the set-up. bytes[0..5] (may be
+ * NULL): the algorithmic bytes each part moves (FP64 values, vectors counted
+ * once). Leaves uv changed. */
+CP_API int cp_bench_mg(cp_instance* inst, int iters, double* ms, double* bytes);
 
 /* Allocation-free secant update (no counterpart in the reference). For
  * callers that cannot allocate device memory -- code running while a CUDA
