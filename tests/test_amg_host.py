@@ -587,3 +587,35 @@ def test_device_kernels_emulated(workdir):
     A0 = (sp.diags(fm) @ em.K @ sp.diags(fm) + sp.diags(1 - fm)).tocsr()
     _, it_bj = _pcg(A0, b, lambda v: em.dinv[0] @ v + np.where(free, 0.0, v))
     assert it * 5 < it_bj, (it, it_bj)
+
+
+@pytest.mark.parametrize("nodes,edges,fixed", [
+    (4, [(0, 1), (1, 2), (2, 3), (3, 0), (0, 2), (1, 3)], ()),   # one 4-node element
+    (5, [(0, 1), (1, 2), (2, 3), (3, 0), (0, 2), (1, 3)], ()),   # plus an isolated node
+    (4, [(0, 1), (1, 2), (2, 3), (3, 0), (0, 2), (1, 3)], tuple(range(8))),  # every DOF prescribed
+    (3, [(0, 1), (1, 2), (0, 2)], (0, 1)),                        # one triangle, one node fixed
+])
+def test_tiny_graphs_coarsen(nodes, edges, fixed):
+    """The fallback the solver takes for meshes at or below the coarse size
+    (min_coarse_dofs 0: coarsen while the graph shrinks) gives at least two
+    levels with consistent maps, and zero prolongator rows on prescribed DOFs."""
+    nb = [[] for _ in range(nodes)]
+    for a, b in edges:
+        nb[a].append(b)
+        nb[b].append(a)
+    adj_pos = np.concatenate([[0], np.cumsum([len(x) for x in nb])]).astype(np.int32)
+    adj = np.array([j for x in nb for j in x] or [0], np.int32)[:adj_pos[-1]]
+    xy = np.random.default_rng(nodes).uniform(size=(nodes, 2))
+    mask = np.ones(2 * nodes, np.uint8)
+    mask[list(fixed)] = 0
+    h = Hierarchy(adj_pos, adj, xy, mask, min_coarse_dofs=0, part_nodes=256)
+    assert len(h) >= 2
+    lev = h.level(0)
+    T = lev["T"].reshape(-1, 3)
+    assert np.all(T[mask == 0] == 0)
+    for lv in range(len(h) - 1):
+        maps = h.device_maps(lv, np.array([0, 32 * (max(len(x) for x in nb) + 1)], np.int32))
+        assert maps["mem_pos"][-1] == h.sizes(lv)[0]
+        assert maps["gal_pos"][-1] == h.sizes(lv)[2]
+        coarse = h.galerkin(lv, np.ones((h.sizes(lv)[2], h.sizes(lv)[1], h.sizes(lv)[1])))
+        assert np.all(np.isfinite(coarse))
