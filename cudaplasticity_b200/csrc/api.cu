@@ -345,10 +345,23 @@ cp::MgArgs mg_args(cp_instance* I) {
     return a;
 }
 
-void cg_fp64_mg(cp_instance* I, double eps, long long max_iter) {
+int mg_body(const cp_instance* I) { return std::max(2, I->body_iters + (I->body_iters & 1)); }
+
+// Kernel count of the WHILE graph once sc_h holds the solve's scalars.
+void mg_count_graph_launches(cp_instance* I) {
+    const int body = mg_body(I);
+    const long long trips = std::max<long long>(1, (I->sc_h->iter + body - 1) / body);
+    I->launches += trips * (body * (long long)cp::mg_launches_per_iteration(I->mg) + 1);
+}
+
+// defer (graph loop only): enqueue the scalars' copy to sc_h and return
+// without waiting; the caller synchronises later (after the secant update,
+// which then follows the solve on the stream with no host round trip in
+// between) and calls mg_count_graph_launches.
+void cg_fp64_mg(cp_instance* I, double eps, long long max_iter, bool defer = false) {
     cp::mg_prepare(I);
     const cp::MgArgs a = mg_args(I);
-    const int body = std::max(2, I->body_iters + (I->body_iters & 1));
+    const int body = mg_body(I);
     I->launches += cp::mg_launch_setup(I->mg, a, I->s());
     if (I->use_graph && !I->gmg) I->gmg = cp::mg_build_while_graph(I->mg, a, body, I->s());
     I->launches += cp::mg_launch_start(I->mg, a, eps * eps, max_iter, I->s());
@@ -356,9 +369,9 @@ void cg_fp64_mg(cp_instance* I, double eps, long long max_iter) {
     if (I->use_graph) {
         CP_CUDA(cudaGraphLaunch(I->gmg, I->s()));
         CP_CUDA(cudaMemcpyAsync(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost, I->s()));
+        if (defer) return;
         CP_CUDA(cudaStreamSynchronize(I->s()));
-        const long long trips = std::max<long long>(1, (I->sc_h->iter + body - 1) / body);
-        I->launches += trips * (body * per_iter + 1);
+        mg_count_graph_launches(I);
         return;
     }
     for (;;) {
@@ -823,7 +836,11 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
                 if (!boost && o.adaptive_cg == 1 && rel_err > 10.0 * o.outer_tol) eps = std::max(o.cg_tol, 1e-2 * rel_err);
                 if (!boost && o.adaptive_cg == 2 && rel_err > o.outer_tol) eps = std::max(o.cg_tol, 1e-1 * rel_err);
                 assemble(I, prec);
-                if (prec == CP_PREC_FP64) {
+                // the multigrid graph loop leaves its scalars for after the update
+                const bool mg_deferred = prec == CP_PREC_FP64 && o.precond == 2 && I->use_graph;
+                if (mg_deferred) {
+                    cg_fp64_mg(I, eps, o.max_cg, true);
+                } else if (prec == CP_PREC_FP64) {
                     if (o.precond == 2) cg_fp64_mg(I, eps, o.max_cg);
                     else cg_fp64(I, eps, o.max_cg, o.precond ? 1 : 0);
                     R.cg_iters += I->sc_h->iter;
@@ -838,6 +855,12 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
                 I->launches += 1;
                 CP_CUDA(cudaMemcpyAsync(I->osc_h, I->osc, sizeof(cp::OuterScalars), cudaMemcpyDeviceToHost, s));
                 CP_CUDA(cudaStreamSynchronize(s));
+                if (mg_deferred) {
+                    mg_count_graph_launches(I);
+                    R.cg_iters += I->sc_h->iter;
+                    R.cg_rel_res = std::sqrt(I->sc_h->rr * I->sc_h->normB_inv);
+                    if (I->sc_h->status == CP_ERR_BREAKDOWN) throw Error{CP_ERR_BREAKDOWN, "CG broke down"};
+                }
                 rel_err = I->osc_h->rel_err;
                 R.outer_iters += 1;
                 CP_CHECK(std::isfinite(rel_err), CP_ERR_BREAKDOWN, "secant iteration produced NaN");
