@@ -70,6 +70,7 @@ struct cp_instance {
     bool mg_ready = false;
     cp::MgDev mg;
     std::vector<void*> mg_allocs;
+    size_t mg_bytes = 0;  // the part of `bytes` the hierarchy holds
     cudaGraphExec_t gmg = nullptr;
     long long launches = 0;  // kernels launched (graph nodes included)
     int last_assembly = -1;  // precision of the last assembly

@@ -768,6 +768,7 @@ T* mg_alloc(cp_instance* I, size_t count) {
     CP_CUDA(cudaMallocAsync(&p, nb, I->s()));
     I->mg_allocs.push_back(p);
     I->bytes += nb;
+    I->mg_bytes += nb;
     return static_cast<T*>(p);
 }
 
@@ -785,6 +786,8 @@ void mg_release(cp_instance* I) {
     I->gmg = nullptr;
     for (void* p : I->mg_allocs) cudaFreeAsync(p, I->s());
     I->mg_allocs.clear();
+    I->bytes -= I->mg_bytes;
+    I->mg_bytes = 0;
     I->mg = MgDev{};
     I->mg_ready = false;
 }
