@@ -781,6 +781,17 @@ T* mg_upload(cp_instance* I, const std::vector<T>& v) {
 
 }  // namespace
 
+size_t mg_footprint(size_t n, size_t blocks) {
+    // level 0: D0^-1, y, z, T0, aggregate, member (128 per node); one map
+    // entry per block (16). Coarse levels: 3x3 values, column, map entry per
+    // block (92) and D^-1, T, b, y, z, aggregate, member, ranges per node
+    // (about 300), a geometric series of at most twice level 1, which has at
+    // most half the nodes and blocks of level 0. The coarsest inverse and its
+    // scratch: at most 2 x 4096^2 doubles, counted as 1 MB (nc <= 160 here
+    // in practice, 0.2 MB).
+    return 128 * n + 16 * blocks + 2 * (300 * (n / 2) + 92 * (blocks / 2)) + (1u << 20);
+}
+
 void mg_release(cp_instance* I) {
     if (I->gmg) cudaGraphExecDestroy(I->gmg);
     I->gmg = nullptr;

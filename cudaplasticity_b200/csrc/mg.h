@@ -91,6 +91,11 @@ int mg_launches_per_iteration(const MgDev& m);
 // while (!converged) { body_iters iterations } as one graph (body_iters even).
 cudaGraphExec_t mg_build_while_graph(const MgDev& m, const MgArgs& a, int body_iters, cudaStream_t s);
 
+// Upper estimate of the device bytes a hierarchy adds to an instance of
+// n_nodes nodes and `blocks` level-0 blocks (nodes + graph edges): level 0's
+// maps and vectors, and coarse levels of at most half the nodes each time.
+size_t mg_footprint(size_t n_nodes, size_t blocks);
+
 // Builds the hierarchy of an instance (host set-up, uploaded once) unless the
 // one it holds was built for the same Dirichlet mask; mg_release frees it.
 void mg_prepare(cp_instance* I);

@@ -490,6 +490,11 @@ CP_API int cp_server_submit(cp_server* s, const cp_mesh_view* mv, const cp_mater
     r->opts = *opts;
     int rc = cp_instance_footprint(mv, opts->precision, &r->footprint);
     if (rc != CP_OK) return rc;
+    if (opts->precond == 2) {  // the multigrid hierarchy, built at the request's first solve
+        // directed neighbour links: at most n_en (n_en - 1) per element
+        const size_t links = 6 * (size_t)mv->count3 + 12 * (size_t)mv->count4 + 56 * (size_t)mv->count8;
+        r->footprint += cp::mg_footprint((size_t)mv->node_count, (size_t)mv->node_count + links);
+    }
     const size_t reserve = (size_t)(s->o.hbm_reserve * (double)s->total_mem);
     std::lock_guard<std::mutex> lock(s->mu);
     if (s->stop) return CP_ERR_CANCELLED;
