@@ -276,11 +276,12 @@ def batched_leg(ctx, window_s=20.0, warm_s=3.0, slots=512, pool_size=768, seed=2
     }
 
 
-def compare_leg(ctx, n_requests, max_outer=100, seed=20261203, lanes=8):
+def compare_leg(ctx, n_requests, max_outer=100, seed=20261203, lanes=8, mg=True):
     """Like for like: the plain FP64 drop-in solves the first n requests of
     the batch stream (DOF 2k-200k) one at a time; the batched mixed-precision engine
     then solves exactly the same requests (fresh instances) to completion, and
-    so does the solve service's FP64 lanes.
+    so does the solve service's FP64 lanes, once with the block-Jacobi PCG of
+    the plain run and (mg) once with the multigrid-preconditioned CG.
     Same solver options and caps for both, wall clock for both, and the error
     of each mixed-precision result against its FP64 result. Requests that hit
     the outer cap count as solved by both (same cap) and are listed."""
@@ -371,6 +372,31 @@ def compare_leg(ctx, n_requests, max_outer=100, seed=20261203, lanes=8):
     fixed["fp64_lanes"] = {"lanes": lanes, "seconds": t_lanes, "solves_per_s": len(ids) / t_lanes,
                            "statuses": sorted(lane_status), "identical_to_plain": bool(same),
                            "speedup_vs_plain": t_plain / t_lanes}
+    if mg:
+        # and once more with the multigrid-preconditioned CG on the lanes: the
+        # same fixed point, reached through other iterates (error stated)
+        srv = cp.Server(fp64_lanes=lanes)
+        mkw = {k: v for k, v in kw.items() if k != "inner_tol"}
+        mkw["precond"] = 2
+        t1 = time.perf_counter()
+        rids = {i: srv.submit(ws[i]["mesh"], ws[i]["material"], ws[i]["rp"], ws[i]["mask"], ws[i]["uv"],
+                              levels=1, precision=cp.CP_PREC_FP64, **mkw) for i in ids}
+        mg_status, mg_errs, mg_cg = set(), {"uv": 0.0, "sig_i": 0.0, "eps_p_i": 0.0}, 0
+        for i in ids:
+            inst, rep, _ = srv.wait(rids[i], timeout=-1.0)
+            mg_status.add(rep["status"])
+            mg_cg += rep["cg_iters"]
+            st = inst.state()
+            for f in mg_errs:
+                nrm = np.linalg.norm(plain[i][0][f])
+                mg_errs[f] = max(mg_errs[f], float(np.linalg.norm(st[f] - plain[i][0][f]) / nrm) if nrm > 0 else 0.0)
+            inst.close()
+        t_mg = time.perf_counter() - t1
+        srv.close()
+        fixed["fp64_lanes_multigrid"] = {"lanes": lanes, "seconds": t_mg, "solves_per_s": len(ids) / t_mg,
+                                         "statuses": sorted(mg_status), "cg_iters": mg_cg,
+                                         "plain_cg_iters": sum(plain[i][1]["cg_iters"] for i in ids),
+                                         "max_rel_err_vs_plain": mg_errs, "speedup_vs_plain": t_plain / t_mg}
     return fixed
 
 
