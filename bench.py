@@ -66,10 +66,26 @@ def build_problem():
     return mesh, mesh.arrays(), mat, rp, mask, uv
 
 
+def reference_mesh():
+    """The same O-grid for the CPU arms, from the numpy restatement of the
+    reference's generator (tests/meshgen.py; digest-pinned to
+    Mesh::genRectWithHole), so that the reference arm maps no product code."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import meshgen
+
+    return meshgen.hole_plate(-100.0, 100.0, -100.0, 100.0, 20.0, 16, 16, rad_n=64)
+
+
 def reference_job_lines(mesh_path):
     return ["mode phases", f"mesh file {mesh_path}", "levels 10", "cg_eps 1e-10", "outer_eps 1e-6",
             "max_outer 100000", "diagram linear 210000 250 2000", "material 210000 0.3 1", "force 2 0 200 0",
             "fixborderhor 0", "fixpoint -100 -100"]
+
+
+def line_config(world):
+    """The `config` of both arms' lines (identical for the same N)."""
+    return dict(WORKLOAD, parallelism=f"replicas x{world}",
+                l2="GPU arm: 512 MB written between steps (L2 flushed); CPU arm: no flush")
 
 
 def dist_env():
@@ -131,19 +147,24 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def cpu_baseline_run(threads=None):
+def cpu_baseline_run(threads=None, first_level_only=False):
     """The reference's own CPU path on the same job (oracle/_ref/cpref), or the
-    oracle restatement where the reference could not be built."""
+    oracle restatement where the reference could not be built. With
+    first_level_only, the job's first load increment alone (20 MPa, one
+    level): the warm-up of the reference arm."""
     import tempfile
 
     import oracle
 
     threads = threads or os.cpu_count()
-    mesh, arrays, _, _, _, _ = build_problem()
+    arrays = reference_mesh()
     with tempfile.TemporaryDirectory() as d:
         path = os.path.join(d, "m.bin")
         oracle.write_mesh(path, arrays["node_xy"], elem4=arrays["elem4"], borders=arrays["borders"])
         lines = reference_job_lines(path)
+        if first_level_only:
+            lines = [("levels 1" if ln.startswith("levels") else "force 2 0 20 0" if ln.startswith("force") else ln)
+                     for ln in lines]
         t0 = time.perf_counter()
         if oracle.have_reference():
             r = oracle.run_reference(lines, threads=threads)
@@ -163,7 +184,9 @@ def run_reference_arm(args):
         return
     steps = []
     for _ in range(max(0, args.warmup)):
-        pass  # CPU code: nothing to warm beyond the first call, which is timed like the others
+        # the first load increment of the same job: pages in the harness and
+        # the job's mesh, starts the OpenMP thread pool
+        cpu_baseline_run(first_level_only=True)
     info = None
     for _ in range(args.steps):
         info = cpu_baseline_run()
@@ -173,12 +196,40 @@ def run_reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(steps),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": WORKLOAD,
+            "data": "synthetic", "config": line_config(1),
+            "solver": "reference CPU path (oracle/_ref/cpref, built from the reference sources): its own phases "
+                      "(fillGlobalStiffness, ConjGradSolver::solve, updateParameters, exitCondition) driven per load "
+                      "level by the harness with the job's tolerances instead of solve()'s fixed 1e-7 / 1e-5; "
+                      "unpreconditioned CG, plain secant iteration",
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": info["cores"], "kind": info["kind"],
-                             "sample": "full 8320-DOF hole-plate solve (10 levels) per step, reference CPU path, all host cores"},
+                             "sample": "full 8320-DOF hole-plate solve (10 levels, CG 1e-10, outer 1e-6) per step, "
+                                       "reference CPU path through its phase functions, all host cores; warm-up "
+                                       "steps solve the first increment only"},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "detail": {"outer_iters": info["outer"], "cg_iters": info["cg"]}}
     print(json.dumps(line), flush=True)
+
+
+def error_vs_reference(state, ref, tight):
+    """The timed solve's result against the reference CPU path's result on the
+    same job (both stopped at outer 1e-6 / CG 1e-10, by different iterations),
+    and the reference's own distance from the tight FP64 fixed point, which
+    bounds what agreement the shared tolerances allow."""
+    import numpy as np
+
+    def rel(a, b):
+        nb = np.linalg.norm(b)
+        return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / nb) if nb > 0 else 0.0
+
+    ours_y = np.asarray(state["psi"]) > 1.0 + 1e-12
+    ref_y = np.asarray(ref["psi"]) > 1.0 + 1e-12
+    tight_y = np.asarray(tight["psi"]) > 1.0 + 1e-12
+    return {"rel_l2": {k: rel(state[k], ref[k]) for k in ("uv", "sig_i", "eps_p_i")},
+            "reference_vs_tight_fp64": {k: rel(ref[k], tight[k]) for k in ("uv", "sig_i", "eps_p_i")},
+            "yielded": int(ours_y.sum()), "yielded_reference": int(ref_y.sum()),
+            "yielded_sets_identical": bool(np.array_equal(ours_y, ref_y)),
+            "yielded_differ": int((ours_y != ref_y).sum()),
+            "yielded_sets_identical_at_tight_fp64": bool(np.array_equal(tight_y, ref_y))}
 
 
 def flush_l2(ctx_dev):
@@ -276,7 +327,7 @@ def batched_leg(ctx, window_s=20.0, warm_s=3.0, slots=512, pool_size=768, seed=2
     }
 
 
-def compare_leg(ctx, n_requests, max_outer=100, seed=20261203, lanes=8, mg=True):
+def compare_leg(ctx, n_requests, max_outer=100, seed=20261203, lanes=8, mg=False):
     """Like for like: the plain FP64 drop-in solves the first n requests of
     the batch stream (DOF 2k-200k) one at a time; the batched mixed-precision engine
     then solves exactly the same requests (fresh instances) to completion, and
@@ -639,12 +690,13 @@ def run_product_arm(args):
                 "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one k_cg_p<double> launch (ncu capture)",
                 "bytes_per_launch": bp, "ms_per_launch": mp, "peak_kind": peak_kind}
 
-    cpu = None
+    cpu = err_ref = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         c = cpu_baseline_run()
         cpu = {"value": 1.0 / c["seconds"], "unit": "solves/s", "cores": c["cores"], "kind": c["kind"],
-               "sample": "one full 8320-DOF hole-plate solve (10 levels, CG 1e-10, outer 1e-6), reference CPU path, "
-                         f"{c['outer']} outer / {c['cg']} CG iterations"}
+               "sample": "one full 8320-DOF hole-plate solve (10 levels, CG 1e-10, outer 1e-6), reference CPU path "
+                         f"through its phase functions, {c['outer']} outer / {c['cg']} CG iterations"}
+        err_ref = error_vs_reference(state, c["state"], tight)
 
     batched = served = roof_batched = None
     if rank == 0 and not args.skip_batched:
@@ -658,19 +710,19 @@ def run_product_arm(args):
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(WORKLOAD, parallelism=f"replicas x{world}", l2="flushed (512 MB write) between steps",
-                           solver=f"FP64, Aitken secant, {PRECOND_NAMES[SOLVE_KW['precond']]}, adaptive CG tolerance "
-                                  "max(1e-10, 0.1 relErr) until relErr <= 1e-6, then 1e-10; levels from the "
-                                  "third on start from the linear extrapolation of the last two",
-                           cg_form=("graph loop: P, U, then the V-cycle (restrict per level, dense coarsest "
-                                    "inverse, prolongation fused into post-smoothing), one kernel each"
-                                    if SOLVE_KW["precond"] == 2 else os.environ.get("CUPLAST_FP64_CG") or
-                                    "one thread-block cluster per linear solve (on chip) where the instance fits")),
+            "config": line_config(world),
+            "solver": f"FP64, Aitken secant, {PRECOND_NAMES[SOLVE_KW['precond']]}, adaptive CG tolerance "
+                      "max(1e-10, 0.1 relErr) until relErr <= 1e-6, then 1e-10; levels from the "
+                      "third on start from the linear extrapolation of the last two",
+            "cg_form": ("graph loop: P, U, then the V-cycle (restrict per level, dense coarsest "
+                        "inverse, prolongation fused into post-smoothing), one kernel each"
+                        if SOLVE_KW["precond"] == 2 else os.environ.get("CUPLAST_FP64_CG") or
+                        "one thread-block cluster per linear solve (on chip) where the instance fits"),
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches), "roofline": roofline, "roofline_this_workload": roof_small,
             "cg_large_mesh": cg_large, "multigrid_parts": mg_parts, "cpu_baseline": cpu, "clocks": clocks.summary(),
-            "accuracy_vs_tight_fp64": accuracy, "batched": batched, "roofline_batched": roof_batched,
+            "accuracy_vs_tight_fp64": accuracy, "error_vs_reference": err_ref, "batched": batched, "roofline_batched": roof_batched,
             "served": served,
             "throughput": dict(throughput, dof_iterations_per_s_headline=2 * arrays["node_xy"].shape[0] *
                                sum(r["cg_iters"] for r in reps) / sum(times)),

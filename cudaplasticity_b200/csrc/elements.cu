@@ -183,10 +183,10 @@ void launch_plastic(const DevMesh& m, const MaterialDev& mat, ElemState& st, cud
 
 // ------------------------------------------------ allocation-free update --
 //
-// Some callers cannot allocate device memory: code that runs while a CUDA
-// graph is being captured (cudaMalloc is not a capturable operation), code
-// inside a framework that owns the whole device memory pool through its own
-// allocator, and real-time loops whose memory budget is fixed up front. For
+// Some callers cannot allocate device memory: code inside a framework that
+// owns the whole device memory pool through its own caching allocator (a
+// cudaMalloc beside it fails or fragments that pool), and embedded or
+// real-time loops whose memory budget is fixed up front. For
 // them cp_secant_update_noalloc runs the fused strain / stress / secant-update
 // kernel (k_update above) on buffers the caller already owns. Its only scratch
 // -- the block partial sums of the exit norm and the reduction's scalars --

@@ -204,15 +204,19 @@ CP_API int cp_bench_assemble(cp_instance* inst, int precision, int iters, double
 CP_API int cp_bench_mg(cp_instance* inst, int iters, double* ms, double* bytes);
 
 /* Allocation-free secant update (no counterpart in the reference). For
- * callers that cannot allocate device memory -- code running while a CUDA
- * graph is captured, code inside a framework whose allocator owns the device
- * memory, loops with a fixed memory budget -- this runs the same fused
+ * callers that cannot allocate device memory -- code inside a framework whose
+ * caching allocator owns the device memory (a cudaMalloc of its own would
+ * fail or fragment that pool), embedded and real-time loops whose memory
+ * budget is fixed up front -- this runs the same fused
  * strain / stress / secant-update / exit-norm kernel as cp_secant_update on
  * buffers the caller owns, and allocates nothing (no cudaMalloc, no cudaFree,
  * no allocating library call). Every pointer except mat and rel_err is a
  * DEVICE pointer on the current device; node_xy, elem4 and uv must be 16-byte
  * aligned. Quad meshes only: count4 <= 1,048,576 elements, larger meshes
- * return CP_ERR_INVALID. In: node_xy (2 * node_count), elem4 (4 * count4), uv
+ * return CP_ERR_INVALID. Every elem4 entry must lie in [0, node_count): the
+ * kernel gathers node_xy and uv at those indices unchecked. The call ends
+ * with a stream synchronisation and a copy of the exit norm to the host.
+ * In: node_xy (2 * node_count), elem4 (4 * count4), uv
  * (2 * node_count), E_c / nu_c (count4, the moduli K was assembled with).
  * Out: E_c, nu_c, psi updated; fields = 9 * count4 doubles, one block of
  * count4 each: exx, eyy, gamma, eps_i, sxx, syy, tau, sig_i, table_s; *rel_err

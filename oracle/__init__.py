@@ -28,11 +28,12 @@ REF_BIN_INP = os.path.join(HERE, "_ref", "cpref_inp")
 _lib = None
 
 
-def build(with_reference=None):
-    """Builds liboracle.so, and _ref/cpref when the reference sources exist."""
-    ref_dir = os.environ.get("CUPLAST_REFERENCE", "/root/reference")
+def build(with_reference=None, ref_dir=None):
+    """Builds liboracle.so, and _ref/cpref when the reference sources exist
+    (ref_dir, else the CUPLAST_REFERENCE environment variable)."""
+    ref_dir = ref_dir or os.environ.get("CUPLAST_REFERENCE", "")
     if with_reference is None:
-        with_reference = os.path.isdir(os.path.join(ref_dir, "src"))
+        with_reference = bool(ref_dir) and os.path.isdir(os.path.join(ref_dir, "src"))
     targets = ["oracle"] + (["ref"] if with_reference else [])
     subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_dir}"] + targets, check=True)
 

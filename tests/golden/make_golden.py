@@ -1,7 +1,7 @@
 """Regenerates the golden fixtures in this directory from the reference.
 
-Run from the repository root in a container where the reference sources are
-available (``python tests/golden/make_golden.py``); it builds the harness
+Run from the repository root with CUPLAST_REFERENCE set to the reference
+checkout (``CUPLAST_REFERENCE=<dir> python tests/golden/make_golden.py``); it builds the harness
 (oracle/_ref/cpref) from them if needed. The fixtures it writes are:
 
 * ``<scenario>.npz`` -- for every reference scenario in tests/scenarios.py:
@@ -33,7 +33,7 @@ import oracle  # noqa: E402
 import scenarios  # noqa: E402
 from oracle import vtk  # noqa: E402
 
-REF = os.environ.get("CUPLAST_REFERENCE", "/root/reference")
+REF = os.environ.get("CUPLAST_REFERENCE", "")
 OUT = os.path.dirname(os.path.abspath(__file__))
 FIELDS = ["uv", "exx", "eyy", "gamma", "eps_i", "sxx", "syy", "tau", "sig_i", "table_s", "psi", "E_c", "nu_c",
           "exx_p", "eyy_p", "gamma_p", "eps_p_i"]
@@ -227,27 +227,30 @@ def inp_fixtures():
 if __name__ == "__main__":
     import tempfile
 
+    if not REF or not os.path.isdir(os.path.join(REF, "src")):
+        sys.exit("set CUPLAST_REFERENCE to the reference checkout (its src/ and data/ are read)")
+
     if "--meshes" in sys.argv:  # only the generator and load-building pins
         if not oracle.have_reference():
-            oracle.build(with_reference=True)
+            oracle.build(with_reference=True, ref_dir=REF)
         mesh_fixtures()
         q8_load_fixtures()
         mesh_tool_fixtures()
         sys.exit(0)
     if "--scenarios" in sys.argv:  # only the named scenario fixtures
         if not oracle.have_reference():
-            oracle.build(with_reference=True)
+            oracle.build(with_reference=True, ref_dir=REF)
         with tempfile.TemporaryDirectory() as d:
             scenario_fixtures(d, only=sys.argv[sys.argv.index("--scenarios") + 1:])
         sys.exit(0)
     if "--inp" in sys.argv:  # only the .inp loader pins
         if not oracle.have_reference():
-            oracle.build(with_reference=True)
+            oracle.build(with_reference=True, ref_dir=REF)
         inp_fixtures()
         sys.exit(0)
 
     if not oracle.have_reference():
-        oracle.build(with_reference=True)
+        oracle.build(with_reference=True, ref_dir=REF)
     with tempfile.TemporaryDirectory() as d:
         scenario_fixtures(d)
     mesh_fixtures()

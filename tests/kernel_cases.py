@@ -1,6 +1,6 @@
 """One kernel at a time, on a fixed input, for profilers (ncu -k <kernel>).
 
-    python -m cudaplasticity_b200.kernel_cases <case> [--repeat R]
+    python tests/kernel_cases.py <case> [--repeat R]
 
 Cases (each prints one JSON line with its host-side facts):
 
@@ -33,8 +33,12 @@ import sys
 
 import numpy as np
 
-from . import CP_PREC_FP64, Context, Instance, Loads, Mesh, material
-from . import _capi as C
+import os
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+from cudaplasticity_b200 import CP_PREC_FP64, Context, Instance, Loads, Mesh, material  # noqa: E402
+from cudaplasticity_b200 import _capi as C  # noqa: E402
 
 
 def _plate(n_circ4, rad_n):

@@ -176,10 +176,15 @@ def test_kirsch_error_norms_and_polar_vtk(drivers, segments, tmp_path):
                        np.abs(s_rp - rp)[k].max() * vol / (np.abs(rp) * area)[k].sum())
     assert polar_err == pytest.approx(expect_polar, rel=1e-8)
     # sigmaError with zero reference stresses: each component's largest
-    # magnitude over its area-weighted mean (signed, as in the reference)
+    # magnitude over its signed area-weighted mean, the largest of the three.
+    # Only the sxx term is well conditioned here: with no y traction and the
+    # plate symmetric about both axes, the area integrals of syy and tau are
+    # zero up to round-off, so their terms are round-off ratios of any size
+    # and sign. The result is at least the sxx term and finite.
     vol = area.sum()
-    expect_cart = max(np.abs(v).max() * vol / (v * area).sum() for v in (sxx, syy, tau))
-    assert cart_err == pytest.approx(expect_cart, rel=1e-8)
+    expect_sxx = np.abs(sxx).max() * vol / (sxx * area).sum()
+    assert np.isfinite(cart_err)
+    assert cart_err >= expect_sxx * (1 - 1e-8)
     # the polar-coordinate VTK: strains from the tensor shear gamma / 2
     v = vtk.read_solution_vtk(out)["cell_fields"]
     for name, ref in zip(("Sigma_rr", "Sigma_phiphi", "Tau_rphi"), (rr, pp, rp)):

@@ -1,10 +1,12 @@
 """The allocation-free secant update (cp_secant_update_noalloc) against the
 regular entry point (cp_secant_update) on the same state, two calls in a row.
 
-It exists for callers that cannot allocate device memory (graph capture, a
-framework-owned allocator, fixed memory budgets): the caller passes device
-buffers it owns, here torch tensors, and the library's only scratch is a
-static device array. This file is collected last on purpose."""
+It exists for callers that cannot allocate device memory (a framework whose
+caching allocator owns the device memory, loops with a fixed memory budget):
+the caller passes device buffers it owns, here torch tensors, and the
+library's only scratch is a static device array. This file is collected last
+on purpose, so that a run stopping at its first failure has already run every
+other test."""
 import ctypes
 import os
 
