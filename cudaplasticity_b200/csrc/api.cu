@@ -296,6 +296,10 @@ void cg_fp64_fused(cp_instance* I, double eps, long long max_iter, int precond) 
     }
     if (I->persistent_fp64 && cp::fused_persistent_fits(a)) {
         // one cooperative launch for the whole solve
+        if (I->test_barrier_ns) {
+            a.barrier_ns = I->test_barrier_ns;
+            a.barrier_skew = 1;
+        }
         cp::fused_launch_persistent(a, eps * eps, max_iter, I->s());
         I->launches += 1;
         CP_CUDA(cudaMemcpyAsync(I->sc_h, I->sc, sizeof(cp::CgScalars), cudaMemcpyDeviceToHost, I->s()));
@@ -540,6 +544,7 @@ CP_API int cp_instance_create(cp_context* ctx, const cp_mesh_view* mv, const cp_
         I->cluster_fp64 = std::strcmp(g, "cluster") == 0 || std::strcmp(g, "cluster2") == 0;
         I->cluster_variant = std::strcmp(g, "cluster2") == 0 ? 2 : 1;
     }
+    if (const char* g = std::getenv("CUPLAST_TEST_BARRIER_NS")) I->test_barrier_ns = std::strtoull(g, nullptr, 10);
     int rc = guarded(ctx, [&] {
         CP_CHECK(mv->node_count > 0 && mv->node_xy, CP_ERR_INVALID, "mesh: no nodes");
         CP_CHECK(mv->count3 >= 0 && mv->count4 >= 0 && mv->count8 >= 0 &&

@@ -67,6 +67,12 @@ struct FusedArgs {
     int precond = 0;
     CgScalars* sc = nullptr;
     double* partials = nullptr;
+    // persistent form only: time limit of each grid-barrier wait, and the
+    // number of extra steps every wait asks for (0; 1 makes each wait ask for
+    // a step that is never released, so that every wait runs out: the
+    // time-out path's test)
+    unsigned long long barrier_ns = 2000000000ull;
+    unsigned int barrier_skew = 0;
 };
 
 void fused_launch_start(const FusedArgs& a, double eps2, long long max_iter, cudaStream_t s);

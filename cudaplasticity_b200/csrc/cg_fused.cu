@@ -299,8 +299,6 @@ __global__ void __launch_bounds__(kThreads) k_f_iter(FusedArgs a, int parity) {
 // the cooperative launch. Every wait is bounded in time: a block that gives up
 // sets CP_ERR_TIMEOUT and returns, and so does every other waiting block.
 
-constexpr unsigned long long kBarrierNs = 2000000000ull;  // 2 s; one step takes microseconds
-
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -318,20 +316,23 @@ __device__ __forceinline__ void grid_release(CgScalars* sc) {
 // step's outcome once for the whole block (another block's time-out may
 // change sc->status at any moment, and every thread of a block must take the
 // same branch): true to go on, with alpha and beta in *view. Gives up after
-// kBarrierNs with CP_ERR_TIMEOUT set.
+// a.barrier_ns (2 s by default; one step takes microseconds) with
+// CP_ERR_TIMEOUT set.
 struct StepView {
     int go;
     double alpha, beta;
 };
 
-__device__ __forceinline__ bool grid_wait(CgScalars* sc, unsigned int target, StepView* view) {
+__device__ __forceinline__ bool grid_wait(const FusedArgs& a, unsigned int step, StepView* view) {
+    CgScalars* sc = a.sc;
+    const unsigned int target = step + a.barrier_skew;
     if (threadIdx.x == 0) {
         const volatile unsigned int* g = &sc->gen;
         int ok = 1;
         if (*g < target) {
             const unsigned long long t0 = global_ns();
             while (*g < target) {
-                if (global_ns() - t0 > kBarrierNs) {
+                if (global_ns() - t0 > a.barrier_ns) {
                     ok = 0;
                     break;
                 }
@@ -363,7 +364,7 @@ __global__ void __launch_bounds__(kThreads) k_f_persistent(FusedArgs a, double e
             init_scalars(sc, t, eps2, max_iter);
             grid_release(sc);
         }
-        if (!grid_wait(sc, ++step, &view)) return;
+        if (!grid_wait(a, ++step, &view)) return;
     }
     {
         double v[2] = {0.0, 0.0};
@@ -372,7 +373,7 @@ __global__ void __launch_bounds__(kThreads) k_f_persistent(FusedArgs a, double e
             w_scalars(sc, t);
             grid_release(sc);
         }
-        if (!grid_wait(sc, ++step, &view)) return;
+        if (!grid_wait(a, ++step, &view)) return;
     }
     for (int it = 0;; ++it) {
         double v[kSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -383,7 +384,7 @@ __global__ void __launch_bounds__(kThreads) k_f_persistent(FusedArgs a, double e
             iter_scalars(sc, t);
             grid_release(sc);
         }
-        if (!grid_wait(sc, ++step, &view)) return;
+        if (!grid_wait(a, ++step, &view)) return;
     }
 }
 

@@ -51,6 +51,11 @@ struct cp_instance {
     // single-launch FP64 CG (cg_fused.cu), allocated on first use
     bool fused_fp64 = true;        // false (CUPLAST_FP64_CG=classic): the two-kernel loop of cg.cu
     bool persistent_fp64 = false;  // CUPLAST_FP64_CG=persistent: one cooperative launch per linear solve
+    // CUPLAST_TEST_BARRIER_NS=<ns> (failure-path tests of the persistent CG):
+    // each grid-barrier wait gives up after <ns> and waits for a step that is
+    // never released, so every wait runs out and the solve ends with
+    // CP_ERR_TIMEOUT
+    unsigned long long test_barrier_ns = 0;
     bool cluster_fp64 = true;      // one thread-block cluster when the instance fits (CUPLAST_FP64_CG other than cluster: off)
     int cluster_variant = 1;       // 2: the second form (CUPLAST_FP64_CG=cluster2)
     int cluster_planned = 0;       // cluster_plan below is computed (once per instance)

@@ -8,6 +8,9 @@ checkout (``CUPLAST_REFERENCE=<dir> python tests/golden/make_golden.py``); it bu
   the reference's CSR structure, right-hand side, Dirichlet mask, the values
   of its first stiffness assembly (run with one thread, so the summation order
   is the element order) and its converged state under tight tolerances;
+* ``config1_bilin.npz``, ``ogrid128x64_hollomon.npz`` -- configuration-size
+  scenarios: the reference's converged state (tight tolerances) of the
+  fields in scenarios.STATE_FIELDS;
 * ``ref_meshes.json`` -- SHA-256 digests of meshes made by the reference's own
   generators (genRectWithHole, genRing, genRectangle);
 * ``ref_holePlatePlastPow.npz`` and ``ref_solverTest.npz`` -- the cell fields
@@ -52,6 +55,23 @@ def scenario_fixtures(workdir, only=None):
         arrays.update(outer_per_level=r["outer_per_level"], cg_per_level=r["cg_per_level"],
                       err_per_level=r["err_per_level"], energy=r["energy"],
                       mesh_digest=np.array(scenarios.mesh_digest(m)))
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **arrays)
+        print(name, "outer", r["outer_per_level"], "cg", r["cg_per_level"])
+
+
+def state_fixtures(workdir, only=None):
+    """Configuration-size scenarios: the reference's converged state under
+    tight tolerances (all host threads), STATE_FIELDS only, float64."""
+    for name, sc in scenarios.SCENARIOS.items():
+        if not sc.get("state_fixture") or (only and name not in only):
+            continue
+        mesh_path = os.path.join(workdir, f"{name}.bin")
+        m, lines = scenarios.scenario_lines(name, mesh_path)
+        oracle.write_mesh(mesh_path, m["node_xy"], elem3=m["elem3"], elem4=m["elem4"], borders=m["borders"])
+        r = oracle.run_reference(lines)
+        arrays = {k: r[k] for k in scenarios.STATE_FIELDS}
+        arrays.update(outer_per_level=r["outer_per_level"], cg_per_level=r["cg_per_level"],
+                      err_per_level=r["err_per_level"], mesh_digest=np.array(scenarios.mesh_digest(m)))
         np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **arrays)
         print(name, "outer", r["outer_per_level"], "cg", r["cg_per_level"])
 
@@ -243,6 +263,12 @@ if __name__ == "__main__":
         with tempfile.TemporaryDirectory() as d:
             scenario_fixtures(d, only=sys.argv[sys.argv.index("--scenarios") + 1:])
         sys.exit(0)
+    if "--states" in sys.argv:  # only the configuration-size state fixtures
+        if not oracle.have_reference():
+            oracle.build(with_reference=True, ref_dir=REF)
+        with tempfile.TemporaryDirectory() as d:
+            state_fixtures(d, only=sys.argv[sys.argv.index("--states") + 1:])
+        sys.exit(0)
     if "--inp" in sys.argv:  # only the .inp loader pins
         if not oracle.have_reference():
             oracle.build(with_reference=True, ref_dir=REF)
@@ -253,6 +279,7 @@ if __name__ == "__main__":
         oracle.build(with_reference=True, ref_dir=REF)
     with tempfile.TemporaryDirectory() as d:
         scenario_fixtures(d)
+        state_fixtures(d)
     mesh_fixtures()
     q8_load_fixtures()
     mesh_tool_fixtures()

@@ -14,7 +14,10 @@ Cases (each prints one JSON line with its host-side facts):
   (run with CUPLAST_FP64_CG=fused CUPLAST_NO_GRAPH=1 so that every launch is
   visible to the profiler);
 * ``cg_large``   -- k_cg_p / k_cg_u on the 2.1M-DOF plate, R iterations
-  (cp_bench_cg);
+  (cp_bench_cg), FP64 values or (``--fp32``) the mixed mode's FP32 ones;
+* ``cg_fused_large`` -- k_f_iter, the FP64 form of instances too large for one
+  cluster: R iterations of one block-Jacobi PCG solve on the 2.1M-DOF plate
+  (run with CUPLAST_NO_GRAPH=1 so that every launch is visible);
 * ``cg_mg``      -- the multigrid-preconditioned solve (cp_solve_opts.precond
   2: set-up kernels, then k_mg_p / k_mg_u / k_mg_restrict0 /
   k_mg_coarse_cycle / k_mg_smooth0 per iteration) of the 64x64 plate from
@@ -57,8 +60,10 @@ def _instance(ctx, n_circ4, rad_n):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("case", choices=["assemble", "update", "cg_cluster", "cg_graph", "cg_large", "cg_mg", "cg_mg_large", "mg_parts"])
+    ap.add_argument("case", choices=["assemble", "update", "cg_cluster", "cg_graph", "cg_large", "cg_fused_large",
+                                     "cg_mg", "cg_mg_large", "mg_parts"])
     ap.add_argument("--repeat", type=int, default=3)
+    ap.add_argument("--fp32", action="store_true", help="cg_large: the mixed mode's FP32 values")
     a = ap.parse_args(argv)
     ctx = Context(0)
     out = {"case": a.case}
@@ -81,6 +86,15 @@ def main(argv=None):
         out.update(nodes=n_nodes, cg_iters=[r["cg_iters"] for r in reps], rel_res=reps[-1]["cg_rel_res"],
                    seconds=[r["seconds"] for r in reps], launches=reps[-1]["kernel_launches"])
         inst.close()
+    elif a.case == "cg_fused_large":
+        inst = _instance(ctx, 256, 1024)
+        n_nodes = inst.sizes()[0]
+        inst.set_field("uv", np.zeros(2 * n_nodes))
+        rep = inst.solve(allow_not_converged=True, cg_tol=1e-12, outer_tol=1e300, max_outer=1, levels=1,
+                         precond=1, max_cg=a.repeat)
+        out.update(nodes=n_nodes, cg_iters=rep["cg_iters"], seconds=rep["seconds"],
+                   launches=rep["kernel_launches"])
+        inst.close()
     elif a.case in ("assemble", "update", "cg_large"):
         inst = _instance(ctx, 256, 1024)
         n_nodes, n_elem, nnz, _ = inst.sizes()
@@ -97,7 +111,8 @@ def main(argv=None):
         else:
             mp, mu, bp, bu = (ctypes.c_double() for _ in range(4))
             inst.set_field("uv", np.zeros(2 * n_nodes))
-            ctx.check(C.lib().cp_bench_cg(inst._h, CP_PREC_FP64, 0, a.repeat, ctypes.byref(mp), ctypes.byref(mu),
+            prec = C.CP_PREC_MIXED if a.fp32 else CP_PREC_FP64
+            ctx.check(C.lib().cp_bench_cg(inst._h, prec, 0, a.repeat, ctypes.byref(mp), ctypes.byref(mu),
                                           ctypes.byref(bp), ctypes.byref(bu)))
             out.update(ms_spmv=mp.value, ms_update=mu.value, bytes_spmv=bp.value, bytes_update=bu.value)
         inst.close()

@@ -97,10 +97,27 @@ SCENARIOS = {
     # the curved border), piecewise diagram
     "ring_q8_pw": dict(mesh=_q8(lambda cp: cp.Mesh.ring(50.0, 100.0, 16, 4, order=2)), reference=True,
                        lines_fn=lambda m: [piecewise_lines(210000.0, 300.0), "material 210000 0.3 1"] + _ring_lines(m)),
+    # Parity at configuration size (state-only fixtures, see STATE_FIELDS):
+    # the benchmark's own job, the 64x64 O-grid plate (4160 nodes, 8320 DOF),
+    # bilinear sy = 250, Et = 2 GPa, 200 MPa in 10 increments ...
+    "config1_bilin": dict(mesh=lambda: _ogrid(16, 64), state_fixture=True, levels=10,
+                          lines=["max_outer 5000", "diagram linear 210000 250 2000", "material 210000 0.3 1"]
+                          + _OGRID_LOADS),
+    # ... and a 128 x 64 O-grid (8320 nodes: more than one thread-block
+    # cluster holds, so the FP64 solve takes the grid-wide form), Hollomon
+    # hardening, 4 increments to 220 MPa
+    "ogrid128x64_hollomon": dict(mesh=lambda: _ogrid(32, 64), state_fixture=True, levels=4,
+                                 lines=["max_outer 5000", "diagram hollomon 210000 250 0.002 0.2",
+                                        "material 210000 0.3 1",
+                                        "force 2 0 220 0", "fixborderhor 0", "fixpoint -100 -100"]),
     # CST extension (no reference counterpart): the hole-plate O-grid split
     "ogrid16_t3": dict(mesh=lambda: meshgen.split_t3(_ogrid(4, 8)), reference=False, levels=10,
                        lines=["diagram linear 210000 250 2000", "material 210000 0.3 1"] + _OGRID_LOADS),
 }
+
+
+# fields kept in the state-only fixtures of the configuration-size scenarios
+STATE_FIELDS = ["uv", "eps_i", "sig_i", "psi", "eps_p_i"]
 
 
 def scenario_lines(name, mesh_path, mode=None, extra=()):

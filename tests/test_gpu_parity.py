@@ -256,3 +256,76 @@ def test_singular_system_terminates(ctx):
     except cp.CuplastError as e:
         assert e.status == cp._capi.CP_ERR_BREAKDOWN
     inst.close()
+
+
+STATE_SCEN = [n for n, s in scenarios.SCENARIOS.items() if s.get("state_fixture")]
+# the benchmark's solver options (bench.py's SOLVE_KW), here under the
+# scenarios' tight tolerances
+BENCH_OPTS = dict(aitken=1, adaptive_cg=2, precond=1, predict=1, max_cg=2_000_000)
+
+
+def state_errors(r, g):
+    """Relative L2 of the state-only fixture fields, normalised as in parity.py."""
+    return {k: field_error(k, r, g) for k in scenarios.STATE_FIELDS}
+
+
+@pytest.mark.parametrize("name,opts", [
+    ("config1_bilin", BENCH_OPTS),
+    ("ogrid128x64_hollomon", BENCH_OPTS),
+    ("ogrid128x64_hollomon", dict(aitken=1, precond=1, max_cg=2_000_000)),
+])
+def test_configuration_size_state_matches_reference(name, opts, ctx, golden_dir, workdir):
+    """Parity at configuration size: the benchmark's 64 x 64 O-grid job (its
+    linear solves run inside one thread-block cluster) and a 128 x 64 O-grid
+    with Hollomon hardening (8320 nodes, more than a cluster holds: the
+    grid-wide one-launch-per-iteration CG), with the benchmark's solver
+    options, against the reference's converged state under tight tolerances:
+    within 1e-10 relative L2 and the identical yielded set."""
+    g = load_golden(golden_dir, name)
+    m, lines = scenario(name, workdir)
+    assert scenarios.mesh_digest(m) == str(g["mesh_digest"])
+    r = product_runner.run(ctx, lines, m, **opts)
+    errs = state_errors(r, g)
+    assert max(errs.values()) <= FP64_TOL, errs
+    assert np.array_equal(yielded(r), yielded(g))
+    assert r["report"]["status"] == 0
+    assert r["report"]["levels_done"] == scenarios.SCENARIOS[name]["levels"]
+
+
+def test_configuration_size_mixed_precision_within_1e8(ctx, golden_dir, workdir):
+    """Configuration 3: the configuration-1 job with FP32 values and inner CG
+    inside FP64 defect correction; u, sigma_i and eps_p_i within 1e-8 of the
+    reference's FP64 state."""
+    g = load_golden(golden_dir, "config1_bilin")
+    m, lines = scenario("config1_bilin", workdir)
+    r = product_runner.run(ctx, lines, m, precision=cp.CP_PREC_MIXED, aitken=1, adaptive_cg=1, inner_tol=1e-3,
+                           precond=1, max_cg=2_000_000)
+    for k in ["uv", "sig_i", "eps_p_i"]:
+        assert field_error(k, r, g) <= MIXED_TOL, (k, field_error(k, r, g))
+    assert np.array_equal(yielded(r, 1e-9), yielded(g, 1e-9))
+
+
+def test_persistent_cg_barrier_time_out_is_reported(ctx, workdir, monkeypatch):
+    """The persistent CG's grid barrier waits are bounded in time. With
+    CUPLAST_TEST_BARRIER_NS every wait asks for a step that no block releases,
+    so each one runs out after 1 ms: the solve returns CP_ERR_TIMEOUT, the
+    kernel ends by itself, and the context stays usable (a normal solve on a
+    fresh instance afterwards)."""
+    m, lines = scenario("config1_bilin", workdir)  # 4160 nodes: 17 blocks wait on one another
+    job, (rp, mask, uv) = product_runner.build_inputs(lines, m)
+    mat = product_runner.material_of(job)
+    monkeypatch.setenv("CUPLAST_FP64_CG", "persistent")
+    monkeypatch.setenv("CUPLAST_TEST_BARRIER_NS", "1000000")
+    inst = cp.Instance(ctx, m, mat)
+    monkeypatch.delenv("CUPLAST_TEST_BARRIER_NS")
+    monkeypatch.delenv("CUPLAST_FP64_CG")
+    inst.set_loads(rp, mask, uv)
+    with pytest.raises(cp.CuplastError) as e:
+        inst.solve(cg_tol=1e-10, outer_tol=1e300, max_outer=1, levels=1)
+    assert e.value.status == cp._capi.CP_ERR_TIMEOUT
+    inst.close()
+    ok = cp.Instance(ctx, m, mat)
+    ok.set_loads(rp, mask, uv)
+    rep = ok.solve(cg_tol=1e-10, outer_tol=1e300, max_outer=1, levels=1, precond=1)
+    assert rep["status"] == 0 and rep["cg_iters"] > 0 and rep["cg_rel_res"] <= 1e-10
+    ok.close()
