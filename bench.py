@@ -517,6 +517,121 @@ def served_leg(rate_hz=10.0, submit_s=20.0, drain_s=25.0, seed=20270101, precisi
     }
 
 
+def fifo_latencies(arrivals, service):
+    """Latencies of requests served one at a time in arrival order by a
+    single server whose service times are `service` (the plain drop-in):
+    start = max(arrival, previous finish)."""
+    fin, lat = 0.0, []
+    for a, s in zip(arrivals, service):
+        fin = max(a, fin) + s
+        lat.append(fin - a)
+    return lat, fin
+
+
+def served_vs_plain_leg(ctx, n_requests, seed=20270101, rates=(10.0, 100.0, 1000.0), budget_s=120.0,
+                        forms=("fp64_lanes", "mixed_batch"), **tol):
+    """The served-vs-plain comparison on the same requests.
+
+    Requests: the first n of the seeded served stream (DOF log-uniform in
+    [2k, 500k], 5-30 load increments, plates and rings, 5-segment diagrams).
+    plain: each request end to end through the public API, one at a time,
+        FP64 drop-in (create the instance from host arrays, loads H2D, solve,
+        every result field D2H, destroy); stops taking new requests once
+        budget_s is spent, and the served forms then run the same prefix.
+    served: the solve service (cp_server) under Poisson arrivals at each rate
+        (seeded), host buffers in and every field out; FP64 requests on its
+        lanes, mixed-precision requests in its continuous batch. Latency =
+        submission to completion (the service's clock); throughput = requests
+        / (last completion - first arrival).
+    The plain drop-in's latencies at the same arrivals follow from its
+    measured service times (one server, arrival order). Each served result
+    is compared with the plain FP64 result of the same request (relative L2
+    of u, sigma_i, eps_p_i; the largest over the requests)."""
+    import random
+
+    import numpy as np
+
+    import cudaplasticity_b200 as cp
+    from cudaplasticity_b200 import workload
+
+    kw = dict(FP64_SERVE_KW, **tol)
+    reqs, plain = [], []
+    t_used = 0.0
+    for i in range(n_requests):
+        if t_used >= budget_s:
+            break
+        w = workload.instance(i, seed=seed, dof_min=2000, dof_max=500000, increments=(5, 30))
+        t0 = time.perf_counter()
+        inst = cp.Instance(ctx, w["mesh"], w["material"])
+        inst.set_loads(w["rp"], w["mask"], w["uv"])
+        rep = inst.solve(allow_not_converged=True, precision=cp.CP_PREC_FP64, levels=w["levels"], **kw)
+        st = inst.state()
+        inst.close()
+        dt = time.perf_counter() - t0
+        t_used += dt
+        reqs.append(w)
+        plain.append({"seconds": dt, "status": rep["status"], "outer": rep["outer_iters"], "cg": rep["cg_iters"],
+                      "state": st})
+    n = len(reqs)
+    service = [p["seconds"] for p in plain]
+    out = {"workload": "first %d requests of the served stream (base seed %d): DOF log-uniform [2k, 500k], 5-30 "
+                       "load increments; CG %g, outer %g; FP64 reference = the plain drop-in's result"
+                       % (n, seed, kw["cg_tol"], kw["outer_tol"]),
+           "requests": n, "dof": [w["params"]["dof"] for w in reqs], "levels": [w["levels"] for w in reqs],
+           "plain_fp64_dropin": {"seconds_total": sum(service), "solves_per_s": n / sum(service),
+                                 "statuses": sorted({p["status"] for p in plain}),
+                                 "outer_iters": [p["outer"] for p in plain], "cg_iters": [p["cg"] for p in plain],
+                                 "seconds": service},
+           "rates": {}}
+
+    def rel(a, b):
+        nb = np.linalg.norm(b)
+        return float(np.linalg.norm(a - b) / nb) if nb > 0 else 0.0
+
+    for rate in rates:
+        rng = random.Random(seed * 1000 + int(rate))
+        arrivals, t = [], 0.0
+        for _ in range(n):
+            t += rng.expovariate(rate)
+            arrivals.append(t)
+        p_lat, p_fin = fifo_latencies(arrivals, service)
+        row = {"plain_fp64_dropin": {"solves_per_s": n / (p_fin - arrivals[0]),
+                                     "p50_s": float(np.percentile(p_lat, 50)),
+                                     "p99_s": float(np.percentile(p_lat, 99))}}
+        for form in forms:
+            srv = cp.Server(fp64_lanes=8)
+            skw = dict(kw, precision=cp.CP_PREC_FP64) if form == "fp64_lanes" else dict(BATCH_KW, **tol)
+            t0 = time.perf_counter()
+            rids = []
+            for w, a in zip(reqs, arrivals):
+                now = time.perf_counter() - t0
+                if a > now:
+                    time.sleep(a - now)
+                rids.append(srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"],
+                                       **skw))
+            lat, errs, statuses, last = [], {"uv": 0.0, "sig_i": 0.0, "eps_p_i": 0.0}, set(), 0.0
+            for k, rid in enumerate(rids):
+                inst, rep, latency = srv.wait(rid, timeout=-1.0)
+                st = inst.state()
+                inst.close()
+                last = max(last, time.perf_counter() - t0)
+                lat.append(latency)
+                statuses.add(rep["status"])
+                for f in errs:
+                    errs[f] = max(errs[f], rel(st[f], plain[k]["state"][f]))
+            srv.close()
+            row[form] = {"solves_per_s": n / (last - arrivals[0]), "p50_s": float(np.percentile(lat, 50)),
+                         "p99_s": float(np.percentile(lat, 99)), "statuses": sorted(statuses),
+                         "max_rel_err_vs_plain_fp64": errs,
+                         "within_1e-8": bool(max(errs.values()) <= 1e-8),
+                         "speedup_vs_plain": (n / (last - arrivals[0])) / (n / (p_fin - arrivals[0]))}
+        out["rates"][str(int(rate))] = row
+        print(json.dumps({"served_vs_plain_rate": rate, **{k: {kk: vv for kk, vv in v.items()
+                                                                if kk in ("solves_per_s", "p50_s", "p99_s")}
+                                                            for k, v in row.items()}}), file=sys.stderr, flush=True)
+    return out
+
+
 def run_product_arm(args):
     import numpy as np
 
