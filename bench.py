@@ -528,12 +528,20 @@ def fifo_latencies(arrivals, service):
     return lat, fin
 
 
-def served_vs_plain_leg(ctx, n_requests, seed=20270101, rates=(10.0, 100.0, 1000.0), budget_s=120.0,
+STREAMS = {"served": dict(seed=20270101, dof_min=2000, dof_max=500000, increments=(5, 30),
+                         text="served stream (DOF log-uniform [2k, 500k], 5-30 load increments)"),
+           "batch": dict(seed=20261203, dof_min=2000, dof_max=200000, increments=None,
+                         text="batch stream (DOF log-uniform [2k, 200k], one load level)")}
+
+
+def served_vs_plain_leg(ctx, n_requests, stream="served", rates=(10.0, 100.0, 1000.0), budget_s=120.0,
                         forms=("fp64_lanes", "mixed_batch"), **tol):
     """The served-vs-plain comparison on the same requests.
 
-    Requests: the first n of the seeded served stream (DOF log-uniform in
-    [2k, 500k], 5-30 load increments, plates and rings, 5-segment diagrams).
+    Requests: the first n of a seeded request stream (STREAMS: the served
+    stream, DOF log-uniform in [2k, 500k] and 5-30 load increments, or the
+    batch stream, DOF in [2k, 200k] and one level; plates and rings,
+    5-segment diagrams).
     plain: each request end to end through the public API, one at a time,
         FP64 drop-in (create the instance from host arrays, loads H2D, solve,
         every result field D2H, destroy); stops taking new requests once
@@ -555,12 +563,15 @@ def served_vs_plain_leg(ctx, n_requests, seed=20270101, rates=(10.0, 100.0, 1000
     from cudaplasticity_b200 import workload
 
     kw = dict(FP64_SERVE_KW, **tol)
+    st_ = STREAMS[stream]
+    seed = st_["seed"]
     reqs, plain = [], []
     t_used = 0.0
     for i in range(n_requests):
         if t_used >= budget_s:
             break
-        w = workload.instance(i, seed=seed, dof_min=2000, dof_max=500000, increments=(5, 30))
+        w = workload.instance(i, seed=seed, dof_min=st_["dof_min"], dof_max=st_["dof_max"],
+                              increments=st_["increments"])
         t0 = time.perf_counter()
         inst = cp.Instance(ctx, w["mesh"], w["material"])
         inst.set_loads(w["rp"], w["mask"], w["uv"])
@@ -574,9 +585,8 @@ def served_vs_plain_leg(ctx, n_requests, seed=20270101, rates=(10.0, 100.0, 1000
                       "state": st})
     n = len(reqs)
     service = [p["seconds"] for p in plain]
-    out = {"workload": "first %d requests of the served stream (base seed %d): DOF log-uniform [2k, 500k], 5-30 "
-                       "load increments; CG %g, outer %g; FP64 reference = the plain drop-in's result"
-                       % (n, seed, kw["cg_tol"], kw["outer_tol"]),
+    out = {"workload": "first %d requests of the %s, base seed %d; CG %g, outer %g; FP64 reference = the plain "
+                       "drop-in's result" % (n, st_["text"], seed, kw["cg_tol"], kw["outer_tol"]),
            "requests": n, "dof": [w["params"]["dof"] for w in reqs], "levels": [w["levels"] for w in reqs],
            "plain_fp64_dropin": {"seconds_total": sum(service), "solves_per_s": n / sum(service),
                                  "statuses": sorted({p["status"] for p in plain}),
@@ -953,6 +963,12 @@ def main():
     ap.add_argument("--serve-window", type=float, default=20.0, help="seconds of arrivals in the served leg")
     ap.add_argument("--batched-probe", type=int, nargs=2, metavar=("N", "TRIPS"),
                     help="profiling aid: N resident batch-stream instances, TRIPS graph trips, then exit")
+    ap.add_argument("--svp", type=int, metavar="N",
+                    help="served-vs-plain leg only: the first N requests of --svp-stream, then exit")
+    ap.add_argument("--svp-stream", default="served", choices=sorted(STREAMS))
+    ap.add_argument("--svp-budget", type=float, default=120.0, help="seconds of plain solves before the prefix stops")
+    ap.add_argument("--svp-outer-tol", type=float, default=1e-6)
+    ap.add_argument("--svp-cg-tol", type=float, default=1e-10)
     ap.add_argument("--precond", type=int, default=SOLVE_KW["precond"], choices=[0, 1, 2],
                     help="linear solver of the headline and of the FP64 served arm: 0 CG, 1 block-Jacobi PCG, "
                          "2 multigrid PCG")
@@ -961,6 +977,15 @@ def main():
     FP64_SERVE_KW["precond"] = args.precond
     if args.batched_probe:
         batched_probe(*args.batched_probe)
+        return
+    if args.svp:
+        import cudaplasticity_b200 as cp
+
+        ctx = cp.Context(0)
+        print(json.dumps({"served_vs_plain": served_vs_plain_leg(
+            ctx, args.svp, stream=args.svp_stream, budget_s=args.svp_budget, outer_tol=args.svp_outer_tol,
+            cg_tol=args.svp_cg_tol)}), flush=True)
+        ctx.close()
         return
     if args.compare:
         import cudaplasticity_b200 as cp

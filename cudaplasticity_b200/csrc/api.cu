@@ -128,12 +128,12 @@ void validate_material(const cp_material& m) {
 template <>
 cp::CgArgs<double> cp_instance::cg_args<double>(int precond) {
     cp::CgArgs<double> a;
-    if (precond && !s64) {
-        s64 = alloc<double2>(n_nodes);
-        minv64 = alloc<double4>(n_nodes);
+    if (precond && !minv64) minv64 = alloc<double4>(n_nodes);
+    if (!rec64a) {
+        rec64a = alloc<double4>(n_nodes);
+        rec64b = alloc<double4>(n_nodes);
     }
     a.precond = precond;
-    a.s = s64;
     a.minv = minv64;
     a.n = n_nodes;
     a.sm_count = sms();
@@ -145,8 +145,8 @@ cp::CgArgs<double> cp_instance::cg_args<double>(int precond) {
     a.mask = mask;
     a.x = u;
     a.r = r64;
-    a.z0 = z64a;
-    a.z1 = z64b;
+    a.rec0 = rec64a;
+    a.rec1 = rec64b;
     a.q = q64;
     a.sc = sc;
     a.partials = partials;
@@ -156,12 +156,8 @@ cp::CgArgs<double> cp_instance::cg_args<double>(int precond) {
 template <>
 cp::CgArgs<float> cp_instance::cg_args<float>(int precond) {
     cp::CgArgs<float> a;
-    if (precond && !s32) {
-        s32 = alloc<float2>(n_nodes);
-        minv32 = alloc<float4>(n_nodes);
-    }
+    if (precond && !minv32) minv32 = alloc<float4>(n_nodes);
     a.precond = precond;
-    a.s = s32;
     a.minv = minv32;
     a.n = n_nodes;
     a.sm_count = sms();
@@ -173,8 +169,8 @@ cp::CgArgs<float> cp_instance::cg_args<float>(int precond) {
     a.mask = mask;
     a.x = u;
     a.r = r32;
-    a.z0 = z32a;
-    a.z1 = z32b;
+    a.rec0 = rec32a;
+    a.rec1 = rec32b;
     a.q = q32;
     a.sc = sc;
     a.partials = partials;
@@ -210,8 +206,8 @@ void ensure_fp32(cp_instance* I) {
     if (I->csr.val32) return;
     I->csr.val32 = I->alloc<float>(4 * (size_t)I->csr.sell_blocks);
     I->r32 = I->alloc<float2>(I->n_nodes);
-    I->z32a = I->alloc<float2>(I->n_nodes);
-    I->z32b = I->alloc<float2>(I->n_nodes);
+    I->rec32a = I->alloc<float4>(I->n_nodes);
+    I->rec32b = I->alloc<float4>(I->n_nodes);
     I->q32 = I->alloc<float2>(I->n_nodes);
 }
 
@@ -428,10 +424,10 @@ void cp::instance_prepare_mixed(cp_instance* I, int precond) {
     const bool fresh = !I->csr.val32;
     ensure_fp32(I);
     if (fresh) {
-        CP_CUDA(cudaMemsetAsync(I->z32a, 0, sizeof(float2) * I->n_nodes, I->s()));
-        CP_CUDA(cudaMemsetAsync(I->z32b, 0, sizeof(float2) * I->n_nodes, I->s()));
+        CP_CUDA(cudaMemsetAsync(I->rec32a, 0, sizeof(float4) * I->n_nodes, I->s()));
+        CP_CUDA(cudaMemsetAsync(I->rec32b, 0, sizeof(float4) * I->n_nodes, I->s()));
     }
-    if (precond) (void)I->cg_args<float>(1);  // allocates s32 / minv32 once
+    if (precond) (void)I->cg_args<float>(1);  // allocates minv32 once
 }
 
 // ------------------------------------------------------------------ C ABI --
@@ -521,7 +517,8 @@ CP_API int cp_instance_footprint(const cp_mesh_view* m, int precision, size_t* b
     b += nnz * 8;                                                              // K (FP64)
     b += n * (16 * 8 + 2);                                                     // u, b, b_full, u_full, r, z, z, q, mask
     b += ne * 18 * 8;                                                          // element state
-    if (precision != CP_PREC_FP64) b += nnz * 4 + n * 8 * 4;
+    b += n * 2 * 32;                                                           // (v, z) records, FP64 two-kernel form
+    if (precision != CP_PREC_FP64) b += nnz * 4 + n * 8 * 4 + n * 2 * 16;
     b += 1 << 20;                                                              // scalars, partials, graphs
     *bytes = b;
     return CP_OK;
@@ -1002,12 +999,12 @@ CP_API int cp_bench_cg(cp_instance* I, int precision, int precond, int iters, do
         // algorithmic bytes per launch (2 DOFs per node, N = 2n):
         //  P: values nnz*sv + block columns nnz/4*4 + read r, z + write z', Kz' (4 N sx)
         //  U: read x (16 n), z', r, Kz' (3 N sx), mask (2 n); write x, r (16 n + N sx)
-        //     [+ block Jacobi: read M^-1 (4 n sx), write s (N sx)]
+        //     and the record's v = M^-1 r (or r) (N sx) [+ block Jacobi: read M^-1 (4 n sx)]
         const double N = 2 * n;
         if (ms_p) *ms_p = tp / iters;
         if (ms_u) *ms_u = tu / iters;
         if (bytes_p) *bytes_p = nnz * sv + nnz + 4 * N * sx;
-        if (bytes_u) *bytes_u = 32 * n + 4 * N * sx + 2 * n + (precond ? 4 * n * sx + N * sx : 0.0);
+        if (bytes_u) *bytes_u = 32 * n + 4 * N * sx + 2 * n + (precond ? 4 * n * sx : 0.0) + N * sx;
     });
 }
 

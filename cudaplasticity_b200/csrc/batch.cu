@@ -418,7 +418,10 @@ __device__ void tile_w(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, 
     }
 }
 
-// ITER: one CG iteration (see the section comment).
+// ITER: one CG iteration (see the section comment). C > 0: the row's blocks
+// are taken C at a time, columns and values loaded together ahead of the C
+// record gathers; C = 0: one unrolled loop.
+template <int C>
 __device__ void tile_iter(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
@@ -448,15 +451,39 @@ __device__ void tile_iter(const BDesc& d, BState* S, BCtl* c, int4 tl, double* s
             if (m.y) r.y -= a * kp.y;
             // w' = K u' with the neighbours' u' from their u, M w, M kp
             float k0 = 0.f, k1 = 0.f;
+            if (C == 0) {
 #pragma unroll 3
-            for (int k = 0; k < wd; ++k) {
-                const long long bi = base + 32LL * k + lane;
-                const int col = __ldg(d.scol + bi);
-                const float4 v = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
-                const float4 c0 = __ldg(go + 2 * (size_t)col), c1 = __ldg(go + 2 * (size_t)col + 1);
-                const float ux = c0.x - a * (c0.z + bt * c1.x), uy = c0.y - a * (c0.w + bt * c1.y);
-                k0 += v.x * ux + v.y * uy;
-                k1 += v.z * ux + v.w * uy;
+                for (int k = 0; k < wd; ++k) {
+                    const long long bi = base + 32LL * k + lane;
+                    const int col = __ldg(d.scol + bi);
+                    const float4 v = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
+                    const float4 c0 = __ldg(go + 2 * (size_t)col), c1 = __ldg(go + 2 * (size_t)col + 1);
+                    const float ux = c0.x - a * (c0.z + bt * c1.x), uy = c0.y - a * (c0.w + bt * c1.y);
+                    k0 += v.x * ux + v.y * uy;
+                    k1 += v.z * ux + v.w * uy;
+                }
+            } else {
+                for (int k0i = 0; k0i < wd; k0i += (C > 0 ? C : 1)) {
+                    int cc[C > 0 ? C : 1];
+                    float4 vv[C > 0 ? C : 1];
+#pragma unroll
+                    for (int j = 0; j < C; ++j) {
+                        if (k0i + j < wd) {
+                            const long long bi = base + 32LL * (k0i + j) + lane;
+                            cc[j] = __ldg(d.scol + bi);
+                            vv[j] = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < C; ++j) {
+                        if (k0i + j < wd) {
+                            const float4 c0 = __ldg(go + 2 * (size_t)cc[j]), c1 = __ldg(go + 2 * (size_t)cc[j] + 1);
+                            const float ux = c0.x - a * (c0.z + bt * c1.x), uy = c0.y - a * (c0.w + bt * c1.y);
+                            k0 += vv[j].x * ux + vv[j].y * uy;
+                            k1 += vv[j].z * ux + vv[j].w * uy;
+                        }
+                    }
+                }
             }
             const float2 w2 = make_float2(k0, k1);
             d.p[n] = p;
@@ -516,7 +543,9 @@ __device__ void tile_iter(const BDesc& d, BState* S, BCtl* c, int4 tl, double* s
 }
 
 // 8 resident blocks per SM (64 registers): the CG iteration is bound by the
-// latency of its gathers, and the occupancy pays for the few spills.
+// latency of its gathers, and the occupancy pays for the few spills. C: the
+// ITER gather form (tile_iter).
+template <int C>
 __global__ void __launch_bounds__(kThreads, 8) k_batch_cg(const BDesc* __restrict__ D, BState* SS,
                                                        const int4* __restrict__ tiles, BCtl* c) {
     __shared__ double sh[2 * kWarps];
@@ -530,7 +559,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_batch_cg(const BDesc* __restric
         const int4 tl = tiles[t];
         BState* S = SS + tl.x;
         const int ph = tile_phase(S, &shp);
-        if (ph == PH_ITER) tile_iter(D[tl.x], S, c, tl, sh, &shf);
+        if (ph == PH_ITER) tile_iter<C>(D[tl.x], S, c, tl, sh, &shf);
         else if (ph == PH_W) tile_w(D[tl.x], S, c, tl, sh, &shf);
         else if (ph == PH_RES) tile_res(D[tl.x], S, c, tl, sh, &shf);
     }
@@ -810,6 +839,21 @@ __global__ void k_batch_cond(BCtl* c, cudaGraphConditionalHandle h) {
 // see kernel nodes of a graph with a conditional node).
 __global__ void k_batch_cond_direct(BCtl* c) { trip_condition(c); }
 
+// The batched CG kernel's ITER gather form: CUPLAST_BATCH_CHUNK = 0 (one
+// unrolled loop) or 3 / 5 (blocks that many at a time), for measurements.
+using BatchCgKernel = void (*)(const BDesc*, BState*, const int4*, BCtl*);
+BatchCgKernel batch_cg_kernel() {
+    static const BatchCgKernel k = [] {
+        const char* e = std::getenv("CUPLAST_BATCH_CHUNK");
+        switch (e ? std::atoi(e) : 0) {
+        case 3: return (BatchCgKernel)k_batch_cg<3>;
+        case 5: return (BatchCgKernel)k_batch_cg<5>;
+        default: return (BatchCgKernel)k_batch_cg<0>;
+        }
+    }();
+    return k;
+}
+
 int bucket_of(int n_slices) {
     int b = 0;
     while ((2 << b) <= n_slices && b + 1 < kBuckets) ++b;
@@ -988,7 +1032,7 @@ void launch_body(cp_batch* b, cudaStream_t s) {
         k_batch_asm<false><<<b->grid_asm, kThreads, b->asm_smem, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl,
                                                                       b->o.max_width);
     for (int k = 0; k < b->o.cg_per_trip; ++k)
-        k_batch_cg<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
+        batch_cg_kernel()<<<b->grid_cg, kThreads, 0, s>>>(b->d_desc, b->d_state, b->d_tiles, b->d_ctl);
 }
 
 // Direct launches: trip after trip with the condition read back each time.
@@ -1094,7 +1138,7 @@ CP_API int cp_batch_create(cp_context* ctx, const cp_batch_opts* opts, cp_batch*
         CP_CUDA(cudaHostGetDevicePointer((void**)&b->d_stop, b->h_stop, 0));
         ensure_tiles(b, 1024);
         int per_sm = 0;
-        CP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cg, kThreads, 0));
+        CP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_cg_kernel(), kThreads, 0));
         if (o.cg_blocks_per_sm > 0) per_sm = std::min(per_sm, o.cg_blocks_per_sm);
         b->grid_cg = ctx->sm_count * std::max(1, per_sm);
         b->asm_smem = (size_t)kWarps * 128 * o.max_width * sizeof(double);

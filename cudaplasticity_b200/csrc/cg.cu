@@ -9,9 +9,14 @@
 // stop when (r, r) / (b, b) <= eps^2.
 //
 // One iteration = two kernels, no host round trip:
-//   P: z' = r + beta z (own node), K z' gathered as K (r + beta z) from the
+//   P: z' = v + beta z (own node), K z' gathered as K (v + beta z) from the
 //      neighbours, (K z', z')          -- the SpMV reads each 2x2 block once
-//   U: x += alpha z', r -= m.alpha K z', (r, r)
+//   U: x += alpha z', r -= m.alpha K z', v' = M r (v' = r without the
+//      preconditioner), (r, r)
+// The neighbours' inputs of P are packed in one record per node, rec[n] =
+// (v, z), double-buffered by iteration parity: P reads (v, z) of parity p
+// and writes z' into the record of parity 1 - p, U writes v' there. A
+// neighbour costs one gather (16 bytes in FP32, 32 in FP64).
 // Scalars live on the device; every cross-block sum is reduced by the last
 // block in index order (deterministic). The loop runs in a CUDA graph whose
 // WHILE node re-launches the body until the device sets "converged".
@@ -19,6 +24,7 @@
 // T is the type of K's values and of the CG recurrences (double, or float in
 // the mixed-precision mode); the solution x always accumulates in FP64, and
 // every dot product is accumulated and reduced in FP64.
+#include <cstdlib>
 #include <mutex>
 #include <unordered_map>
 
@@ -48,6 +54,24 @@ __device__ __forceinline__ double4 load_block<double>(const double* __restrict__
 template <>
 __device__ __forceinline__ float4 load_block<float>(const float* __restrict__ val, long long b) {
     return __ldg(reinterpret_cast<const float4*>(val + 4 * b));
+}
+
+// Node c's record (v, z) of the parity being read.
+template <typename T>
+__device__ __forceinline__ typename Vec4<T>::type load_rec(const typename Vec4<T>::type* rec, int c) {
+    return rec[c];
+}
+template <>
+__device__ __forceinline__ double4 load_rec<double>(const double4* rec, int c) {
+    const double2* p = reinterpret_cast<const double2*>(rec + c);
+    const double2 lo = p[0], hi = p[1];
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+
+// The two halves of a record, written separately: v by U, z by P.
+template <typename T>
+__device__ __forceinline__ typename Vec2<T>::type* rec_half(typename Vec4<T>::type* rec, int n, int half) {
+    return reinterpret_cast<typename Vec2<T>::type*>(rec + n) + half;
 }
 
 // One warp per slice of 32 nodes, one thread per node: the loop over slices
@@ -89,10 +113,11 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(CgArgs<T> a, const VA* __r
             rt.x = (T)r0;
             rt.y = (T)r1;
             a.r[n] = rt;
-            V2 zz;
-            zz.x = (T)0;
-            zz.y = (T)0;
-            a.z0[n] = zz;
+            typename Vec4<T>::type rec;
+            rec.x = rt.x;
+            rec.y = rt.y;
+            rec.z = (T)0;
+            rec.w = (T)0;
             s_rr += (double)rt.x * (double)rt.x + (double)rt.y * (double)rt.y;
             if (PRE) {
                 // inverse of the node's 2x2 diagonal block (block 0), restricted
@@ -113,9 +138,11 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(CgArgs<T> a, const VA* __r
                 V2 sv;
                 sv.x = mi.x * rt.x + mi.y * rt.y;
                 sv.y = mi.z * rt.x + mi.w * rt.y;
-                a.s[n] = sv;
+                rec.x = sv.x;
+                rec.y = sv.y;
                 s_rho += (double)rt.x * (double)sv.x + (double)rt.y * (double)sv.y;
             }
+            a.rec0[n] = rec;
             s_r64 += r0 * r0 + r1 * r1;
             s_bb += bb.x * bb.x + bb.y * bb.y;
         }
@@ -164,16 +191,19 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(CgArgs<T> a, const VA* __r
     }
 }
 
-// P: z' = r + beta z (own node); K z' gathered as K (r + beta z); (K z', z').
-template <typename T, bool PRE>
+// P: z' = v + beta z (own node); K z' gathered as K (v + beta z); (K z', z').
+// C > 0: the blocks of a row are taken C at a time, their columns and values
+// loaded together before the C record gathers; C = 0: one loop, unrolled.
+template <typename T, bool PRE, int C>
 __global__ void __launch_bounds__(kThreads) k_cg_p(CgArgs<T> a, int parity) {
     using V2 = typename Vec2<T>::type;
+    using V4 = typename Vec4<T>::type;
     __shared__ double sh[kThreads / 32];
     __shared__ bool last;
     CgScalars* sc = a.sc;
     if (sc->converged || sc->status) return;
-    const V2* __restrict__ zo = parity ? a.z1 : a.z0;
-    V2* __restrict__ zn = parity ? a.z0 : a.z1;
+    const V4* __restrict__ ro = parity ? a.rec1 : a.rec0;
+    V4* __restrict__ rn = parity ? a.rec0 : a.rec1;
     const T beta = (T)sc->beta;
     double dot = 0.0;
     CP_SLICE_LOOP(a.n) {
@@ -181,23 +211,47 @@ __global__ void __launch_bounds__(kThreads) k_cg_p(CgArgs<T> a, int parity) {
         const int base = a.slice_ptr[sl], w = (a.slice_ptr[sl + 1] - base) >> 5;
         if (n < a.n) {
             T k0 = (T)0, k1 = (T)0;
+            if (C == 0) {
 #pragma unroll 3
-            for (int k = 0; k < w; ++k) {
-                const long long b = base + 32LL * k + lane;
-                const int c = __ldg(a.scol + b);
-                const auto v = load_block<T>(a.val, b);
-                const V2 rc = PRE ? a.s[c] : a.r[c], zc = zo[c];
-                const T wx = rc.x + beta * zc.x, wy = rc.y + beta * zc.y;
-                k0 += v.x * wx + v.y * wy;
-                k1 += v.z * wx + v.w * wy;
+                for (int k = 0; k < w; ++k) {
+                    const long long b = base + 32LL * k + lane;
+                    const int c = __ldg(a.scol + b);
+                    const auto v = load_block<T>(a.val, b);
+                    const V4 g = load_rec<T>(ro, c);
+                    const T wx = g.x + beta * g.z, wy = g.y + beta * g.w;
+                    k0 += v.x * wx + v.y * wy;
+                    k1 += v.z * wx + v.w * wy;
+                }
+            } else {
+                for (int k0i = 0; k0i < w; k0i += (C > 0 ? C : 1)) {
+                    int cc[C > 0 ? C : 1];
+                    V4 vv[C > 0 ? C : 1];
+#pragma unroll
+                    for (int j = 0; j < C; ++j) {
+                        if (k0i + j < w) {
+                            const long long b = base + 32LL * (k0i + j) + lane;
+                            cc[j] = __ldg(a.scol + b);
+                            vv[j] = load_block<T>(a.val, b);
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < C; ++j) {
+                        if (k0i + j < w) {
+                            const V4 g = load_rec<T>(ro, cc[j]);
+                            const T wx = g.x + beta * g.z, wy = g.y + beta * g.w;
+                            k0 += vv[j].x * wx + vv[j].y * wy;
+                            k1 += vv[j].z * wx + vv[j].w * wy;
+                        }
+                    }
+                }
             }
-            const V2 rn = PRE ? a.s[n] : a.r[n], zon = zo[n];
+            const V4 own = load_rec<T>(ro, n);
             V2 zz, qq;
-            zz.x = rn.x + beta * zon.x;
-            zz.y = rn.y + beta * zon.y;
+            zz.x = own.x + beta * own.z;
+            zz.y = own.y + beta * own.w;
             qq.x = k0;
             qq.y = k1;
-            zn[n] = zz;
+            *rec_half<T>(rn, n, 1) = zz;
             a.q[n] = qq;
             dot += (double)k0 * (double)zz.x + (double)k1 * (double)zz.y;
         }
@@ -222,12 +276,12 @@ __global__ void __launch_bounds__(kThreads) k_cg_u(CgArgs<T> a, int parity) {
     __shared__ bool last;
     CgScalars* sc = a.sc;
     if (sc->converged || sc->status) return;
-    const V2* __restrict__ zn = parity ? a.z0 : a.z1;
+    typename Vec4<T>::type* __restrict__ rn = parity ? a.rec0 : a.rec1;
     const double alpha = sc->alpha;
     const T alpha_t = (T)alpha;
     double dot = 0.0, dot_s = 0.0;
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < a.n; n += gridDim.x * blockDim.x) {
-        const V2 z = zn[n], q = a.q[n];
+        const V2 z = *rec_half<T>(rn, n, 1), q = a.q[n];
         const uchar2 m = a.mask[n];
         double2 x = a.x[n];
         x.x += alpha * (double)z.x;
@@ -243,8 +297,10 @@ __global__ void __launch_bounds__(kThreads) k_cg_u(CgArgs<T> a, int parity) {
             V2 sv;
             sv.x = mi.x * r.x + mi.y * r.y;
             sv.y = mi.z * r.x + mi.w * r.y;
-            a.s[n] = sv;
+            *rec_half<T>(rn, n, 0) = sv;
             dot_s += (double)r.x * (double)sv.x + (double)r.y * (double)sv.y;
+        } else {
+            *rec_half<T>(rn, n, 0) = r;
         }
     }
     __shared__ double sh2[2 * kThreads / 32];
@@ -319,9 +375,32 @@ void cg_launch_init(const CgArgs<T>& a, const void* valA, bool valA_is_fp64, dou
     CP_CUDA(cudaGetLastError());
 }
 
+// Blocks per gather chunk of P (0: the unrolled loop). CUPLAST_CG_CHUNK
+// overrides the default, for measurements.
+template <typename T>
+int p_chunk() {
+    static const int c = [] {
+        const char* e = std::getenv("CUPLAST_CG_CHUNK");
+        const int v = e ? std::atoi(e) : -1;
+        return (v == 0 || v == 3 || v == 5 || v == 9) ? v : (sizeof(T) == 4 ? 5 : 3);
+    }();
+    return c;
+}
+
+template <typename T, bool PRE>
+void (*p_kernel(int c))(CgArgs<T>, int) {
+    switch (c) {
+    case 0: return k_cg_p<T, PRE, 0>;
+    case 3: return k_cg_p<T, PRE, 3>;
+    case 9: return k_cg_p<T, PRE, 9>;
+    default: return k_cg_p<T, PRE, 5>;
+    }
+}
+
 template <typename T>
 void cg_launch_p(const CgArgs<T>& a, int parity, cudaStream_t s) {
-    auto kp = a.precond ? k_cg_p<T, true> : k_cg_p<T, false>;
+    const int c = p_chunk<T>();
+    auto kp = a.precond ? p_kernel<T, true>(c) : p_kernel<T, false>(c);
     const int gp = resident_grid(kp, a.n, kThreads, a.sm_count);
     CP_CHECK(gp <= a.max_blocks, CP_ERR_INVALID, "partials buffer too small");
     kp<<<gp, kThreads, 0, s>>>(a, parity);

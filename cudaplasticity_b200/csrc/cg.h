@@ -40,11 +40,12 @@ struct CgArgs {
     const uchar2* mask = nullptr;   // 1 = free DOF
     double2* x = nullptr;           // solution, accumulated in FP64
     V2* r = nullptr;
-    V2* s = nullptr;                // preconditioned residual M^-1 r (block Jacobi only)
     typename Vec4<T>::type* minv = nullptr;  // inverse 2x2 diagonal blocks (block Jacobi only)
     int precond = 0;                // 0: plain CG (reference), 1: 2x2 block-Jacobi PCG
-    V2* z0 = nullptr;
-    V2* z1 = nullptr;
+    // per node (v, z): v = M^-1 r (r without the preconditioner), z the
+    // direction; by iteration parity
+    typename Vec4<T>::type* rec0 = nullptr;
+    typename Vec4<T>::type* rec1 = nullptr;
     V2* q = nullptr;
     CgScalars* sc = nullptr;
     double* partials = nullptr;     // >= 3 * max_blocks doubles

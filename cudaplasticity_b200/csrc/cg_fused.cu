@@ -18,6 +18,7 @@
 // scalars stay on the device; the loop runs in a CUDA graph with a WHILE
 // node, as in cg.cu.
 #include <cstddef>
+#include <cstdlib>
 #include <mutex>
 #include <unordered_map>
 
@@ -188,7 +189,9 @@ __device__ __forceinline__ void w_scalars(CgScalars* sc, const double* t) {
 }
 
 // One iteration (see the file comment); parity selects the record buffers.
-template <bool P>
+// C > 0: the row's blocks are taken C at a time, their columns and values
+// loaded together ahead of the C record gathers; C = 0: one unrolled loop.
+template <bool P, int C = 0>
 __device__ __forceinline__ void iter_body(const FusedArgs& a, int parity, double al, double bt, double* v) {
     const double2* __restrict__ go = parity ? a.gB : a.gA;
     double2* __restrict__ gn = parity ? a.gA : a.gB;
@@ -210,16 +213,42 @@ __device__ __forceinline__ void iter_body(const FusedArgs& a, int parity, double
         if (m.x) r.x -= al * kp.x;
         if (m.y) r.y -= al * kp.y;
         double k0 = 0.0, k1 = 0.0;
+        if (C == 0) {
 #pragma unroll 3
-        for (int k = 0; k < wd; ++k) {
-            const long long bi = base + 32LL * k + lane;
-            const int col = __ldg(a.scol + bi);
-            const double2 lo = load_lo(a.val, bi), hi = load_hi(a.val, bi);
-            const double2 uc = ld_other<P>(go + 3 * (size_t)col), mwc = ld_other<P>(go + 3 * (size_t)col + 1),
-                          mkc = ld_other<P>(go + 3 * (size_t)col + 2);
-            const double ux = uc.x - al * (mwc.x + bt * mkc.x), uy = uc.y - al * (mwc.y + bt * mkc.y);
-            k0 += lo.x * ux + lo.y * uy;
-            k1 += hi.x * ux + hi.y * uy;
+            for (int k = 0; k < wd; ++k) {
+                const long long bi = base + 32LL * k + lane;
+                const int col = __ldg(a.scol + bi);
+                const double2 lo = load_lo(a.val, bi), hi = load_hi(a.val, bi);
+                const double2 uc = ld_other<P>(go + 3 * (size_t)col), mwc = ld_other<P>(go + 3 * (size_t)col + 1),
+                              mkc = ld_other<P>(go + 3 * (size_t)col + 2);
+                const double ux = uc.x - al * (mwc.x + bt * mkc.x), uy = uc.y - al * (mwc.y + bt * mkc.y);
+                k0 += lo.x * ux + lo.y * uy;
+                k1 += hi.x * ux + hi.y * uy;
+            }
+        } else {
+            for (int k0i = 0; k0i < wd; k0i += (C > 0 ? C : 1)) {
+                int cc[C > 0 ? C : 1];
+                double2 lo[C > 0 ? C : 1], hi[C > 0 ? C : 1];
+#pragma unroll
+                for (int j = 0; j < C; ++j) {
+                    if (k0i + j < wd) {
+                        const long long bi = base + 32LL * (k0i + j) + lane;
+                        cc[j] = __ldg(a.scol + bi);
+                        lo[j] = load_lo(a.val, bi);
+                        hi[j] = load_hi(a.val, bi);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < C; ++j) {
+                    if (k0i + j < wd) {
+                        const double2* rc = go + 3 * (size_t)cc[j];
+                        const double2 uc = ld_other<P>(rc), mwc = ld_other<P>(rc + 1), mkc = ld_other<P>(rc + 2);
+                        const double ux = uc.x - al * (mwc.x + bt * mkc.x), uy = uc.y - al * (mwc.y + bt * mkc.y);
+                        k0 += lo[j].x * ux + lo[j].y * uy;
+                        k1 += hi[j].x * ux + hi[j].y * uy;
+                    }
+                }
+            }
         }
         const double2 w = make_double2(k0, k1);
         a.p[n] = p;
@@ -276,16 +305,28 @@ __global__ void __launch_bounds__(kThreads) k_f_w(FusedArgs a) {
     if (threadIdx.x == 0) w_scalars(sc, t);
 }
 
-__global__ void __launch_bounds__(kThreads) k_f_iter(FusedArgs a, int parity) {
+template <int C>
+__device__ __forceinline__ void iter_kernel_body(const FusedArgs& a, int parity) {
     __shared__ double sh[2 * kThreads / 32];
     __shared__ bool last;
     CgScalars* sc = a.sc;
     if (sc->converged || sc->status) return;
     double v[kSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    iter_body<false>(a, parity, sc->alpha, sc->beta, v);
+    iter_body<false, C>(a, parity, sc->alpha, sc->beta, v);
     double t[kSums];
     if (!reduce_sums(a, v, 5, t, sh, &last)) return;
     if (threadIdx.x == 0) iter_scalars(sc, t);
+}
+
+// C as in iter_body; k_f_iter4 asks the compiler for 4 resident blocks per
+// SM (a 64-register cap).
+template <int C>
+__global__ void __launch_bounds__(kThreads) k_f_iter(FusedArgs a, int parity) {
+    iter_kernel_body<C>(a, parity);
+}
+template <int C>
+__global__ void __launch_bounds__(kThreads, 4) k_f_iter4(FusedArgs a, int parity) {
+    iter_kernel_body<C>(a, parity);
 }
 
 // ---------------------------------------------------- persistent form --
@@ -350,6 +391,7 @@ __device__ __forceinline__ bool grid_wait(const FusedArgs& a, unsigned int step,
     return view->go != 0;
 }
 
+template <int C>
 __global__ void __launch_bounds__(kThreads) k_f_persistent(FusedArgs a, double eps2, long long max_iter) {
     __shared__ double sh[2 * kThreads / 32];
     __shared__ bool last;
@@ -379,7 +421,7 @@ __global__ void __launch_bounds__(kThreads) k_f_persistent(FusedArgs a, double e
         double v[kSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         const double al = view.alpha, bt = view.beta;
         __syncthreads();  // everyone has read the view before thread 0 overwrites it
-        iter_body<true>(a, it & 1, al, bt, v);
+        iter_body<true, C>(a, it & 1, al, bt, v);
         if (reduce_sums(a, v, 5, t, sh, &last) && threadIdx.x == 0) {
             iter_scalars(sc, t);
             grid_release(sc);
@@ -414,6 +456,39 @@ int fused_grid(K kernel, int n, int sm_count) {
     return g < 1 ? 1 : (int)g;
 }
 
+// The iteration kernel's form: CUPLAST_FUSED_FORM = 0 (one unrolled loop),
+// 1 (blocks 3 at a time), 2 (one loop, 4 blocks per SM), 3 (3 at a time, 4
+// blocks per SM), for measurements; the default is set below.
+constexpr int kDefaultForm = 0;
+using IterKernel = void (*)(FusedArgs, int);
+using PersistentKernel = void (*)(FusedArgs, double, long long);
+
+int form() {
+    static const int f = [] {
+        const char* e = std::getenv("CUPLAST_FUSED_FORM");
+        const int v = e ? std::atoi(e) : kDefaultForm;
+        return (v >= 0 && v <= 3) ? v : kDefaultForm;
+    }();
+    return f;
+}
+
+// the persistent form takes its blocks C at a time as the iteration kernel
+// does, so that both sum in the same order
+PersistentKernel persistent_kernel() {
+    return (form() == 1 || form() == 3) ? (PersistentKernel)k_f_persistent<3> : (PersistentKernel)k_f_persistent<0>;
+}
+IterKernel iter_kernel() {
+    static const IterKernel k = [] {
+        switch (form()) {
+        case 1: return (IterKernel)k_f_iter<3>;
+        case 2: return (IterKernel)k_f_iter4<0>;
+        case 3: return (IterKernel)k_f_iter4<3>;
+        default: return (IterKernel)k_f_iter<0>;
+        }
+    }();
+    return k;
+}
+
 }  // namespace
 
 void fused_launch_start(const FusedArgs& a, double eps2, long long max_iter, cudaStream_t s) {
@@ -426,7 +501,7 @@ void fused_launch_start(const FusedArgs& a, double eps2, long long max_iter, cud
 
 bool fused_persistent_fits(const FusedArgs& a) {
     const long long need = (a.n + kThreads - 1) / kThreads;
-    return need <= fused_grid(k_f_persistent, a.n, a.sm_count) && need <= fused_grid(k_f_iter, a.n, a.sm_count);
+    return need <= fused_grid(persistent_kernel(), a.n, a.sm_count) && need <= fused_grid(iter_kernel(), a.n, a.sm_count);
 }
 
 void fused_launch_persistent(const FusedArgs& a, double eps2, long long max_iter, cudaStream_t s) {
@@ -438,13 +513,14 @@ void fused_launch_persistent(const FusedArgs& a, double eps2, long long max_iter
     CP_CUDA(cudaMemsetAsync(&a.sc->ticket, 0, 2 * sizeof(unsigned int), s));
     FusedArgs args = a;
     void* params[] = {&args, &eps2, &max_iter};
-    CP_CUDA(cudaLaunchCooperativeKernel((const void*)k_f_persistent, dim3(g), dim3(kThreads), params, 0, s));
+    CP_CUDA(cudaLaunchCooperativeKernel((const void*)persistent_kernel(), dim3(g), dim3(kThreads), params, 0, s));
 }
 
 void fused_launch_iteration(const FusedArgs& a, int parity, cudaStream_t s) {
-    const int g = fused_grid(k_f_iter, a.n, a.sm_count);
+    const IterKernel k = iter_kernel();
+    const int g = fused_grid(k, a.n, a.sm_count);
     CP_CHECK(g <= a.max_blocks, CP_ERR_INVALID, "partials buffer too small");
-    k_f_iter<<<g, kThreads, 0, s>>>(a, parity);
+    k<<<g, kThreads, 0, s>>>(a, parity);
     CP_CUDA(cudaGetLastError());
 }
 

@@ -30,8 +30,10 @@ struct cp_instance {
     int n_nodes = 0, n_elem = 0;
     double2 *u = nullptr, *b = nullptr, *b_full = nullptr, *u_full = nullptr;
     uchar2* mask = nullptr;
-    double2 *r64 = nullptr, *z64a = nullptr, *z64b = nullptr, *q64 = nullptr, *s64 = nullptr;
-    float2 *r32 = nullptr, *z32a = nullptr, *z32b = nullptr, *q32 = nullptr, *s32 = nullptr;
+    double2 *r64 = nullptr, *z64a = nullptr, *z64b = nullptr, *q64 = nullptr;
+    float2 *r32 = nullptr, *q32 = nullptr;
+    double4 *rec64a = nullptr, *rec64b = nullptr;  // (v, z) records of the two-kernel CG (cg.cu), by parity
+    float4 *rec32a = nullptr, *rec32b = nullptr;
     double4* minv64 = nullptr;
     float4* minv32 = nullptr;
     cp::ElemState st{};

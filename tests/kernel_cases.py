@@ -8,8 +8,10 @@ Cases (each prints one JSON line with its host-side facts):
   2.1M DOF), R launches (cp_bench_assemble: CUDA events around them);
 * ``update``     -- k_update (strain, stress, secant update, exit norm) on the
   same plate, R launches after one linear solve;
-* ``cg_cluster`` -- k_c_solve: one PCG solve of the 64x64 O-grid plate
-  (8320 DOF) from zero, the whole solve in one thread-block cluster;
+* ``cg_cluster`` -- k_c_solve: R block-Jacobi PCG solves of the 64x64 O-grid
+  plate (8320 DOF) from zero (with the assembly and the secant update of a
+  one-iteration cp_solve around each), the whole solve in one thread-block
+  cluster; prints the time per CG iteration;
 * ``cg_graph``   -- the same solve with one k_f_iter launch per iteration
   (run with CUPLAST_FP64_CG=fused CUPLAST_NO_GRAPH=1 so that every launch is
   visible to the profiler);
@@ -118,9 +120,14 @@ def main(argv=None):
         inst.close()
     else:
         inst = _instance(ctx, 16, 64)
-        inst.assemble(CP_PREC_FP64)
-        it, rel = inst.cg_solve(1e-10)
-        out.update(nodes=inst.sizes()[0], cg_iters=it, rel_res=rel)
+        reps = []
+        for _ in range(a.repeat):
+            inst.set_field("uv", np.zeros(2 * inst.sizes()[0]))
+            reps.append(inst.solve(cg_tol=1e-10, outer_tol=1e300, max_outer=1, levels=1, precond=1,
+                                   max_cg=100000))
+        out.update(nodes=inst.sizes()[0], cg_iters=[r["cg_iters"] for r in reps],
+                   rel_res=reps[-1]["cg_rel_res"], seconds=[r["seconds"] for r in reps],
+                   us_per_iter=min(r["seconds"] / max(1, r["cg_iters"]) for r in reps) * 1e6)
         inst.close()
     ctx.close()
     print(json.dumps(out), flush=True)

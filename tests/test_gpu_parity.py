@@ -144,22 +144,24 @@ def test_persistent_cg_matches_graph_loop(name, ctx, golden_dir, workdir, monkey
 @pytest.mark.parametrize("name", ["hole12_pow", "ogrid16_bilin", "hole12_q8_pow"])
 def test_cluster_cg_matches_reference(name, ctx, golden_dir, workdir, monkeypatch):
     """The FP64 CG inside one thread-block cluster (the default where the
-    instance fits the cluster's shared memory): the converged state within
+    instance fits the cluster's shared memory), in both its forms
+    (CUPLAST_FP64_CG=cluster, cluster2): the converged state within
     1e-10 of the reference's, as the other solvers, and the same number of
     outer iterations as the grid-wide CG loop (CUPLAST_FP64_CG=fused, read at
     instance creation) within a couple (the summation order differs)."""
     m, lines = scenario(name, workdir)
     monkeypatch.setenv("CUPLAST_FP64_CG", "fused")
     base = product_runner.run(ctx, lines, m, precond=1)
-    monkeypatch.setenv("CUPLAST_FP64_CG", "cluster")
-    for precond in (0, 1):
-        r = product_runner.run(ctx, lines, m, precond=precond)
-        g = load_golden(golden_dir, name)
-        k, err, errs = worst(r, g)
-        assert err <= FP64_TOL, (name, precond, k, err, errs)
-        assert np.array_equal(yielded(r), yielded(g))
-    assert abs(r["report"]["outer_iters"] - base["report"]["outer_iters"]) <= 2
-    assert r["report"]["status"] == 0
+    for form in ("cluster", "cluster2"):
+        monkeypatch.setenv("CUPLAST_FP64_CG", form)
+        for precond in (0, 1):
+            r = product_runner.run(ctx, lines, m, precond=precond)
+            g = load_golden(golden_dir, name)
+            k, err, errs = worst(r, g)
+            assert err <= FP64_TOL, (name, form, precond, k, err, errs)
+            assert np.array_equal(yielded(r), yielded(g))
+        assert abs(r["report"]["outer_iters"] - base["report"]["outer_iters"]) <= 2
+        assert r["report"]["status"] == 0
 
 
 @pytest.mark.parametrize("name", ["ogrid16_bilin", "ogrid16_hollomon", "ogrid8_q8_bilin"])
@@ -273,6 +275,9 @@ def state_errors(r, g):
     ("config1_bilin", BENCH_OPTS),
     ("ogrid128x64_hollomon", BENCH_OPTS),
     ("ogrid128x64_hollomon", dict(aitken=1, precond=1, max_cg=2_000_000)),
+    # the aggregation-multigrid preconditioned FP64 CG (an extension)
+    ("config1_bilin", dict(aitken=1, adaptive_cg=1, precond=2, max_cg=2_000_000)),
+    ("ogrid128x64_hollomon", dict(aitken=1, adaptive_cg=1, precond=2, max_cg=2_000_000)),
 ])
 def test_configuration_size_state_matches_reference(name, opts, ctx, golden_dir, workdir):
     """Parity at configuration size: the benchmark's 64 x 64 O-grid job (its
