@@ -517,6 +517,87 @@ def served_leg(rate_hz=10.0, submit_s=20.0, drain_s=25.0, seed=20270101, precisi
     }
 
 
+CONFIG2 = dict(workload="hole_plate_ogrid1024x1024_q4_2099200dof_hollomon", n_circ=1024, n_rad=1024,
+               nodes=1049600, dof=2099200, elements=1048576, E_mpa=210000, nu=0.3, sigma_y=250, eps0=0.002,
+               n_exp=0.2, traction_mpa=220, increments=20, cg_tol=1e-10, outer_tol=1e-6)
+
+
+def config2_leg(ctx, cpu=True, cpu_cg_eps=1e-4):
+    """Configuration 2 end to end: the 1024 x 1024 O-grid plate (2.1M DOF),
+    Hollomon hardening sy (1 + eps_p / eps0)^n, 220 MPa in 20 increments, CG
+    1e-10, outer 1e-6, one FP64 solve through the drop-in (host arrays in,
+    every field out) with the headline's solver options.
+
+    CPU baseline: the reference cannot run this mesh as shipped (its band
+    matrix would take about 138 GB), so the reference-composed CSR-direct
+    harness (oracle/_ref/cpref_csr, mode phases_csr: the reference's calcBs,
+    initConditions, SparseSLAE, formC / formKe4, ConjGradSolver::solve,
+    updateParameters, exitCondition, with the element matrices added straight
+    into CSR) runs the first outer step of the first increment with a loose
+    CG tolerance, on all host cores: its set-up, assembly, CG-iteration and
+    update times. The CPU estimate of the full solve applies those per-step
+    and per-iteration times to the GPU solve's outer and CG iteration counts
+    (an estimate at equal iteration counts, not a measured CPU solve)."""
+    import numpy as np
+
+    import cudaplasticity_b200 as cp
+
+    mesh = cp.Mesh.rect_with_hole(-100.0, 100.0, -100.0, 100.0, 20.0, 256, 256, rad_n=1024)
+    arrays = mesh.arrays()
+    rp, mask, uv = cp.Loads().set_force(2, 0.0, 220.0).fix_border_hor(0).fix_point(-100.0, -100.0).build(mesh)
+    mat = cp.material(210000.0, 0.3, diagram="hollomon", sigma_y=250.0, eps0=0.002, n=0.2)
+    kw = dict(SOLVE_KW, levels=20, max_cg=5_000_000, max_outer=20000)
+    t0 = time.perf_counter()
+    inst = cp.Instance(ctx, arrays, mat)
+    inst.set_loads(rp, mask, uv)
+    rep = inst.solve(allow_not_converged=True, **kw)
+    st = inst.state()
+    inst.close()
+    wall = time.perf_counter() - t0
+    out = {"config": CONFIG2, "solver": "FP64 drop-in, Aitken secant, block-Jacobi PCG, adaptive CG rule 2, "
+                                         "level predictor (the headline's options)",
+           "gpu": {"seconds_e2e": wall, "seconds_device": rep["seconds"], "status": rep["status"],
+                   "outer_iters": rep["outer_iters"], "cg_iters": rep["cg_iters"], "levels_done": rep["levels_done"],
+                   "rel_err": rep["rel_err"], "kernel_launches": rep["kernel_launches"],
+                   "us_per_cg_iter": 1e6 * rep["seconds"] / max(1, rep["cg_iters"]),
+                   "yielded": int((np.asarray(st["psi"]) > 1.0 + 1e-12).sum())}}
+    if cpu:
+        import tempfile
+
+        import oracle
+
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import meshgen
+
+        if not os.path.exists(oracle.REF_BIN_CSR):
+            out["cpu_prefix"] = {"unavailable": "oracle/_ref/cpref_csr not built"}
+            return out
+        m = meshgen.hole_plate(-100.0, 100.0, -100.0, 100.0, 20.0, 256, 256, rad_n=1024)
+        threads = os.cpu_count()
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "m.bin")
+            oracle.write_mesh(path, m["node_xy"], elem4=m["elem4"], borders=m["borders"])
+            lines = ["mode phases_csr", f"mesh file {path}", "levels 20", f"cg_eps {cpu_cg_eps}", "outer_eps 1e-6",
+                     "max_outer 100000", "prefix_outer 1", "diagram hollomon 210000 250 0.002 0.2",
+                     "material 210000 0.3 1", "force 2 0 220 0", "fixborderhor 0", "fixpoint -100 -100"]
+            t1 = time.perf_counter()
+            r = oracle.run_reference(lines, threads=threads, binary=oracle.REF_BIN_CSR)
+            cwall = time.perf_counter() - t1
+        cg_it = int(r["cg_per_level"].sum())
+        per_it = float(r["cg_seconds"][0]) / max(1, cg_it)
+        per_outer = float(r["assembly_seconds"][0] + r["update_seconds"][0])
+        est = float(r["setup_seconds"][0]) + per_outer * rep["outer_iters"] + per_it * rep["cg_iters"]
+        out["cpu_prefix"] = {"kind": "reference (CSR-direct composition)", "cores": threads,
+                             "sample": f"first outer step of increment 1, CG {cpu_cg_eps:g} from zero, "
+                                       f"{cg_it} CG iterations", "wall_s": cwall,
+                             "setup_s": float(r["setup_seconds"][0]), "assembly_s": float(r["assembly_seconds"][0]),
+                             "update_s": float(r["update_seconds"][0]), "cg_s": float(r["cg_seconds"][0]),
+                             "ms_per_cg_iter": 1e3 * per_it,
+                             "estimated_full_solve_s_at_gpu_iteration_counts": est,
+                             "gpu_speedup_vs_estimate": est / wall}
+    return out
+
+
 def fifo_latencies(arrivals, service):
     """Latencies of requests served one at a time in arrival order by a
     single server whose service times are `service` (the plain drop-in):
@@ -963,6 +1044,8 @@ def main():
     ap.add_argument("--serve-window", type=float, default=20.0, help="seconds of arrivals in the served leg")
     ap.add_argument("--batched-probe", type=int, nargs=2, metavar=("N", "TRIPS"),
                     help="profiling aid: N resident batch-stream instances, TRIPS graph trips, then exit")
+    ap.add_argument("--config2", action="store_true",
+                    help="configuration 2 only (2.1M-DOF Hollomon plate, 20 increments) and its CPU prefix, then exit")
     ap.add_argument("--svp", type=int, metavar="N",
                     help="served-vs-plain leg only: the first N requests of --svp-stream, then exit")
     ap.add_argument("--svp-stream", default="served", choices=sorted(STREAMS))
@@ -977,6 +1060,13 @@ def main():
     FP64_SERVE_KW["precond"] = args.precond
     if args.batched_probe:
         batched_probe(*args.batched_probe)
+        return
+    if args.config2:
+        import cudaplasticity_b200 as cp
+
+        ctx = cp.Context(0)
+        print(json.dumps({"config2": config2_leg(ctx, cpu=not args.skip_cpu)}), flush=True)
+        ctx.close()
         return
     if args.svp:
         import cudaplasticity_b200 as cp

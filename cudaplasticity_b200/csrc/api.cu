@@ -147,6 +147,7 @@ cp::CgArgs<double> cp_instance::cg_args<double>(int precond) {
     a.r = r64;
     a.rec0 = rec64a;
     a.rec1 = rec64b;
+    a.zn = z64a;  // shared with the multigrid solve, which never runs at the same time
     a.q = q64;
     a.sc = sc;
     a.partials = partials;
@@ -171,6 +172,7 @@ cp::CgArgs<float> cp_instance::cg_args<float>(int precond) {
     a.r = r32;
     a.rec0 = rec32a;
     a.rec1 = rec32b;
+    a.zn = z32;
     a.q = q32;
     a.sc = sc;
     a.partials = partials;
@@ -208,6 +210,7 @@ void ensure_fp32(cp_instance* I) {
     I->r32 = I->alloc<float2>(I->n_nodes);
     I->rec32a = I->alloc<float4>(I->n_nodes);
     I->rec32b = I->alloc<float4>(I->n_nodes);
+    I->z32 = I->alloc<float2>(I->n_nodes);
     I->q32 = I->alloc<float2>(I->n_nodes);
 }
 
@@ -278,7 +281,7 @@ void cg_fp64_fused(cp_instance* I, double eps, long long max_iter, int precond) 
     a.partials = I->f_partials;
     if (I->cluster_fp64) {
         if (!I->cluster_planned) {
-            I->cluster_plan = cp::cluster_cg_plan(a, I->csr.max_width, I->cluster_variant);
+            I->cluster_plan = cp::cluster_cg_plan(a, I->csr.max_width);
             I->cluster_planned = 1;
         }
         if (I->cluster_plan.ctas > 0) {
@@ -538,8 +541,7 @@ CP_API int cp_instance_create(cp_context* ctx, const cp_mesh_view* mv, const cp_
     if (const char* g = std::getenv("CUPLAST_FP64_CG")) {
         I->fused_fp64 = std::strcmp(g, "classic") != 0;
         I->persistent_fp64 = std::strcmp(g, "persistent") == 0;
-        I->cluster_fp64 = std::strcmp(g, "cluster") == 0 || std::strcmp(g, "cluster2") == 0;
-        I->cluster_variant = std::strcmp(g, "cluster2") == 0 ? 2 : 1;
+        I->cluster_fp64 = std::strcmp(g, "cluster") == 0;
     }
     if (const char* g = std::getenv("CUPLAST_TEST_BARRIER_NS")) I->test_barrier_ns = std::strtoull(g, nullptr, 10);
     int rc = guarded(ctx, [&] {
@@ -999,12 +1001,12 @@ CP_API int cp_bench_cg(cp_instance* I, int precision, int precond, int iters, do
         // algorithmic bytes per launch (2 DOFs per node, N = 2n):
         //  P: values nnz*sv + block columns nnz/4*4 + read r, z + write z', Kz' (4 N sx)
         //  U: read x (16 n), z', r, Kz' (3 N sx), mask (2 n); write x, r (16 n + N sx)
-        //     and the record's v = M^-1 r (or r) (N sx) [+ block Jacobi: read M^-1 (4 n sx)]
+        //     and the record (v', z') (2 N sx) [+ block Jacobi: read M^-1 (4 n sx)]
         const double N = 2 * n;
         if (ms_p) *ms_p = tp / iters;
         if (ms_u) *ms_u = tu / iters;
         if (bytes_p) *bytes_p = nnz * sv + nnz + 4 * N * sx;
-        if (bytes_u) *bytes_u = 32 * n + 4 * N * sx + 2 * n + (precond ? 4 * n * sx : 0.0) + N * sx;
+        if (bytes_u) *bytes_u = 32 * n + 4 * N * sx + 2 * n + (precond ? 4 * n * sx : 0.0) + 2 * N * sx;
     });
 }
 

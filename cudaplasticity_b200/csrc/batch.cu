@@ -839,16 +839,17 @@ __global__ void k_batch_cond(BCtl* c, cudaGraphConditionalHandle h) {
 // see kernel nodes of a graph with a conditional node).
 __global__ void k_batch_cond_direct(BCtl* c) { trip_condition(c); }
 
-// The batched CG kernel's ITER gather form: CUPLAST_BATCH_CHUNK = 0 (one
-// unrolled loop) or 3 / 5 (blocks that many at a time), for measurements.
+// The batched CG kernel's ITER gather form: CUPLAST_BATCH_CHUNK = 3 (blocks
+// 3 at a time: the default, 5 % faster per trip of 512 instances than one
+// unrolled loop), 0 (one unrolled loop) or 5, for measurements.
 using BatchCgKernel = void (*)(const BDesc*, BState*, const int4*, BCtl*);
 BatchCgKernel batch_cg_kernel() {
     static const BatchCgKernel k = [] {
         const char* e = std::getenv("CUPLAST_BATCH_CHUNK");
-        switch (e ? std::atoi(e) : 0) {
-        case 3: return (BatchCgKernel)k_batch_cg<3>;
+        switch (e ? std::atoi(e) : 3) {
+        case 0: return (BatchCgKernel)k_batch_cg<0>;
         case 5: return (BatchCgKernel)k_batch_cg<5>;
-        default: return (BatchCgKernel)k_batch_cg<0>;
+        default: return (BatchCgKernel)k_batch_cg<3>;
         }
     }();
     return k;

@@ -14,9 +14,10 @@
 //   U: x += alpha z', r -= m.alpha K z', v' = M r (v' = r without the
 //      preconditioner), (r, r)
 // The neighbours' inputs of P are packed in one record per node, rec[n] =
-// (v, z), double-buffered by iteration parity: P reads (v, z) of parity p
-// and writes z' into the record of parity 1 - p, U writes v' there. A
-// neighbour costs one gather (16 bytes in FP32, 32 in FP64).
+// (v, z), double-buffered by iteration parity: P reads (v, z) of parity p and
+// writes z' to a plain vector, U writes the whole record (v', z') of parity
+// 1 - p (whole records: no partially written L2 sectors). A neighbour costs
+// one gather (16 bytes in FP32, 32 in FP64).
 // Scalars live on the device; every cross-block sum is reduced by the last
 // block in index order (deterministic). The loop runs in a CUDA graph whose
 // WHILE node re-launches the body until the device sets "converged".
@@ -68,11 +69,6 @@ __device__ __forceinline__ double4 load_rec<double>(const double4* rec, int c) {
     return make_double4(lo.x, lo.y, hi.x, hi.y);
 }
 
-// The two halves of a record, written separately: v by U, z by P.
-template <typename T>
-__device__ __forceinline__ typename Vec2<T>::type* rec_half(typename Vec4<T>::type* rec, int n, int half) {
-    return reinterpret_cast<typename Vec2<T>::type*>(rec + n) + half;
-}
 
 // One warp per slice of 32 nodes, one thread per node: the loop over slices
 // advances whole warps, so the trip count is warp-uniform.
@@ -203,7 +199,6 @@ __global__ void __launch_bounds__(kThreads) k_cg_p(CgArgs<T> a, int parity) {
     CgScalars* sc = a.sc;
     if (sc->converged || sc->status) return;
     const V4* __restrict__ ro = parity ? a.rec1 : a.rec0;
-    V4* __restrict__ rn = parity ? a.rec0 : a.rec1;
     const T beta = (T)sc->beta;
     double dot = 0.0;
     CP_SLICE_LOOP(a.n) {
@@ -251,7 +246,7 @@ __global__ void __launch_bounds__(kThreads) k_cg_p(CgArgs<T> a, int parity) {
             zz.y = own.y + beta * own.w;
             qq.x = k0;
             qq.y = k1;
-            *rec_half<T>(rn, n, 1) = zz;
+            a.zn[n] = zz;
             a.q[n] = qq;
             dot += (double)k0 * (double)zz.x + (double)k1 * (double)zz.y;
         }
@@ -277,11 +272,12 @@ __global__ void __launch_bounds__(kThreads) k_cg_u(CgArgs<T> a, int parity) {
     CgScalars* sc = a.sc;
     if (sc->converged || sc->status) return;
     typename Vec4<T>::type* __restrict__ rn = parity ? a.rec0 : a.rec1;
+    using V4 = typename Vec4<T>::type;
     const double alpha = sc->alpha;
     const T alpha_t = (T)alpha;
     double dot = 0.0, dot_s = 0.0;
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < a.n; n += gridDim.x * blockDim.x) {
-        const V2 z = *rec_half<T>(rn, n, 1), q = a.q[n];
+        const V2 z = a.zn[n], q = a.q[n];
         const uchar2 m = a.mask[n];
         double2 x = a.x[n];
         x.x += alpha * (double)z.x;
@@ -292,16 +288,22 @@ __global__ void __launch_bounds__(kThreads) k_cg_u(CgArgs<T> a, int parity) {
         if (m.y) r.y -= alpha_t * q.y;
         a.r[n] = r;
         dot += (double)r.x * (double)r.x + (double)r.y * (double)r.y;
+        V4 rec;
+        rec.z = z.x;
+        rec.w = z.y;
         if (PRE) {
             const auto mi = a.minv[n];
             V2 sv;
             sv.x = mi.x * r.x + mi.y * r.y;
             sv.y = mi.z * r.x + mi.w * r.y;
-            *rec_half<T>(rn, n, 0) = sv;
+            rec.x = sv.x;
+            rec.y = sv.y;
             dot_s += (double)r.x * (double)sv.x + (double)r.y * (double)sv.y;
         } else {
-            *rec_half<T>(rn, n, 0) = r;
+            rec.x = r.x;
+            rec.y = r.y;
         }
+        rn[n] = rec;
     }
     __shared__ double sh2[2 * kThreads / 32];
     const double2 bs = block_sum2(dot, dot_s, sh2);
@@ -382,7 +384,7 @@ int p_chunk() {
     static const int c = [] {
         const char* e = std::getenv("CUPLAST_CG_CHUNK");
         const int v = e ? std::atoi(e) : -1;
-        return (v == 0 || v == 3 || v == 5 || v == 9) ? v : (sizeof(T) == 4 ? 5 : 3);
+        return (v == 0 || v == 3 || v == 5 || v == 9) ? v : 0;
     }();
     return c;
 }

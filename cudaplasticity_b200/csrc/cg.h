@@ -46,6 +46,7 @@ struct CgArgs {
     // direction; by iteration parity
     typename Vec4<T>::type* rec0 = nullptr;
     typename Vec4<T>::type* rec1 = nullptr;
+    V2* zn = nullptr;               // z' from P to U
     V2* q = nullptr;
     CgScalars* sc = nullptr;
     double* partials = nullptr;     // >= 3 * max_blocks doubles
@@ -91,9 +92,8 @@ struct ClusterPlan {
     int spc = 0;       // slices of 32 nodes per CTA (one warp each)
     int wmax = 0;      // widest node row, in blocks
     size_t smem = 0;   // dynamic shared memory per CTA
-    int variant = 1;   // 1: k_c_solve; 2: k_c_solve2 (opt-in second form)
 };
-ClusterPlan cluster_cg_plan(const FusedArgs& a, int max_width, int variant = 1);
+ClusterPlan cluster_cg_plan(const FusedArgs& a, int max_width);
 void cluster_cg_launch(const FusedArgs& a, const ClusterPlan& plan, double eps2, long long max_iter, cudaStream_t s);
 
 template <typename T>

@@ -300,264 +300,6 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1)
     }
 }
 
-// ------------------------------------------------- second form (opt-in) --
-//
-// The same solve with the per-iteration chain shortened, selected by
-// CUPLAST_FP64_CG=cluster2 until measured against the form above:
-//   - each warp publishes its own partial sums (no CTA barrier to combine
-//     them), and after the cluster barrier every warp of every CTA reduces
-//     all warps' partials itself, in one fixed order through one fixed
-//     shuffle tree, so every thread holds the same scalars (no broadcast, no
-//     second barrier): the only barrier of an iteration is the cluster's;
-//   - the neighbours' record addresses are precomputed per block (one 8-byte
-//     shared load instead of two dependent ones), and the gather is unrolled
-//     to the compile-time row width WMAX so that its loads issue together.
-// Shared memory of one CTA (dynamic part):
-//   kval [spc][WMAX][32] double4, kptr [spc][WMAX][32] const double2*,
-//   rec [2][spc * 32][3] double2, wpart [2][spc][8] double.
-struct Smem2 {
-    double4* kval;
-    const double2** kptr;
-    double2* rec;
-    double* wpart;
-};
-
-template <int WMAX>
-__device__ __forceinline__ Smem2 carve2(unsigned char* base, int spc) {
-    Smem2 s;
-    const size_t nb = (size_t)spc * WMAX * 32;
-    s.kval = reinterpret_cast<double4*>(base);
-    s.kptr = reinterpret_cast<const double2**>(base + nb * sizeof(double4));
-    s.rec = reinterpret_cast<double2*>(base + nb * (sizeof(double4) + sizeof(void*)));
-    s.wpart = reinterpret_cast<double*>(base + nb * (sizeof(double4) + sizeof(void*)) +
-                                        2 * (size_t)spc * 32 * 3 * sizeof(double2));
-    return s;
-}
-
-size_t smem_bytes2(int spc, int wmax) {
-    const size_t nb = (size_t)spc * wmax * 32;
-    return nb * (sizeof(double4) + sizeof(void*)) + 2 * (size_t)spc * 32 * 3 * sizeof(double2) +
-           2 * (size_t)spc * 8 * sizeof(double);
-}
-
-// Totals of K sums over every warp of every CTA (parts[c] = CTA c's partials
-// of this parity, 8 doubles per warp), the same in every warp.
-template <int K>
-__device__ __forceinline__ void all_totals(double* const* parts, int ctas, int nw, double* tot) {
-    const int lane = threadIdx.x & 31;
-    double acc[K];
-#pragma unroll
-    for (int i = 0; i < K; ++i) acc[i] = 0.0;
-    for (int e = lane; e < ctas * nw; e += 32) {
-        const double* p = parts[e / nw] + 8 * (e % nw);
-#pragma unroll
-        for (int i = 0; i < K; ++i) acc[i] += p[i];
-    }
-#pragma unroll
-    for (int i = 0; i < K; ++i) tot[i] = warp_sum(acc[i]);
-}
-
-// This warp's sums of K values per thread into wpart (lane 0 writes).
-template <int K>
-__device__ __forceinline__ void warp_partials(const double* v, double* wpart) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-        const double s = warp_sum(v[i]);
-        if (lane == 0) wpart[i] = s;
-    }
-}
-
-template <int WMAX>
-__global__ void __launch_bounds__(kMaxWarps * 32, 1)
-    k_c_solve2(FusedArgs a, ClusterPlan shp, double eps2, long long max_iter) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double* part_of[2][kMaxCluster];
-
-    cgr::cluster_group cl = cgr::this_cluster();
-    const int rank = (int)cl.block_rank();
-    const int spc = shp.spc, ctas = shp.ctas, nw = spc;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int n_slices = (a.n + 31) / 32;
-    const int sl = rank * spc + w;
-    const int n = 32 * sl + lane;
-    const bool act = sl < n_slices && n < a.n;
-    const int loc = w * 32 + lane;
-    Smem2 S = carve2<WMAX>(smem_raw, spc);
-    const size_t rec_half = (size_t)spc * 32 * 3;  // double2 per parity buffer
-    if (threadIdx.x < ctas) {
-        part_of[0][threadIdx.x] = cl.map_shared_rank(S.wpart, (int)threadIdx.x);
-        part_of[1][threadIdx.x] = cl.map_shared_rank(S.wpart + 8 * spc, (int)threadIdx.x);
-    }
-    int wd = 0;
-    if (sl < n_slices) wd = (a.slice_ptr[sl + 1] - a.slice_ptr[sl]) >> 5;
-    if (act) {
-        const int base = a.slice_ptr[sl];
-        for (int k = 0; k < wd; ++k) {
-            const long long bi = base + 32LL * k + lane;
-            const int col = __ldg(a.scol + bi);
-            const double2 lo = __ldg(reinterpret_cast<const double2*>(a.val + 4 * bi));
-            const double2 hi = __ldg(reinterpret_cast<const double2*>(a.val + 4 * bi) + 1);
-            const int cr = (col >> 5) / spc;
-            const size_t q = ((size_t)w * WMAX + k) * 32 + lane;
-            S.kval[q] = make_double4(lo.x, lo.y, hi.x, hi.y);
-            S.kptr[q] = cl.map_shared_rank(S.rec, cr) + 3 * (size_t)(col - cr * spc * 32);
-        }
-    }
-    double2 x = make_double2(0.0, 0.0), bb = x, r = x, p = x, kp = x, wv = x, u = x, mw = x, mk = x;
-    uchar2 m = make_uchar2(0, 0);
-    double4 minv = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (act) {
-        x = a.x[n];
-        bb = a.b[n];
-        m = a.mask[n];
-        S.rec[rec_half + 3 * (size_t)loc] = x;
-    }
-    cl.sync();
-
-    auto apply_m = [&](double2 v) {
-        if (a.precond) return mvec(minv, v);
-        return make_double2(m.x ? v.x : 0.0, m.y ? v.y : 0.0);
-    };
-    auto gather0 = [&](size_t off) {  // sum_k K_k (first double2 of the record at offset off)
-        double k0 = 0.0, k1 = 0.0;
-#pragma unroll
-        for (int k = 0; k < WMAX; ++k) {
-            if (k < wd) {
-                const size_t q = ((size_t)w * WMAX + k) * 32 + lane;
-                const double4 kv = S.kval[q];
-                const double2 v = S.kptr[q][off];
-                k0 += kv.x * v.x + kv.y * v.y;
-                k1 += kv.z * v.x + kv.w * v.y;
-            }
-        }
-        return make_double2(k0, k1);
-    };
-
-    double v[kSums] = {0.0, 0.0, 0.0, 0.0, 0.0}, tot[kSums];
-    if (act) {
-        const double2 kx = gather0(rec_half);
-        r = make_double2(m.x ? bb.x - kx.x : 0.0, m.y ? bb.y - kx.y : 0.0);
-        if (a.precond) {
-            const double4 d = S.kval[((size_t)w * WMAX) * 32 + lane];
-            if (m.x && m.y) {
-                const double det = d.x * d.w - d.y * d.z;
-                minv = make_double4(d.w / det, -d.y / det, -d.z / det, d.x / det);
-            } else if (m.x) {
-                minv.x = 1.0 / d.x;
-            } else if (m.y) {
-                minv.w = 1.0 / d.w;
-            }
-        }
-        u = apply_m(r);
-        S.rec[3 * (size_t)loc] = u;
-        S.rec[3 * (size_t)loc + 2] = make_double2(0.0, 0.0);
-        v[0] = r.x * r.x + r.y * r.y;
-        v[1] = bb.x * bb.x + bb.y * bb.y;
-    }
-    warp_partials<2>(v, S.wpart + 8 * w);
-    cl.sync();
-    all_totals<2>(part_of[0], ctas, nw, tot);
-    const double rr0 = tot[0], bnorm2 = tot[1];
-    const double normB_inv = bnorm2 > 0.0 ? 1.0 / bnorm2 : 0.0;
-    int status = 0, converged = (rr0 == 0.0 || rr0 * normB_inv <= eps2) ? 1 : 0;
-    if (!(rr0 == rr0) || !(bnorm2 == bnorm2)) status = CP_ERR_BREAKDOWN;
-    double rr = rr0, rho = 0.0, alpha = 0.0, beta = 0.0;
-    long long iter = 0;
-    if (!converged && !status) {
-        v[0] = v[1] = 0.0;
-        if (act) {
-            wv = gather0(0);
-            mw = apply_m(wv);
-            S.rec[3 * (size_t)loc + 1] = mw;
-            v[0] = r.x * u.x + r.y * u.y;
-            v[1] = wv.x * u.x + wv.y * u.y;
-        }
-        warp_partials<2>(v, S.wpart + 8 * spc + 8 * w);
-        cl.sync();
-        all_totals<2>(part_of[1], ctas, nw, tot);
-        rho = tot[0];
-        alpha = tot[0] / tot[1];
-        if (!(tot[1] > 0.0) || !(alpha == alpha)) status = CP_ERR_BREAKDOWN;
-    }
-    int parity = 0;
-    while (!converged && !status) {
-        const size_t go = parity ? rec_half : 0, gn = parity ? 0 : rec_half;
-        double t[kSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        if (act) {
-            const double al = alpha, bt = beta;
-            const double2 u0 = u;
-            p = make_double2(u0.x + bt * p.x, u0.y + bt * p.y);
-            kp = make_double2(wv.x + bt * kp.x, wv.y + bt * kp.y);
-            u = make_double2(u0.x - al * (mw.x + bt * mk.x), u0.y - al * (mw.y + bt * mk.y));
-            x.x += al * p.x;
-            x.y += al * p.y;
-            if (m.x) r.x -= al * kp.x;
-            if (m.y) r.y -= al * kp.y;
-            double k0 = 0.0, k1 = 0.0;
-#pragma unroll
-            for (int k = 0; k < WMAX; ++k) {
-                if (k < wd) {
-                    const size_t q = ((size_t)w * WMAX + k) * 32 + lane;
-                    const double4 kv = S.kval[q];
-                    const double2* rc = S.kptr[q] + go;
-                    const double2 uc = rc[0], mwc = rc[1], mkc = rc[2];
-                    const double ux = uc.x - al * (mwc.x + bt * mkc.x), uy = uc.y - al * (mwc.y + bt * mkc.y);
-                    k0 += kv.x * ux + kv.y * uy;
-                    k1 += kv.z * ux + kv.w * uy;
-                }
-            }
-            wv = make_double2(k0, k1);
-            mw = apply_m(wv);
-            mk = apply_m(kp);
-            S.rec[gn + 3 * (size_t)loc] = u;
-            S.rec[gn + 3 * (size_t)loc + 1] = mw;
-            S.rec[gn + 3 * (size_t)loc + 2] = mk;
-            t[0] = r.x * u.x + r.y * u.y;
-            t[1] = wv.x * u.x + wv.y * u.y;
-            t[2] = r.x * r.x + r.y * r.y;
-            t[3] = (wv.x * p.x + wv.y * p.y) + (kp.x * u.x + kp.y * u.y);
-            t[4] = kp.x * p.x + kp.y * p.y;
-        }
-        warp_partials<kSums>(t, S.wpart + 8 * spc * parity + 8 * w);
-        cl.sync();
-        all_totals<kSums>(part_of[parity], ctas, nw, tot);
-        const double g = tot[0], rn = tot[2];
-        const double b2 = g / rho;
-        const double den = tot[1] + b2 * tot[3] + b2 * b2 * tot[4];
-        ++iter;
-        rr = rn;
-        beta = b2;
-        alpha = g / den;
-        rho = g;
-        if (rn * normB_inv <= eps2) converged = 1;
-        else if (iter >= max_iter) status = CP_ERR_NOT_CONVERGED;
-        else if (!(den > 0.0) || !(g > 0.0)) status = CP_ERR_BREAKDOWN;
-        if (!(rn == rn)) status = CP_ERR_BREAKDOWN;
-        parity ^= 1;
-    }
-    cl.sync();
-    if (act) a.x[n] = x;
-    if (rank == 0 && threadIdx.x == 0) {
-        CgScalars* sc = a.sc;
-        sc->rr = rr;
-        sc->bb = bnorm2;
-        sc->res64 = rr0;
-        sc->normB_inv = normB_inv;
-        sc->eps2 = eps2;
-        sc->iter = iter;
-        sc->max_iter = max_iter;
-        sc->converged = converged;
-        sc->status = status;
-        sc->lin_done = 0;
-        sc->alpha = alpha;
-        sc->beta = beta;
-        sc->rho = rho;
-        sc->ticket = 0;
-    }
-}
-
-
 // Sets the launch attributes of kernel k and checks that a cluster of the
 // shape can be scheduled.
 template <typename K>
@@ -612,27 +354,19 @@ void launch_cluster(K k, const FusedArgs& a, const ClusterPlan& shp, double eps2
 }  // namespace
 
 // The cluster shape for an instance, or ctas = 0 when it does not fit.
-ClusterPlan cluster_cg_plan(const FusedArgs& a, int wmax, int variant) {
+ClusterPlan cluster_cg_plan(const FusedArgs& a, int wmax) {
     ClusterPlan s;
     const int n_slices = (a.n + 31) / 32;
-    const int wcap = variant == 2 ? (wmax <= 9 ? 9 : wmax <= 13 ? 13 : wmax <= 21 ? 21 : 0) : wmax;
-    if (wcap == 0) return s;
     for (int ctas : {16, 8}) {
         const int spc = (n_slices + ctas - 1) / ctas;
         if (spc > kMaxWarps) continue;
-        const size_t smem = variant == 2 ? smem_bytes2(spc, wcap) : smem_bytes(spc, wcap);
+        const size_t smem = smem_bytes(spc, wmax);
         if (smem > (size_t)kSmemCap) continue;
-        bool ok = false;
-        if (variant != 2) ok = cluster_fits(k_c_solve, ctas, spc, smem);
-        else if (wcap == 9) ok = cluster_fits(k_c_solve2<9>, ctas, spc, smem);
-        else if (wcap == 13) ok = cluster_fits(k_c_solve2<13>, ctas, spc, smem);
-        else ok = cluster_fits(k_c_solve2<21>, ctas, spc, smem);
-        if (!ok) continue;
+        if (!cluster_fits(k_c_solve, ctas, spc, smem)) continue;
         s.ctas = ctas;
         s.spc = spc;
-        s.wmax = wcap;
+        s.wmax = wmax;
         s.smem = smem;
-        s.variant = variant == 2 ? 2 : 1;
         return s;
     }
     return s;
@@ -641,10 +375,7 @@ ClusterPlan cluster_cg_plan(const FusedArgs& a, int wmax, int variant) {
 void cluster_cg_launch(const FusedArgs& a, const ClusterPlan& shp, double eps2, long long max_iter, cudaStream_t s) {
     CP_CHECK(shp.ctas > 0 && shp.spc * 32 * shp.ctas >= a.n, CP_ERR_INVALID,
              "cluster CG: the instance does not fit one cluster");
-    if (shp.variant != 2) launch_cluster(k_c_solve, a, shp, eps2, max_iter, s);
-    else if (shp.wmax == 9) launch_cluster(k_c_solve2<9>, a, shp, eps2, max_iter, s);
-    else if (shp.wmax == 13) launch_cluster(k_c_solve2<13>, a, shp, eps2, max_iter, s);
-    else launch_cluster(k_c_solve2<21>, a, shp, eps2, max_iter, s);
+    launch_cluster(k_c_solve, a, shp, eps2, max_iter, s);
 }
 
 }  // namespace cp

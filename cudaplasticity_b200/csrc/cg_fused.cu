@@ -457,9 +457,10 @@ int fused_grid(K kernel, int n, int sm_count) {
 }
 
 // The iteration kernel's form: CUPLAST_FUSED_FORM = 0 (one unrolled loop),
-// 1 (blocks 3 at a time), 2 (one loop, 4 blocks per SM), 3 (3 at a time, 4
-// blocks per SM), for measurements; the default is set below.
-constexpr int kDefaultForm = 0;
+// 1 (blocks 3 at a time: the default, 20 % faster than 0 on the 2.1M-DOF
+// plate), 2 (one loop, 4 blocks per SM), 3 (3 at a time, 4 blocks per SM),
+// 4 / 5 (2 / 5 at a time), for measurements.
+constexpr int kDefaultForm = 1;
 using IterKernel = void (*)(FusedArgs, int);
 using PersistentKernel = void (*)(FusedArgs, double, long long);
 
@@ -467,7 +468,7 @@ int form() {
     static const int f = [] {
         const char* e = std::getenv("CUPLAST_FUSED_FORM");
         const int v = e ? std::atoi(e) : kDefaultForm;
-        return (v >= 0 && v <= 3) ? v : kDefaultForm;
+        return (v >= 0 && v <= 5) ? v : kDefaultForm;
     }();
     return f;
 }
@@ -475,15 +476,22 @@ int form() {
 // the persistent form takes its blocks C at a time as the iteration kernel
 // does, so that both sum in the same order
 PersistentKernel persistent_kernel() {
-    return (form() == 1 || form() == 3) ? (PersistentKernel)k_f_persistent<3> : (PersistentKernel)k_f_persistent<0>;
+    switch (form()) {
+    case 0: case 2: return (PersistentKernel)k_f_persistent<0>;
+    case 4: return (PersistentKernel)k_f_persistent<2>;
+    case 5: return (PersistentKernel)k_f_persistent<5>;
+    default: return (PersistentKernel)k_f_persistent<3>;
+    }
 }
 IterKernel iter_kernel() {
     static const IterKernel k = [] {
         switch (form()) {
-        case 1: return (IterKernel)k_f_iter<3>;
+        case 0: return (IterKernel)k_f_iter<0>;
         case 2: return (IterKernel)k_f_iter4<0>;
         case 3: return (IterKernel)k_f_iter4<3>;
-        default: return (IterKernel)k_f_iter<0>;
+        case 4: return (IterKernel)k_f_iter<2>;
+        case 5: return (IterKernel)k_f_iter<5>;
+        default: return (IterKernel)k_f_iter<3>;
         }
     }();
     return k;

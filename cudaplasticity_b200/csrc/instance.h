@@ -31,7 +31,7 @@ struct cp_instance {
     double2 *u = nullptr, *b = nullptr, *b_full = nullptr, *u_full = nullptr;
     uchar2* mask = nullptr;
     double2 *r64 = nullptr, *z64a = nullptr, *z64b = nullptr, *q64 = nullptr;
-    float2 *r32 = nullptr, *q32 = nullptr;
+    float2 *r32 = nullptr, *z32 = nullptr, *q32 = nullptr;
     double4 *rec64a = nullptr, *rec64b = nullptr;  // (v, z) records of the two-kernel CG (cg.cu), by parity
     float4 *rec32a = nullptr, *rec32b = nullptr;
     double4* minv64 = nullptr;
@@ -59,7 +59,6 @@ struct cp_instance {
     // CP_ERR_TIMEOUT
     unsigned long long test_barrier_ns = 0;
     bool cluster_fp64 = true;      // one thread-block cluster when the instance fits (CUPLAST_FP64_CG other than cluster: off)
-    int cluster_variant = 1;       // 2: the second form (CUPLAST_FP64_CG=cluster2)
     int cluster_planned = 0;       // cluster_plan below is computed (once per instance)
     double2* pred_u = nullptr;     // level predictor (cp_solve_opts.predict): the last level's u and psi
     double* pred_psi = nullptr;

@@ -24,6 +24,10 @@ REF_BIN = os.path.join(HERE, "_ref", "cpref")
 # the same harness with the reference's Mesh.cu built at -O0, for its .inp
 # loader (see the Makefile)
 REF_BIN_INP = os.path.join(HERE, "_ref", "cpref_inp")
+# the harness built with the solver's source for its phases_csr mode (the
+# reference's element arithmetic added straight into CSR: meshes whose band
+# matrix does not fit)
+REF_BIN_CSR = os.path.join(HERE, "_ref", "cpref_csr")
 
 _lib = None
 

@@ -32,6 +32,17 @@
  *   displpoint x y ux uy | gravity g dx dy | fixdof d (extra Dirichlet DOF, value 0)
  *   cg_eps e | outer_eps e | max_outer n | levels k (load factors k/n for k=1..n)
  *   dump_k 1 | dump_csr 1
+ *   prefix_outer n                           (phases / phases_csr: stop after n outer iterations in all)
+ *
+ * mode phases_csr is mode phases with one change, for meshes whose band
+ * matrix does not fit in host memory (the reference's fillGlobalStiffness
+ * assembles into a StripSLAE of N x (2W + 1) doubles, W about 4 n_r on the
+ * ring-numbered O-grid: about 138 GB for the 1024 x 1024 plate): each
+ * element's C and Ke come from the reference's own formC / formKe4, and Ke
+ * is added straight into the CSR values through a table of CSR positions
+ * built once from the reference's SparseSLAE. Everything else (calcBs,
+ * initConditions, ConjGradSolver::solve, updateParameters, exitCondition)
+ * is the reference's. 4-node elements only.
  */
 #include <unistd.h>
 #include <csetjmp>
@@ -55,7 +66,14 @@
 
 #define private public
 #define protected public
+#ifdef CPREF_SOLVER_SOURCE
+/* the phases_csr build (cpref_csr): the solver's source in this unit, so
+ * that its file-local element routines (formKe4) can be called; linked
+ * without the separately compiled PlasticitySolver object */
+#include "PlasticitySolver.cu"
+#else
 #include "PlasticitySolver.cuh"
+#endif
 #include "ConjGradSolver.h"
 #undef private
 #undef protected
@@ -106,6 +124,7 @@ struct Job {
     bool dumpK = false, dumpCsr = false;
     std::vector<int> fixDofs;
     std::vector<std::vector<std::string>> loads;
+    long long prefixOuter = 0;
 };
 
 static std::vector<std::string> split(const std::string& s) {
@@ -137,6 +156,7 @@ static Job parseJob(const char* path) {
         else if (k == "dump_k") j.dumpK = atoi(w[1].c_str()) != 0;
         else if (k == "dump_csr") j.dumpCsr = atoi(w[1].c_str()) != 0;
         else if (k == "fixdof") j.fixDofs.push_back(atoi(w[1].c_str()));
+        else if (k == "prefix_outer") j.prefixOuter = atoll(w[1].c_str());
         else j.loads.push_back(w);
     }
     return j;
@@ -315,6 +335,51 @@ static void dumpState(FILE* f, PlasticitySolver& ps, int E, int N) {
     cpbin_put(f, "eps_p_i", 'd', E, ps.intE_p);
 }
 
+#ifdef CPREF_SOLVER_SOURCE
+/* CSR position of every (local row, local column) DOF pair of every 4-node
+ * element: 64 per element, row-major over the element's 8 DOFs. */
+static std::vector<int> csrSlots4(const Mesh& mesh, const SparseSLAE& sp) {
+    std::vector<int> slots((size_t)mesh.count4 * 64);
+#pragma omp parallel for
+    for (long long e = 0; e < (long long)mesh.count4; ++e) {
+        for (int a = 0; a < 8; ++a) {
+            const int gi = 2 * mesh.elem4[4 * e + a / 2] + a % 2;
+            for (int b = 0; b < 8; ++b) {
+                const int gj = 2 * mesh.elem4[4 * e + b / 2] + b % 2;
+                int pos = -1;
+                for (int q = sp.rows[gi]; q < sp.rows[gi + 1]; ++q)
+                    if (sp.cols[q] == gj) { pos = q; break; }
+                slots[(size_t)e * 64 + 8 * a + b] = pos;
+            }
+        }
+    }
+    return slots;
+}
+
+/* fillGlobalStiffness with the band matrix replaced by the CSR slot table
+ * (see the file comment); the per-element arithmetic is the reference's. */
+static void fillCsrDirect(PlasticitySolver& ps, SparseSLAE& spK, const std::vector<int>& slots) {
+    const Mesh& mesh = ps.mesh;
+    const int nnz = spK.rows[2 * mesh.nodeCount];
+    std::memset(spK.data, 0, sizeof(double) * (size_t)nnz);
+#pragma omp parallel for
+    for (int e = mesh.elemPos[0]; e < mesh.elemPos[1]; ++e) {
+        StaticMatrix<3, 3, double> Ce;
+        (*ps.formC)(Ce, ps.E_c[e], ps.nu_c[e]);
+        std::memcpy(ps.C + e, &Ce, sizeof(Ce));
+        SymMatrix<8, double> Ke;
+        formKe4(Ke, e, ps.B4, ps.detJ4, Ce, ps.m.h);
+        const int le = e - mesh.elemPos[0];
+        for (int a = 0; a < 8; ++a)
+            for (int b = 0; b < 8; ++b) {
+                const double v = a >= b ? Ke(a, b) : Ke(b, a);
+#pragma omp atomic
+                spK.data[slots[(size_t)le * 64 + 8 * a + b]] += v;
+            }
+    }
+}
+#endif
+
 int main(int argc, char** argv) {
     if (argc != 3) { fprintf(stderr, "usage: cpref job.txt out.bin\n"); return 2; }
     Job j = parseJob(argv[1]);
@@ -363,11 +428,20 @@ int main(int argc, char** argv) {
     }
 
     /* Phase driver: the body of solveCPU with caller tolerances. */
+    const bool csrDirect = (j.mode == "phases_csr");
+#ifndef CPREF_SOLVER_SOURCE
+    if (csrDirect) { fprintf(stderr, "phases_csr: use the cpref_csr build\n"); return 4; }
+#endif
+    if (csrDirect && (ps.mesh.count3 || ps.mesh.count8)) { fprintf(stderr, "phases_csr: 4-node meshes only\n"); return 4; }
     double t0 = omp_get_wtime();
-    StripSLAE K(N, 2 * ps.mesh.findMaxIndexDiff() + 1);
-    K.factN = N;
+    StripSLAE K(csrDirect ? 1 : N, csrDirect ? 1 : 2 * ps.mesh.findMaxIndexDiff() + 1);
+    K.factN = csrDirect ? 1 : N;
     ps.calcBs();
     SparseSLAE spK(ps.mesh, 2);
+#ifdef CPREF_SOLVER_SOURCE
+    std::vector<int> slots;
+    if (csrDirect) slots = csrSlots4(ps.mesh, spK);
+#endif
     ps.initConditions(spK);
     for (int d : j.fixDofs) ps.kinMask[d] = false;
     std::vector<double> rpFull(spK.rp, spK.rp + N), uvFull(ps.uv.begin(), ps.uv.begin() + N);
@@ -384,8 +458,11 @@ int main(int argc, char** argv) {
 
     std::vector<int> outerPerLevel, cgPerLevel;
     std::vector<double> errPerLevel;
-    long long cgTotal = 0;
+    long long cgTotal = 0, outerTotal = 0;
+    double tAsm = 0, tCg = 0, tUpd = 0;
+    const double tSetup = omp_get_wtime() - t0;
     bool elastic = (j.mode == "elastic");
+    bool stopped = false;
     for (int lev = 1; lev <= j.levels; ++lev) {
         double lam = (double)lev / j.levels;
         for (int i = 0; i < N; ++i) spK.rp[i] = lam * rpFull[i];
@@ -395,20 +472,34 @@ int main(int argc, char** argv) {
         long long cgLevel = 0;
         double relErr = 0.;
         do {
+            double ta = omp_get_wtime();
+#ifdef CPREF_SOLVER_SOURCE
+            if (csrDirect) fillCsrDirect(ps, spK, slots);
+            else
+#endif
             ps.fillGlobalStiffness(K, spK);
+            double tb = omp_get_wtime();
             if (j.dumpK && lev == 1 && iter == 0) cpbin_put(out, "k_data", 'd', spK.rows[N], spK.data);
             size_t inner = 0;
             cjs.solve(ps.uv.data(), ps.kinMask, inner, j.cgEps);
+            double tc = omp_get_wtime();
             cgLevel += (long long)inner;
             ps.updateParameters(iter);
             relErr = ps.exitCondition();
+            double td = omp_get_wtime();
+            tAsm += tb - ta;
+            tCg += tc - tb;
+            tUpd += td - tc;
             ++iter;
+            ++outerTotal;
+            if (j.prefixOuter && outerTotal >= j.prefixOuter) { stopped = true; break; }
             if (elastic) break;
         } while (relErr > j.outerEps && iter < j.maxOuter);
         outerPerLevel.push_back(iter);
         cgPerLevel.push_back((int)cgLevel);
         errPerLevel.push_back(relErr);
         cgTotal += cgLevel;
+        if (stopped) break;
     }
     ps.calcPlastDeform();
     double wall = omp_get_wtime() - t0;
@@ -417,6 +508,10 @@ int main(int argc, char** argv) {
     cpbin_put(out, "cg_per_level", 'i', cgPerLevel.size(), cgPerLevel.data());
     cpbin_put(out, "err_per_level", 'd', errPerLevel.size(), errPerLevel.data());
     cpbin_put_d(out, "wall_seconds", wall);
+    cpbin_put_d(out, "setup_seconds", tSetup);
+    cpbin_put_d(out, "assembly_seconds", tAsm);
+    cpbin_put_d(out, "cg_seconds", tCg);
+    cpbin_put_d(out, "update_seconds", tUpd);
     cpbin_put_d(out, "energy", ps.deformEnergy());
     cpbin_put_i(out, "threads", omp_get_max_threads());
     fclose(out);

@@ -144,15 +144,14 @@ def test_persistent_cg_matches_graph_loop(name, ctx, golden_dir, workdir, monkey
 @pytest.mark.parametrize("name", ["hole12_pow", "ogrid16_bilin", "hole12_q8_pow"])
 def test_cluster_cg_matches_reference(name, ctx, golden_dir, workdir, monkeypatch):
     """The FP64 CG inside one thread-block cluster (the default where the
-    instance fits the cluster's shared memory), in both its forms
-    (CUPLAST_FP64_CG=cluster, cluster2): the converged state within
+    instance fits the cluster's shared memory): the converged state within
     1e-10 of the reference's, as the other solvers, and the same number of
     outer iterations as the grid-wide CG loop (CUPLAST_FP64_CG=fused, read at
     instance creation) within a couple (the summation order differs)."""
     m, lines = scenario(name, workdir)
     monkeypatch.setenv("CUPLAST_FP64_CG", "fused")
     base = product_runner.run(ctx, lines, m, precond=1)
-    for form in ("cluster", "cluster2"):
+    for form in ("cluster",):
         monkeypatch.setenv("CUPLAST_FP64_CG", form)
         for precond in (0, 1):
             r = product_runner.run(ctx, lines, m, precond=precond)
