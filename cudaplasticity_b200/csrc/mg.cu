@@ -787,8 +787,8 @@ size_t mg_footprint(size_t n, size_t blocks) {
     // block (92) and D^-1, T, b, y, z, aggregate, member, ranges per node
     // (about 300), a geometric series of at most twice level 1, which has at
     // most half the nodes and blocks of level 0. The coarsest inverse and its
-    // scratch: at most 2 x 4096^2 doubles, counted as 1 MB (nc <= 160 here
-    // in practice, 0.2 MB).
+    // scratch: at most 2 x kMgMaxCoarsest^2 doubles = 1 MB (mg_prepare
+    // rejects a coarser bottom level).
     return 128 * n + 16 * blocks + 2 * (300 * (n / 2) + 92 * (blocks / 2)) + (1u << 20);
 }
 
@@ -826,7 +826,7 @@ void mg_prepare(cp_instance* I) {
     MgDev m;
     m.L = L;
     m.nc = 3 * H.levels[L - 1].n_nodes;
-    CP_CHECK(m.nc <= 4096, CP_ERR_UNSUPPORTED, "multigrid: coarsest level too large");
+    CP_CHECK(m.nc <= kMgMaxCoarsest, CP_ERR_UNSUPPORTED, "multigrid: coarsest level too large");
     for (int l = 0; l < L; ++l) {
         const amg::Level& F = H.levels[l];
         MgLevel& D = m.lv[l];

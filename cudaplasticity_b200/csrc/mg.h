@@ -20,7 +20,8 @@ struct cp_instance;
 
 namespace cp {
 
-constexpr int kMgMaxLevels = 10;
+constexpr int kMgMaxLevels = 16;
+constexpr int kMgMaxCoarsest = 256;  // coarsest DOFs accepted: its inverse and scratch stay within 1 MB
 constexpr int kMgMaxCoarse = 160;  // coarsest DOFs whose inversion runs in shared memory
 constexpr int kMgMinCoarse = 150;  // coarsening stops at this many DOFs
 constexpr int kMgPartNodes = 256;  // level-0 node ranges that no aggregate crosses
