@@ -699,7 +699,12 @@ def served_vs_plain_leg(ctx, n_requests, stream="served", rates=(10.0, 100.0, 10
                                      "p99_s": float(np.percentile(p_lat, 99))}}
         for form in forms:
             srv = cp.Server(fp64_lanes=8)
-            skw = dict(kw, precision=cp.CP_PREC_FP64) if form == "fp64_lanes" else dict(BATCH_KW, **tol)
+            if form == "fp64_lanes":
+                skw = dict(kw, precision=cp.CP_PREC_FP64)
+            elif form == "fp64_lanes_mg":  # the lanes with the multigrid-preconditioned CG
+                skw = dict(kw, precision=cp.CP_PREC_FP64, precond=2)
+            else:
+                skw = dict(BATCH_KW, **tol)
             t0 = time.perf_counter()
             rids = []
             for w, a in zip(reqs, arrivals):

@@ -151,8 +151,9 @@ def test_cluster_cg_matches_reference(name, ctx, golden_dir, workdir, monkeypatc
     m, lines = scenario(name, workdir)
     monkeypatch.setenv("CUPLAST_FP64_CG", "fused")
     base = product_runner.run(ctx, lines, m, precond=1)
-    for form in ("cluster",):
-        monkeypatch.setenv("CUPLAST_FP64_CG", form)
+    monkeypatch.setenv("CUPLAST_FP64_CG", "cluster")
+    for form in ("0", "1"):  # both kernel forms (CUPLAST_CLUSTER_FORM, read when an instance is planned)
+        monkeypatch.setenv("CUPLAST_CLUSTER_FORM", form)
         for precond in (0, 1):
             r = product_runner.run(ctx, lines, m, precond=precond)
             g = load_golden(golden_dir, name)
