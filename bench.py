@@ -16,20 +16,25 @@ the reference). ``--impl reference`` runs the reference implementation's own
 CPU path (oracle/_ref/cpref, built from its sources) on the same job with all
 host cores.
 
-Beside the headline, the line carries the batched and served forms on the
-seeded request streams of cudaplasticity_b200/workload.py:
+Beside the headline, the line carries:
+  error_vs_reference  the timed result against the reference CPU path's
+           result on the same job;
+  roofline (CG GB/s)  the FP64 CG iteration of the 2.1M-DOF plate (k_f_iter),
+           CUDA events, against the measured HBM copy peak; the FP32 SpMV
+           beside it;
+  served_vs_plain  the metric's comparison: the first requests of the
+           seeded batch stream (cudaplasticity_b200/workload.py: DOF
+           log-uniform in [2k, 200k], plates and rings, 5-segment diagrams)
+           solved one at a time through the plain FP64 drop-in, and through
+           the solve service (cp_server, FP64 lanes) under Poisson arrivals
+           at 10, 100 and 1000 requests/s: solves/s, p50/p99 latency and each
+           result's error against the plain FP64 result;
   batched  closed-loop saturation throughput of the batched mixed-precision
-           engine: a batch of 512 resident instances of the batch stream
-           (DOF log-uniform in [2k, 200k], plates and rings, 5-segment
-           diagrams), refilled from the stream as solves finish, converged
-           solves counted over a fixed window; the SpMV sweep over all 512
-           resident instances timed live (CG GB/s);
-  plain    the plain FP64 drop-in, one request at a time, on a seeded sample
-           of the requests the batched window completed (same solver
-           options), and the mixed-precision results' error against it;
-  served   the solve service (cp_server) under Poisson arrivals of the served stream
-           requests (DOF log-uniform in [2k, 500k], 5-30 load increments),
-           host buffers in and results out: solves/s and p50/p99 latency.
+           engine (512 resident batch-stream instances) and its CG
+           iteration's live roofline;
+  config2  configuration 2 end to end: the 2.1M-DOF Hollomon plate, 20
+           increments, through the drop-in, and the reference-composed CPU
+           per-iteration rate on the same mesh.
 
 Multi-GPU: the path does not shard (one solve is one small instance), so N GPUs
 run N independent replicas ("replicas only"); value = solves of all ranks /
@@ -451,77 +456,6 @@ def compare_leg(ctx, n_requests, max_outer=100, seed=20261203, lanes=8, mg=False
     return fixed
 
 
-def served_leg(rate_hz=10.0, submit_s=20.0, drain_s=25.0, seed=20270101, precision="mixed"):
-    """The solve service under Poisson arrivals of served-stream requests
-    (DOF 2k-500k, 5-30 load increments); precision "mixed" sends them to the
-    batch, "fp64" to the FP64 lanes (cp_solve, several at once)."""
-    import random
-
-    import numpy as np
-
-    import cudaplasticity_b200 as cp
-    from cudaplasticity_b200 import workload
-
-    rng = random.Random(seed)
-    srv = cp.Server()
-    kw = dict(BATCH_KW) if precision == "mixed" else dict(FP64_SERVE_KW, precision=cp.CP_PREC_FP64)
-    ids, t_sub, h2d = [], [], 0
-    t0 = time.perf_counter()
-    k = 0
-    next_t = rng.expovariate(rate_hz)
-    while next_t < submit_s:
-        w = workload.instance(k, seed=seed, dof_min=2000, dof_max=500000, increments=(5, 30))
-        now = time.perf_counter() - t0
-        if next_t > now:
-            time.sleep(next_t - now)
-        ids.append(srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"], **kw))
-        t_sub.append(time.perf_counter() - t0)
-        h2d += sum(w["mesh"][a].nbytes for a in ("node_xy", "elem4")) + w["rp"].nbytes + w["mask"].nbytes + w["uv"].nbytes
-        k += 1
-        next_t += rng.expovariate(rate_hz)
-    deadline = t0 + submit_s + drain_s
-    lat, statuses, d2h, last_done = [], [], 0, 0.0
-    pending = list(ids)
-    while pending and time.perf_counter() < deadline:
-        still = []
-        for rid in pending:
-            try:
-                inst, rep, latency = srv.wait(rid, timeout=0.0)
-            except cp.CuplastError as e:
-                if e.status == cp._capi.CP_ERR_BUSY:
-                    still.append(rid)
-                    continue
-                raise
-            st = inst.state()
-            d2h += sum(v.nbytes for v in st.values())
-            inst.close()
-            lat.append(latency)
-            statuses.append(rep["status"])
-            last_done = time.perf_counter() - t0
-        pending = still
-        time.sleep(0.02)
-    stats = srv.stats()
-    srv.close()
-    n = len(lat)
-    return {
-        "workload": "served stream: Poisson arrivals, DOF log-uniform [2k, 500k], 5-30 load increments, "
-                    f"{'mixed precision (batch)' if precision == 'mixed' else 'FP64 (lanes)'}, CG 1e-10, outer 1e-6",
-        "rate_hz": rate_hz, "submitted": len(ids), "completed": n,
-        "solves_per_s": n / last_done if last_done > 0 else 0.0,
-        "p50_s": float(np.percentile(lat, 50)) if n else None,
-        "p99_s": float(np.percentile(lat, 99)) if n else None,
-        "censored": len(ids) - n, "statuses": sorted(set(statuses)),
-        "h2d_bytes": int(h2d), "d2h_bytes": int(d2h), "server": {k: stats[k] for k in
-                                                               ("admitted", "completed", "runs", "trips",
-                                                                "busy_seconds", "peak_bytes")},
-    }
-
-
-CONFIG2 = dict(workload="hole_plate_ogrid1024x1024_q4_2099200dof_hollomon", n_circ=1024, n_rad=1024,
-               nodes=1049600, dof=2099200, elements=1048576, E_mpa=210000, nu=0.3, sigma_y=250, eps0=0.002,
-               n_exp=0.2, traction_mpa=220, increments=20, cg_tol=1e-10, outer_tol=1e-6)
-
-
 def config2_leg(ctx, cpu=True, cpu_cg_eps=1e-2):
     """Configuration 2 end to end: the 1024 x 1024 O-grid plate (2.1M DOF),
     Hollomon hardening sy (1 + eps_p / eps0)^n, 220 MPa in 20 increments, CG
@@ -890,6 +824,11 @@ def run_product_arm(args):
     for prec, name in ((cp.CP_PREC_FP64, "fp64"), (cp.CP_PREC_MIXED, "fp32")):
         binst.set_field("uv", np.zeros_like(brp))
         rows[name] = bench_cg(binst, prec, 0, 100)
+    # the FP64 CG iteration that instances too large for one cluster run
+    # (configuration 2): one k_f_iter launch per block-Jacobi PCG iteration
+    binst.set_field("uv", np.zeros_like(brp))
+    fms, fby = ctypes.c_double(), ctypes.c_double()
+    binst.ctx.check(cp._capi.lib().cp_bench_cg_fused(binst._h, 1, 200, ctypes.byref(fms), ctypes.byref(fby)))
     # elements assembled per second (fillGlobalStiffness on the 1,048,576-element
     # mesh, CUDA events around the launches) and DOF-iterations per second
     throughput = {"assembly_mesh": "1024x1024 O-grid plate, 1,048,576 Q4, FP64 values"}
@@ -915,11 +854,20 @@ def run_product_arm(args):
     throughput["dof_iterations_per_s_2M"] = 2 * big_nodes / ((mp + mu) * 1e-3)
     cg_large = {k: {"spmv_gbs": b / (m * 1e-3) / 1e9, "update_gbs": c / (n * 1e-3) / 1e9, "ms_spmv": m,
                     "ms_update": n, "us_per_cg_iter": 1e3 * (m + n)} for k, (m, n, b, c) in rows.items()}
-    roofline = {"bound": "hbm", "kernel": "k_cg_p<double> (SpMV+dot) on the 2.1M-DOF 1024x1024 O-grid plate",
-                "achieved": bp / (mp * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-                "frac": bp / (mp * 1e-3) / 1e9 / peak, "traffic": 402.7e6,
-                "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one k_cg_p<double> launch (ncu capture)",
-                "bytes_per_launch": bp, "ms_per_launch": mp, "peak_kind": peak_kind}
+    # "CG GB/s": the FP64 CG iteration of the 2.1M-DOF plate (k_f_iter, the
+    # kernel that takes 90 % of a configuration-2 solve), live CUDA events
+    roofline = {"bound": "hbm", "kernel": "k_f_iter (FP64 block-Jacobi PCG iteration, one launch) on the 2.1M-DOF "
+                                          "1024x1024 O-grid plate",
+                "achieved": fby.value / (fms.value * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": fby.value / (fms.value * 1e-3) / 1e9 / peak, "traffic": 622.5e6,
+                "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one k_f_iter launch on this mesh "
+                                "(ncu capture, profiles/k_f_iter_2M.md)",
+                "bytes_per_launch": fby.value, "ms_per_launch": fms.value, "peak_kind": peak_kind}
+    mp32, mu32, bp32, bu32 = rows["fp32"]
+    roof_fp32 = {"bound": "hbm", "kernel": "k_cg_p<float> (mixed precision SpMV + direction) on the 2.1M-DOF plate",
+                 "achieved": bp32 / (mp32 * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                 "frac": bp32 / (mp32 * 1e-3) / 1e9 / peak, "traffic": None, "bytes_per_launch": bp32,
+                 "ms_per_launch": mp32, "peak_kind": peak_kind}
 
     cpu = err_ref = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -929,13 +877,17 @@ def run_product_arm(args):
                          f"through its phase functions, {c['outer']} outer / {c['cg']} CG iterations"}
         err_ref = error_vs_reference(state, c["state"], tight)
 
-    batched = served = roof_batched = None
+    batched = served = roof_batched = config2 = None
     if rank == 0 and not args.skip_batched:
         batched = batched_leg(ctx, window_s=args.batched_window)
         roof_batched = cg_kernel_roofline(ctx)
     if rank == 0 and not args.skip_served:
-        served = served_leg(rate_hz=args.serve_rate, submit_s=args.serve_window, drain_s=args.serve_window + 5,
-                            precision=args.serve_precision)
+        # the metric: the same requests served and one at a time through the
+        # plain FP64 drop-in, at three Poisson rates
+        served = served_vs_plain_leg(ctx, args.serve_requests, stream="batch", budget_s=args.serve_budget,
+                                     forms=("fp64_lanes",), max_outer=300)
+    if rank == 0 and not args.skip_config2:
+        config2 = config2_leg(ctx, cpu=not args.skip_cpu, cpu_cg_eps=0.1)
 
     launches = sum(r["kernel_launches"] for r in reps)
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -951,10 +903,11 @@ def run_product_arm(args):
                         "one thread-block cluster per linear solve (on chip) where the instance fits"),
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": int(launches), "roofline": roofline, "roofline_this_workload": roof_small,
+            "gpu_launches": int(launches), "roofline": roofline, "roofline_headline": roof_small,
+            "roofline_fp32_spmv": roof_fp32,
             "cg_large_mesh": cg_large, "multigrid_parts": mg_parts, "cpu_baseline": cpu, "clocks": clocks.summary(),
-            "accuracy_vs_tight_fp64": accuracy, "error_vs_reference": err_ref, "batched": batched, "roofline_batched": roof_batched,
-            "served": served,
+            "accuracy_vs_tight_fp64": accuracy, "error_vs_reference": err_ref, "batched": batched,
+            "roofline_batched": roof_batched, "served_vs_plain": served, "config2": config2,
             "throughput": dict(throughput, dof_iterations_per_s_headline=2 * arrays["node_xy"].shape[0] *
                                sum(r["cg_iters"] for r in reps) / sum(times)),
             "detail": {"outer_iters": reps[-1]["outer_iters"], "cg_iters": reps[-1]["cg_iters"],
@@ -1063,10 +1016,10 @@ def main():
     ap.add_argument("--compare", type=int, metavar="N",
                     help="like-for-like run only: the first N batch-stream requests, plain FP64 one at a time vs batched")
     ap.add_argument("--compare-max-outer", type=int, default=100)
-    ap.add_argument("--serve-rate", type=float, default=10.0, help="Poisson arrival rate of the served leg")
-    ap.add_argument("--serve-precision", default="mixed", choices=["mixed", "fp64"],
-                    help="served leg: mixed-precision batch or FP64 lanes")
-    ap.add_argument("--serve-window", type=float, default=20.0, help="seconds of arrivals in the served leg")
+    ap.add_argument("--serve-requests", type=int, default=24, help="requests in the served-vs-plain leg")
+    ap.add_argument("--serve-budget", type=float, default=60.0,
+                    help="seconds of plain solves after which the served-vs-plain sample stops growing")
+    ap.add_argument("--skip-config2", action="store_true", help="omit the configuration-2 leg")
     ap.add_argument("--batched-probe", type=int, nargs=2, metavar=("N", "TRIPS"),
                     help="profiling aid: N resident batch-stream instances, TRIPS graph trips, then exit")
     ap.add_argument("--config2", action="store_true",

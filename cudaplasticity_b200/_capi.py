@@ -139,6 +139,7 @@ _SIGS = {
     "cpx_mesh_split_t3": (c_int, [c_p]),
     "cpx_mesh_load_inp": (c_int, [c_p, ctypes.c_char_p]),
     "cp_bench_assemble": (c_int, [c_p, c_int, c_int, P_double, P_double]),
+    "cp_bench_cg_fused": (c_int, [c_p, c_int, c_int, P_double, P_double]),
     "cp_bench_mg": (c_int, [c_p, c_int, P_double, P_double]),
     "cpx_mesh_renum_by_direction": (c_int, [c_p, c_double, c_double]),
     "cpx_mesh_smooth_ring": (c_int, [c_p, c_int]),

@@ -247,8 +247,9 @@ void run_cg_loop(cp_instance* I, const cp::CgArgs<T>& a, cudaGraphExec_t g) {
     }
 }
 
-// FP64 CG, one launch per iteration (cg_fused.cu).
-void cg_fp64_fused(cp_instance* I, double eps, long long max_iter, int precond) {
+// Arguments of the one-launch FP64 CG (cg_fused.cu) of this instance; its
+// vectors are allocated on first use.
+cp::FusedArgs fused_args(cp_instance* I, int precond) {
     const int n = I->n_nodes;
     if (!I->f_r) {
         I->f_r = I->alloc<double2>(n);
@@ -279,6 +280,13 @@ void cg_fp64_fused(cp_instance* I, double eps, long long max_iter, int precond) 
     a.precond = precond;
     a.sc = I->sc;
     a.partials = I->f_partials;
+    return a;
+}
+
+// FP64 CG, one launch per iteration (cg_fused.cu), or the whole solve in one
+// thread-block cluster where the instance fits.
+void cg_fp64_fused(cp_instance* I, double eps, long long max_iter, int precond) {
+    cp::FusedArgs a = fused_args(I, precond);
     if (I->cluster_fp64) {
         if (!I->cluster_planned) {
             I->cluster_plan = cp::cluster_cg_plan(a, I->csr.max_width);
@@ -1007,6 +1015,40 @@ CP_API int cp_bench_cg(cp_instance* I, int precision, int precond, int iters, do
         if (ms_u) *ms_u = tu / iters;
         if (bytes_p) *bytes_p = nnz * sv + nnz + 4 * N * sx;
         if (bytes_u) *bytes_u = 32 * n + 4 * N * sx + 2 * n + (precond ? 4 * n * sx : 0.0) + 2 * N * sx;
+    });
+}
+
+CP_API int cp_bench_cg_fused(cp_instance* I, int precond, int iters, double* ms_iter, double* bytes_iter) {
+    if (I && I->in_batch) return CP_ERR_BUSY;
+    if (!I || iters <= 0 || (precond & ~1)) return CP_ERR_INVALID;
+    return guarded(I->ctx, [&] {
+        CP_CHECK(I->loads_set, CP_ERR_INVALID, "loads not set");
+        cudaStream_t s = I->s();
+        assemble(I, CP_PREC_FP64);
+        cp::FusedArgs a = fused_args(I, precond);
+        std::vector<cudaEvent_t> ev((size_t)iters + 1);
+        for (auto& e : ev) CP_CUDA(cudaEventCreate(&e));
+        cp::fused_launch_start(a, 0.0, (long long)iters + 8, s);
+        for (int it = 0; it < iters; ++it) {
+            CP_CUDA(cudaEventRecord(ev[it], s));
+            cp::fused_launch_iteration(a, it & 1, s);
+        }
+        CP_CUDA(cudaEventRecord(ev[iters], s));
+        CP_CUDA(cudaEventSynchronize(ev.back()));
+        double t = 0;
+        for (int it = 0; it < iters; ++it) {
+            float x = 0;
+            CP_CUDA(cudaEventElapsedTime(&x, ev[it], ev[it + 1]));
+            t += x;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        // algorithmic bytes of one iteration: 8 per value and one 4-byte
+        // column per 2x2 block; per node read r, w, p, kp, x and the own
+        // 48-byte record, write them back (256), the mask and the
+        // block-Jacobi inverse (34 with, 2 without)
+        const double n = I->n_nodes, nnz = (double)I->csr.nnz;
+        if (ms_iter) *ms_iter = t / iters;
+        if (bytes_iter) *bytes_iter = nnz * 8 + nnz + n * (256 + (precond ? 34 : 2));
     });
 }
 

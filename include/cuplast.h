@@ -187,6 +187,17 @@ CP_API int cp_solve(cp_instance* inst, const cp_solve_opts* opts, cp_solve_repor
  * Jacobi). Leaves uv changed. */
 CP_API int cp_bench_cg(cp_instance* inst, int precision, int precond, int iters, double* ms_spmv, double* ms_update,
                        double* bytes_spmv, double* bytes_update);
+/* Measurement entry point of the FP64 CG form that instances too large for
+ * one thread-block cluster run (one launch per iteration; no counterpart in
+ * the reference, whose ConjGradCuda::solve, src/ConjGradCuda.cu:185-231,
+ * launches three kernels and synchronises per iteration): assembles K at the
+ * current state, starts a (block-Jacobi with precond 1) CG from the current
+ * uv and runs `iters` iterations as direct launches with CUDA events around
+ * each. Outputs the mean duration of one iteration in milliseconds and the
+ * algorithmic bytes one iteration moves: the values and one 4-byte column per
+ * 2x2 block, and per node the vectors read and written once. Leaves uv
+ * changed. */
+CP_API int cp_bench_cg_fused(cp_instance* inst, int precond, int iters, double* ms_iter, double* bytes_iter);
 /* Measurement entry point: runs the assembly (fillGlobalStiffness) `iters`
  * times as direct launches with CUDA events around each, from the current
  * secant moduli. Outputs the mean duration in milliseconds and the
