@@ -878,16 +878,25 @@ def run_product_arm(args):
         err_ref = error_vs_reference(state, c["state"], tight)
 
     batched = served = roof_batched = config2 = None
-    if rank == 0 and not args.skip_batched:
-        batched = batched_leg(ctx, window_s=args.batched_window)
-        roof_batched = cg_kernel_roofline(ctx)
+    def aux(name, fn):
+        """An auxiliary leg: its failure is reported in the line, which is still printed."""
+        try:
+            return fn()
+        except Exception as exc:  # noqa: BLE001
+            print(json.dumps({"leg_failed": name, "error": repr(exc)}), file=sys.stderr, flush=True)
+            return {"error": repr(exc)}
+
     if rank == 0 and not args.skip_served:
         # the metric: the same requests served and one at a time through the
         # plain FP64 drop-in, at three Poisson rates
-        served = served_vs_plain_leg(ctx, args.serve_requests, stream="batch", budget_s=args.serve_budget,
-                                     forms=("fp64_lanes",), max_outer=300)
+        served = aux("served_vs_plain", lambda: served_vs_plain_leg(
+            ctx, args.serve_requests, stream="batch", budget_s=args.serve_budget, forms=("fp64_lanes",),
+            max_outer=300))
+    if rank == 0 and not args.skip_batched:
+        batched = aux("batched", lambda: batched_leg(ctx, window_s=args.batched_window))
+        roof_batched = aux("roofline_batched", lambda: cg_kernel_roofline(ctx))
     if rank == 0 and not args.skip_config2:
-        config2 = config2_leg(ctx, cpu=not args.skip_cpu, cpu_cg_eps=0.1)
+        config2 = aux("config2", lambda: config2_leg(ctx, cpu=not args.skip_cpu, cpu_cg_eps=0.1))
 
     launches = sum(r["kernel_launches"] for r in reps)
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,

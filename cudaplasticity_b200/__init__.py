@@ -521,10 +521,25 @@ class _Handed(Instance):
     ones still open)."""
 
     def __init__(self, server, handle, n_nodes, n_elem, count3, count4, count8=0):
-        self.ctx = server.ctx
+        self.ctx = _HandedContext(server.ctx, handle)
         self._server = server
         self._h = handle
         self.n_nodes, self.n_elem, self.count3, self.count4, self.count8 = n_nodes, n_elem, count3, count4, count8
+
+
+class _HandedContext:
+    """Error reporting for a handed-back instance: its messages live on the
+    service's context that the instance belongs to."""
+
+    def __init__(self, ctx, handle):
+        self._ctx, self._ih = ctx, handle
+
+    def error(self):
+        return C.lib().cp_instance_last_error(self._ih).decode()
+
+    def check(self, st):
+        if st != C.CP_OK:
+            raise CuplastError(st, self.error())
 
 
 _LIVE_SERVERS = weakref.WeakSet()

@@ -84,6 +84,7 @@ _SIGS = {
     "cp_context_create": (c_int, [c_int, ctypes.POINTER(c_p)]),
     "cp_context_destroy": (c_int, [c_p]),
     "cp_context_last_error": (ctypes.c_char_p, [c_p]),
+    "cp_instance_last_error": (ctypes.c_char_p, [c_p]),
     "cp_context_synchronize": (c_int, [c_p]),
     "cp_instance_create": (c_int, [c_p, ctypes.POINTER(cp_mesh_view), ctypes.POINTER(cp_material),
                                    ctypes.POINTER(c_p)]),

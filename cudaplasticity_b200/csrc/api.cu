@@ -510,6 +510,10 @@ CP_API int cp_context_destroy(cp_context* ctx) {
 
 CP_API const char* cp_context_last_error(const cp_context* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
+CP_API const char* cp_instance_last_error(const cp_instance* inst) {
+    return inst && inst->ctx ? inst->ctx->last_error.c_str() : "";
+}
+
 CP_API int cp_context_synchronize(cp_context* ctx) {
     if (!ctx) return CP_ERR_INVALID;
     return guarded(ctx, [&] { CP_CUDA(cudaStreamSynchronize(ctx->stream)); });

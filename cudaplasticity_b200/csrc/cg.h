@@ -92,7 +92,6 @@ struct ClusterPlan {
     int spc = 0;       // slices of 32 nodes per CTA (one warp each)
     int wmax = 0;      // widest node row, in blocks
     size_t smem = 0;   // dynamic shared memory per CTA
-    int form = 0;      // kernel form (cg_cluster.cu)
 };
 ClusterPlan cluster_cg_plan(const FusedArgs& a, int max_width);
 void cluster_cg_launch(const FusedArgs& a, const ClusterPlan& plan, double eps2, long long max_iter, cudaStream_t s);

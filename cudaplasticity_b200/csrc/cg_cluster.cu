@@ -21,8 +21,6 @@
 // so the iterates agree with them to rounding, not bit for bit.
 #include <cooperative_groups.h>
 
-#include <cstdlib>
-
 #include "cg.h"
 #include "common.cuh"
 #include "internal.h"
@@ -46,12 +44,10 @@ __device__ __forceinline__ double2 mvec(const double4& m, double2 v) {
 //   kval [spc][wmax][32] double4  block values, 2x2 row-major
 //   rec  [2][spc * 32][3] double2 published (u, M w, M kp) by parity
 //   part [2][8] double            this CTA's partial sums by parity
-//   kloc [spc][wmax][32] int      form 0: owner rank << 16 | owner-local node index
-//   kptr [spc][wmax][32] pointer  form 1: the neighbour's parity-0 record, mapped
+//   kloc [spc][wmax][32] int      owner rank << 16 | owner-local node index
 struct Smem {
     double4* kval;
     int* kloc;
-    const double2** kptr;
     double2* rec;
     double* part;
 };
@@ -64,14 +60,12 @@ __device__ __forceinline__ Smem carve(unsigned char* base, int spc, int wmax) {
     s.part = reinterpret_cast<double*>(base + nb * sizeof(double4) + 2 * (size_t)spc * 32 * 3 * sizeof(double2));
     s.kloc = reinterpret_cast<int*>(base + nb * sizeof(double4) + 2 * (size_t)spc * 32 * 3 * sizeof(double2) +
                                     16 * sizeof(double));
-    s.kptr = reinterpret_cast<const double2**>(s.kloc);
     return s;
 }
 
-size_t smem_bytes(int spc, int wmax, int form) {
+size_t smem_bytes(int spc, int wmax) {
     const size_t nb = (size_t)spc * wmax * 32;
-    return nb * sizeof(double4) + 2 * (size_t)spc * 32 * 3 * sizeof(double2) + 16 * sizeof(double) +
-           nb * (form ? sizeof(void*) : sizeof(int));
+    return nb * sizeof(double4) + 2 * (size_t)spc * 32 * 3 * sizeof(double2) + 16 * sizeof(double) + nb * sizeof(int);
 }
 
 // Block-wide sums of kSums values per thread into part[0..kSums) of this CTA
@@ -107,14 +101,6 @@ __device__ __forceinline__ void cluster_totals(double* const* part_of, int ctas,
     __syncthreads();
 }
 
-// FORM 0: neighbour records located through (owner rank, local index) and
-// a table of mapped record bases, one loop over a row's blocks, the
-// cluster totals reduced by warp 0 and broadcast through shared memory.
-// FORM 1: the neighbour's mapped record address stored per block (one
-// shared load instead of two dependent ones), the row loop unrolled by 3 so
-// that several remote loads are in flight, and every warp reducing the
-// cluster totals itself after the cluster barrier (no broadcast barrier).
-template <int FORM>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
     k_c_solve(FusedArgs a, ClusterPlan shp, double eps2, long long max_iter) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -153,8 +139,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1)
             const int cr = (col >> 5) / spc;
             const size_t q = ((size_t)w * wmax + k) * 32 + lane;
             S.kval[q] = make_double4(lo.x, lo.y, hi.x, hi.y);
-            if (FORM == 0) S.kloc[q] = (cr << 16) | (col - cr * spc * 32);
-            else S.kptr[q] = cl.map_shared_rank(S.rec, cr) + 3 * (size_t)(col - cr * spc * 32);
+            S.kloc[q] = (cr << 16) | (col - cr * spc * 32);
         }
     }
     // ---- own data in registers
@@ -180,13 +165,8 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1)
         for (int k = 0; k < wd; ++k) {
             const size_t q = ((size_t)w * wmax + k) * 32 + lane;
             const double4 kv = S.kval[q];
-            double2 v;
-            if (FORM == 0) {
-                const int lc = S.kloc[q];
-                v = rec_of[lc >> 16][half + 3 * (size_t)(lc & 0xffff)];
-            } else {
-                v = S.kptr[q][half];
-            }
+            const int lc = S.kloc[q];
+            const double2 v = rec_of[lc >> 16][half + 3 * (size_t)(lc & 0xffff)];
             k0 += kv.x * v.x + kv.y * v.y;
             k1 += kv.z * v.x + kv.w * v.y;
         }
@@ -257,28 +237,15 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1)
             if (m.x) r.x -= al * kp.x;
             if (m.y) r.y -= al * kp.y;
             double k0 = 0.0, k1 = 0.0;
-            if (FORM == 0) {
-                for (int k = 0; k < wd; ++k) {
-                    const size_t q = ((size_t)w * wmax + k) * 32 + lane;
-                    const double4 kv = S.kval[q];
-                    const int lc = S.kloc[q];
-                    const double2* rc = rec_of[lc >> 16] + go + 3 * (size_t)(lc & 0xffff);
-                    const double2 uc = rc[0], mwc = rc[1], mkc = rc[2];
-                    const double ux = uc.x - al * (mwc.x + bt * mkc.x), uy = uc.y - al * (mwc.y + bt * mkc.y);
-                    k0 += kv.x * ux + kv.y * uy;
-                    k1 += kv.z * ux + kv.w * uy;
-                }
-            } else {
-#pragma unroll 3
-                for (int k = 0; k < wd; ++k) {
-                    const size_t q = ((size_t)w * wmax + k) * 32 + lane;
-                    const double4 kv = S.kval[q];
-                    const double2* rc = S.kptr[q] + go;
-                    const double2 uc = rc[0], mwc = rc[1], mkc = rc[2];
-                    const double ux = uc.x - al * (mwc.x + bt * mkc.x), uy = uc.y - al * (mwc.y + bt * mkc.y);
-                    k0 += kv.x * ux + kv.y * uy;
-                    k1 += kv.z * ux + kv.w * uy;
-                }
+            for (int k = 0; k < wd; ++k) {
+                const size_t q = ((size_t)w * wmax + k) * 32 + lane;
+                const double4 kv = S.kval[q];
+                const int lc = S.kloc[q];
+                const double2* rc = rec_of[lc >> 16] + go + 3 * (size_t)(lc & 0xffff);
+                const double2 uc = rc[0], mwc = rc[1], mkc = rc[2];
+                const double ux = uc.x - al * (mwc.x + bt * mkc.x), uy = uc.y - al * (mwc.y + bt * mkc.y);
+                k0 += kv.x * ux + kv.y * uy;
+                k1 += kv.z * ux + kv.w * uy;
             }
             wv = make_double2(k0, k1);
             mw = apply_m(wv);
@@ -296,21 +263,10 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1)
         // publishes them with the records
         cta_sums(t, S.part + 8 * parity, wsum);
         cl.sync();
-        double tt[kSums];
-        if (FORM == 0) {
-            cluster_totals(part_of[parity], ctas, tot);
-#pragma unroll
-            for (int i = 0; i < kSums; ++i) tt[i] = tot[i];
-        } else {
-            // every warp sums the CTAs' partials in rank order through the
-            // same shuffle tree, so all threads hold the same totals
-            const double* pp = part_of[parity][lane < ctas ? lane : 0];
-#pragma unroll
-            for (int i = 0; i < kSums; ++i) tt[i] = warp_sum(lane < ctas ? pp[i] : 0.0);
-        }
-        const double g = tt[0], rn = tt[2];
+        cluster_totals(part_of[parity], ctas, tot);
+        const double g = tot[0], rn = tot[2];
         const double b2 = g / rho;
-        const double den = tt[1] + b2 * tt[3] + b2 * b2 * tt[4];
+        const double den = tot[1] + b2 * tot[3] + b2 * b2 * tot[4];
         ++iter;
         rr = rn;
         beta = b2;
@@ -395,32 +351,22 @@ void launch_cluster(K k, const FusedArgs& a, const ClusterPlan& shp, double eps2
     CP_CUDA(cudaLaunchKernelEx(&cfg, k, a, shp, eps2, max_iter));
 }
 
-// The kernel's form (see k_c_solve), read when an instance is planned:
-// CUPLAST_CLUSTER_FORM, for measurements.
-int cluster_form() {
-    const char* e = std::getenv("CUPLAST_CLUSTER_FORM");
-    return (e && std::atoi(e) == 1) ? 1 : 0;
-}
-
 }  // namespace
 
 // The cluster shape for an instance, or ctas = 0 when it does not fit.
 ClusterPlan cluster_cg_plan(const FusedArgs& a, int wmax) {
     ClusterPlan s;
     const int n_slices = (a.n + 31) / 32;
-    const int form = cluster_form();
     for (int ctas : {16, 8}) {
         const int spc = (n_slices + ctas - 1) / ctas;
         if (spc > kMaxWarps) continue;
-        const size_t smem = smem_bytes(spc, wmax, form);
+        const size_t smem = smem_bytes(spc, wmax);
         if (smem > (size_t)kSmemCap) continue;
-        if (!(form ? cluster_fits(k_c_solve<1>, ctas, spc, smem) : cluster_fits(k_c_solve<0>, ctas, spc, smem)))
-            continue;
+        if (!cluster_fits(k_c_solve, ctas, spc, smem)) continue;
         s.ctas = ctas;
         s.spc = spc;
         s.wmax = wmax;
         s.smem = smem;
-        s.form = form;
         return s;
     }
     return s;
@@ -429,8 +375,7 @@ ClusterPlan cluster_cg_plan(const FusedArgs& a, int wmax) {
 void cluster_cg_launch(const FusedArgs& a, const ClusterPlan& shp, double eps2, long long max_iter, cudaStream_t s) {
     CP_CHECK(shp.ctas > 0 && shp.spc * 32 * shp.ctas >= a.n, CP_ERR_INVALID,
              "cluster CG: the instance does not fit one cluster");
-    if (shp.form) launch_cluster(k_c_solve<1>, a, shp, eps2, max_iter, s);
-    else launch_cluster(k_c_solve<0>, a, shp, eps2, max_iter, s);
+    launch_cluster(k_c_solve, a, shp, eps2, max_iter, s);
 }
 
 }  // namespace cp

@@ -138,6 +138,10 @@ CP_API int cp_device_count(int* count);
 CP_API int cp_context_create(int device, cp_context** out);
 CP_API int cp_context_destroy(cp_context* ctx);
 CP_API const char* cp_context_last_error(const cp_context* ctx);
+/* The message of the last error on the context an instance belongs to (for
+ * instances a solve service hands back, whose contexts are the service's;
+ * no counterpart in the reference). */
+CP_API const char* cp_instance_last_error(const cp_instance* inst);
 CP_API int cp_context_synchronize(cp_context* ctx);
 
 /* ----------------------------------------------------------- instance --- */

@@ -152,16 +152,14 @@ def test_cluster_cg_matches_reference(name, ctx, golden_dir, workdir, monkeypatc
     monkeypatch.setenv("CUPLAST_FP64_CG", "fused")
     base = product_runner.run(ctx, lines, m, precond=1)
     monkeypatch.setenv("CUPLAST_FP64_CG", "cluster")
-    for form in ("0", "1"):  # both kernel forms (CUPLAST_CLUSTER_FORM, read when an instance is planned)
-        monkeypatch.setenv("CUPLAST_CLUSTER_FORM", form)
-        for precond in (0, 1):
-            r = product_runner.run(ctx, lines, m, precond=precond)
-            g = load_golden(golden_dir, name)
-            k, err, errs = worst(r, g)
-            assert err <= FP64_TOL, (name, form, precond, k, err, errs)
-            assert np.array_equal(yielded(r), yielded(g))
-        assert abs(r["report"]["outer_iters"] - base["report"]["outer_iters"]) <= 2
-        assert r["report"]["status"] == 0
+    for precond in (0, 1):
+        r = product_runner.run(ctx, lines, m, precond=precond)
+        g = load_golden(golden_dir, name)
+        k, err, errs = worst(r, g)
+        assert err <= FP64_TOL, (name, precond, k, err, errs)
+        assert np.array_equal(yielded(r), yielded(g))
+    assert abs(r["report"]["outer_iters"] - base["report"]["outer_iters"]) <= 2
+    assert r["report"]["status"] == 0
 
 
 @pytest.mark.parametrize("name", ["ogrid16_bilin", "ogrid16_hollomon", "ogrid8_q8_bilin"])
