@@ -67,6 +67,11 @@ struct cp_server {
     cp_context* ctx_setup = nullptr;
     cp_batch* batch = nullptr;
     std::vector<cp_context*> lane_ctx;    // one per FP64 lane
+    // The context of every instance handed back to a caller: the lanes' and
+    // the set-up contexts keep working (and capture CUDA graphs on their
+    // streams) while callers read results, so a result moves to this
+    // context, whose stream only the callers use, before it is handed over.
+    cp_context* ctx_out = nullptr;
     std::vector<std::thread> lanes;
     std::deque<ReqP> lane_q;              // admitted FP64 requests, not yet on a lane
     std::vector<ReqP> lane_cur;           // the request each lane is solving (or null)
@@ -180,6 +185,9 @@ void lane(cp_server* s, int k) {
             }
             const int st = cp_solve(inst, &r->opts, &rep);
             if (st != CP_OK && rep.status == CP_OK) rep.status = st;
+            // nothing of this instance stays in flight on the lane's stream
+            if (cudaStreamSynchronize(inst->ctx->stream) != cudaSuccess && rep.status == CP_OK) rep.status = CP_ERR_CUDA;
+            inst->ctx = s->ctx_out;
         }
         std::lock_guard<std::mutex> lock(s->mu);
         s->lane_cur[k] = nullptr;
@@ -222,6 +230,10 @@ void scheduler(cp_server* s) {
                 s->inflight.erase(it);
                 s->inflight_bytes -= r->footprint;
                 r->rep = reps[i];
+                if (r->inst) {  // the run has ended: hand the instance over on the callers' context
+                    cudaStreamSynchronize(r->inst->ctx->stream);
+                    r->inst->ctx = s->ctx_out;
+                }
                 complete(s, r);
             }
             if (rc != CP_OK) {
@@ -383,6 +395,7 @@ CP_API int cp_server_create(const cp_server_opts* opts, cp_server** out) {
     s->o = o;
     int rc = cp_context_create(o.device, &s->ctx_run);
     if (rc == CP_OK) rc = cp_context_create(o.device, &s->ctx_setup);
+    if (rc == CP_OK) rc = cp_context_create(o.device, &s->ctx_out);
     if (rc == CP_OK) rc = cp_batch_create(s->ctx_run, &o.batch, &s->batch);
     for (int k = 0; rc == CP_OK && k < o.fp64_lanes; ++k) {
         cp_context* c = nullptr;
@@ -398,6 +411,7 @@ CP_API int cp_server_create(const cp_server_opts* opts, cp_server** out) {
     if (rc != CP_OK) {
         for (cp_context* c : s->lane_ctx) cp_context_destroy(c);
         if (s->batch) cp_batch_destroy(s->batch);
+        if (s->ctx_out) cp_context_destroy(s->ctx_out);
         if (s->ctx_setup) cp_context_destroy(s->ctx_setup);
         if (s->ctx_run) cp_context_destroy(s->ctx_run);
         delete s;
@@ -421,6 +435,7 @@ CP_API int cp_server_create(const cp_server_opts* opts, cp_server** out) {
             if (t.joinable()) t.join();
         for (cp_context* c : s->lane_ctx) cp_context_destroy(c);
         cp_batch_destroy(s->batch);
+        cp_context_destroy(s->ctx_out);
         cp_context_destroy(s->ctx_setup);
         cp_context_destroy(s->ctx_run);
         delete s;
@@ -450,6 +465,7 @@ CP_API int cp_server_destroy(cp_server* s) {
     }
     s->cv_done.notify_all();
     for (cp_context* c : s->lane_ctx) cp_context_destroy(c);
+    cp_context_destroy(s->ctx_out);
     cp_context_destroy(s->ctx_setup);
     cp_context_destroy(s->ctx_run);
     delete s;
