@@ -21,6 +21,8 @@
 // so the iterates agree with them to rounding, not bit for bit.
 #include <cooperative_groups.h>
 
+#include <cstdlib>
+
 #include "cg.h"
 #include "common.cuh"
 #include "internal.h"
@@ -34,7 +36,7 @@ namespace cgr = cooperative_groups;
 constexpr int kMaxCluster = 16;
 constexpr int kMaxWarps = 16;  // slices per CTA (512 threads)
 constexpr int kSums = 5;
-constexpr int kSmemCap = 200 * 1024;  // dynamic shared memory per CTA
+constexpr int kSmemCap = 220 * 1024;  // dynamic shared memory per CTA
 
 __device__ __forceinline__ double2 mvec(const double4& m, double2 v) {
     return make_double2(m.x * v.x + m.y * v.y, m.z * v.x + m.w * v.y);
@@ -357,7 +359,18 @@ void launch_cluster(K k, const FusedArgs& a, const ClusterPlan& shp, double eps2
 ClusterPlan cluster_cg_plan(const FusedArgs& a, int wmax) {
     ClusterPlan s;
     const int n_slices = (a.n + 31) / 32;
-    for (int ctas : {16, 8}) {
+    // cluster sizes tried in order; CUPLAST_CLUSTER_CTAS = 2..16 forces one
+    // (for measurements)
+    int order[2] = {16, 8}, n_order = 2;
+    if (const char* e = std::getenv("CUPLAST_CLUSTER_CTAS")) {
+        const int c = std::atoi(e);
+        if (c >= 2 && c <= kMaxCluster) {
+            order[0] = c;
+            n_order = 1;
+        }
+    }
+    for (int oi = 0; oi < n_order; ++oi) {
+        const int ctas = order[oi];
         const int spc = (n_slices + ctas - 1) / ctas;
         if (spc > kMaxWarps) continue;
         const size_t smem = smem_bytes(spc, wmax);
