@@ -456,6 +456,11 @@ def compare_leg(ctx, n_requests, max_outer=100, seed=20261203, lanes=8, mg=False
     return fixed
 
 
+CONFIG2 = dict(workload="hole_plate_ogrid1024x1024_q4_2099200dof_hollomon", n_circ=1024, n_rad=1024,
+               nodes=1049600, dof=2099200, elements=1048576, E_mpa=210000, nu=0.3, sigma_y=250, eps0=0.002,
+               n_exp=0.2, traction_mpa=220, increments=20, cg_tol=1e-10, outer_tol=1e-6)
+
+
 def config2_leg(ctx, cpu=True, cpu_cg_eps=1e-2):
     """Configuration 2 end to end: the 1024 x 1024 O-grid plate (2.1M DOF),
     Hollomon hardening sy (1 + eps_p / eps0)^n, 220 MPa in 20 increments, CG

@@ -26,7 +26,8 @@ Cases (each prints one JSON line with its host-side facts):
   zero, R linear solves;
 * ``cg_mg_large`` -- the same on the 2.1M-DOF plate, one linear solve to 1e-6;
 * ``mg_parts``   -- cp_bench_mg on the 2.1M-DOF plate: the set-up once, then
-  R iterations with CUDA events around P, U, R0, the coarse levels and S0.
+  R iterations with CUDA events around P, U, R0, the coarse levels and S0;
+  ``mg_parts_small`` the same on the 64x64 plate.
 
 The inputs are the benchmark's (bilinear steel, top traction), built the
 same way; nothing here is timed for a report.
@@ -63,14 +64,14 @@ def _instance(ctx, n_circ4, rad_n):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("case", choices=["assemble", "update", "cg_cluster", "cg_graph", "cg_large", "cg_fused_large",
-                                     "cg_mg", "cg_mg_large", "mg_parts"])
+                                     "cg_mg", "cg_mg_large", "mg_parts", "mg_parts_small"])
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--fp32", action="store_true", help="cg_large: the mixed mode's FP32 values")
     a = ap.parse_args(argv)
     ctx = Context(0)
     out = {"case": a.case}
-    if a.case == "mg_parts":
-        inst = _instance(ctx, 256, 1024)
+    if a.case in ("mg_parts", "mg_parts_small"):
+        inst = _instance(ctx, 256, 1024) if a.case == "mg_parts" else _instance(ctx, 16, 64)
         ms, by = (ctypes.c_double * 6)(), (ctypes.c_double * 6)()
         inst.set_field("uv", np.zeros(2 * inst.sizes()[0]))
         ctx.check(C.lib().cp_bench_mg(inst._h, a.repeat, ms, by))
