@@ -181,6 +181,18 @@ cp::CgArgs<float> cp_instance::cg_args<float>(int precond) {
 
 namespace {
 
+// Adaptive rule 2's factor (the linear tolerance is factor x relErr until
+// the outer tolerance is met). CUPLAST_RULE2_FACTOR overrides 0.1, for
+// measurements.
+double rule2_factor() {
+    static const double f = [] {
+        const char* e = std::getenv("CUPLAST_RULE2_FACTOR");
+        const double v = e ? std::atof(e) : 0.0;
+        return (v > 0.0 && v < 1.0) ? v : 0.1;
+    }();
+    return f;
+}
+
 int fail(cp_context* ctx, const Error& e) {
     if (ctx) ctx->last_error = e.msg;
     return e.status;
@@ -850,7 +862,8 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
                 // linear tolerance: tight once the secant iteration is close
                 double eps = boost ? std::max(o.cg_tol, kBoostTol) : o.cg_tol;
                 if (!boost && o.adaptive_cg == 1 && rel_err > 10.0 * o.outer_tol) eps = std::max(o.cg_tol, 1e-2 * rel_err);
-                if (!boost && o.adaptive_cg == 2 && rel_err > o.outer_tol) eps = std::max(o.cg_tol, 1e-1 * rel_err);
+                if (!boost && o.adaptive_cg == 2 && rel_err > o.outer_tol)
+                    eps = std::max(o.cg_tol, rule2_factor() * rel_err);
                 assemble(I, prec);
                 // the multigrid graph loop leaves its scalars for after the update
                 const bool mg_deferred = prec == CP_PREC_FP64 && o.precond == 2 && I->use_graph;

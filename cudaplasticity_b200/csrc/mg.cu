@@ -27,6 +27,7 @@
 // value is produced by one thread in a fixed order and every cross-block sum
 // is reduced by the last block in index order: the solve is deterministic.
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "amg.h"
@@ -630,7 +631,17 @@ int grid_small(long long n, int sms) {
 // Level 1 at most this many nodes: levels 1 .. L-1 run in one block.
 constexpr int kMgOneBlockNodes = 4096;
 
-bool one_block_coarse(const MgDev& m) { return m.L >= 3 && m.lv[1].n <= kMgOneBlockNodes; }
+// CUPLAST_MG_ONE_BLOCK=0 runs the coarse levels as one kernel per level step
+// whatever their size (for measurements).
+int one_block_limit() {
+    static const int lim = [] {
+        const char* e = std::getenv("CUPLAST_MG_ONE_BLOCK");
+        return (e && e[0] == '0') ? 0 : kMgOneBlockNodes;
+    }();
+    return lim;
+}
+
+bool one_block_coarse(const MgDev& m) { return m.L >= 3 && m.lv[1].n <= one_block_limit(); }
 
 // The V-cycle from U's y0 to S0's z, in three parts: R0, the coarse levels,
 // S0. `ev` (optional): events recorded after R0 and after the coarse levels.
