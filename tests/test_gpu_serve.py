@@ -160,6 +160,40 @@ def test_fp64_lanes_equal_cp_solve_alone_next_to_the_batch():
         ctx.close()
 
 
+def test_results_read_while_lanes_start_their_next_requests():
+    """Requests larger than one thread-block cluster holds run the graph-loop
+    CG, whose first solve on an instance captures a CUDA graph on the lane's
+    stream. The caller reads each result (every field, device to host) as
+    soon as it completes, while the two lanes already set up and capture the
+    next requests: every read succeeds and equals cp_solve alone bit for bit
+    (the outer cap keeps the test short; capped results compare too)."""
+    gen = dict(dof_min=20000, dof_max=40000)
+    kw = dict(FP64_KW, max_outer=3)
+    ws = [workload.instance(i, **gen) for i in range(80, 88)]
+    ctx = cp.Context(0)
+    ref = []
+    for w in ws:
+        inst = cp.Instance(ctx, w["mesh"], w["material"])
+        inst.set_loads(w["rp"], w["mask"], w["uv"])
+        rep = inst.solve(allow_not_converged=True, levels=w["levels"], **kw)
+        ref.append((inst.state(), rep))
+        inst.close()
+    srv = cp.Server(fp64_lanes=2)
+    try:
+        ids = [srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"],
+                          precision=cp.CP_PREC_FP64, **kw) for w in ws]
+        for k, rid in enumerate(ids):
+            inst, rep, _ = srv.wait(rid, timeout=600.0)
+            st = inst.state()
+            inst.close()
+            assert rep["status"] == ref[k][1]["status"], (k, rep)
+            for f in cp.FIELDS + ["uv"]:
+                assert np.array_equal(st[f], ref[k][0][f]), (k, f)
+    finally:
+        srv.close()
+        ctx.close()
+
+
 def test_destroy_with_fp64_solves_in_flight_returns():
     """Closing the server cancels the lanes' solves at their next outer
     iteration and the requests still queued."""
