@@ -909,7 +909,7 @@ def run_product_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": line_config(world),
             "solver": f"FP64, Aitken secant, {PRECOND_NAMES[SOLVE_KW['precond']]}, adaptive CG tolerance "
-                      "max(1e-10, 0.1 relErr) until relErr <= 1e-6, then 1e-10; levels from the "
+                      "max(1e-10, 0.2 relErr) until relErr <= 1e-6, then 1e-10; levels from the "
                       "third on start from the linear extrapolation of the last two",
             "cg_form": ("graph loop: P, U, then the V-cycle (restrict per level, dense coarsest "
                         "inverse, prolongation fused into post-smoothing), one kernel each"

@@ -182,13 +182,13 @@ cp::CgArgs<float> cp_instance::cg_args<float>(int precond) {
 namespace {
 
 // Adaptive rule 2's factor (the linear tolerance is factor x relErr until
-// the outer tolerance is met). CUPLAST_RULE2_FACTOR overrides 0.1, for
+// the outer tolerance is met): kRule2Factor, or CUPLAST_RULE2_FACTOR for
 // measurements.
 double rule2_factor() {
     static const double f = [] {
         const char* e = std::getenv("CUPLAST_RULE2_FACTOR");
         const double v = e ? std::atof(e) : 0.0;
-        return (v > 0.0 && v < 1.0) ? v : 0.1;
+        return (v > 0.0 && v < 1.0) ? v : cp::kRule2Factor;
     }();
     return f;
 }

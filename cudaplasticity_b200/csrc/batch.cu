@@ -194,7 +194,7 @@ __device__ __forceinline__ int tile_phase(const BState* S, int* sh) {
 // early steps, tight within 10x of the outer tolerance; 2 looser, tight once
 // the outer tolerance is met.
 __device__ __forceinline__ double next_eps(const BDesc& d, double rel_err) {
-    if (d.adaptive == 2) return rel_err > d.outer_tol ? fmax(d.cg_tol, 1e-1 * rel_err) : d.cg_tol;
+    if (d.adaptive == 2) return rel_err > d.outer_tol ? fmax(d.cg_tol, kRule2Factor * rel_err) : d.cg_tol;
     return (d.adaptive && rel_err > 10.0 * d.outer_tol) ? fmax(d.cg_tol, 1e-2 * rel_err) : d.cg_tol;
 }
 

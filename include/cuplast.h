@@ -104,7 +104,7 @@ typedef struct {
     double inner_tol;    /* mixed precision: relative tolerance of each FP32 inner solve */
     int adaptive_cg;     /* linear tolerance follows the outer error (inexact early steps; the converged result
                             meets the same criterion): 1: max(cg_tol, 1e-2 relErr) while relErr > 10 outer_tol;
-                            2: max(cg_tol, 1e-1 relErr) while relErr > outer_tol (fewer CG iterations, a few
+                            2: max(cg_tol, 0.2 relErr) while relErr > outer_tol (fewer CG iterations, a few
                             more outer ones) */
     int precond;         /* 0: unpreconditioned CG as the reference; 1: 2x2 block-Jacobi PCG (same solution);
                             2: PCG with one aggregation-multigrid V-cycle (CP_PREC_FP64 only, else
