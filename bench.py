@@ -813,7 +813,7 @@ def run_product_arm(args):
     if t_iter is None:
         roof_small = {"kernel": "k_c_solve", "error": small_error}
     else:
-        roof_small = {"bound": "hbm", "kernel": "k_c_solve (FP64 PCG in one 16-CTA cluster, per CG iteration)",
+        roof_small = {"bound": "hbm", "kernel": "k_c_solve (FP64 PCG in one thread-block cluster, per CG iteration)",
                       "achieved": b_iter / t_iter / 1e9, "peak": peak, "unit": "GB/s",
                       "frac": b_iter / t_iter / 1e9 / peak, "traffic": None, "bytes_per_launch": b_iter,
                       "ms_per_launch": t_iter * 1e3, "peak_kind": peak_kind,
