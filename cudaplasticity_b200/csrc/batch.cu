@@ -421,7 +421,7 @@ __device__ void tile_w(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, 
 // ITER: one CG iteration (see the section comment). C > 0: the row's blocks
 // are taken C at a time, columns and values loaded together ahead of the C
 // record gathers; C = 0: one unrolled loop.
-template <int C>
+template <int C, bool ST = false>
 __device__ void tile_iter(const BDesc& d, BState* S, BCtl* c, int4 tl, double* sh, int* shf) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sl0 = tl.y * tl.z, sl1 = min(sl0 + tl.z, d.n_slices);
@@ -470,8 +470,8 @@ __device__ void tile_iter(const BDesc& d, BState* S, BCtl* c, int4 tl, double* s
                     for (int j = 0; j < C; ++j) {
                         if (k0i + j < wd) {
                             const long long bi = base + 32LL * (k0i + j) + lane;
-                            cc[j] = __ldg(d.scol + bi);
-                            vv[j] = __ldg(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
+                            cc[j] = ld_stream<ST>(d.scol + bi);
+                            vv[j] = ld_stream<ST>(reinterpret_cast<const float4*>(d.val32 + 4 * bi));
                         }
                     }
 #pragma unroll
@@ -545,7 +545,7 @@ __device__ void tile_iter(const BDesc& d, BState* S, BCtl* c, int4 tl, double* s
 // 8 resident blocks per SM (64 registers): the CG iteration is bound by the
 // latency of its gathers, and the occupancy pays for the few spills. C: the
 // ITER gather form (tile_iter).
-template <int C>
+template <int C, bool ST = false>
 __global__ void __launch_bounds__(kThreads, 8) k_batch_cg(const BDesc* __restrict__ D, BState* SS,
                                                        const int4* __restrict__ tiles, BCtl* c) {
     __shared__ double sh[2 * kWarps];
@@ -559,7 +559,7 @@ __global__ void __launch_bounds__(kThreads, 8) k_batch_cg(const BDesc* __restric
         const int4 tl = tiles[t];
         BState* S = SS + tl.x;
         const int ph = tile_phase(S, &shp);
-        if (ph == PH_ITER) tile_iter<C>(D[tl.x], S, c, tl, sh, &shf);
+        if (ph == PH_ITER) tile_iter<C, ST>(D[tl.x], S, c, tl, sh, &shf);
         else if (ph == PH_W) tile_w(D[tl.x], S, c, tl, sh, &shf);
         else if (ph == PH_RES) tile_res(D[tl.x], S, c, tl, sh, &shf);
     }
@@ -849,7 +849,7 @@ BatchCgKernel batch_cg_kernel() {
         switch (e ? std::atoi(e) : 3) {
         case 0: return (BatchCgKernel)k_batch_cg<0>;
         case 5: return (BatchCgKernel)k_batch_cg<5>;
-        default: return (BatchCgKernel)k_batch_cg<3>;
+        default: return stream_loads() ? (BatchCgKernel)k_batch_cg<3, true> : (BatchCgKernel)k_batch_cg<3>;
         }
     }();
     return k;

@@ -57,6 +57,20 @@ __device__ __forceinline__ float4 load_block<float>(const float* __restrict__ va
     return __ldg(reinterpret_cast<const float4*>(val + 4 * b));
 }
 
+// The same with the streaming hint of ld_stream.
+template <typename T, bool ST>
+__device__ __forceinline__ typename Vec4<T>::type load_block_st(const T* __restrict__ val, long long b) {
+    using V4 = typename Vec4<T>::type;
+    if constexpr (ST) return __ldcs(reinterpret_cast<const V4*>(val + 4 * b));
+    else return load_block<T>(val, b);
+}
+template <>
+__device__ __forceinline__ double4 load_block_st<double, true>(const double* __restrict__ val, long long b) {
+    const double2* p = reinterpret_cast<const double2*>(val + 4 * b);
+    const double2 lo = __ldcs(p), hi = __ldcs(p + 1);
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+
 // Node c's record (v, z) of the parity being read.
 template <typename T>
 __device__ __forceinline__ typename Vec4<T>::type load_rec(const typename Vec4<T>::type* rec, int c) {
@@ -190,7 +204,7 @@ __global__ void __launch_bounds__(kThreads) k_cg_init(CgArgs<T> a, const VA* __r
 // P: z' = v + beta z (own node); K z' gathered as K (v + beta z); (K z', z').
 // C > 0: the blocks of a row are taken C at a time, their columns and values
 // loaded together before the C record gathers; C = 0: one loop, unrolled.
-template <typename T, bool PRE, int C>
+template <typename T, bool PRE, int C, bool ST>
 __global__ void __launch_bounds__(kThreads) k_cg_p(CgArgs<T> a, int parity) {
     using V2 = typename Vec2<T>::type;
     using V4 = typename Vec4<T>::type;
@@ -210,8 +224,8 @@ __global__ void __launch_bounds__(kThreads) k_cg_p(CgArgs<T> a, int parity) {
 #pragma unroll 3
                 for (int k = 0; k < w; ++k) {
                     const long long b = base + 32LL * k + lane;
-                    const int c = __ldg(a.scol + b);
-                    const auto v = load_block<T>(a.val, b);
+                    const int c = ld_stream<ST>(a.scol + b);
+                    const auto v = load_block_st<T, ST>(a.val, b);
                     const V4 g = load_rec<T>(ro, c);
                     const T wx = g.x + beta * g.z, wy = g.y + beta * g.w;
                     k0 += v.x * wx + v.y * wy;
@@ -225,8 +239,8 @@ __global__ void __launch_bounds__(kThreads) k_cg_p(CgArgs<T> a, int parity) {
                     for (int j = 0; j < C; ++j) {
                         if (k0i + j < w) {
                             const long long b = base + 32LL * (k0i + j) + lane;
-                            cc[j] = __ldg(a.scol + b);
-                            vv[j] = load_block<T>(a.val, b);
+                            cc[j] = ld_stream<ST>(a.scol + b);
+                            vv[j] = load_block_st<T, ST>(a.val, b);
                         }
                     }
 #pragma unroll
@@ -358,6 +372,14 @@ int resident_grid(K kernel, long long units, int per_block, int sm_count) {
 
 }  // namespace
 
+bool stream_loads() {
+    static const bool v = [] {
+        const char* e = std::getenv("CUPLAST_STREAM_LOADS");
+        return e && e[0] == '1';
+    }();
+    return v;
+}
+
 template <typename T>
 void cg_launch_init(const CgArgs<T>& a, const void* valA, bool valA_is_fp64, double eps2, long long max_iter,
                     int relative_to_r0, double outer_eps2, cudaStream_t s) {
@@ -391,11 +413,12 @@ int p_chunk() {
 
 template <typename T, bool PRE>
 void (*p_kernel(int c))(CgArgs<T>, int) {
+    if (stream_loads()) return k_cg_p<T, PRE, 0, true>;
     switch (c) {
-    case 0: return k_cg_p<T, PRE, 0>;
-    case 3: return k_cg_p<T, PRE, 3>;
-    case 9: return k_cg_p<T, PRE, 9>;
-    default: return k_cg_p<T, PRE, 5>;
+    case 0: return k_cg_p<T, PRE, 0, false>;
+    case 3: return k_cg_p<T, PRE, 3, false>;
+    case 9: return k_cg_p<T, PRE, 9, false>;
+    default: return k_cg_p<T, PRE, 5, false>;
     }
 }
 

@@ -191,7 +191,7 @@ __device__ __forceinline__ void w_scalars(CgScalars* sc, const double* t) {
 // One iteration (see the file comment); parity selects the record buffers.
 // C > 0: the row's blocks are taken C at a time, their columns and values
 // loaded together ahead of the C record gathers; C = 0: one unrolled loop.
-template <bool P, int C = 0>
+template <bool P, int C = 0, bool ST = false>
 __device__ __forceinline__ void iter_body(const FusedArgs& a, int parity, double al, double bt, double* v) {
     const double2* __restrict__ go = parity ? a.gB : a.gA;
     double2* __restrict__ gn = parity ? a.gA : a.gB;
@@ -233,9 +233,10 @@ __device__ __forceinline__ void iter_body(const FusedArgs& a, int parity, double
                 for (int j = 0; j < C; ++j) {
                     if (k0i + j < wd) {
                         const long long bi = base + 32LL * (k0i + j) + lane;
-                        cc[j] = __ldg(a.scol + bi);
-                        lo[j] = load_lo(a.val, bi);
-                        hi[j] = load_hi(a.val, bi);
+                        cc[j] = ld_stream<ST>(a.scol + bi);
+                        const double2* vp = reinterpret_cast<const double2*>(a.val + 4 * bi);
+                        lo[j] = ld_stream<ST>(vp);
+                        hi[j] = ld_stream<ST>(vp + 1);
                     }
                 }
 #pragma unroll
@@ -305,24 +306,24 @@ __global__ void __launch_bounds__(kThreads) k_f_w(FusedArgs a) {
     if (threadIdx.x == 0) w_scalars(sc, t);
 }
 
-template <int C>
+template <int C, bool ST = false>
 __device__ __forceinline__ void iter_kernel_body(const FusedArgs& a, int parity) {
     __shared__ double sh[2 * kThreads / 32];
     __shared__ bool last;
     CgScalars* sc = a.sc;
     if (sc->converged || sc->status) return;
     double v[kSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    iter_body<false, C>(a, parity, sc->alpha, sc->beta, v);
+    iter_body<false, C, ST>(a, parity, sc->alpha, sc->beta, v);
     double t[kSums];
     if (!reduce_sums(a, v, 5, t, sh, &last)) return;
     if (threadIdx.x == 0) iter_scalars(sc, t);
 }
 
-// C as in iter_body; k_f_iter4 asks the compiler for 4 resident blocks per
-// SM (a 64-register cap).
-template <int C>
+// C and ST as in iter_body; k_f_iter4 asks the compiler for 4 resident
+// blocks per SM (a 64-register cap).
+template <int C, bool ST = false>
 __global__ void __launch_bounds__(kThreads) k_f_iter(FusedArgs a, int parity) {
-    iter_kernel_body<C>(a, parity);
+    iter_kernel_body<C, ST>(a, parity);
 }
 template <int C>
 __global__ void __launch_bounds__(kThreads, 4) k_f_iter4(FusedArgs a, int parity) {
@@ -491,7 +492,7 @@ IterKernel iter_kernel() {
         case 3: return (IterKernel)k_f_iter4<3>;
         case 4: return (IterKernel)k_f_iter<2>;
         case 5: return (IterKernel)k_f_iter<5>;
-        default: return (IterKernel)k_f_iter<3>;
+        default: return stream_loads() ? (IterKernel)k_f_iter<3, true> : (IterKernel)k_f_iter<3>;
         }
     }();
     return k;

@@ -93,4 +93,17 @@ __device__ __forceinline__ double2 block_reduce_array2(const volatile double* p,
     return block_sum2(a, b, sh);
 }
 
+// Loads of data a kernel streams through once (matrix values, block
+// columns): ST = true marks them evict-first (ld.global.cs), so that they do
+// not push the gathered neighbour records out of L1 / L2; ST = false reads
+// them through the read-only path.
+template <bool ST, typename V>
+__device__ __forceinline__ V ld_stream(const V* p) {
+    if constexpr (ST) return __ldcs(p);
+    else return __ldg(p);
+}
+
+// CUPLAST_STREAM_LOADS=1 selects the ST = true kernels (measurements).
+bool stream_loads();
+
 }  // namespace cp
