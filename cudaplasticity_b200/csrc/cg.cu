@@ -375,7 +375,7 @@ int resident_grid(K kernel, long long units, int per_block, int sm_count) {
 bool stream_loads() {
     static const bool v = [] {
         const char* e = std::getenv("CUPLAST_STREAM_LOADS");
-        return e && e[0] == '1';
+        return !(e && e[0] == '0');
     }();
     return v;
 }

@@ -492,7 +492,7 @@ IterKernel iter_kernel() {
         case 3: return (IterKernel)k_f_iter4<3>;
         case 4: return (IterKernel)k_f_iter<2>;
         case 5: return (IterKernel)k_f_iter<5>;
-        default: return stream_loads() ? (IterKernel)k_f_iter<3, true> : (IterKernel)k_f_iter<3>;
+        default: return (IterKernel)k_f_iter<3>;
         }
     }();
     return k;
