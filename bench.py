@@ -1074,6 +1074,7 @@ def main():
     ap.add_argument("--svp-cg-tol", type=float, default=1e-10)
     ap.add_argument("--svp-max-outer", type=int, default=2000, help="outer-iteration cap per load level, both arms")
     ap.add_argument("--svp-forms", default="fp64_lanes,mixed_batch")
+    ap.add_argument("--svp-rates", default="10,100,1000", help="Poisson arrival rates (requests/s), comma-separated")
     ap.add_argument("--precond", type=int, default=SOLVE_KW["precond"], choices=[0, 1, 2],
                     help="linear solver of the headline and of the FP64 served arm: 0 CG, 1 block-Jacobi PCG, "
                          "2 multigrid PCG")
@@ -1096,6 +1097,7 @@ def main():
         ctx = cp.Context(0)
         print(json.dumps({"served_vs_plain": served_vs_plain_leg(
             ctx, args.svp, stream=args.svp_stream, budget_s=args.svp_budget, forms=tuple(args.svp_forms.split(",")),
+            rates=tuple(float(x) for x in args.svp_rates.split(",")),
             outer_tol=args.svp_outer_tol, cg_tol=args.svp_cg_tol, max_outer=args.svp_max_outer)}), flush=True)
         ctx.close()
         return

@@ -859,6 +859,11 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
             int prec = boost ? CP_PREC_MIXED : o.precision;
             for (int it = 0; it < o.max_outer; ++it) {
                 CP_CHECK(!I->cancel.load(std::memory_order_relaxed), CP_ERR_CANCELLED, "solve cancelled");
+                if (cudaStream_t ns = I->ctx->restream.exchange(nullptr)) {
+                    CP_CUDA(cudaStreamSynchronize(s));  // nothing of this solve left on the old stream
+                    I->ctx->stream = ns;
+                    s = ns;
+                }
                 // linear tolerance: tight once the secant iteration is close
                 double eps = boost ? std::max(o.cg_tol, kBoostTol) : o.cg_tol;
                 if (!boost && o.adaptive_cg == 1 && rel_err > 10.0 * o.outer_tol) eps = std::max(o.cg_tol, 1e-2 * rel_err);

@@ -19,6 +19,10 @@ struct cp_context {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string last_error;
+    // Set from another thread (the solve service's oldest-first priorities):
+    // cp_solve moves to this stream at its next outer iteration, after the
+    // current one has drained.
+    std::atomic<cudaStream_t> restream{nullptr};
 };
 
 struct cp_instance {

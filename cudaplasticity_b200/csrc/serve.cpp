@@ -67,6 +67,15 @@ struct cp_server {
     cp_context* ctx_setup = nullptr;
     cp_batch* batch = nullptr;
     std::vector<cp_context*> lane_ctx;    // one per FP64 lane
+    // Oldest first: each lane has one stream per priority level, and the
+    // running requests in submission order take the levels from the highest
+    // down (the last level shared by the rest), reassigned whenever a lane
+    // starts or ends a request; a running solve moves to its new stream at
+    // its next outer iteration. lane_own[k] is the stream lane_ctx[k] was
+    // created with (restored before the context is destroyed).
+    std::vector<std::vector<cudaStream_t>> lane_streams;
+    std::vector<cudaStream_t> lane_own;
+    std::vector<int> lane_level;          // the level each lane's request runs at (-1: idle)
     // The context of every instance handed back to a caller: the lanes' and
     // the set-up contexts keep working (and capture CUDA graphs on their
     // streams) while callers read results, so a result moves to this
@@ -113,6 +122,38 @@ void stop_thread(cp_server* s) {
 }
 
 bool is_lane_request(const cp_solve_opts& o) { return o.precision != CP_PREC_MIXED; }
+
+// Reassigns the levels of the running requests (s->mu held).
+void relevel(cp_server* s) {
+    if (s->lane_streams.empty()) return;
+    std::vector<std::pair<long long, int>> run;
+    for (size_t j = 0; j < s->lane_cur.size(); ++j)
+        if (s->lane_cur[j]) run.emplace_back(s->lane_cur[j]->id, (int)j);
+        else s->lane_level[j] = -1;
+    std::sort(run.begin(), run.end());
+    for (size_t i = 0; i < run.size(); ++i) {
+        const int j = run[i].second;
+        const int lv = (int)std::min(i, s->lane_streams[j].size() - 1);
+        if (lv != s->lane_level[j]) {
+            s->lane_level[j] = lv;
+            s->lane_ctx[j]->restream.store(s->lane_streams[j][lv]);
+        }
+    }
+}
+
+// Gives every lane context its own stream back and destroys the priority
+// streams (before the lane contexts are destroyed).
+void release_lane_streams(cp_server* s) {
+    for (size_t k = 0; k < s->lane_own.size() && k < s->lane_ctx.size(); ++k) {
+        cudaStreamSynchronize(s->lane_ctx[k]->stream);
+        s->lane_ctx[k]->stream = s->lane_own[k];
+    }
+    for (auto& v : s->lane_streams)
+        for (cudaStream_t st : v) cudaStreamDestroy(st);
+    for (cp_context* c : s->lane_ctx) c->restream.store(nullptr);
+    s->lane_streams.clear();
+    s->lane_own.clear();
+}
 
 void stop_all_at_exit() {
     std::lock_guard<std::mutex> lock(g_live_mu);
@@ -173,6 +214,13 @@ void lane(cp_server* s, int k) {
             r = s->lane_q.front();
             s->lane_q.pop_front();
             s->lane_cur[k] = r;
+            if (!s->lane_streams.empty()) {
+                s->lane_level[k] = -1;
+                relevel(s);
+                // this lane's stream is idle between requests: take the level now
+                s->lane_ctx[k]->restream.store(nullptr);
+                s->lane_ctx[k]->stream = s->lane_streams[k][s->lane_level[k]];
+            }
         }
         cp_instance* inst = nullptr;
         int rc = setup(s->lane_ctx[k], r, &inst);
@@ -191,6 +239,7 @@ void lane(cp_server* s, int k) {
         }
         std::lock_guard<std::mutex> lock(s->mu);
         s->lane_cur[k] = nullptr;
+        relevel(s);
         s->inflight_bytes -= r->footprint;
         if (rc != CP_OK) {
             r->status = rc;
@@ -403,12 +452,31 @@ CP_API int cp_server_create(const cp_server_opts* opts, cp_server** out) {
         if (rc == CP_OK) s->lane_ctx.push_back(c);
     }
     s->lane_cur.assign(s->lane_ctx.size(), nullptr);
+    {
+        const char* e = std::getenv("CUPLAST_LANE_PRIORITY");
+        int least = 0, greatest = 0;
+        if (rc == CP_OK && !(e && e[0] == '0') && cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess &&
+            greatest < least) {
+            for (cp_context* c : s->lane_ctx) {
+                s->lane_own.push_back(c->stream);
+                std::vector<cudaStream_t> v;
+                for (int p = greatest; p <= least && rc == CP_OK; ++p) {  // greatest priority first
+                    cudaStream_t st = nullptr;
+                    if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, p) != cudaSuccess) rc = CP_ERR_CUDA;
+                    else v.push_back(st);
+                }
+                s->lane_streams.push_back(v);
+            }
+            s->lane_level.assign(s->lane_ctx.size(), -1);
+        }
+    }
     if (rc == CP_OK) {
         size_t f = 0, t = 0;
         if (cudaMemGetInfo(&f, &t) != cudaSuccess) rc = CP_ERR_CUDA;
         s->total_mem = t;
     }
     if (rc != CP_OK) {
+        release_lane_streams(s);
         for (cp_context* c : s->lane_ctx) cp_context_destroy(c);
         if (s->batch) cp_batch_destroy(s->batch);
         if (s->ctx_out) cp_context_destroy(s->ctx_out);
@@ -433,6 +501,7 @@ CP_API int cp_server_create(const cp_server_opts* opts, cp_server** out) {
         if (s->th.joinable()) s->th.join();
         for (auto& t : s->lanes)
             if (t.joinable()) t.join();
+        release_lane_streams(s);
         for (cp_context* c : s->lane_ctx) cp_context_destroy(c);
         cp_batch_destroy(s->batch);
         cp_context_destroy(s->ctx_out);
@@ -464,6 +533,7 @@ CP_API int cp_server_destroy(cp_server* s) {
         }
     }
     s->cv_done.notify_all();
+    release_lane_streams(s);
     for (cp_context* c : s->lane_ctx) cp_context_destroy(c);
     cp_context_destroy(s->ctx_out);
     cp_context_destroy(s->ctx_setup);
