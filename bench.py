@@ -555,7 +555,7 @@ STREAMS = {"served": dict(seed=20270101, dof_min=2000, dof_max=500000, increment
 
 
 def served_vs_plain_leg(ctx, n_requests, stream="served", rates=(10.0, 100.0, 1000.0), budget_s=120.0,
-                        forms=("fp64_lanes", "mixed_batch"), deadline_factor=1.5, **tol):
+                        forms=("fp64_lanes", "mixed_batch"), deadline_factor=1.5, lanes=8, **tol):
     """The served-vs-plain comparison on the same requests.
 
     Requests: the first n of a seeded request stream (STREAMS: the served
@@ -637,7 +637,7 @@ def served_vs_plain_leg(ctx, n_requests, stream="served", rates=(10.0, 100.0, 10
         row = {"plain_fp64_dropin": {"solves_per_s": plain_sps, "p50_s": float(np.percentile(p_lat, 50)),
                                      "p99_s": float(np.percentile(p_lat, 99))}}
         for form in forms:
-            srv = cp.Server(fp64_lanes=8)
+            srv = cp.Server(fp64_lanes=lanes)
             if form == "fp64_lanes":
                 skw = dict(kw, precision=cp.CP_PREC_FP64)
             elif form == "fp64_lanes_mg":  # the lanes with the multigrid-preconditioned CG
@@ -1075,6 +1075,7 @@ def main():
     ap.add_argument("--svp-max-outer", type=int, default=2000, help="outer-iteration cap per load level, both arms")
     ap.add_argument("--svp-forms", default="fp64_lanes,mixed_batch")
     ap.add_argument("--svp-rates", default="10,100,1000", help="Poisson arrival rates (requests/s), comma-separated")
+    ap.add_argument("--svp-lanes", type=int, default=8, help="FP64 lanes of the solve service")
     ap.add_argument("--precond", type=int, default=SOLVE_KW["precond"], choices=[0, 1, 2],
                     help="linear solver of the headline and of the FP64 served arm: 0 CG, 1 block-Jacobi PCG, "
                          "2 multigrid PCG")
@@ -1097,7 +1098,7 @@ def main():
         ctx = cp.Context(0)
         print(json.dumps({"served_vs_plain": served_vs_plain_leg(
             ctx, args.svp, stream=args.svp_stream, budget_s=args.svp_budget, forms=tuple(args.svp_forms.split(",")),
-            rates=tuple(float(x) for x in args.svp_rates.split(",")),
+            rates=tuple(float(x) for x in args.svp_rates.split(",")), lanes=args.svp_lanes,
             outer_tol=args.svp_outer_tol, cg_tol=args.svp_cg_tol, max_outer=args.svp_max_outer)}), flush=True)
         ctx.close()
         return
