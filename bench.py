@@ -687,6 +687,78 @@ def served_vs_plain_leg(ctx, n_requests, stream="served", rates=(10.0, 100.0, 10
     return out
 
 
+def sharded_service_leg(device, rank, world, dist, n_requests=24, stream="batch", lanes=8, max_outer=300):
+    """Instance sharding across GPUs: the first n requests of a seeded stream
+    split over the ranks (longest-processing-time first on DOF x increments,
+    cudaplasticity_b200.shard), each rank solving its share as one burst
+    through the solve service's FP64 lanes on its own GPU; no collective on
+    the data path, the per-request records meet on the host (object
+    all-gather). Every rank runs it (collectives in the same order);
+    throughput = requests / the slowest rank's span. The checksums (sum |u|
+    per request) are those of the same requests solved on one GPU: the
+    kernels' reductions run in a fixed order."""
+    import numpy as np
+
+    import cudaplasticity_b200 as cp
+    from cudaplasticity_b200 import shard, workload
+
+    st_ = STREAMS[stream]
+    reqs = [workload.instance(i, seed=st_["seed"], dof_min=st_["dof_min"], dof_max=st_["dof_max"],
+                              increments=st_["increments"]) for i in range(n_requests)]
+    costs = [shard.request_cost(w["params"]["dof"], w["levels"]) for w in reqs]
+    parts = shard.partition(costs, world)
+    kw = dict(FP64_SERVE_KW, max_outer=max_outer, precision=cp.CP_PREC_FP64)
+    srv = cp.Server(device=device, fp64_lanes=lanes)
+
+    def submit(w):
+        return srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"], **kw)
+
+    def wait(rid):
+        inst, rep, lat = srv.wait(rid, timeout=-1.0)
+        u = inst.field("uv")
+        inst.close()
+        return {"status": rep["status"], "outer": rep["outer_iters"], "cg": rep["cg_iters"], "latency": lat,
+                "checksum": float(np.abs(u).sum()), "rank": rank}
+
+    try:
+        if dist is not None:
+            dist.barrier()
+        recs = shard.run_share(parts[rank], lambda i: reqs[i], submit, wait)
+    finally:
+        srv.close()
+    merged = shard.gather_records(recs, dist)
+    out = shard.summarize(merged, n_requests, world)
+    out.update(workload="first %d requests of the %s as one burst; FP64 lanes (%d per GPU), CG %g, outer %g, outer "
+                        "cap %d" % (n_requests, st_["text"], lanes, kw["cg_tol"], kw["outer_tol"], max_outer),
+               split="longest-processing-time first on DOF x increments",
+               shares=[{"rank": r, "requests": parts[r], "seconds": max((merged[i]["done_at"] for i in parts[r]),
+                                                                         default=0.0)} for r in range(world)],
+               checksums=[merged[i]["checksum"] for i in range(n_requests)])
+    return out
+
+
+def run_sharded(args):
+    """bench.py --sharded N [under torchrun]: the sharded-service leg alone."""
+    import cudaplasticity_b200 as cp  # noqa: F401  (loads the library before the process group)
+
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist_mod
+
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = dist_mod
+    out = sharded_service_leg(local, rank, world, dist, n_requests=args.sharded)
+    if rank == 0:
+        print(json.dumps({"sharded_service": out}), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def run_product_arm(args):
     import numpy as np
 
@@ -917,16 +989,25 @@ def run_product_arm(args):
             print(json.dumps({"leg_failed": name, "error": repr(exc)}), file=sys.stderr, flush=True)
             return {"error": repr(exc)}
 
-    if rank == 0 and not args.skip_served:
+    sharded = None
+    if world > 1 and not args.skip_served:
+        # every rank: its share of the batch-stream requests on its own GPU
+        try:
+            sharded = sharded_service_leg(device, rank, world, dist, n_requests=args.serve_requests)
+        except Exception as exc:  # noqa: BLE001
+            sharded = {"error": repr(exc)}
+    # the single-GPU comparisons (N = 1 figures; with N > 1 the ranks have
+    # left after the sharded leg)
+    if rank == 0 and world == 1 and not args.skip_served:
         # the metric: the same requests served and one at a time through the
         # plain FP64 drop-in, at three Poisson rates
         served = aux("served_vs_plain", lambda: served_vs_plain_leg(
             ctx, args.serve_requests, stream="batch", budget_s=args.serve_budget, forms=("fp64_lanes",),
             max_outer=300))
-    if rank == 0 and not args.skip_batched:
+    if rank == 0 and world == 1 and not args.skip_batched:
         batched = aux("batched", lambda: batched_leg(ctx, window_s=args.batched_window))
         roof_batched = aux("roofline_batched", lambda: cg_kernel_roofline(ctx))
-    if rank == 0 and not args.skip_config2:
+    if rank == 0 and world == 1 and not args.skip_config2:
         config2 = aux("config2", lambda: config2_leg(ctx, cpu=not args.skip_cpu, cpu_cg_eps=0.1))
 
     launches = sum(r["kernel_launches"] for r in reps)
@@ -950,6 +1031,7 @@ def run_product_arm(args):
             "multigrid_parts": mg_parts, "cpu_baseline": cpu, "clocks": clocks.summary(),
             "accuracy_vs_tight_fp64": accuracy, "error_vs_reference": err_ref, "batched": batched,
             "roofline_batched": roof_batched, "served_vs_plain": served, "config2": config2,
+            "sharded_service": sharded,
             "throughput": dict(throughput, dof_iterations_per_s_headline=2 * arrays["node_xy"].shape[0] *
                                sum(r["cg_iters"] for r in reps) / sum(times)),
             "detail": {"outer_iters": reps[-1]["outer_iters"], "cg_iters": reps[-1]["cg_iters"],
@@ -1076,6 +1158,8 @@ def main():
     ap.add_argument("--svp-forms", default="fp64_lanes,mixed_batch")
     ap.add_argument("--svp-rates", default="10,100,1000", help="Poisson arrival rates (requests/s), comma-separated")
     ap.add_argument("--svp-lanes", type=int, default=8, help="FP64 lanes of the solve service")
+    ap.add_argument("--sharded", type=int, metavar="N",
+                    help="sharded-service leg only (the first N batch-stream requests split over the ranks), then exit")
     ap.add_argument("--precond", type=int, default=SOLVE_KW["precond"], choices=[0, 1, 2],
                     help="linear solver of the headline and of the FP64 served arm: 0 CG, 1 block-Jacobi PCG, "
                          "2 multigrid PCG")
@@ -1091,6 +1175,9 @@ def main():
         ctx = cp.Context(0)
         print(json.dumps({"config2": config2_leg(ctx, cpu=not args.skip_cpu)}), flush=True)
         ctx.close()
+        return
+    if args.sharded:
+        run_sharded(args)
         return
     if args.svp:
         import cudaplasticity_b200 as cp

@@ -48,3 +48,117 @@ def test_single_process_is_identity():
 
     assert max_over_ranks(3.0) == 3.0
     assert replica_throughput(1, 4, 2.0) == pytest.approx(2.0)
+
+
+# ---- instance sharding of the batched / served workloads (no GPU) ----
+
+def test_partition_is_lpt_deterministic_and_covers_every_request():
+    from cudaplasticity_b200.shard import partition
+
+    parts = partition([5, 4, 3, 3, 3], 2)
+    # 5 -> rank 0; 4 -> 1; 3 -> 1 (4 < 5); 3 -> 0 (5 < 7); 3 -> 1 (7 < 8)
+    assert parts == [[0, 3], [1, 2, 4]]
+    assert partition([5, 4, 3, 3, 3], 2) == parts
+    costs = [float((7 * i) % 11 + 1) for i in range(40)]
+    for world in (1, 2, 3, 8):
+        ps = partition(costs, world)
+        assert len(ps) == world
+        assert sorted(i for p in ps for i in p) == list(range(40))
+        assert all(p == sorted(p) for p in ps)
+        loads = [sum(costs[i] for i in p) for p in ps]
+        # LPT: no rank carries more than the mean plus the largest single cost
+        assert max(loads) <= sum(costs) / world + max(costs)
+    assert partition([], 3) == [[], [], []]
+    with pytest.raises(ValueError):
+        partition([1.0], 0)
+
+
+def test_request_cost_counts_increments():
+    from cudaplasticity_b200.shard import request_cost
+
+    assert request_cost(1000, 1) == 1000.0
+    assert request_cost(1000, 5) == 5000.0
+    assert request_cost(1000, 0) == 1000.0
+
+
+class _FakeGather:
+    """An all-gather over ranks whose records are given up front."""
+
+    def __init__(self, parts):
+        self.parts = parts
+
+    def get_world_size(self):
+        return len(self.parts)
+
+    def all_gather_object(self, out, obj):
+        for k, p in enumerate(self.parts):
+            out[k] = p
+
+
+def test_gather_rejects_a_request_solved_twice():
+    from cudaplasticity_b200.shard import gather_records
+
+    with pytest.raises(RuntimeError):
+        gather_records({}, _FakeGather([{0: {"status": 0}}, {0: {"status": 0}}]))
+    merged = gather_records({}, _FakeGather([{0: {"a": 1}}, {1: {"a": 2}}]))
+    assert merged == {0: {"a": 1}, 1: {"a": 2}}
+
+
+def _shard_rank(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    from cudaplasticity_b200 import shard
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        n = 7
+        costs = [float(i % 3 + 1) for i in range(n)]
+        parts = shard.partition(costs, world)
+        ticks = iter(range(1000))
+        solved = []
+
+        def build(i):
+            return {"index": i, "cost": costs[i]}
+
+        def submit(req):
+            solved.append(req["index"])
+            return req["index"]
+
+        def wait(rid):
+            return {"status": 0 if rid != 5 else 4, "latency": 0.1 * (rid + 1), "checksum": rid * 1.5,
+                    "rank": rank}
+
+        recs = shard.run_share(parts[rank], build, submit, wait, clock=lambda: float(next(ticks)))
+        merged = shard.gather_records(recs, dist)
+        summ = shard.summarize(merged, n, world)
+        out[rank] = (sorted(solved), parts, sorted(merged), [merged[i]["rank"] for i in range(n)],
+                     [merged[i]["checksum"] for i in range(n)], summ)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_split_the_requests_and_merge_the_records():
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_shard_rank, args=(2, port, out), nprocs=2, join=True)
+        res = dict(out)
+    solved0, parts, keys0, owner, checks, summ0 = res[0]
+    solved1, _, keys1, _, _, summ1 = res[1]
+    # each rank solved exactly its share, the shares are disjoint and complete
+    assert solved0 == parts[0] and solved1 == parts[1]
+    assert sorted(solved0 + solved1) == list(range(7))
+    # every rank holds the same merged records, with the right owners
+    assert keys0 == keys1 == list(range(7))
+    assert owner == [0 if i in parts[0] else 1 for i in range(7)]
+    assert checks == [i * 1.5 for i in range(7)]
+    assert summ0 == summ1
+    assert summ0["statuses"] == [0, 4]
+    assert summ0["requests"] == 7 and summ0["ranks"] == 2
+    # the span is the slowest rank's: done_at counts clock ticks after the first submission
+    longest = max(len(p) for p in parts)
+    assert summ0["seconds"] == pytest.approx(float(longest))
+    assert summ0["solves_per_s"] == pytest.approx(7 / float(longest))
