@@ -703,12 +703,18 @@ def sharded_service_leg(device, rank, world, dist, n_requests=24, stream="batch"
     from cudaplasticity_b200 import shard, workload
 
     st_ = STREAMS[stream]
-    reqs = [workload.instance(i, seed=st_["seed"], dof_min=st_["dof_min"], dof_max=st_["dof_max"],
-                              increments=st_["increments"]) for i in range(n_requests)]
-    costs = [shard.request_cost(w["params"]["dof"], w["levels"]) for w in reqs]
-    parts = shard.partition(costs, world)
     kw = dict(FP64_SERVE_KW, max_outer=max_outer, precision=cp.CP_PREC_FP64)
-    srv = cp.Server(device=device, fp64_lanes=lanes)
+    # every rank takes the barrier and the all-gather whatever fails locally,
+    # so that no rank waits on a collective that another rank skipped
+    err, recs, srv, parts = None, {}, None, None
+    try:
+        reqs = [workload.instance(i, seed=st_["seed"], dof_min=st_["dof_min"], dof_max=st_["dof_max"],
+                                  increments=st_["increments"]) for i in range(n_requests)]
+        costs = [shard.request_cost(w["params"]["dof"], w["levels"]) for w in reqs]
+        parts = shard.partition(costs, world)
+        srv = cp.Server(device=device, fp64_lanes=lanes)
+    except Exception as exc:  # noqa: BLE001
+        err = repr(exc)
 
     def submit(w):
         return srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"], **kw)
@@ -720,13 +726,20 @@ def sharded_service_leg(device, rank, world, dist, n_requests=24, stream="batch"
         return {"status": rep["status"], "outer": rep["outer_iters"], "cg": rep["cg_iters"], "latency": lat,
                 "checksum": float(np.abs(u).sum()), "rank": rank}
 
-    try:
-        if dist is not None:
-            dist.barrier()
-        recs = shard.run_share(parts[rank], lambda i: reqs[i], submit, wait)
-    finally:
+    if dist is not None:
+        dist.barrier()
+    if err is None:
+        try:
+            recs = shard.run_share(parts[rank], lambda i: reqs[i], submit, wait)
+        except Exception as exc:  # noqa: BLE001
+            err = repr(exc)
+    if srv is not None:
         srv.close()
-    merged = shard.gather_records(recs, dist)
+    got = shard.gather_objects({"records": recs, "error": err}, dist)
+    errors = [f"rank {r}: {g['error']}" for r, g in enumerate(got) if g["error"]]
+    if errors:
+        return {"error": "; ".join(errors)}
+    merged = shard.merge_records([g["records"] for g in got])
     out = shard.summarize(merged, n_requests, world)
     out.update(workload="first %d requests of the %s as one burst; FP64 lanes (%d per GPU), CG %g, outer %g, outer "
                         "cap %d" % (n_requests, st_["text"], lanes, kw["cg_tol"], kw["outer_tol"], max_outer),

@@ -59,13 +59,19 @@ def run_share(indices, build, submit, wait, clock=time.perf_counter):
     return out
 
 
-def gather_records(records, dist=None):
-    """Merges every rank's {index: record} into one dict, on every rank (an
-    object all-gather; ``records`` itself when ``dist`` is None)."""
+def gather_objects(obj, dist=None):
+    """[obj of rank 0, obj of rank 1, ...] on every rank (an object
+    all-gather; [obj] when ``dist`` is None)."""
     if dist is None:
-        return dict(records)
+        return [obj]
     parts = [None] * dist.get_world_size()
-    dist.all_gather_object(parts, dict(records))
+    dist.all_gather_object(parts, obj)
+    return parts
+
+
+def merge_records(parts):
+    """One {index: record} from the ranks' record dicts; an index on two
+    ranks is an error."""
     merged = {}
     for p in parts:
         for k, v in p.items():
@@ -73,6 +79,11 @@ def gather_records(records, dist=None):
                 raise RuntimeError(f"request {k} was solved on two ranks")
             merged[k] = v
     return merged
+
+
+def gather_records(records, dist=None):
+    """Merges every rank's {index: record} into one dict, on every rank."""
+    return merge_records(gather_objects(dict(records), dist))
 
 
 def summarize(merged, n_requests, world):
