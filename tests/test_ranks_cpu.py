@@ -162,3 +162,74 @@ def test_two_gloo_ranks_split_the_requests_and_merge_the_records():
     longest = max(len(p) for p in parts)
     assert summ0["seconds"] == pytest.approx(float(longest))
     assert summ0["solves_per_s"] == pytest.approx(7 / float(longest))
+
+
+def _bench_shard_rank(rank, world, port, fail_rank, out):
+    """bench.py's sharded leg with a stand-in solve service (no GPU): the
+    batch-stream meshes are built by the library's host code, the solves are
+    faked; ``fail_rank``'s service fails to start."""
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+
+    import bench
+    import cudaplasticity_b200 as cp
+
+    class FakeInstance:
+        def __init__(self, n):
+            self.n = n
+
+        def field(self, name):
+            return np.full(2 * self.n, 0.5)
+
+        def close(self):
+            pass
+
+    class FakeServer:
+        def __init__(self, device=0, fp64_lanes=8):
+            if rank == fail_rank:
+                raise RuntimeError("service failed to start")
+            self.meshes = []
+
+        def submit(self, mesh, material, rp, mask, uv, **kw):
+            self.meshes.append(len(mesh["node_xy"]))
+            return len(self.meshes) - 1
+
+        def wait(self, rid, timeout=-1.0):
+            rep = {"status": 0, "outer_iters": 3, "cg_iters": 10}
+            return FakeInstance(self.meshes[rid]), rep, 0.01
+
+        def close(self):
+            pass
+
+    cp.Server = FakeServer
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        out[rank] = bench.sharded_service_leg(0, rank, world, dist, n_requests=4)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("fail_rank", [-1, 1])
+def test_bench_sharded_leg_on_two_gloo_ranks(fail_rank):
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_bench_shard_rank, args=(2, port, fail_rank, out), nprocs=2, join=True)
+        res = dict(out)
+    if fail_rank >= 0:
+        # both ranks finish (no collective left waiting) and report the failure
+        assert "rank 1: RuntimeError('service failed to start')" in res[0]["error"]
+        assert res[0] == res[1]
+        return
+    r0 = res[0]
+    assert r0["requests"] == 4 and r0["ranks"] == 2 and r0["statuses"] == [0]
+    shares = sorted(i for s in r0["shares"] for i in s["requests"])
+    assert shares == [0, 1, 2, 3]
+    # checksum = sum |u| of the stand-in result, 0.5 per DOF
+    from cudaplasticity_b200 import workload
+
+    dofs = [workload.instance(i, seed=20261203)["params"]["dof"] for i in range(4)]
+    assert r0["checksums"] == pytest.approx([0.5 * d for d in dofs])
