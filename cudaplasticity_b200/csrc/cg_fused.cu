@@ -310,6 +310,7 @@ template <int C, bool ST = false>
 __device__ __forceinline__ void iter_kernel_body(const FusedArgs& a, int parity) {
     __shared__ double sh[2 * kThreads / 32];
     __shared__ bool last;
+    pdl_enter();  // scheduled early by fused_launch_iteration
     CgScalars* sc = a.sc;
     if (sc->converged || sc->status) return;
     double v[kSums] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -525,12 +526,29 @@ void fused_launch_persistent(const FusedArgs& a, double eps2, long long max_iter
     CP_CUDA(cudaLaunchCooperativeKernel((const void*)persistent_kernel(), dim3(g), dim3(kThreads), params, 0, s));
 }
 
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("CUPLAST_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 void fused_launch_iteration(const FusedArgs& a, int parity, cudaStream_t s) {
     const IterKernel k = iter_kernel();
     const int g = fused_grid(k, a.n, a.sm_count);
     CP_CHECK(g <= a.max_blocks, CP_ERR_INVALID, "partials buffer too small");
-    k<<<g, kThreads, 0, s>>>(a, parity);
-    CP_CUDA(cudaGetLastError());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(g);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    CP_CUDA(cudaLaunchKernelEx(&cfg, k, a, parity));
 }
 
 // "while (!converged) { body_iters x iteration }" as a graph with a WHILE

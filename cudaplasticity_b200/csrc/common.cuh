@@ -110,4 +110,20 @@ __device__ __forceinline__ V ld_stream(const V* p) {
 // (345 against 347 ms for 3000 iterations) and keeps the read-only path.
 bool stream_loads();
 
+// Whether the CG iteration kernels launch with programmatic stream
+// serialization: the next grid is scheduled while the current one finishes
+// and waits for it on the device (cudaGridDependencySynchronize), hiding the
+// launch gap of latency-bound iterations. CUPLAST_PDL=0 launches them
+// plainly (measurements).
+bool pdl_enabled();
+
+// The first statements of a kernel launched that way: nothing of the
+// previous grid is read before it has completed and its writes are visible;
+// then the next grid may be scheduled. Without the launch attribute both
+// return at once.
+__device__ __forceinline__ void pdl_enter() {
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
+}
+
 }  // namespace cp
