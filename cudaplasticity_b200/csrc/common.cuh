@@ -110,8 +110,8 @@ __device__ __forceinline__ V ld_stream(const V* p) {
 // (345 against 347 ms for 3000 iterations) and keeps the read-only path.
 bool stream_loads();
 
-// Whether the CG iteration kernels launch with programmatic stream
-// serialization: the next grid is scheduled while the current one finishes
+// Whether the one-launch FP64 CG iterations (cg_fused.cu) launch with
+// programmatic stream serialization: the next grid is scheduled while the current one finishes
 // and waits for it on the device (cudaGridDependencySynchronize), hiding the
 // launch gap of latency-bound iterations. CUPLAST_PDL=0 launches them
 // plainly (measurements).
