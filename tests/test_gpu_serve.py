@@ -206,3 +206,43 @@ def test_destroy_with_fp64_solves_in_flight_returns():
     t0 = time.time()
     srv.close()
     assert time.time() - t0 < 60.0
+
+
+def test_sharded_shares_equal_requests_solved_alone():
+    """The instance sharding of cudaplasticity_b200.shard, its two shares run
+    one after the other through one service (what two ranks do on two GPUs):
+    every request is solved once, and its result equals the same request
+    solved alone with cp_solve, bit for bit."""
+    from cudaplasticity_b200 import shard
+
+    ws = [workload.instance(i, increments=(1, 3), **GEN) for i in range(80, 86)]
+    ctx = cp.Context(0)
+    ref = [alone_fp64(ctx, w) for w in ws]
+    parts = shard.partition([shard.request_cost(w["params"]["dof"], w["levels"]) for w in ws], 2)
+    assert sorted(parts[0] + parts[1]) == list(range(len(ws))) and parts[0] and parts[1]
+    srv = cp.Server(fp64_lanes=3)
+    results = {}
+    try:
+        def submit(w):
+            return srv.submit(w["mesh"], w["material"], w["rp"], w["mask"], w["uv"], levels=w["levels"],
+                              precision=cp.CP_PREC_FP64, **FP64_KW)
+
+        def wait(rid):
+            inst, rep, latency = srv.wait(rid, timeout=600.0)
+            results[rid] = (inst.state(), rep)
+            inst.close()
+            return {"status": rep["status"], "latency": latency, "rid": rid}
+
+        recs = [shard.run_share(p, lambda i: ws[i], submit, wait) for p in parts]
+    finally:
+        srv.close()
+        ctx.close()
+    merged = shard.merge_records(recs)
+    summ = shard.summarize(merged, len(ws), 2)
+    assert summ["requests"] == len(ws) and summ["seconds"] > 0
+    for k in range(len(ws)):
+        st, rep = results[merged[k]["rid"]]
+        assert rep["status"] == ref[k][1]["status"], (k, rep, ref[k][1])
+        for f in cp.FIELDS + ["uv"]:
+            assert np.array_equal(st[f], ref[k][0][f]), (k, f)
+        assert rep["cg_iters"] == ref[k][1]["cg_iters"]
