@@ -978,7 +978,11 @@ def run_product_arm(args):
                 "frac": fby.value / (fms.value * 1e-3) / 1e9 / peak, "traffic": 622.5e6,
                 "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one k_f_iter launch on this mesh "
                                 "(ncu capture, profiles/k_f_iter_2M.md)",
-                "bytes_per_launch": fby.value, "ms_per_launch": fms.value, "peak_kind": peak_kind}
+                "bytes_per_launch": fby.value, "ms_per_launch": fms.value, "peak_kind": peak_kind,
+                "why_this_kernel": "the metric's CG GB/s: the dominant kernel of the configuration-2 solve "
+                                   "(k_f_iter, 114 us x 924k iterations of its 105 s); the headline step's own "
+                                   "kernel, k_c_solve, keeps the instance on chip and is latency-bound, so its "
+                                   "HBM fraction is reported apart as roofline_headline"}
     mp32, mu32, bp32, bu32 = rows["fp32"]
     roof_fp32 = {"bound": "hbm", "kernel": "k_cg_p<float> (mixed precision SpMV + direction) on the 2.1M-DOF plate",
                  "achieved": bp32 / (mp32 * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
