@@ -56,7 +56,7 @@ WORKLOAD = dict(workload="hole_plate_ogrid64x64_q4_8320dof", plate_mm=200, hole_
                 nodes=4160, dof=8320, elements=4096, E_mpa=210000, nu=0.3, sigma_y=250, E_t=2000, traction_mpa=200,
                 increments=10, cg_tol=1e-10, outer_tol=1e-6)
 SOLVE_KW = dict(cg_tol=1e-10, outer_tol=1e-6, max_outer=2000, levels=10, aitken=1, adaptive_cg=2, precond=1,
-                max_cg=2_000_000, predict=1)
+                max_cg=2_000_000, predict=1, recycle=6)
 PRECOND_NAMES = {0: "unpreconditioned CG", 1: "block-Jacobi PCG", 2: "aggregation-multigrid V-cycle PCG"}
 METRIC = "converged solves/s (200 mm plate, 20 mm hole, 64x64 O-grid, 8320 DOF, FP64, <=1e-6 outer / 1e-10 CG)"
 
@@ -1034,7 +1034,9 @@ def run_product_arm(args):
             "config": line_config(world),
             "solver": f"FP64, Aitken secant, {PRECOND_NAMES[SOLVE_KW['precond']]}, adaptive CG tolerance "
                       "max(1e-10, 0.2 relErr) until relErr <= 1e-6, then 1e-10; levels from the "
-                      "third on start from the linear extrapolation of the last two",
+                      "third on start from the linear extrapolation of the last two"
+                      + ("; each linear solve starts from the Galerkin projection onto the level's last "
+                         f"{SOLVE_KW['recycle']} solution increments" if SOLVE_KW["recycle"] else ""),
             "cg_form": ("graph loop: P, U, then the V-cycle (restrict per level, dense coarsest "
                         "inverse, prolongation fused into post-smoothing), one kernel each"
                         if SOLVE_KW["precond"] == 2 else os.environ.get("CUPLAST_FP64_CG") or
@@ -1177,11 +1179,14 @@ def main():
     ap.add_argument("--svp-lanes", type=int, default=8, help="FP64 lanes of the solve service")
     ap.add_argument("--sharded", type=int, metavar="N",
                     help="sharded-service leg only (the first N batch-stream requests split over the ranks), then exit")
+    ap.add_argument("--recycle", type=int, default=SOLVE_KW["recycle"], choices=range(0, 7),
+                    help="initial guesses from the last N solution increments of a load level (0: off)")
     ap.add_argument("--precond", type=int, default=SOLVE_KW["precond"], choices=[0, 1, 2],
                     help="linear solver of the headline and of the FP64 served arm: 0 CG, 1 block-Jacobi PCG, "
                          "2 multigrid PCG")
     args = ap.parse_args()
     SOLVE_KW["precond"] = args.precond
+    SOLVE_KW["recycle"] = args.recycle
     FP64_SERVE_KW["precond"] = args.precond
     if args.batched_probe:
         batched_probe(*args.batched_probe)

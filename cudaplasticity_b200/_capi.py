@@ -49,7 +49,7 @@ class cp_mesh_view(ctypes.Structure):
 class cp_solve_opts(ctypes.Structure):
     _fields_ = [("precision", c_int), ("cg_tol", c_double), ("outer_tol", c_double), ("max_outer", c_int),
                 ("max_cg", c_ll), ("levels", c_int), ("aitken", c_int), ("inner_tol", c_double),
-                ("adaptive_cg", c_int), ("precond", c_int), ("predict", c_int)]
+                ("adaptive_cg", c_int), ("precond", c_int), ("predict", c_int), ("recycle", c_int)]
 
 
 class cp_solve_report(ctypes.Structure):

@@ -418,6 +418,52 @@ void cg_fp64(cp_instance* I, double eps, long long max_iter, int precond = 0) {
     run_cg_loop(I, a, I->g64[precond]);
 }
 
+// Initial guesses from the level's solution increments (recycle.h): the
+// arguments with the m-slot ring's increments newest first.
+cp::RecycleArgs recycle_args(cp_instance* I, int m) {
+    if (!I->rec_w) {
+        I->rec_w = I->alloc<double2>((size_t)cp::kRecycleMax * I->n_nodes);
+        I->rec_u0 = I->alloc<double2>(I->n_nodes);
+        I->rec_part = I->alloc<double>((size_t)cp::recycle_grid(I->n_nodes, I->sms()) * cp::kRecycleStride);
+        I->rec_y = I->alloc<double>(cp::kRecycleMax);
+        I->rec_ticket = I->alloc<unsigned int>(1);
+        CP_CUDA(cudaMemsetAsync(I->rec_ticket, 0, sizeof(unsigned int), I->s()));
+        CP_CUDA(cudaMemsetAsync(I->rec_y, 0, cp::kRecycleMax * sizeof(double), I->s()));
+    }
+    cp::RecycleArgs a;
+    a.n = I->n_nodes;
+    a.slice_ptr = I->csr.slice_ptr;
+    a.scol = I->csr.scol;
+    a.val = I->csr.val64;
+    a.u = I->u;
+    a.b = I->b;
+    a.mask = I->mask;
+    a.w = I->rec_w;
+    a.u0 = I->rec_u0;
+    a.partials = I->rec_part;
+    a.ticket = I->rec_ticket;
+    a.y = I->rec_y;
+    a.cnt = std::min(I->rec_cnt, m);
+    for (int i = 0; i < a.cnt; ++i) a.slot[i] = ((I->rec_head - 1 - i) % m + m) % m;
+    return a;
+}
+
+// Before a linear solve: u0 = u and, with increments in the ring, u += W y.
+void recycle_before(cp_instance* I, int m) {
+    const cp::RecycleArgs a = recycle_args(I, m);
+    cp::recycle_project(a, I->sms(), I->s());
+    I->launches += a.cnt > 0 ? 2 : 1;
+}
+
+// After it: the increment u - u0 goes into the ring.
+void recycle_after(cp_instance* I, int m) {
+    const cp::RecycleArgs a = recycle_args(I, m);
+    cp::recycle_push(a, I->rec_head, I->sms(), I->s());
+    I->launches += 1;
+    I->rec_head = (I->rec_head + 1) % m;
+    I->rec_cnt = std::min(I->rec_cnt + 1, m);
+}
+
 // Mixed precision: FP64 defect correction around FP32 CG. Each step computes
 // r = m.(b - K64 u) in FP64 and runs CG on K32 from that residual (FP32
 // recurrences, u accumulated in FP64) to a relative reduction inner_tol; stops
@@ -546,6 +592,7 @@ CP_API int cp_instance_footprint(const cp_mesh_view* m, int precision, size_t* b
     b += ne * 18 * 8;                                                          // element state
     b += n * 2 * 32;                                                           // (v, z) records, FP64 two-kernel form
     if (precision != CP_PREC_FP64) b += nnz * 4 + n * 8 * 4 + n * 2 * 16;
+    b += n * 16 * (cp::kRecycleMax + 1);                                       // solution increments (recycle)
     b += 1 << 20;                                                              // scalars, partials, graphs
     *bytes = b;
     return CP_OK;
@@ -824,6 +871,9 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
     if (o.precond < 0 || o.precond > 2) return CP_ERR_INVALID;
     if (o.precond == 2 && o.precision != CP_PREC_FP64) return CP_ERR_UNSUPPORTED;  // multigrid: FP64 only
     if (o.adaptive_cg < 0 || o.adaptive_cg > 2 || o.predict < 0 || o.predict > 1) return CP_ERR_INVALID;
+    if (o.recycle < 0 || o.recycle > cp::kRecycleMax) return CP_ERR_INVALID;
+    // the increments' ring holds o.recycle slots; FP64 linear solves with precond 0 or 1 only
+    const int m_rec = o.precond == 2 ? 0 : o.recycle;
     // floatBoost's first phase (solveCUDA_FD, src/PlasticitySolver.cu:660-679):
     // CG 1e-4 and relErr 1e-4 in reduced precision
     constexpr double kBoostTol = 1e-4;
@@ -852,6 +902,8 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
             grid1d(2LL * I->n_elem, I->sms(), g);
             k_zero_double<<<g, 256, 0, s>>>(I->st.res_prev, 2LL * I->n_elem);  // res_prev, res_cur adjacent
             I->launches += 2;
+            I->rec_cnt = 0;  // increments of this level only
+            I->rec_head = 0;
             double rel_err = 1.0, w_prev = 1.0;
             bool converged = false;
             // floatBoost: the reduced-precision phase, then FP64 from its state
@@ -875,8 +927,13 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
                 if (mg_deferred) {
                     cg_fp64_mg(I, eps, o.max_cg, true);
                 } else if (prec == CP_PREC_FP64) {
-                    if (o.precond == 2) cg_fp64_mg(I, eps, o.max_cg);
-                    else cg_fp64(I, eps, o.max_cg, o.precond ? 1 : 0);
+                    if (o.precond == 2) {
+                        cg_fp64_mg(I, eps, o.max_cg);
+                    } else {
+                        if (m_rec > 0) recycle_before(I, m_rec);
+                        cg_fp64(I, eps, o.max_cg, o.precond ? 1 : 0);
+                        if (m_rec > 0) recycle_after(I, m_rec);
+                    }
                     R.cg_iters += I->sc_h->iter;
                     R.cg_rel_res = std::sqrt(I->sc_h->rr * I->sc_h->normB_inv);
                     if (I->sc_h->status == CP_ERR_BREAKDOWN) throw Error{CP_ERR_BREAKDOWN, "CG broke down"};
@@ -915,6 +972,8 @@ CP_API int cp_solve(cp_instance* I, const cp_solve_opts* opts, cp_solve_report* 
                         boost = false;
                         prec = CP_PREC_FP64;
                         w_prev = 1.0;
+                        I->rec_cnt = 0;
+                        I->rec_head = 0;
                         int g2;
                         grid1d(2LL * I->n_elem, I->sms(), g2);
                         k_zero_double<<<g2, 256, 0, s>>>(I->st.res_prev, 2LL * I->n_elem);

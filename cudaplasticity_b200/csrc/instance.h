@@ -12,6 +12,7 @@
 #include "cg.h"
 #include "internal.h"
 #include "mg.h"
+#include "recycle.h"
 
 struct cp_context {
     int device = 0;
@@ -66,6 +67,13 @@ struct cp_instance {
     int cluster_planned = 0;       // cluster_plan below is computed (once per instance)
     double2* pred_u = nullptr;     // level predictor (cp_solve_opts.predict): the last level's u and psi
     double* pred_psi = nullptr;
+    // initial guesses from the level's solution increments (cp_solve_opts.recycle, recycle.h), allocated on
+    // first use: the increments (a ring of kRecycleMax), the warm start before the correction, partial sums,
+    // the coefficients and a ticket; rec_cnt increments in use, rec_head the next slot to write
+    double2 *rec_w = nullptr, *rec_u0 = nullptr;
+    double *rec_part = nullptr, *rec_y = nullptr;
+    unsigned int* rec_ticket = nullptr;
+    int rec_cnt = 0, rec_head = 0;
     cp::ClusterPlan cluster_plan;
     double2 *f_r = nullptr, *f_w = nullptr, *f_p = nullptr, *f_kp = nullptr, *f_g = nullptr;
     double* f_partials = nullptr;

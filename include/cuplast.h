@@ -113,6 +113,10 @@ typedef struct {
     int predict;         /* 1: from the third load level on, start from the linear extrapolation of the last two
                             levels' displacements and secant moduli (a predictor; each level still converges to
                             the same criterion) */
+    int recycle;         /* 0..6, CP_PREC_FP64 with precond 0 or 1: each linear solve of a load level starts
+                            from the last solution corrected by the Galerkin projection of the error onto the
+                            level's last `recycle` solution increments (fewer CG iterations; each solve stops on
+                            the same criterion, so the fixed point is unchanged). 0: off (the reference) */
 } cp_solve_opts;
 
 typedef struct {

@@ -177,6 +177,36 @@ def test_level_predictor_and_loose_adaptive_rule_reach_the_same_fixed_point(name
     assert r["report"]["levels_done"] == scenarios.SCENARIOS[name].get("levels", 1)
 
 
+@pytest.mark.parametrize("name", ["ogrid16_bilin", "ogrid16_hollomon", "ogrid8_q8_bilin"])
+def test_recycled_initial_guesses_reach_the_same_fixed_point(name, ctx, golden_dir, workdir):
+    """cp_solve_opts.recycle: each FP64 linear solve of a load level starts
+    from the last solution corrected by the Galerkin projection onto the
+    level's recent solution increments. The path changes, not the fixed
+    point: the FP64 bar against the reference's fixture, with the
+    benchmark's other options."""
+    g = load_golden(golden_dir, name)
+    m, lines = scenario(name, workdir)
+    r = product_runner.run(ctx, lines, m, recycle=6, **BENCH_OPTS)
+    k, err, errs = worst(r, g)
+    assert err <= FP64_TOL, (k, err, errs)
+    assert np.array_equal(yielded(r), yielded(g))
+    assert r["report"]["status"] == 0
+
+
+def test_recycle_takes_fewer_cg_iterations_at_configuration_size(ctx, golden_dir, workdir):
+    """On the benchmark's job the recycled initial guesses cut the CG
+    iterations (a CPU model of the same solver: 39.3k -> 27.6k) and keep the
+    converged state within the FP64 bar; a count outside 0..6 is rejected."""
+    g = load_golden(golden_dir, "config1_bilin")
+    m, lines = scenario("config1_bilin", workdir)
+    base = product_runner.run(ctx, lines, m, **BENCH_OPTS)
+    r = product_runner.run(ctx, lines, m, recycle=6, **BENCH_OPTS)
+    assert max(state_errors(r, g).values()) <= FP64_TOL
+    assert r["report"]["cg_iters"] < 0.9 * base["report"]["cg_iters"], (r["report"], base["report"])
+    with pytest.raises(cp.CuplastError):
+        product_runner.run(ctx, lines, m, recycle=7, **BENCH_OPTS)
+
+
 @pytest.mark.parametrize("name", ["hole12_pow", "ogrid16_bilin"])
 def test_float_boost_reaches_the_fp64_fixed_point(name, ctx, golden_dir, workdir):
     """The reference's floatBoost scheme (CP_PREC_FLOAT_BOOST; solveCUDA_FD,
@@ -259,8 +289,9 @@ def test_singular_system_terminates(ctx):
 
 
 STATE_SCEN = [n for n, s in scenarios.SCENARIOS.items() if s.get("state_fixture")]
-# the benchmark's solver options (bench.py's SOLVE_KW), here under the
-# scenarios' tight tolerances
+# the benchmark's solver options (bench.py's SOLVE_KW) without the recycled
+# initial guesses (the tests add recycle=6, the benchmark's value, where they
+# compare with and without), here under the scenarios' tight tolerances
 BENCH_OPTS = dict(aitken=1, adaptive_cg=2, precond=1, predict=1, max_cg=2_000_000)
 
 
@@ -273,6 +304,9 @@ def state_errors(r, g):
     ("config1_bilin", BENCH_OPTS),
     ("ogrid128x64_hollomon", BENCH_OPTS),
     ("ogrid128x64_hollomon", dict(aitken=1, precond=1, max_cg=2_000_000)),
+    # initial guesses from the recent solution increments (cluster and grid-wide CG)
+    ("config1_bilin", dict(BENCH_OPTS, recycle=6)),
+    ("ogrid128x64_hollomon", dict(BENCH_OPTS, recycle=6)),
     # the aggregation-multigrid preconditioned FP64 CG (an extension)
     ("config1_bilin", dict(aitken=1, adaptive_cg=1, precond=2, max_cg=2_000_000)),
     ("ogrid128x64_hollomon", dict(aitken=1, adaptive_cg=1, precond=2, max_cg=2_000_000)),
