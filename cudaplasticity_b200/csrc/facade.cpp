@@ -379,6 +379,7 @@ double PlasticitySolver::run(bool elastic) {
     o.predict = predict ? 1 : 0;
     o.precond = precond;
     o.inner_tol = innerTol;
+    o.recycle = recycle;
     if (elastic) o.outer_tol = 1e300;  // one linear solve + stress update (solveElast)
     int st = cp_solve(inst_, &o, &report_);
     if (st != CP_OK && st != CP_ERR_NOT_CONVERGED) check(st);

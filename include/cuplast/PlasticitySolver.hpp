@@ -36,6 +36,8 @@ public:
     int precond = 0;         // linear solver (cp_solve_opts): 0 CG as the reference, 1 2x2 block-Jacobi PCG,
                              // 2 aggregation-multigrid PCG (FP64; not with floatBoost)
     double innerTol = 1e-4;  // floatBoost's first phase: FP32 inner solves' relative tolerance
+    int recycle = 0;         // 0..6: FP64 linear solves start from the projection onto the level's last
+                             // `recycle` solution increments (cp_solve_opts.recycle; same fixed point)
     int device = 0;
 
     PlasticitySolver(const Material& material, Mesh& mesh, const LoadConditions& loadConditions);
