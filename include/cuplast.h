@@ -116,7 +116,8 @@ typedef struct {
     int recycle;         /* 0..6, CP_PREC_FP64 with precond 0 or 1: each linear solve of a load level starts
                             from the last solution corrected by the Galerkin projection of the error onto the
                             level's last `recycle` solution increments (fewer CG iterations; each solve stops on
-                            the same criterion, so the fixed point is unchanged). 0: off (the reference) */
+                            the same criterion, so the fixed point is unchanged). 0: off (the reference).
+                            cp_solve only; a batch ignores it */
 } cp_solve_opts;
 
 typedef struct {
