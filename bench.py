@@ -253,7 +253,7 @@ BATCH_KW = dict(cg_tol=1e-10, outer_tol=1e-6, max_outer=2000, max_cg=5_000_000, 
                 inner_tol=1e-3)
 # the FP64 lanes of the solve service: the same tolerances in FP64
 FP64_SERVE_KW = dict(cg_tol=1e-10, outer_tol=1e-6, max_outer=2000, max_cg=5_000_000, precond=1, aitken=1,
-                     adaptive_cg=1)
+                     adaptive_cg=1, recycle=6)
 
 
 def batched_leg(ctx, window_s=20.0, warm_s=3.0, slots=512, pool_size=768, seed=20261203):
@@ -611,9 +611,10 @@ def served_vs_plain_leg(ctx, n_requests, stream="served", rates=(10.0, 100.0, 10
               file=sys.stderr, flush=True)
     n = len(reqs)
     service = [p["seconds"] for p in plain]
-    out = {"workload": "first %d requests of the %s, base seed %d; CG %g, outer %g, outer cap %d; FP64 reference = "
-                       "the plain drop-in's result" % (n, st_["text"], seed, kw["cg_tol"], kw["outer_tol"],
-                                                       kw["max_outer"]),
+    out = {"workload": "first %d requests of the %s, base seed %d; CG %g, outer %g, outer cap %d, recycled "
+                       "initial guesses %d (both arms); FP64 reference = the plain drop-in's result"
+                       % (n, st_["text"], seed, kw["cg_tol"], kw["outer_tol"], kw["max_outer"],
+                          kw.get("recycle", 0)),
            "requests": n, "dof": [w["params"]["dof"] for w in reqs], "levels": [w["levels"] for w in reqs],
            "plain_fp64_dropin": {"seconds_total": sum(service), "solves_per_s": n / sum(service),
                                  "statuses": sorted({p["status"] for p in plain}),
@@ -1187,6 +1188,7 @@ def main():
     args = ap.parse_args()
     SOLVE_KW["precond"] = args.precond
     SOLVE_KW["recycle"] = args.recycle
+    FP64_SERVE_KW["recycle"] = args.recycle
     FP64_SERVE_KW["precond"] = args.precond
     if args.batched_probe:
         batched_probe(*args.batched_probe)
