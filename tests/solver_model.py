@@ -75,12 +75,13 @@ def chol_drop_solve(a, h, tol=1e-10):
 class PlateModel:
     """The FP64 solve of one Q4 mesh under a bilinear diagram (plane stress)."""
 
-    def __init__(self, node_xy, elem4, rp, mask, uv, E, nu, sigma_t, k_t, h=1.0):
+    def __init__(self, node_xy, elem4, rp, mask, uv, E, nu, sigma_t, k_t, h=1.0, diagram=None):
         self.xy = np.asarray(node_xy, float).reshape(-1, 2)
         self.el = np.asarray(elem4, np.int64).reshape(-1, 4)
         self.n, self.ne = self.xy.shape[0], self.el.shape[0]
         self.N = 2 * self.n
         self.E, self.nu, self.sy, self.kt, self.h = E, nu, sigma_t, k_t, h
+        self.diagram = diagram  # f(eps_i) -> sigma; None: bilinear (sigma_t, k_t)
         self.rp = np.asarray(rp, float)
         self.mask = np.asarray(mask).astype(bool)
         self.uv = np.asarray(uv, float)
@@ -160,12 +161,14 @@ class PlateModel:
             rho = rn
 
     def _diagram(self, eps):
+        if self.diagram is not None:
+            return self.diagram(eps)
         et = self.sy / self.E
         return np.where(eps < et, eps * self.E, self.sy + (eps - et) * self.kt)
 
-    def solve(self, levels=10, outer_tol=1e-6, cg_tol=1e-10, recycle=0, max_outer=2000):
+    def solve(self, levels=10, outer_tol=1e-6, cg_tol=1e-10, recycle=0, max_outer=2000, rule=2):
         """Returns (outer iterations, CG iterations, u) with the benchmark's
-        options (Aitken, adaptive rule 2, level predictor, block-Jacobi)."""
+        options (Aitken, adaptive rule 2 or 1, level predictor, block-Jacobi)."""
         E, nu = self.E, self.nu
         psi = np.ones(self.ne)
         ec, nuc = E / psi, 0.5 * (1 - (1 - 2 * nu) / psi)
@@ -188,7 +191,10 @@ class PlateModel:
             rel, w_prev = 1.0, 1.0
             incs = []
             for it in range(max_outer):
-                eps = max(cg_tol, 0.2 * rel) if rel > outer_tol else cg_tol
+                if rule == 2:
+                    eps = max(cg_tol, 0.2 * rel) if rel > outer_tol else cg_tol
+                else:
+                    eps = max(cg_tol, 1e-2 * rel) if rel > 10 * outer_tol else cg_tol
                 k = self._assemble(ec, nuc)
                 x0 = u
                 if recycle and incs:
