@@ -131,7 +131,10 @@ class PlateModel:
         inv[oy, 3] = 1 / c[oy]
         return inv
 
-    def _pcg(self, k, b, x, eps):
+    def _pcg(self, k, b, x, eps, defl=None):
+        """Block-Jacobi PCG; with ``defl`` (a matrix W of directions) the
+        deflated variant: every search direction is made K-orthogonal to W
+        (Saad, Yeung, Erhel and Guyomarc'h, 2000)."""
         inv = self._block_jacobi(k)
 
         def apply_m(v):
@@ -139,12 +142,22 @@ class PlateModel:
             return np.stack([inv[:, 0] * v2[:, 0] + inv[:, 1] * v2[:, 1],
                              inv[:, 2] * v2[:, 0] + inv[:, 3] * v2[:, 1]], 1).ravel()
 
+        project = None
+        if defl is not None:
+            kw = np.where(self.mask[:, None], k @ defl, 0.0)
+            ev, vec = np.linalg.eigh(defl.T @ kw)
+            keep = ev > 1e-10 * ev.max()
+            ginv = (vec[:, keep] / ev[keep]) @ vec[:, keep].T
+
+            def project(v):
+                return v - defl @ (ginv @ (kw.T @ v))
+
         r = np.where(self.mask, b - k @ x, 0.0)
         nb = b @ b
         if r @ r == 0 or (r @ r) / nb <= eps * eps:
             return x, 0
         z = apply_m(r)
-        p = z.copy()
+        p = project(z) if project else z.copy()
         rho = r @ z
         it = 0
         while True:
@@ -157,7 +170,7 @@ class PlateModel:
                 return x, it
             z = apply_m(r)
             rn = r @ z
-            p = z + (rn / rho) * p
+            p = (project(z) if project else z) + (rn / rho) * p
             rho = rn
 
     def _diagram(self, eps):
@@ -166,9 +179,11 @@ class PlateModel:
         et = self.sy / self.E
         return np.where(eps < et, eps * self.E, self.sy + (eps - et) * self.kt)
 
-    def solve(self, levels=10, outer_tol=1e-6, cg_tol=1e-10, recycle=0, max_outer=2000, rule=2):
+    def solve(self, levels=10, outer_tol=1e-6, cg_tol=1e-10, recycle=0, max_outer=2000, rule=2, deflate=False):
         """Returns (outer iterations, CG iterations, u) with the benchmark's
-        options (Aitken, adaptive rule 2 or 1, level predictor, block-Jacobi)."""
+        options (Aitken, adaptive rule 2 or 1, level predictor, block-Jacobi).
+        ``deflate`` (with ``recycle``): the linear solves also deflate the
+        recycled increments (not in the product yet)."""
         E, nu = self.E, self.nu
         psi = np.ones(self.ne)
         ec, nuc = E / psi, 0.5 * (1 - (1 - 2 * nu) / psi)
@@ -196,13 +211,13 @@ class PlateModel:
                 else:
                     eps = max(cg_tol, 1e-2 * rel) if rel > 10 * outer_tol else cg_tol
                 k = self._assemble(ec, nuc)
-                x0 = u
+                x0, w = u, None
                 if recycle and incs:
                     w = np.stack(incs[::-1][:recycle], 1)  # newest first
                     r0 = np.where(self.mask, b - k @ u, 0.0)
                     y = chol_drop_solve(w.T @ (k @ w), w.T @ r0)
                     x0 = u + w @ y
-                u_new, ncg = self._pcg(k, b, x0, eps)
+                u_new, ncg = self._pcg(k, b, x0, eps, defl=w if deflate else None)
                 incs.append(u_new - u)
                 u = u_new
                 tot_cg += ncg

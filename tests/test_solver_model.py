@@ -45,3 +45,20 @@ def test_model_reproduces_the_gpu_counts_and_the_recycling_gain(model):
     assert cg6 < 0.75 * cg0
     # both stop at outer 1e-6 through different iterates: close, not equal
     assert np.linalg.norm(u6 - u0) / np.linalg.norm(u0) < 1e-4
+
+
+def test_deflation_model_on_a_small_plate():
+    """The deflated variant (a candidate for the cluster CG) on a 16 x 16
+    O-grid: the same fixed point within the stop rule, no more CG iterations
+    than the recycled initial guesses alone."""
+    import cudaplasticity_b200 as cp
+
+    mesh = cp.Mesh.rect_with_hole(-100.0, 100.0, -100.0, 100.0, 20.0, 4, 4, rad_n=16)
+    loads = cp.Loads().set_force(2, 0.0, 200.0).fix_border_hor(0).fix_point(-100.0, -100.0)
+    rp, mask, uv = loads.build(mesh)
+    a = mesh.arrays()
+    m = PlateModel(a["node_xy"], a["elem4"], rp, mask, uv, 210000.0, 0.3, 250.0, 2000.0)
+    o1, c1, u1 = m.solve(recycle=6)
+    o2, c2, u2 = m.solve(recycle=6, deflate=True)
+    assert c2 <= c1
+    assert np.linalg.norm(u2 - u1) / np.linalg.norm(u1) < 1e-4
