@@ -173,6 +173,7 @@ _SIGS = {
     "cpx_amg_level_get": (c_int, [c_p, c_int, P_int, P_int, P_int, P_double]),
     "cpx_amg_galerkin": (c_int, [c_p, c_int, P_double, P_double]),
     "cpx_amg_device_maps": (c_int, [c_p, c_int, P_int, P_int, P_int, P_int, P_int, P_int, P_int, P_int]),
+    "cpx_recycle_solve": (c_int, [P_double, c_int, P_double]),
 }
 
 _lib = None

@@ -2,6 +2,7 @@
 #include "common.cuh"
 #include "internal.h"
 #include "recycle.h"
+#include "../../include/cuplast_host.h"
 
 namespace cp {
 
@@ -14,7 +15,7 @@ constexpr int kRecThreads = 256;
 // diagonal is not positive); dropped increments get y = 0. One thread.
 constexpr double kDrop = 1e-10;
 
-__device__ void small_solve(const double* t, int cnt, double* y) {
+__host__ __device__ void small_solve(const double* t, int cnt, double* y) {
     double A[kRecycleMax][kRecycleMax], S[kRecycleMax][kRecycleMax], L[kRecycleMax][kRecycleMax];
     double h[kRecycleMax], d[kRecycleMax], z[kRecycleMax], yy[kRecycleMax];
     bool keep[kRecycleMax], ok[kRecycleMax];
@@ -205,6 +206,12 @@ void recycle_project(const RecycleArgs& a, int sm_count, cudaStream_t s) {
     CP_CUDA(cudaGetLastError());
 }
 
+int recycle_solve_host(const double* sums, int cnt, double* y) {
+    if (!sums || !y || cnt < 0 || cnt > kRecycleMax) return CP_ERR_INVALID;
+    small_solve(sums, cnt, y);
+    return CP_OK;
+}
+
 void recycle_push(const RecycleArgs& a, int slot, int sm_count, cudaStream_t s) {
     CP_CHECK(slot >= 0 && slot < kRecycleMax, CP_ERR_INVALID, "recycle: bad slot");
     k_recycle_push<<<node_grid(a.n, sm_count), kRecThreads, 0, s>>>(a, slot);
@@ -212,3 +219,5 @@ void recycle_push(const RecycleArgs& a, int slot, int sm_count, cudaStream_t s) 
 }
 
 }  // namespace cp
+
+CP_API int cpx_recycle_solve(const double* sums, int cnt, double* y) { return cp::recycle_solve_host(sums, cnt, y); }

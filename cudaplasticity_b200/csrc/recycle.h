@@ -47,6 +47,8 @@ struct RecycleArgs {
 int recycle_grid(int n, int sm_count);
 // u0 = u, then (cnt > 0) the Gram sums, the small solve and u += W y.
 void recycle_project(const RecycleArgs& a, int sm_count, cudaStream_t s);
+// The small solve on the host (the device's code; cpx_recycle_solve).
+int recycle_solve_host(const double* sums, int cnt, double* y);
 // w[slot] = u - u0 after the linear solve.
 void recycle_push(const RecycleArgs& a, int slot, int sm_count, cudaStream_t s);
 

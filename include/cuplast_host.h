@@ -117,6 +117,12 @@ CP_API int cpx_amg_galerkin(const cpx_amg* h, int level, const double* fine, dou
 CP_API int cpx_amg_device_maps(const cpx_amg* h, int level, const int* slice_ptr, int* counts, int* rp, int* ci,
                                int* mem_pos, int* mem, int* gal_pos, int* gal);
 
+/* The small solve of the recycled initial guesses (cp_solve_opts.recycle),
+ * the same code the device runs: sums holds the Gram entries d_j . K d_k
+ * (j <= k) at k (k + 1) / 2 + j, then the right-hand sides d_j . r0 at 21 + j;
+ * cnt (0..6) increments; y receives 6 coefficients (0 for dropped ones). */
+CP_API int cpx_recycle_solve(const double* sums, int cnt, double* y);
+
 #ifdef __cplusplus
 }
 #endif

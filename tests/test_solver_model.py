@@ -62,3 +62,39 @@ def test_deflation_model_on_a_small_plate():
     o2, c2, u2 = m.solve(recycle=6, deflate=True)
     assert c2 <= c1
     assert np.linalg.norm(u2 - u1) / np.linalg.norm(u1) < 1e-4
+
+
+def test_library_small_solve_matches_the_model():
+    """cpx_recycle_solve runs the device's small solve on the host: it
+    agrees with the model's Cholesky-with-drop on random Gram systems, with
+    and without dependent increments, for every count 0..6."""
+    import ctypes
+
+    from cudaplasticity_b200 import _capi as C
+
+    lib = C.lib()
+    rng = np.random.default_rng(11)
+    for trial in range(40):
+        cnt = trial % 7
+        n = 30
+        k = rng.standard_normal((n, n))
+        k = k @ k.T + n * np.eye(n)
+        w = rng.standard_normal((n, max(cnt, 1)))[:, :cnt]
+        if cnt >= 3 and trial % 2:
+            w[:, 2] = w[:, 0] - 0.5 * w[:, 1]  # a dependent increment
+        r0 = rng.standard_normal(n)
+        g = w.T @ k @ w
+        h = w.T @ r0
+        sums = np.zeros(27)
+        for kk in range(cnt):
+            for j in range(kk + 1):
+                sums[kk * (kk + 1) // 2 + j] = g[j, kk]
+            sums[21 + kk] = h[kk]
+        y = np.zeros(6)
+        st = lib.cpx_recycle_solve(sums.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cnt,
+                                   y.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        assert st == 0
+        want = chol_drop_solve(g, h) if cnt else np.zeros(0)
+        np.testing.assert_allclose(y[:cnt], want, rtol=1e-9, atol=1e-12)
+        assert np.all(y[cnt:] == 0.0)
+    assert lib.cpx_recycle_solve(None, 1, None) != 0
